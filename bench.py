@@ -1,0 +1,463 @@
+#!/usr/bin/env python
+"""Benchmark of the two-phase VOF step on the 200^3 dam break (2000 steps).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A bench "step" is one solver time step (the loop body of voftrial1.cu:1361-1401)
+over the whole 200^3 grid; the metric is Mcell-updates/s = cells * steps / s.
+
+ours (default): the CUDA library through its C-ABI.
+  value      device-resident throughput: W warm-up steps, then K steps through
+             captured CUDA graphs bracketed by a barrier, synchronize and CUDA
+             events on the library's stream; max over ranks.
+  e2e        the same K steps through the public API with host buffers: upload
+             of F,u,v,w,p from pinned memory, per step vof_run + an async FP64
+             liquid-volume readback (8 bytes), final download of F; all inside
+             the timed region.
+  roofline   the dominant kernel (largest share of the step, timed live with
+             CUDA events around each phase on the library's stream) against the
+             measured HBM copy bandwidth in MEASURED_PEAKS.json.
+  cpu_baseline  the FP64 CPU restatement (oracle/, OpenMP on every host core)
+             on a bounded sample of the same workload.
+reference: the reference's own voftrial1.cu kernels (oracle/_ref, built from
+  the reference source; the reference has no CPU implementation of the path),
+  sm_100a build and README build, better of the two; rank 0 only.
+
+Multi-GPU: independent replicas, one 200^3 problem per rank (weak scaling, no
+data-path collective); value = cells * steps * N / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+for _p in (str(ROOT), str(ROOT / "cuda-lbm-ibm-fvm_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "Mcell-updates/s at 200^3"
+UNIT = "Mcell-updates/s"
+
+# Algorithmic DRAM bytes per interior cell of one launch of each kernel
+# (FP32 fields, stencil neighbours counted once).
+ALG_BYTES = {
+    "predict": 28,   # read F,u,v,w; write u*,v*,w*
+    "rhs": 20,       # read F,u*,v*,w*; write rhs
+    "jacobi": 12,    # read rhs,p; write p'
+    "correct": 32,   # read u*,v*,w*,p,F; write u,v,w
+    "sweep1": 12,    # read F, face velocity; write F
+    "sweep2": 12,
+    "sweep3": 12,
+}
+KERNEL_NAMES = {
+    "predict": "k_predict", "rhs": "k_rhs", "jacobi": "k_jacobi", "correct": "k_correct",
+    "sweep1": "k_fct", "sweep2": "k_fct", "sweep3": "k_fct",
+}
+STEP_MODEL_BYTES = 188  # B per cell-step of the fused plain path (10 sweeps, FP32)
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=200, help="grid cells per side (default 200)")
+    ap.add_argument("--profile-steps", type=int, default=6)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0,
+                    help="target CPU time of the CPU-baseline sample (0 disables)")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines: list[str] = []
+        self._thr = None
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self._thr = threading.Thread(target=self._read, daemon=True)
+        self._thr.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self._thr:
+            self._thr.join(timeout=2)
+        return summarize_clocks(self.lines)
+
+
+def summarize_clocks(lines) -> dict:
+    sm, smax, power = [], [], []
+    reasons = set()
+    names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    for ln in lines:
+        parts = [x.strip() for x in ln.split(",")]
+        if len(parts) < 9:
+            continue
+        try:
+            sm.append(float(parts[1]))
+            smax.append(float(parts[2]))
+            power.append(float(parts[3]))
+        except ValueError:
+            continue
+        for name, val in zip(names, parts[5:9]):
+            if val.lower().startswith("active"):
+                reasons.add(name)
+    if not sm:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+            "samples": len(sm), "power_w_max": max(power)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def workload_params(V, n):
+    # 0.1 m box, rho 1000/50, nu 1e-6/1.5e-5, dt 4e-6, 10 Jacobi sweeps; gravity
+    # -9.81 along z (the reference's kernels add gx,gy,gz from the parameters).
+    return V.default_params(n, gx=0.0, gy=0.0, gz=-9.81)
+
+
+def workload_state(prm):
+    from vof_b200 import ic
+
+    F = ic.dam_break(prm, height=ic.noisy_height(prm, seed=1))
+    return ic.rest_state(prm, F)
+
+
+def workload_config(prm, steps, world):
+    return {
+        "workload": f"dam_break_{prm.nx}^3_plain_fp32",
+        "grid": [prm.nx, prm.ny, prm.nz],
+        "steps_timed": steps,
+        "dt": float(prm.dt),
+        "jacobi_iters": prm.jacobi_iters,
+        "gravity": [float(prm.gx), float(prm.gy), float(prm.gz)],
+        "ic": "liquid x<0.04, y<0.04, z<0.06+0.5*dx*U(-1,1) (splitmix64 seed 1), u=v=w=p=0",
+        "l2_policy": "inputs larger than L2: 10 resident fields x %.0f MB" % (prm.nTot * 4 / 1e6),
+        "parallelism": "single" if world == 1 else f"replicas x{world}",
+    }
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def measured_traffic():
+    """Per-launch DRAM bytes of each kernel at 200^3 from the committed ncu summary."""
+    p = ROOT / "profiles" / "traffic_200.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return {}
+    return {}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas: barrier + max over ranks only)
+# ---------------------------------------------------------------------------
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int, device=None):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier(device_ids=[device.index] if device is not None and device.type == "cuda" else None)
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline
+# ---------------------------------------------------------------------------
+def cpu_baseline(prm, state, seconds: float) -> dict | None:
+    if seconds <= 0:
+        return None
+    from oracle import oracle as orc
+
+    cores = os.cpu_count() or 1
+    cells = prm.nx * prm.ny * prm.nz
+    st = {k: state[k] for k in ("F", "u", "v", "w", "p")}
+    t0 = time.perf_counter()
+    st = orc.run_f64(prm, st, 1, 1, nthreads=cores)
+    t1 = time.perf_counter()
+    per = max(t1 - t0, 1e-6)
+    n = int(min(20, max(1, round(seconds / per))))
+    t0 = time.perf_counter()
+    orc.run_f64(prm, st, 2, n, nthreads=cores)
+    el = time.perf_counter() - t0
+    cpu = "unknown"
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                cpu = ln.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    return {"value": cells * n / el / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"FP64 CPU restatement (oracle/vof_oracle.cpp, OpenMP {cores} threads, {cpu}): "
+                      f"steps 2..{n + 1} of the {prm.nx}^3 workload after 1 warm-up step, {el:.2f} s"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    import vof_b200 as V
+
+    rank, world, local = dist_env()
+    if world != args.gpus:
+        print(f"warning: --gpus {args.gpus} but WORLD_SIZE {world}", file=sys.stderr)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    prm = workload_params(V, args.n)
+    state = workload_state(prm)
+    cells = prm.nx * prm.ny * prm.nz
+    K, W = args.steps, max(3, args.warmup)
+    stream = torch.cuda.current_stream(dev)
+    props = torch.cuda.get_device_properties(dev)
+    gpu_id = None
+    try:
+        gpu_id = "GPU-" + str(props.uuid)
+    except Exception:
+        pass
+
+    solver = V.Solver(prm, stream=stream.cuda_stream)
+    solver.upload_state(**state)
+    istep = 1
+    solver.run(istep, W)  # warm-up; also captures the three per-order graphs
+    istep += W
+
+    barrier(world, dev)
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(gpu_id)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.run(istep, K)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier(world, dev)
+    ms = e0.elapsed_time(e1)
+    istep += K
+    ms_max = max_over_ranks(ms, world, dev)
+    value = world * cells * K / (ms_max / 1e3) / 1e6
+    vol = solver.reduce("volume")
+    nonfinite = solver.reduce("nonfinite")
+
+    # per-phase CUDA-event timing on the library's stream (live, same state)
+    phases = {}
+    for q in range(max(3, args.profile_steps)):
+        for name, (pms, nl) in solver.step_timed(istep).items():
+            phases.setdefault(name, []).append((pms, nl))
+        istep += 1
+    phase_ms = {k: statistics.median(x[0] for x in v) for k, v in phases.items()}
+    phase_launches = {k: v[0][1] for k, v in phases.items()}
+    dom = max(phase_ms, key=lambda k: phase_ms[k])
+    per_launch_s = phase_ms[dom] / phase_launches[dom] / 1e3
+    peak, peak_src = measured_peaks()
+    achieved = ALG_BYTES[dom] * cells / per_launch_s / 1e9
+    traffic = measured_traffic().get(KERNEL_NAMES[dom] + ":" + dom)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": KERNEL_NAMES[dom],
+                "phase": dom, "alg_bytes_per_cell": ALG_BYTES[dom], "units_per_launch": cells,
+                "launch_ms": round(per_launch_s * 1e3, 5), "peak_source": peak_src}
+    step_ms = ms_max / K
+    step_roofline = {"model_bytes_per_cell_step": STEP_MODEL_BYTES,
+                     "achieved_gbs": round(STEP_MODEL_BYTES * cells / (step_ms / 1e3) / 1e9, 1),
+                     "frac_of_peak": round(STEP_MODEL_BYTES * cells / (step_ms / 1e3) / 1e9 / peak, 4)}
+
+    # e2e through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        lib = V.lib()
+        host = {k: torch.from_numpy(state[k]).pin_memory() for k in V.STATE_FIELDS}
+        vols = torch.zeros(K, dtype=torch.float64).pin_memory()
+        Fout = torch.empty(prm.shape, dtype=torch.float32).pin_memory()
+        solver2 = V.Solver(prm, stream=stream.cuda_stream)
+        solver2.run(1, 3)  # graph capture outside the timed region
+        barrier(world, dev)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for k in V.STATE_FIELDS:
+            solver2._check(lib.vof_upload(solver2._ctx, V.FIELDS[k], C.c_void_p(host[k].data_ptr()), 0),
+                           "vof_upload")
+        vptr = vols.data_ptr()
+        for s in range(K):
+            solver2.run(1 + s, 1)
+            solver2.reduce_async("volume", vptr + 8 * s)
+        solver2.download("F", Fout.numpy())  # synchronizes the stream
+        a1.record(stream)
+        a1.synchronize()
+        wall = time.perf_counter() - t0
+        e2e_ms = max_over_ranks(a0.elapsed_time(a1), world, dev)
+        solver2.close()
+        nbytes = prm.nTot * 4
+        e2e = {"value": round(world * cells * K / (e2e_ms / 1e3) / 1e6, 1), "unit": UNIT,
+               "h2d_bytes_per_step": 5 * nbytes / K, "d2h_bytes_per_step": (nbytes + 8 * K) / K,
+               "ms": round(e2e_ms, 3), "wall_ms": round(wall * 1e3, 3),
+               "api": "vof_upload x5 (pinned) + K x (vof_run 1 step + vof_reduce_async volume) + vof_download F",
+               "final_volume": float(vols[-1])}
+
+    cpu = cpu_baseline(prm, state, args.cpu_seconds) if (rank == 0 and world == 1) else None
+
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": round(step_ms, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": workload_config(prm, K, world),
+        "roofline": roofline, "step_roofline": step_roofline,
+        "cpu_baseline": cpu, "clocks": clk, "e2e": e2e,
+        "gpu_launches": solver.kernels_per_step * K,
+        "phases_ms": {k: round(v, 5) for k, v in phase_ms.items()},
+        "phase_launches": phase_launches,
+        "check": {"volume_after": vol, "nonfinite": nonfinite},
+        "device": props.name,
+    }
+    solver.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    import vof_b200 as V
+    from oracle import oracle as orc
+
+    variants = [v for v in ("sm100a", "readme") if orc.ref_available(v)]
+    if not variants:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference harness oracle/_ref not built (needs the reference source at build time)"}))
+        return
+    import torch
+
+    torch.cuda.set_device(local)
+    props = torch.cuda.get_device_properties(local)
+    gpu_id = None
+    try:
+        gpu_id = "GPU-" + str(props.uuid)
+    except Exception:
+        pass
+    prm = workload_params(V, args.n)
+    state = workload_state(prm)
+    cells = prm.nx * prm.ny * prm.nz
+    K, W = args.steps, max(3, args.warmup)
+    results = {}
+    clk = None
+    for var in variants:
+        clocks = ClockSampler(gpu_id)
+        clocks.start()
+        ms, _ = orc.ref_time(prm, state, 1, W, K, variant=var)
+        c = clocks.stop()
+        results[var] = {"ms": ms, "value": cells * K / (ms / 1e3) / 1e6, "clocks": c}
+    best = max(results, key=lambda v: results[v]["value"])
+    clk = results[best]["clocks"]
+    value = results[best]["value"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": 1,
+        "steps": K, "warmup": W, "ms_per_step": round(results[best]["ms"] / K, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": workload_config(prm, K, 1),
+        "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": None, "kind": "reference",
+                         "sample": f"voftrial1.cu's own kernels ({best} build) on {props.name}, "
+                                   f"{K} steps after {W}; the reference has no CPU implementation of the path"},
+        "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "variants": {v: {"value": round(r["value"], 1), "ms_per_step": round(r["ms"] / K, 5)}
+                     for v, r in results.items()},
+        "clocks": clk, "gpu_launches": orc.ref_lib(best).ref_kernels_per_step(prm.jacobi_iters) * K,
+        "device": props.name,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

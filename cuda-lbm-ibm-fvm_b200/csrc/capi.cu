@@ -1,0 +1,416 @@
+// capi.cu -- the extern "C" boundary declared in include/vof.h.
+//
+// Owns the device buffers (the reference's DeviceFields, voftrial1.cu:1176-1226),
+// converts between the reference layout and the padded internal layout, and
+// sequences the step (voftrial1.cu:1361-1401) on the caller's stream, directly
+// or through captured CUDA graphs.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <new>
+
+#include "../../include/vof.h"
+#include "plain_step.h"
+#include "reduce.h"
+
+using vof::Geom;
+
+static_assert(sizeof(vof_params) == 136, "vof_params layout is part of the ABI");
+static_assert(VOF_PHASES == vof::PLAIN_PHASES, "phase count");
+
+struct vof_ctx {
+    vof_params prm;
+    Geom g;
+    int device;
+    cudaStream_t stream;        // caller's stream (may be the legacy default stream)
+    cudaStream_t cap_stream;    // private stream used only for graph capture
+    vof::PlainBuffers b;
+    int p_parity;               // which of p0/p1 holds the current pressure
+    float* fields[VOF_NUM_FIELDS - 1];  // all but P (P depends on parity)
+    double* d_red_scratch;
+    double* d_red_result;
+    double* h_red_result;       // pinned, for vof_reduce
+    cudaGraphExec_t graph[3][2];  // [istep % 3][p parity at step start]
+    int last_cuda_error;
+    size_t bytes;
+    size_t elems;               // padded elements per field
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+        else prev = -1;
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+int fail_cuda(vof_ctx* c, cudaError_t e) {
+    if (c) c->last_cuda_error = (int)e;
+    return VOF_E_CUDA;
+}
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// Largest interior extent accepted: keeps int32 indexing of the padded
+// layout and the reference's int nTot (voftrial1.cu:40) from overflowing.
+constexpr long long kMaxCells = 2000000000LL;
+
+int validate(const vof_params* p) {
+    if (!p) return VOF_E_INVALID;
+    if (p->nx < 1 || p->ny < 1 || p->nz < 1) return VOF_E_SIZE;
+    const long long pxl = round_up(p->nx + 2, 32);
+    const long long tot = pxl * (p->ny + 2) * (long long)(p->nz + 2);
+    if (tot > kMaxCells) return VOF_E_SIZE;
+    if (p->imin != 1 || p->jmin != 1 || p->kmin != 1 || p->imax != p->nx || p->jmax != p->ny ||
+        p->kmax != p->nz)
+        return VOF_E_INVALID;
+    if (p->nTot != (p->nx + 2) * (p->ny + 2) * (p->nz + 2)) return VOF_E_INVALID;
+    if (!(p->dt > 0.0f) || !(p->dx > 0.0f) || !(p->dy > 0.0f) || !(p->dz > 0.0f)) return VOF_E_INVALID;
+    if (p->jacobi_iters < 0 || p->jacobi_iters > 100000) return VOF_E_INVALID;
+    if (p->mode != VOF_MODE_PLAIN && p->mode != VOF_MODE_MIXED && p->mode != VOF_MODE_FP64)
+        return VOF_E_INVALID;
+    return VOF_OK;
+}
+
+float* field_ptr(vof_ctx* c, int field) {
+    if (field == VOF_FIELD_P) return c->p_parity ? c->b.p1 : c->b.p0;
+    if (field < 0 || field >= VOF_NUM_FIELDS) return nullptr;
+    const int slot = field < VOF_FIELD_P ? field : field - 1;
+    return c->fields[slot];
+}
+
+void free_ctx(vof_ctx* c) {
+    if (!c) return;
+    for (int r = 0; r < 3; ++r)
+        for (int q = 0; q < 2; ++q)
+            if (c->graph[r][q]) cudaGraphExecDestroy(c->graph[r][q]);
+    for (int f = 0; f < VOF_NUM_FIELDS - 1; ++f)
+        if (c->fields[f]) cudaFree(c->fields[f]);
+    if (c->b.p0) cudaFree(c->b.p0);
+    if (c->b.p1) cudaFree(c->b.p1);
+    if (c->d_red_scratch) cudaFree(c->d_red_scratch);
+    if (c->d_red_result) cudaFree(c->d_red_result);
+    if (c->h_red_result) cudaFreeHost(c->h_red_result);
+    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+    delete c;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vof_abi_version(void) { return VOF_ABI_VERSION; }
+
+const char* vof_error_string(int status) {
+    switch (status) {
+        case VOF_OK: return "ok";
+        case VOF_E_INVALID: return "invalid argument";
+        case VOF_E_SIZE: return "grid size out of range";
+        case VOF_E_NOMEM: return "out of memory";
+        case VOF_E_CUDA: return "CUDA error (see vof_last_cuda_error)";
+        case VOF_E_NOT_CONVERGED: return "iterative solve did not converge";
+        case VOF_E_NONFINITE: return "non-finite value in the state";
+        case VOF_E_STATE: return "call not valid in the current state";
+        case VOF_E_UNSUPPORTED: return "unsupported mode or feature";
+        default: return "unknown status";
+    }
+}
+
+int vof_params_finalize(vof_params* p) {
+    if (!p) return VOF_E_INVALID;
+    if (p->nx < 1 || p->ny < 1 || p->nz < 1) return VOF_E_SIZE;
+    // voftrial1.cu:1262-1270, 1285-1291 (float expressions kept).
+    p->imin = 1;
+    p->imax = p->imin + p->nx - 1;
+    p->jmin = 1;
+    p->jmax = p->jmin + p->ny - 1;
+    p->kmin = 1;
+    p->kmax = p->kmin + p->nz - 1;
+    p->dx = p->Lx / static_cast<float>(p->nx);
+    p->dy = p->Ly / static_cast<float>(p->ny);
+    p->dz = p->Lz / static_cast<float>(p->nz);
+    p->dxi = 1.0f / p->dx;
+    p->dyi = 1.0f / p->dy;
+    p->dzi = 1.0f / p->dz;
+    const long long tot = (long long)(p->nx + 2) * (p->ny + 2) * (p->nz + 2);
+    if (tot > 0x7fffffffLL) return VOF_E_SIZE;
+    p->nTot = (int)tot;
+    return VOF_OK;
+}
+
+int vof_params_init(vof_params* p, int nx, int ny, int nz) {
+    if (!p) return VOF_E_INVALID;
+    memset(p, 0, sizeof(*p));
+    p->nx = nx;
+    p->ny = ny;
+    p->nz = nz;
+    // voftrial1.cu:1272-1283
+    p->Lx = 0.1f;
+    p->Ly = 0.1f;
+    p->Lz = 0.1f;
+    p->rho_l = 1000.0f;
+    p->rho_g = 50.0f;
+    p->nu_l = 1.0e-6f;
+    p->nu_g = 1.5e-5f;
+    p->sigma = 0.007f;
+    p->gx = 0.0f;
+    p->gy = -5.0f;
+    p->gz = 0.0f;
+    p->dt = 4.0e-6f;
+    p->jacobi_iters = 10;  // voftrial1.cu:1371
+    p->mode = VOF_MODE_PLAIN;
+    p->inner_sweeps = 32;
+    p->max_outer = 200;
+    p->tol = 1e-8;
+    return vof_params_finalize(p);
+}
+
+int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
+    if (!out) return VOF_E_INVALID;
+    *out = nullptr;
+    int st = validate(p);
+    if (st != VOF_OK) return st;
+    if (p->mode != VOF_MODE_PLAIN) return VOF_E_UNSUPPORTED;
+
+    vof_ctx* c = new (std::nothrow) vof_ctx;
+    if (!c) return VOF_E_NOMEM;
+    memset(c, 0, sizeof(*c));
+    c->prm = *p;
+    c->stream = (cudaStream_t)stream;
+    cudaError_t e = cudaGetDevice(&c->device);
+    if (e != cudaSuccess) {
+        free_ctx(c);
+        return VOF_E_CUDA;
+    }
+
+    Geom& g = c->g;
+    g.nx = p->nx;
+    g.ny = p->ny;
+    g.nz = p->nz;
+    g.px = round_up(p->nx + 2, 32);
+    g.py = p->ny + 2;
+    g.plane = g.px * g.py;
+    g.dt = p->dt;
+    g.dx = p->dx;
+    g.dy = p->dy;
+    g.dz = p->dz;
+    g.dxi = p->dxi;
+    g.dyi = p->dyi;
+    g.dzi = p->dzi;
+    g.rho_l = p->rho_l;
+    g.rho_g = p->rho_g;
+    g.nu_l = p->nu_l;
+    g.nu_g = p->nu_g;
+    g.gx = p->gx;
+    g.gy = p->gy;
+    g.gz = p->gz;
+    if (!vof::plain_supported(g)) {
+        free_ctx(c);
+        return VOF_E_SIZE;
+    }
+
+    c->elems = (size_t)g.plane * (size_t)(p->nz + 2);
+    const size_t fbytes = c->elems * sizeof(float);
+    auto alloc = [&](void** ptr, size_t bytes) -> bool {
+        if (cudaMalloc(ptr, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        c->bytes += bytes;
+        return cudaMemsetAsync(*ptr, 0, bytes, c->stream) == cudaSuccess;
+    };
+    bool ok = true;
+    for (int f = 0; f < VOF_NUM_FIELDS - 1 && ok; ++f) ok = alloc((void**)&c->fields[f], fbytes);
+    ok = ok && alloc((void**)&c->b.p0, fbytes) && alloc((void**)&c->b.p1, fbytes);
+    ok = ok && alloc((void**)&c->d_red_scratch, sizeof(double) * vof::RED_SCRATCH_DOUBLES);
+    ok = ok && alloc((void**)&c->d_red_result, sizeof(double) * vof::RED_RESULT_DOUBLES);
+    if (ok && cudaMallocHost((void**)&c->h_red_result, sizeof(double) * 4) != cudaSuccess) ok = false;
+    if (!ok) {
+        free_ctx(c);
+        return VOF_E_NOMEM;
+    }
+    c->b.F = c->fields[VOF_FIELD_F];
+    c->b.u = c->fields[VOF_FIELD_U];
+    c->b.v = c->fields[VOF_FIELD_V];
+    c->b.w = c->fields[VOF_FIELD_W];
+    c->b.us = c->fields[VOF_FIELD_USTAR - 1];
+    c->b.vs = c->fields[VOF_FIELD_VSTAR - 1];
+    c->b.ws = c->fields[VOF_FIELD_WSTAR - 1];
+    c->b.rhs = c->fields[VOF_FIELD_RHS - 1];
+    c->p_parity = 0;
+
+    const int maxn = p->nx > p->ny ? (p->nx > p->nz ? p->nx : p->nz) : (p->ny > p->nz ? p->ny : p->nz);
+    if ((e = vof::plain_configure(maxn)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(c->stream)) != cudaSuccess) {
+        c->last_cuda_error = (int)e;
+        free_ctx(c);
+        return VOF_E_CUDA;
+    }
+    *out = c;
+    return VOF_OK;
+}
+
+void vof_destroy(vof_ctx* ctx) {
+    if (!ctx) return;
+    DeviceGuard dg(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    free_ctx(ctx);
+}
+
+int vof_get_params(const vof_ctx* ctx, vof_params* out) {
+    if (!ctx || !out) return VOF_E_INVALID;
+    *out = ctx->prm;
+    return VOF_OK;
+}
+
+int vof_upload(vof_ctx* ctx, int field, const float* src, int src_is_device) {
+    if (!ctx || !src) return VOF_E_INVALID;
+    float* dst = field_ptr(ctx, field);
+    if (!dst) return VOF_E_INVALID;
+    DeviceGuard dg(ctx->device);
+    const Geom& g = ctx->g;
+    const size_t w = (size_t)(g.nx + 2) * sizeof(float);
+    cudaError_t e = cudaMemcpy2DAsync(dst, (size_t)g.px * sizeof(float), src, w, w,
+                                      (size_t)(g.ny + 2) * (g.nz + 2),
+                                      src_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                      ctx->stream);
+    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
+}
+
+int vof_download(vof_ctx* ctx, int field, float* dst, int dst_is_device) {
+    if (!ctx || !dst) return VOF_E_INVALID;
+    float* src = field_ptr(ctx, field);
+    if (!src) return VOF_E_INVALID;
+    DeviceGuard dg(ctx->device);
+    const Geom& g = ctx->g;
+    const size_t w = (size_t)(g.nx + 2) * sizeof(float);
+    cudaError_t e = cudaMemcpy2DAsync(dst, w, src, (size_t)g.px * sizeof(float), w,
+                                      (size_t)(g.ny + 2) * (g.nz + 2),
+                                      dst_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                      ctx->stream);
+    if (e == cudaSuccess && !dst_is_device) e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
+}
+
+int vof_step(vof_ctx* ctx, int istep) {
+    if (!ctx) return VOF_E_INVALID;
+    DeviceGuard dg(ctx->device);
+    cudaError_t e = vof::plain_step(ctx->g, ctx->b, istep, ctx->prm.jacobi_iters, &ctx->p_parity,
+                                    ctx->stream);
+    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
+}
+
+int vof_run(vof_ctx* ctx, int istep0, int nsteps) {
+    if (!ctx || nsteps < 0) return VOF_E_INVALID;
+    DeviceGuard dg(ctx->device);
+    for (int s = 0; s < nsteps; ++s) {
+        const int istep = istep0 + s;
+        const int r = ((istep % 3) + 3) % 3;
+        const int par = ctx->p_parity;
+        if (!ctx->graph[r][par]) {
+            cudaGraph_t graph = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return fail_cuda(ctx, e);
+            int tmp_parity = par;
+            cudaError_t le = vof::plain_step(ctx->g, ctx->b, istep, ctx->prm.jacobi_iters, &tmp_parity,
+                                             ctx->cap_stream);
+            e = cudaStreamEndCapture(ctx->cap_stream, &graph);
+            if (le != cudaSuccess) e = le;
+            if (e != cudaSuccess) {
+                if (graph) cudaGraphDestroy(graph);
+                return fail_cuda(ctx, e);
+            }
+            e = cudaGraphInstantiate(&ctx->graph[r][par], graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                ctx->graph[r][par] = nullptr;
+                return fail_cuda(ctx, e);
+            }
+        }
+        cudaError_t e = cudaGraphLaunch(ctx->graph[r][par], ctx->stream);
+        if (e != cudaSuccess) return fail_cuda(ctx, e);
+        ctx->p_parity = par ^ (ctx->prm.jacobi_iters & 1);
+    }
+    return VOF_OK;
+}
+
+int vof_step_timed(vof_ctx* ctx, int istep, float* phase_ms, int* launches, int nphase) {
+    if (!ctx || nphase < 0) return VOF_E_INVALID;
+    DeviceGuard dg(ctx->device);
+    cudaEvent_t ev[vof::PLAIN_PHASES + 1] = {};
+    cudaError_t e = cudaSuccess;
+    for (int q = 0; q <= vof::PLAIN_PHASES && e == cudaSuccess; ++q) e = cudaEventCreate(&ev[q]);
+    if (e == cudaSuccess)
+        e = vof::plain_step(ctx->g, ctx->b, istep, ctx->prm.jacobi_iters, &ctx->p_parity, ctx->stream, ev);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev[vof::PLAIN_PHASES]);
+    const int n = nphase < VOF_PHASES ? nphase : VOF_PHASES;
+    for (int q = 0; q < n && e == cudaSuccess; ++q) {
+        float ms = 0.0f;
+        e = cudaEventElapsedTime(&ms, ev[q], ev[q + 1]);
+        if (phase_ms) phase_ms[q] = ms;
+        if (launches) launches[q] = vof::plain_phase_launches(q, ctx->prm.jacobi_iters);
+    }
+    for (int q = 0; q <= vof::PLAIN_PHASES; ++q)
+        if (ev[q]) cudaEventDestroy(ev[q]);
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    return n;
+}
+
+const char* vof_phase_name(int phase) {
+    static const char* names[VOF_PHASES] = {"predict", "rhs", "jacobi", "correct", "sweep1", "sweep2", "sweep3"};
+    return (phase >= 0 && phase < VOF_PHASES) ? names[phase] : nullptr;
+}
+
+int vof_sync(vof_ctx* ctx) {
+    if (!ctx) return VOF_E_INVALID;
+    DeviceGuard dg(ctx->device);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
+}
+
+int vof_reduce_async(vof_ctx* ctx, int what, double* host_out) {
+    if (!ctx || !host_out) return VOF_E_INVALID;
+    if (what < 0 || what >= VOF_NUM_REDUCTIONS) return VOF_E_INVALID;
+    DeviceGuard dg(ctx->device);
+    vof::ReduceInputs in;
+    in.F = ctx->b.F;
+    in.u = ctx->b.u;
+    in.v = ctx->b.v;
+    in.w = ctx->b.w;
+    in.p = ctx->p_parity ? ctx->b.p1 : ctx->b.p0;
+    in.rhs = ctx->b.rhs;
+    cudaError_t e = vof::reduce_launch(ctx->g, in, what, ctx->d_red_scratch, ctx->d_red_result,
+                                       ctx->stream);
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    e = cudaMemcpyAsync(host_out, ctx->d_red_result + vof::reduce_result_slot(what), sizeof(double),
+                        cudaMemcpyDeviceToHost, ctx->stream);
+    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
+}
+
+int vof_reduce(vof_ctx* ctx, int what, double* out) {
+    if (!ctx || !out) return VOF_E_INVALID;
+    int st = vof_reduce_async(ctx, what, ctx->h_red_result);
+    if (st != VOF_OK) return st;
+    st = vof_sync(ctx);
+    if (st != VOF_OK) return st;
+    *out = ctx->h_red_result[0];
+    return VOF_OK;
+}
+
+int vof_last_cuda_error(const vof_ctx* ctx) { return ctx ? ctx->last_cuda_error : 0; }
+
+int vof_kernels_per_step(const vof_ctx* ctx) {
+    if (!ctx) return VOF_E_INVALID;
+    return vof::plain_kernels_per_step(ctx->prm.jacobi_iters);
+}
+
+size_t vof_device_bytes(const vof_ctx* ctx) { return ctx ? ctx->bytes : 0; }
+
+}  // extern "C"

@@ -1,0 +1,57 @@
+// plain_step.h -- host-side interface of the FP32 drop-in step kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "vof_device.cuh"
+
+namespace vof {
+
+// Device buffers of one context, padded layout (vof_device.cuh).
+struct PlainBuffers {
+    float* F;
+    float* u;
+    float* v;
+    float* w;
+    float* us;   // predictor outputs; entries outside the updated range stay 0
+    float* vs;
+    float* ws;
+    float* rhs;  // rho/dt * div(u*)
+    float* p0;   // Jacobi ping-pong pair (DeviceFields::p / ::pt)
+    float* p1;
+};
+
+// Raise the dynamic shared-memory limit of the FCT kernels for lines of up to
+// max_line interior cells.  Call once per device before the first step.
+cudaError_t plain_configure(int max_line);
+
+// True when every FCT line tile of this grid fits in shared memory.
+bool plain_supported(const Geom& g);
+
+// Bytes of dynamic shared memory of one FCT tile for lines of n cells.
+size_t fct_smem_bytes(int n);
+
+// Kernel launches per plain step.
+int plain_kernels_per_step(int jacobi_iters);
+
+// Phases of one plain step, in launch order.
+enum {
+    PHASE_PREDICT = 0,
+    PHASE_RHS = 1,
+    PHASE_JACOBI = 2,
+    PHASE_CORRECT = 3,
+    PHASE_SWEEP1 = 4,
+    PHASE_SWEEP2 = 5,
+    PHASE_SWEEP3 = 6,
+    PLAIN_PHASES = 7
+};
+
+// Enqueue one plain step on stream s.  *p_parity (0/1) selects which of
+// p0/p1 holds the current pressure iterate and is updated for the ping-pong.
+// ev: NULL, or PLAIN_PHASES+1 events recorded around the phases.
+cudaError_t plain_step(const Geom& g, const PlainBuffers& b, int istep, int jacobi_iters,
+                       int* p_parity, cudaStream_t s, cudaEvent_t* ev = nullptr);
+
+// Kernel launches of one phase.
+int plain_phase_launches(int phase, int jacobi_iters);
+
+}  // namespace vof

@@ -1,0 +1,230 @@
+// reduce.cu -- FP64 diagnostics over the step state (no reference counterpart:
+// voftrial1.cu computes no reductions; the volume, divergence and residual
+// monitors are additions of this library).
+//
+// Every reduction is deterministic: pass 1 runs a fixed grid of RED_BLOCKS
+// blocks over a fixed cell->thread mapping, each block reducing with warp
+// shuffles into one FP64 partial; pass 2 is one block that folds the partials
+// in a fixed order.  The same inputs give the same bits on every run.
+#include "reduce.h"
+
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace vof {
+
+constexpr int RED_THREADS = 256;
+
+enum Op { OP_SUM = 0, OP_MAX = 1, OP_MIN = 2 };
+
+__device__ __forceinline__ double combine(double a, double b, int op) {
+    return op == OP_SUM ? a + b : (op == OP_MAX ? fmax(a, b) : fmin(a, b));
+}
+
+__device__ __forceinline__ double identity(int op) {
+    return op == OP_SUM ? 0.0 : (op == OP_MAX ? -INFINITY : INFINITY);
+}
+
+// Block reduction of NV values per thread into partial[NV*blockIdx.x + v].
+template <int NV>
+__device__ void block_reduce_store(double (&val)[NV], const int (&op)[NV], double* partial) {
+    __shared__ double sh[NV][RED_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        double x = val[v];
+        for (int o = 16; o > 0; o >>= 1) x = combine(x, __shfl_down_sync(0xffffffffu, x, o), op[v]);
+        if (lane == 0) sh[v][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            double x = sh[v][0];
+            for (int q = 1; q < RED_THREADS / 32; ++q) x = combine(x, sh[v][q], op[v]);
+            partial[(size_t)NV * blockIdx.x + v] = x;
+        }
+    }
+}
+
+// Interior-cell iterator: linear index over nx*ny*nz, grid-stride.
+#define FOR_INTERIOR(g, i, j, k)                                                        \
+    for (long long t_ = (long long)blockIdx.x * blockDim.x + threadIdx.x,               \
+                   n_ = (long long)(g).nx * (g).ny * (g).nz;                            \
+         t_ < n_; t_ += (long long)gridDim.x * blockDim.x)                              \
+        for (int i = 1 + (int)(t_ % (g).nx), j = 1 + (int)((t_ / (g).nx) % (g).ny),      \
+                 k = 1 + (int)(t_ / ((long long)(g).nx * (g).ny)), once_ = 1;           \
+             once_; once_ = 0)
+
+__global__ void __launch_bounds__(RED_THREADS) k_red_field(Geom g, const float* __restrict__ a,
+                                                           double* partial) {
+    // v0 = sum, v1 = max, v2 = min over interior cells.
+    double val[3] = {0.0, -INFINITY, INFINITY};
+    const int op[3] = {OP_SUM, OP_MAX, OP_MIN};
+    FOR_INTERIOR(g, i, j, k) {
+        const double x = (double)a[gidx(g, i, j, k)];
+        val[0] += x;
+        val[1] = fmax(val[1], x);
+        val[2] = fmin(val[2], x);
+    }
+    block_reduce_store<3>(val, op, partial);
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_red_div(Geom g, const float* __restrict__ u,
+                                                         const float* __restrict__ v,
+                                                         const float* __restrict__ w,
+                                                         double* partial) {
+    double val[2] = {0.0, 0.0};
+    const int op[2] = {OP_SUM, OP_MAX};
+    const double dxi = g.dxi, dyi = g.dyi, dzi = g.dzi;
+    FOR_INTERIOR(g, i, j, k) {
+        const int id = gidx(g, i, j, k);
+        const double d = ((double)u[id + 1] - (double)u[id]) * dxi +
+                         ((double)v[id + g.px] - (double)v[id]) * dyi +
+                         ((double)w[id + g.plane] - (double)w[id]) * dzi;
+        val[0] += d * d;
+        val[1] = fmax(val[1], fabs(d));
+    }
+    block_reduce_store<2>(val, op, partial);
+}
+
+// Residual of the pressure system A p = b, b = rhs - mean(rhs), with A the
+// Neumann operator of the Jacobi sweep (voftrial1.cu:424-430):
+// (A p)_c = sum over non-wall neighbours nb of a_nb (p_nb - p_c).
+__global__ void __launch_bounds__(RED_THREADS) k_red_resid(Geom g, const float* __restrict__ rhs,
+                                                           const float* __restrict__ p,
+                                                           const double* __restrict__ mean,
+                                                           double* partial) {
+    double val[2] = {0.0, 0.0};
+    const int op[2] = {OP_SUM, OP_SUM};
+    const double m = *mean;
+    const double cx = (double)g.dxi * g.dxi, cy = (double)g.dyi * g.dyi, cz = (double)g.dzi * g.dzi;
+    FOR_INTERIOR(g, i, j, k) {
+        const int id = gidx(g, i, j, k);
+        const double pc = p[id];
+        double ap = 0.0;
+        if (i != g.nx) ap += cx * ((double)p[id + 1] - pc);
+        if (i != 1) ap += cx * ((double)p[id - 1] - pc);
+        if (j != g.ny) ap += cy * ((double)p[id + g.px] - pc);
+        if (j != 1) ap += cy * ((double)p[id - g.px] - pc);
+        if (k != g.nz) ap += cz * ((double)p[id + g.plane] - pc);
+        if (k != 1) ap += cz * ((double)p[id - g.plane] - pc);
+        const double b = (double)rhs[id] - m;
+        const double r = b - ap;
+        val[0] += r * r;
+        val[1] += b * b;
+    }
+    block_reduce_store<2>(val, op, partial);
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_red_nonfinite(Geom g, const float* __restrict__ f0,
+                                                               const float* __restrict__ f1,
+                                                               const float* __restrict__ f2,
+                                                               const float* __restrict__ f3,
+                                                               const float* __restrict__ f4,
+                                                               double* partial) {
+    double val[1] = {0.0};
+    const int op[1] = {OP_SUM};
+    const long long n = (long long)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % (g.nx + 2));
+        const int j = (int)((t / (g.nx + 2)) % (g.ny + 2));
+        const int k = (int)(t / ((long long)(g.nx + 2) * (g.ny + 2)));
+        const int id = gidx(g, i, j, k);
+        val[0] += (double)(!isfinite(f0[id])) + (double)(!isfinite(f1[id])) +
+                  (double)(!isfinite(f2[id])) + (double)(!isfinite(f3[id])) +
+                  (double)(!isfinite(f4[id]));
+    }
+    block_reduce_store<1>(val, op, partial);
+}
+
+// Pass 2: fold nblk partials of NV values; result[v] for each v.  Optional
+// post-processing: MODE_MEAN divides result[0] by count, MODE_SQRT takes the
+// square root of result[0], MODE_RATIO = sqrt(result[0] / result[1]),
+// MODE_VOLUME multiplies result[0] by the cell volume.
+enum Post { POST_NONE = 0, POST_MEAN = 1, POST_SQRT = 2, POST_RATIO = 3, POST_SCALE = 4 };
+
+__global__ void __launch_bounds__(RED_THREADS) k_red_finish(const double* __restrict__ partial,
+                                                            int nblk, int nv, int op0, int op1,
+                                                            int op2, int post, double scale,
+                                                            double* result) {
+    __shared__ double sh[3][RED_THREADS];
+    const int ops[3] = {op0, op1, op2};
+    for (int v = 0; v < nv; ++v) {
+        double x = identity(ops[v]);
+        for (int b = threadIdx.x; b < nblk; b += RED_THREADS)
+            x = combine(x, partial[(size_t)nv * b + v], ops[v]);
+        sh[v][threadIdx.x] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r[3];
+        for (int v = 0; v < nv; ++v) {
+            double x = sh[v][0];
+            for (int q = 1; q < RED_THREADS; ++q) x = combine(x, sh[v][q], ops[v]);
+            r[v] = x;
+        }
+        double out0 = r[0];
+        if (post == POST_MEAN) out0 = r[0] * scale;
+        else if (post == POST_SQRT) out0 = sqrt(r[0]);
+        else if (post == POST_RATIO) out0 = (r[1] > 0.0) ? sqrt(r[0] / r[1]) : 0.0;
+        else if (post == POST_SCALE) out0 = r[0] * scale;
+        result[0] = out0;
+        for (int v = 1; v < nv; ++v) result[v] = r[v];
+    }
+}
+
+cudaError_t reduce_launch(const Geom& g, const ReduceInputs& in, int what, double* d_scratch,
+                          double* d_result, cudaStream_t s) {
+    const int nblk = RED_BLOCKS;
+    double* part = d_scratch;
+    const double ncell = (double)g.nx * g.ny * g.nz;
+    switch (what) {
+        case RED_VOLUME:
+        case RED_F_MIN:
+        case RED_F_MAX: {
+            k_red_field<<<nblk, RED_THREADS, 0, s>>>(g, in.F, part);
+            const double vol = (double)g.dx * (double)g.dy * (double)g.dz;
+            // result[0] = volume, [1] = max, [2] = min
+            k_red_finish<<<1, RED_THREADS, 0, s>>>(part, nblk, 3, OP_SUM, OP_MAX, OP_MIN,
+                                                   POST_SCALE, vol, d_result);
+            break;
+        }
+        case RED_DIV_L2:
+        case RED_DIV_MAX:
+            k_red_div<<<nblk, RED_THREADS, 0, s>>>(g, in.u, in.v, in.w, part);
+            k_red_finish<<<1, RED_THREADS, 0, s>>>(part, nblk, 2, OP_SUM, OP_MAX, OP_SUM,
+                                                   POST_SQRT, 1.0, d_result);
+            break;
+        case RED_PRES_RESID: {
+            // mean(rhs) into d_result[3], then the residual ratio into d_result[0].
+            k_red_field<<<nblk, RED_THREADS, 0, s>>>(g, in.rhs, part);
+            k_red_finish<<<1, RED_THREADS, 0, s>>>(part, nblk, 3, OP_SUM, OP_MAX, OP_MIN,
+                                                   POST_MEAN, 1.0 / ncell, d_result + 3);
+            k_red_resid<<<nblk, RED_THREADS, 0, s>>>(g, in.rhs, in.p, d_result + 3, part);
+            k_red_finish<<<1, RED_THREADS, 0, s>>>(part, nblk, 2, OP_SUM, OP_SUM, OP_SUM,
+                                                   POST_RATIO, 1.0, d_result);
+            break;
+        }
+        case RED_NONFINITE:
+            k_red_nonfinite<<<nblk, RED_THREADS, 0, s>>>(g, in.F, in.u, in.v, in.w, in.p, part);
+            k_red_finish<<<1, RED_THREADS, 0, s>>>(part, nblk, 1, OP_SUM, OP_SUM, OP_SUM,
+                                                   POST_NONE, 1.0, d_result);
+            break;
+        default:
+            return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+int reduce_result_slot(int what) {
+    switch (what) {
+        case RED_F_MAX: return 1;
+        case RED_F_MIN: return 2;
+        case RED_DIV_MAX: return 1;
+        default: return 0;
+    }
+}
+
+}  // namespace vof

@@ -1,0 +1,58 @@
+// vof_device.cuh -- device-side geometry, padded layout and the scalar
+// helpers of the reference (voftrial1.cu:52-70), shared by every kernel TU.
+//
+// Layout in HBM (internal, padded): cell (i,j,k), i in [0,nx+1] ... is at
+//     ((k * py) + j) * px + i,   px = round_up(nx+2, 32), py = ny+2,
+// so every x-row starts on a 128-byte boundary (TMA-legal strides, aligned
+// vector loads).  The reference layout (voftrial1.cu:66-70) has px = nx+2 and
+// is converted only at the C-ABI boundary (vof_upload / vof_download).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace vof {
+
+// Everything a step kernel needs, passed by value (kernel parameter space).
+struct Geom {
+    int nx, ny, nz;      // interior cells
+    int px, py;          // x pitch (elements) and y extent (ny+2) of the padded layout
+    int plane;           // px*py
+    // Physics/geometry constants, the float values of Params (voftrial1.cu:27-41).
+    float dt, dx, dy, dz, dxi, dyi, dzi;
+    float rho_l, rho_g, nu_l, nu_g;
+    float gx, gy, gz;
+};
+
+__host__ __device__ __forceinline__ int gidx(const Geom& g, int i, int j, int k) {
+    return (k * g.py + j) * g.px + i;
+}
+
+__host__ __device__ __forceinline__ int clampi(int v, int lo, int hi) {
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+// median3f / clamp01f (voftrial1.cu:52-60).  The expression a+b+c-mx-mn is
+// evaluated left to right in FP32, which rounds v to a multiple of 2^-23 on
+// [0,1) and maps tiny negatives to tiny values of either sign; the step's
+// results depend on that, so the expression is kept as it is.
+__host__ __device__ __forceinline__ float median3f(float a, float b, float c) {
+    const float mx = fmaxf(fmaxf(a, b), c);
+    const float mn = fminf(fminf(a, b), c);
+    return a + b + c - mx - mn;
+}
+
+__host__ __device__ __forceinline__ float clamp01f(float v) {
+    return median3f(0.0f, 1.0f, v);
+}
+
+// rho and nu from the volume fraction (voftrial1.cu:95-104), same operand order.
+__device__ __forceinline__ float rho_of(const Geom& g, float F) {
+    const float f = clamp01f(F);
+    return g.rho_g * (1.0f - f) + g.rho_l * f;
+}
+__device__ __forceinline__ float nu_of(const Geom& g, float F) {
+    const float f = clamp01f(F);
+    return g.nu_l * f + g.nu_g * (1.0f - f);
+}
+
+}  // namespace vof

@@ -1,0 +1,78 @@
+"""Build recipe for libvof_b200.so (sm_100a) -- nvcc only, no JIT cache.
+
+The shared library is written next to this file, inside the source tree, so it
+travels with the repository to the machine that runs it.  Object files go to
+``cuda-lbm-ibm-fvm_b200/_build``.
+
+``plain_step.cu`` is compiled with ``-fmad=false``: the FP32 drop-in step keeps
+the reference's per-point expressions without FMA contraction, which makes it
+bit-identical to the CPU restatement (oracle/) and to the reference's kernels
+compiled the same way.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG_DIR = Path(__file__).resolve().parent
+SRC_DIR = PKG_DIR.parent / "csrc"
+BUILD_DIR = PKG_DIR.parent / "_build"
+INCLUDE_DIR = PKG_DIR.parent.parent / "include"
+LIB_PATH = PKG_DIR / "libvof_b200.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + str(INCLUDE_DIR),
+          "-Xptxas", "-warn-spills"]
+
+# source -> extra flags
+SOURCES = {
+    "plain_step.cu": ["-fmad=false", "-DVOF_FMAD_FALSE"],
+    "reduce.cu": [],
+    "capi.cu": [],
+}
+HEADERS = ["vof_device.cuh", "plain_step.h", "reduce.h"]
+
+
+def nvcc() -> str:
+    exe = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(exe):
+        raise RuntimeError("nvcc not found: cannot build libvof_b200.so")
+    return exe
+
+
+def _stale(target: Path, deps) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(Path(d).stat().st_mtime > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile every CUDA source for sm_100a and link libvof_b200.so."""
+    BUILD_DIR.mkdir(parents=True, exist_ok=True)
+    headers = [SRC_DIR / h for h in HEADERS] + [INCLUDE_DIR / "vof.h"]
+    objs = []
+    for src, extra in SOURCES.items():
+        s = SRC_DIR / src
+        o = BUILD_DIR / (src + ".o")
+        objs.append(o)
+        if force or _stale(o, [s, *headers, Path(__file__)]):
+            cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", str(s), "-o", str(o)]
+            if verbose:
+                print(" ".join(cmd), file=sys.stderr)
+            subprocess.run(cmd, check=True)
+    if force or _stale(LIB_PATH, objs):
+        tmp = LIB_PATH.with_suffix(".so.tmp")
+        cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *map(str, objs), "-o", str(tmp)]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -1,0 +1,202 @@
+/*
+ * vof.h -- C-ABI of the B200 two-phase VOF step library (libvof_b200.so).
+ *
+ * The library replaces the time-loop body of voftrial1.cu
+ * (voftrial1.cu:1361-1401): rho/nu from the volume fraction, the explicit
+ * momentum predictor, the Jacobi pressure sweeps, the velocity correction,
+ * the free-slip velocity boundary conditions, the three directionally split
+ * FCT sweeps of the volume fraction in the istep-dependent order, the final
+ * clamp and the zero-gradient volume-fraction boundary conditions.
+ *
+ * Conventions (they differ from the reference's host launchers on purpose):
+ *  - Every entry point returns an int status: VOF_OK (0) or a negative
+ *    VOF_E_* code.  The library never calls exit().  The CUDA error behind a
+ *    VOF_E_CUDA is kept and returned by vof_last_cuda_error().
+ *  - All work is enqueued on the stream given to vof_create (a cudaStream_t
+ *    passed as void*; NULL means the legacy default stream, which is what the
+ *    reference uses).  vof_step and vof_run do not synchronise the host.
+ *  - One context per host thread.  Fields cross the boundary in the
+ *    reference's own layout: (nx+2)(ny+2)(nz+2) floats, i fastest, one ghost
+ *    layer (voftrial1.cu:66-70); the context keeps a padded copy internally.
+ */
+#ifndef VOF_B200_H
+#define VOF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VOF_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define VOF_OK               0
+#define VOF_E_INVALID      (-1)  /* bad argument (null pointer, bad field id, ...) */
+#define VOF_E_SIZE         (-2)  /* grid size out of the supported range         */
+#define VOF_E_NOMEM        (-3)  /* device or pinned host allocation failed        */
+#define VOF_E_CUDA         (-4)  /* a CUDA runtime call failed                     */
+#define VOF_E_NOT_CONVERGED (-5) /* iterative solve hit its iteration cap          */
+#define VOF_E_NONFINITE    (-6)  /* watchdog found NaN/Inf in the state            */
+#define VOF_E_STATE        (-7)  /* call not valid in the current context state    */
+#define VOF_E_UNSUPPORTED  (-8)  /* feature not built / mode not available         */
+
+/* ---- solver modes ------------------------------------------------------ */
+#define VOF_MODE_PLAIN  0   /* FP32, jacobi_iters Jacobi sweeps: the drop-in path */
+#define VOF_MODE_MIXED  1   /* FP64 defect correction over a BF16-stored/FP32 inner solve */
+#define VOF_MODE_FP64   2   /* same convergent projection, every field in FP64    */
+
+/* ---- field identifiers (vof_upload / vof_download) --------------------- */
+#define VOF_FIELD_F      0  /* volume fraction (DeviceFields::F)      */
+#define VOF_FIELD_U      1  /* x face velocity, u[i] on face i-1/2    */
+#define VOF_FIELD_V      2
+#define VOF_FIELD_W      3
+#define VOF_FIELD_P      4  /* pressure (current Jacobi iterate)      */
+#define VOF_FIELD_USTAR  5  /* predictor output of the last step      */
+#define VOF_FIELD_VSTAR  6
+#define VOF_FIELD_WSTAR  7
+#define VOF_FIELD_RHS    8  /* rho/dt * div(u*) of the last step (no reference buffer) */
+#define VOF_NUM_FIELDS   9
+
+/* ---- reductions (vof_reduce) -------------------------------------------- */
+#define VOF_RED_VOLUME      0  /* sum over interior cells of F*dx*dy*dz (FP64)         */
+#define VOF_RED_DIV_L2      1  /* sqrt(sum of (div u)^2) over interior cells (FP64)    */
+#define VOF_RED_DIV_MAX     2  /* max |div u| over interior cells                      */
+#define VOF_RED_PRES_RESID  3  /* ||b - A p|| / ||b|| of the last pressure system,
+                                  b = rhs with its mean removed (FP64)                 */
+#define VOF_RED_NONFINITE   4  /* number of NaN/Inf values in F,u,v,w,p (as a double)  */
+#define VOF_RED_F_MIN       5  /* min of F over interior cells                         */
+#define VOF_RED_F_MAX       6  /* max of F over interior cells                         */
+#define VOF_NUM_REDUCTIONS  7
+
+/*
+ * Mirrors struct Params (voftrial1.cu:27-41) field for field and in the same
+ * order, followed by the additions this library needs.
+ */
+typedef struct vof_params {
+    int nx, ny, nz;
+    int imin, imax;
+    int jmin, jmax;
+    int kmin, kmax;
+    float Lx, Ly, Lz;
+    float rho_l, rho_g;
+    float nu_l, nu_g;
+    float sigma;            /* stored and reported; no kernel reads it (as in the reference) */
+    float gx, gy, gz;
+    float dt;
+    float dx, dy, dz;
+    float dxi, dyi, dzi;
+    int nTot;
+    /* ---- additions (no counterpart in Params) ---- */
+    int jacobi_iters;       /* plain mode: sweeps per step; voftrial1.cu:1371 hardcodes 10 */
+    int mode;               /* VOF_MODE_*                                                   */
+    int inner_sweeps;       /* mixed/fp64 modes: smoothing sweeps per inner solve (default 32) */
+    int max_outer;          /* mixed/fp64 modes: cap on defect-correction iterations        */
+    double tol;             /* mixed/fp64 modes: target ||b-Ap||/||b|| (default 1e-8)       */
+} vof_params;
+
+typedef struct vof_ctx vof_ctx;
+
+/* Library ABI version (VOF_ABI_VERSION of the build). */
+int vof_abi_version(void);
+
+/* Short static description of a status code. */
+const char* vof_error_string(int status);
+
+/*
+ * Fill *p for an nx x ny x nz grid the way voftrial1.cu:1262-1291 fills
+ * cpar_host (same float expressions for dx and dxi), with the reference's
+ * constants: 0.1 m box, rho 1000/50, nu 1e-6/1.5e-5, sigma 0.007,
+ * g = (0,-5,0), dt 4e-6, plus jacobi_iters = 10 and mode = VOF_MODE_PLAIN.
+ * Callers change gx/gy/gz, dt, ... afterwards and call vof_params_finalize.
+ */
+int vof_params_init(vof_params* p, int nx, int ny, int nz);
+
+/*
+ * Recompute the derived members (imin..kmax, dx..dzi, nTot) from nx,ny,nz
+ * and Lx,Ly,Lz with the reference's float expressions (voftrial1.cu:1268-1291).
+ */
+int vof_params_finalize(vof_params* p);
+
+/*
+ * Create a context: validates *p, allocates every device buffer zero-filled
+ * (voftrial1.cu:1200-1203, 1306-1326) in the padded internal layout.
+ * `stream` is a cudaStream_t (NULL = legacy default stream).
+ * Replaces: DeviceFields + alloc_field + cudaMemcpyToSymbol(cpar)
+ * (voftrial1.cu:1176-1203, :1293, :1303-1326).
+ */
+int vof_create(const vof_params* p, void* stream, vof_ctx** out);
+
+/* Release every buffer of the context (voftrial1.cu:1205-1226). NULL is a no-op. */
+void vof_destroy(vof_ctx* ctx);
+
+/* Copy of the parameters the context runs with. */
+int vof_get_params(const vof_ctx* ctx, vof_params* out);
+
+/*
+ * Copy one field from `src` (reference layout, nTot floats) into the context.
+ * src_is_device != 0: src is a device pointer; otherwise host memory (pinned
+ * or pageable).  Stream-ordered; host memory must stay valid until the
+ * stream reaches the copy (vof_sync).
+ */
+int vof_upload(vof_ctx* ctx, int field, const float* src, int src_is_device);
+
+/* Copy one field out of the context into `dst` (reference layout, nTot floats). */
+int vof_download(vof_ctx* ctx, int field, float* dst, int dst_is_device);
+
+/*
+ * One time step, exactly the sequence of voftrial1.cu:1364-1401 for the
+ * given istep (the value the reference's loop has after `++istep`, so the
+ * first step is istep = 1; istep % 3 picks the FCT sweep order,
+ * voftrial1.cu:1384-1396).
+ */
+int vof_step(vof_ctx* ctx, int istep);
+
+/*
+ * Steps istep0 .. istep0+nsteps-1 through captured CUDA graphs (one per
+ * sweep order and Jacobi-buffer parity).  Same results as nsteps vof_step calls.
+ */
+int vof_run(vof_ctx* ctx, int istep0, int nsteps);
+
+/*
+ * Per-phase timing (no reference counterpart; voftrial1.cu times only the
+ * whole loop, voftrial1.cu:1359, 1416-1420).  Runs one vof_step with CUDA
+ * events recorded on the context's stream around each phase, waits for it,
+ * and writes the milliseconds of phase q to phase_ms[q] and its kernel
+ * launches to launches[q] (either may be NULL) for q < min(nphase,
+ * VOF_PHASES).  Phases: predict, rhs, jacobi, correct, sweep1, sweep2, sweep3.
+ */
+#define VOF_PHASES 7
+int vof_step_timed(vof_ctx* ctx, int istep, float* phase_ms, int* launches, int nphase);
+
+/* Name of phase q of vof_step_timed ("predict", "jacobi", ...), NULL if out of range. */
+const char* vof_phase_name(int phase);
+
+/* Wait for all work enqueued on the context's stream. */
+int vof_sync(vof_ctx* ctx);
+
+/* Blocking reduction over the current state (VOF_RED_*); result in *out. */
+int vof_reduce(vof_ctx* ctx, int what, double* out);
+
+/*
+ * Stream-ordered reduction: the result is written to *host_out (which should
+ * be pinned host memory) when the stream reaches this point; the host must
+ * vof_sync before reading it.  No host synchronisation inside.
+ */
+int vof_reduce_async(vof_ctx* ctx, int what, double* host_out);
+
+/* cudaError_t of the most recent failing CUDA call in this context (0 if none). */
+int vof_last_cuda_error(const vof_ctx* ctx);
+
+/* Number of kernel launches one vof_step enqueues for the current settings. */
+int vof_kernels_per_step(const vof_ctx* ctx);
+
+/* Device bytes held by the context. */
+size_t vof_device_bytes(const vof_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VOF_B200_H */

@@ -1,0 +1,153 @@
+"""ctypes loaders of the checkers under oracle/ -- TEST INFRASTRUCTURE ONLY.
+
+Imported by tests/, __graft_entry__.smoke() and bench.py (CPU-baseline leg and
+``--impl reference``); never by the library.
+
+  * ``run_f32`` / ``run_f64``: the CPU restatement of the reference step
+    (vof_oracle.cpp), FP32 without FMA contraction, or FP64.
+  * ``ref_run`` / ``ref_time``: the reference's own kernels (voftrial1.cu
+    compiled with ref_harness.cu into oracle/_ref/); GPU only.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ORACLE_DIR = Path(__file__).resolve().parent
+ORACLE_LIB = ORACLE_DIR / "_build" / "liboracle.so"
+REF_LIBS = {
+    "sm100a": ORACLE_DIR / "_ref" / "libvofref_sm100a.so",   # nvcc -O3 sm_100a (default -fmad=true)
+    "nofma": ORACLE_DIR / "_ref" / "libvofref_nofma.so",     # same, -fmad=false
+    "readme": ORACLE_DIR / "_ref" / "libvofref_readme.so",   # README flags, PTX JIT
+}
+REFERENCE_SRC = Path(os.environ.get("VOF_REFERENCE_DIR", "/root/reference"))
+
+STATE = ("F", "u", "v", "w", "p")
+
+_oracle = None
+_refs = {}
+
+
+def build(ref: bool | None = None) -> None:
+    """make the oracle (always) and the reference harness (when its source exists)."""
+    targets = ["oracle"]
+    if ref is None:
+        ref = (REFERENCE_SRC / "voftrial1.cu").exists()
+    if ref:
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), f"REF_DIR={REFERENCE_SRC}", *targets], check=True)
+
+
+def _params_type():
+    sys.path.insert(0, str(ORACLE_DIR.parent / "cuda-lbm-ibm-fvm_b200"))
+    from vof_b200 import Params  # the ctypes mirror of vof_params
+    return Params
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        if not ORACLE_LIB.exists():
+            build(ref=False)
+        Params = _params_type()
+        lib = C.CDLL(str(ORACLE_LIB))
+        for name, T in (("oracle_run_f32", C.c_float), ("oracle_run_f64", C.c_double)):
+            fn = getattr(lib, name)
+            fn.restype = C.c_int
+            fn.argtypes = [C.POINTER(Params)] + [C.POINTER(T)] * 5 + [C.c_int, C.c_int] + \
+                [C.POINTER(T)] * 4 + [C.c_int]
+        lib.oracle_clamp01f.restype = C.c_float
+        lib.oracle_clamp01f.argtypes = [C.c_float]
+        lib.oracle_clamp01d.restype = C.c_double
+        lib.oracle_clamp01d.argtypes = [C.c_double]
+        lib.oracle_max_threads.restype = C.c_int
+        _oracle = lib
+    return _oracle
+
+
+def _ptr(a, T):
+    return a.ctypes.data_as(C.POINTER(T)) if a is not None else None
+
+
+def _run(fn, T, dtype, prm, state, istep0, nsteps, nthreads, extras):
+    st = {k: np.ascontiguousarray(state[k], dtype=dtype).copy() for k in STATE}
+    ex = {k: np.zeros(prm.shape, dtype=dtype) for k in ("ustar", "vstar", "wstar", "rhs")} if extras else {}
+    rc = fn(C.byref(prm), *(_ptr(st[k], T) for k in STATE), istep0, nsteps,
+            *(_ptr(ex.get(k), T) for k in ("ustar", "vstar", "wstar", "rhs")), int(nthreads))
+    if rc != 0:
+        raise RuntimeError(f"oracle run failed: {rc}")
+    st.update(ex)
+    return st
+
+
+def run_f32(prm, state, istep0: int, nsteps: int, nthreads: int = 0, extras: bool = False) -> dict:
+    """nsteps reference steps in FP32 (IEEE, no FMA) on a copy of `state`."""
+    return _run(oracle_lib().oracle_run_f32, C.c_float, np.float32, prm, state, istep0, nsteps, nthreads, extras)
+
+
+def run_f64(prm, state, istep0: int, nsteps: int, nthreads: int = 0, extras: bool = False) -> dict:
+    """nsteps reference steps in FP64 on a copy of `state` (promoted to float64)."""
+    return _run(oracle_lib().oracle_run_f64, C.c_double, np.float64, prm, state, istep0, nsteps, nthreads, extras)
+
+
+def clamp01f(x: float) -> float:
+    return oracle_lib().oracle_clamp01f(x)
+
+
+def max_threads() -> int:
+    return oracle_lib().oracle_max_threads()
+
+
+# ---- the reference's own kernels (GPU) ------------------------------------
+def ref_available(variant: str = "sm100a") -> bool:
+    return REF_LIBS[variant].exists()
+
+
+def ref_lib(variant: str = "sm100a"):
+    if variant not in _refs:
+        path = REF_LIBS[variant]
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (needs the reference source; see oracle/Makefile)")
+        Params = _params_type()
+        lib = C.CDLL(str(path))
+        F = C.POINTER(C.c_float)
+        lib.ref_run.restype = C.c_int
+        lib.ref_run.argtypes = [C.POINTER(Params)] + [F] * 5 + [C.c_int, C.c_int] + [F] * 3
+        lib.ref_time.restype = C.c_int
+        lib.ref_time.argtypes = [C.POINTER(Params)] + [F] * 5 + [C.c_int, C.c_int, C.c_int,
+                                                                 C.POINTER(C.c_double), F]
+        lib.ref_kernels_per_step.restype = C.c_int
+        lib.ref_kernels_per_step.argtypes = [C.c_int]
+        _refs[variant] = lib
+    return _refs[variant]
+
+
+def ref_run(prm, state, istep0: int, nsteps: int, variant: str = "sm100a", extras: bool = False) -> dict:
+    lib = ref_lib(variant)
+    st = {k: np.ascontiguousarray(state[k], dtype=np.float32).copy() for k in STATE}
+    ex = {k: np.zeros(prm.shape, dtype=np.float32) for k in ("ustar", "vstar", "wstar")} if extras else {}
+    rc = lib.ref_run(C.byref(prm), *(_ptr(st[k], C.c_float) for k in STATE), istep0, nsteps,
+                     *(_ptr(ex.get(k), C.c_float) for k in ("ustar", "vstar", "wstar")))
+    if rc != 0:
+        raise RuntimeError(f"ref_run failed: {rc}")
+    st.update(ex)
+    return st
+
+
+def ref_time(prm, state, istep0: int, warmup: int, nsteps: int, variant: str = "sm100a",
+             want_F: bool = False):
+    """Milliseconds of nsteps reference steps (CUDA events), and F if asked."""
+    lib = ref_lib(variant)
+    st = {k: np.ascontiguousarray(state[k], dtype=np.float32) for k in STATE}
+    ms = C.c_double()
+    Fo = np.zeros(prm.shape, dtype=np.float32) if want_F else None
+    rc = lib.ref_time(C.byref(prm), *(_ptr(st[k], C.c_float) for k in STATE), istep0, warmup, nsteps,
+                      C.byref(ms), _ptr(Fo, C.c_float))
+    if rc != 0:
+        raise RuntimeError(f"ref_time failed: {rc}")
+    return ms.value, Fo

@@ -1,0 +1,270 @@
+"""Parity of the CUDA step (through the C-ABI) with the oracle and the reference.
+
+Tolerances:
+  * vs the FP32 CPU restatement (oracle, no FMA): bit-identical (np.array_equal,
+    so +0 == -0) for F, u, v, w, p, u*, v*, w* and rhs.
+  * vs the reference's kernels built with -fmad=false: bit-identical.
+  * vs the reference's kernels built with nvcc defaults (FMA contraction):
+    max-abs and relative-L2 bounds stated in each test.
+  * vs the FP64 oracle: relative-L2 bounds stated in each test.
+"""
+import numpy as np
+import pytest
+
+from vof_b200 import ic
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("F", "u", "v", "w", "p")
+
+
+def run_gpu(V, prm, state, istep0, nsteps, use_graph=False, extras=False):
+    with V.Solver(prm) as s:
+        s.upload_state(**state)
+        if use_graph:
+            s.run(istep0, nsteps)
+        else:
+            for t in range(nsteps):
+                s.step(istep0 + t)
+        out = s.state()
+        if extras:
+            for k in ("ustar", "vstar", "wstar", "rhs"):
+                out[k] = s.download(k)
+    return out
+
+
+def assert_bitwise(got, want, keys, ctx=""):
+    for k in keys:
+        g, w = got[k], want[k]
+        if not np.array_equal(g, w):
+            bad = np.argwhere(g != w)
+            kk, jj, ii = bad[0]
+            raise AssertionError(
+                f"{ctx} field {k}: {len(bad)} cells differ; first (k,j,i)=({kk},{jj},{ii}) "
+                f"got {g[kk, jj, ii]!r} want {w[kk, jj, ii]!r}")
+
+
+def rel_l2(a, b):
+    a = a.astype(np.float64)
+    b = b.astype(np.float64)
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+CASES = [
+    # (nx, ny, nz, seed, dt, vel_scale)
+    (16, 12, 10, 1, 1e-3, 1.0),
+    (17, 9, 13, 2, 5e-4, 2.0),
+    (32, 32, 32, 3, 4e-6, 1.0),
+    (1, 3, 2, 4, 1e-3, 1.0),
+    (40, 33, 21, 5, 2e-4, 3.0),
+]
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed,dt,vs", CASES)
+def test_random_state_bitwise_vs_oracle(cuda, V, orc, nx, ny, nz, seed, dt, vs):
+    prm = V.default_params(nx, ny, nz, dt=dt, gy=0.0, gz=-9.81)
+    state = ic.random_state(prm, seed=seed, vel_scale=vs)
+    got = run_gpu(V, prm, state, 1, 3, extras=True)  # istep 1,2,3: all sweep orders
+    want = orc.run_f32(prm, state, 1, 3, extras=True)
+    assert_bitwise(got, want, STATE + ("ustar", "vstar", "wstar", "rhs"), f"{nx}x{ny}x{nz}")
+
+
+@pytest.mark.parametrize("istep", [1, 2, 3])
+def test_each_sweep_order_bitwise(cuda, V, orc, istep):
+    prm = V.default_params(20, 18, 16, dt=5e-4)
+    state = ic.random_state(prm, seed=100 + istep, vel_scale=1.5)
+    got = run_gpu(V, prm, state, istep, 1)
+    want = orc.run_f32(prm, state, istep, 1)
+    assert_bitwise(got, want, STATE, f"istep={istep}")
+
+
+@pytest.mark.parametrize("iters", [0, 1, 7, 10])
+def test_jacobi_iteration_counts(cuda, V, orc, iters):
+    prm = V.default_params(12, 14, 10, dt=1e-3, jacobi_iters=iters)
+    state = ic.random_state(prm, seed=7, vel_scale=1.0)
+    got = run_gpu(V, prm, state, 1, 4)
+    want = orc.run_f32(prm, state, 1, 4)
+    assert_bitwise(got, want, STATE, f"iters={iters}")
+    got_g = run_gpu(V, prm, state, 1, 4, use_graph=True)
+    assert_bitwise(got_g, want, STATE, f"graph iters={iters}")
+
+
+def test_graph_run_equals_steps(cuda, V):
+    prm = V.default_params(24, 24, 24, dt=2e-4)
+    state = ic.random_state(prm, seed=9, vel_scale=1.0)
+    a = run_gpu(V, prm, state, 5, 7, use_graph=False)
+    b = run_gpu(V, prm, state, 5, 7, use_graph=True)
+    assert_bitwise(a, b, STATE, "graph vs step")
+
+
+def test_dam_break_32_200_steps(cuda, V, orc):
+    """The 32^3 dam break of 200 steps (gravity -9.81 along z)."""
+    prm = V.default_params(32, gy=0.0, gz=-9.81)
+    state = ic.rest_state(prm, ic.dam_break(prm))
+    got = run_gpu(V, prm, state, 1, 200, use_graph=True)
+    want = orc.run_f32(prm, state, 1, 200)
+    assert_bitwise(got, want, STATE, "32^3 x 200")
+    ref64 = orc.run_f64(prm, state, 1, 200)
+    # FP32 vs FP64 after 200 steps (measured ~1e-5; bound 1e-4 rel-L2, p modulo its mean)
+    for k in ("F", "u", "v", "w"):
+        assert rel_l2(got[k], ref64[k]) < 1e-4, k
+    pm = got["p"][1:-1, 1:-1, 1:-1].astype(np.float64)
+    qm = ref64["p"][1:-1, 1:-1, 1:-1]
+    assert rel_l2(pm - pm.mean(), qm - qm.mean()) < 1e-4
+    vol0 = state["F"][1:-1, 1:-1, 1:-1].sum(dtype=np.float64)
+    vol1 = got["F"][1:-1, 1:-1, 1:-1].sum(dtype=np.float64)
+    assert abs(vol1 / vol0 - 1.0) < 1e-5  # measured -5.4e-7 in FP32
+
+
+def test_invariants_after_step(cuda, V):
+    prm = V.default_params(18, 16, 14, dt=5e-4)
+    state = ic.random_state(prm, seed=21, vel_scale=1.0)
+    got = run_gpu(V, prm, state, 2, 1)
+    u, v, w, F = got["u"], got["v"], got["w"], got["F"]
+    # wall-normal face velocities are exactly 0 (voftrial1.cu:980-986, 1012-1018, 1044-1050)
+    assert np.all(u[:, :, 1] == 0) and np.all(u[:, :, -1] == 0)
+    assert np.all(v[:, 1, :] == 0) and np.all(v[:, -1, :] == 0)
+    assert np.all(w[1, :, :] == 0) and np.all(w[-1, :, :] == 0)
+    # F ghosts equal the clamped interior index (apply_bc_F composition)
+    ci = np.clip(np.arange(prm.nx + 2), 1, prm.nx)
+    cj = np.clip(np.arange(prm.ny + 2), 1, prm.ny)
+    ck = np.clip(np.arange(prm.nz + 2), 1, prm.nz)
+    assert np.array_equal(F, F[np.ix_(ck, cj, ci)])
+    assert F.min() >= -1e-6 and F.max() <= 1.0
+
+
+def test_reductions_match_numpy(cuda, V):
+    prm = V.default_params(30, 26, 22, dt=5e-4)
+    state = ic.random_state(prm, seed=31, vel_scale=1.0)
+    with V.Solver(prm) as s:
+        s.upload_state(**state)
+        s.step(1)
+        st = s.state()
+        rhs = s.download("rhs").astype(np.float64)
+        red = {k: s.reduce(k) for k in V.REDUCTIONS}
+    F = st["F"][1:-1, 1:-1, 1:-1].astype(np.float64)
+    vol = F.sum() * float(prm.dx) * float(prm.dy) * float(prm.dz)
+    assert red["volume"] == pytest.approx(vol, rel=1e-12)
+    assert red["f_min"] == F.min() and red["f_max"] == F.max()
+    u, v, w = (st[k].astype(np.float64) for k in "uvw")
+    div = ((u[1:-1, 1:-1, 2:] - u[1:-1, 1:-1, 1:-1]) * float(prm.dxi)
+           + (v[1:-1, 2:, 1:-1] - v[1:-1, 1:-1, 1:-1]) * float(prm.dyi)
+           + (w[2:, 1:-1, 1:-1] - w[1:-1, 1:-1, 1:-1]) * float(prm.dzi))
+    assert red["div_l2"] == pytest.approx(np.sqrt((div ** 2).sum()), rel=1e-10)
+    assert red["div_max"] == pytest.approx(np.abs(div).max(), rel=1e-12)
+    # residual of the pressure system with the mean-free rhs
+    p = st["p"].astype(np.float64)
+    b = rhs[1:-1, 1:-1, 1:-1] - rhs[1:-1, 1:-1, 1:-1].mean()
+    Ap = np.zeros_like(b)
+    c = p[1:-1, 1:-1, 1:-1]
+    cx, cy, cz = float(prm.dxi) ** 2, float(prm.dyi) ** 2, float(prm.dzi) ** 2
+    Ap[:, :, :-1] += cx * (p[1:-1, 1:-1, 2:-1] - c[:, :, :-1])
+    Ap[:, :, 1:] += cx * (p[1:-1, 1:-1, 1:-2] - c[:, :, 1:])
+    Ap[:, :-1, :] += cy * (p[1:-1, 2:-1, 1:-1] - c[:, :-1, :])
+    Ap[:, 1:, :] += cy * (p[1:-1, 1:-2, 1:-1] - c[:, 1:, :])
+    Ap[:-1, :, :] += cz * (p[2:-1, 1:-1, 1:-1] - c[:-1, :, :])
+    Ap[1:, :, :] += cz * (p[1:-2, 1:-1, 1:-1] - c[1:, :, :])
+    want = np.linalg.norm(b - Ap) / np.linalg.norm(b)
+    assert red["pres_resid"] == pytest.approx(want, rel=1e-9)
+    assert red["nonfinite"] == 0.0
+
+
+def test_reductions_deterministic(cuda, V):
+    prm = V.default_params(64, 48, 40, dt=5e-4)
+    state = ic.random_state(prm, seed=41)
+    with V.Solver(prm) as s:
+        s.upload_state(**state)
+        s.step(1)
+        a = [s.reduce(k) for k in V.REDUCTIONS]
+        b = [s.reduce(k) for k in V.REDUCTIONS]
+    assert a == b
+
+
+def test_nonfinite_watchdog(cuda, V):
+    prm = V.default_params(10, 10, 10)
+    state = ic.random_state(prm, seed=3)
+    state["u"][3, 4, 5] = np.nan
+    state["F"][2, 2, 2] = np.inf
+    with V.Solver(prm) as s:
+        s.upload_state(**state)
+        assert s.reduce("nonfinite") == 2.0
+
+
+def test_upload_download_roundtrip_and_device_pointers(cuda, V):
+    import torch
+
+    prm = V.default_params(13, 11, 9)
+    state = ic.random_state(prm, seed=5)
+    with V.Solver(prm) as s:
+        for k in STATE:
+            s.upload(k, state[k])
+        for k in STATE:
+            assert np.array_equal(s.download(k), state[k])
+        t = torch.from_numpy(state["w"] * 2).cuda()
+        s.upload("w", device_ptr=t.data_ptr())
+        o = torch.zeros_like(t)
+        s.download_device("w", o.data_ptr())
+        torch.cuda.synchronize()
+        assert torch.equal(o, t)
+
+
+def test_user_stream(cuda, V, orc):
+    import torch
+
+    prm = V.default_params(16, 16, 16, dt=5e-4)
+    state = ic.random_state(prm, seed=8)
+    st = torch.cuda.Stream()
+    with V.Solver(prm, stream=st.cuda_stream) as s:
+        s.upload_state(**state)
+        s.run(1, 3)
+        s.sync()
+        got = s.state()
+    want = orc.run_f32(prm, state, 1, 3)
+    assert_bitwise(got, want, STATE, "user stream")
+
+
+def test_argument_errors(cuda, V):
+    prm = V.default_params(8, 8, 8)
+    with V.Solver(prm) as s:
+        with pytest.raises(V.VofError) as e:
+            s._check(s._lib.vof_upload(s._ctx, 99, None, 0), "upload")
+        assert e.value.status == V.E_INVALID
+        assert s._lib.vof_reduce(s._ctx, 99, None) == V.E_INVALID
+        assert s._lib.vof_run(s._ctx, 1, -1) == V.E_INVALID
+
+
+# ---- the reference's own kernels (oracle/_ref) -------------------------------
+def _need_ref(orc, variant):
+    if not orc.ref_available(variant):
+        pytest.skip(f"reference harness {variant} not built (needs the reference source at build time)")
+
+
+@pytest.mark.parametrize("nx,ny,nz,seed,dt,vs", CASES[:3])
+def test_bitwise_vs_reference_kernels_nofma(cuda, V, orc, nx, ny, nz, seed, dt, vs):
+    _need_ref(orc, "nofma")
+    prm = V.default_params(nx, ny, nz, dt=dt, gy=0.0, gz=-9.81)
+    state = ic.random_state(prm, seed=seed, vel_scale=vs)
+    ref = orc.ref_run(prm, state, 1, 3, variant="nofma", extras=True)
+    got = run_gpu(V, prm, state, 1, 3, extras=True)
+    assert_bitwise(got, ref, STATE + ("ustar", "vstar", "wstar"), "vs reference -fmad=false")
+
+
+def test_dam_break_vs_reference_kernels(cuda, V, orc):
+    """32^3 dam break, 200 steps, against the reference's default (FMA) build.
+    Bounds: rel-L2 <= 1e-5 for F, u, v, w and for p modulo its mean;
+    max-abs |dF| <= 1e-4."""
+    _need_ref(orc, "sm100a")
+    prm = V.default_params(32, gy=0.0, gz=-9.81)
+    state = ic.rest_state(prm, ic.dam_break(prm))
+    ref = orc.ref_run(prm, state, 1, 200, variant="sm100a")
+    got = run_gpu(V, prm, state, 1, 200, use_graph=True)
+    for k in ("F", "u", "v", "w"):
+        assert rel_l2(got[k], ref[k]) <= 1e-5, (k, rel_l2(got[k], ref[k]))
+    assert np.abs(got["F"].astype(np.float64) - ref["F"]).max() <= 1e-4
+    pm = got["p"][1:-1, 1:-1, 1:-1].astype(np.float64)
+    qm = ref["p"][1:-1, 1:-1, 1:-1].astype(np.float64)
+    assert rel_l2(pm - pm.mean(), qm - qm.mean()) <= 1e-5
+    if orc.ref_available("nofma"):
+        ref_nf = orc.ref_run(prm, state, 1, 200, variant="nofma")
+        assert_bitwise(got, ref_nf, STATE, "32^3 x 200 vs reference -fmad=false")
