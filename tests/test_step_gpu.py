@@ -234,6 +234,36 @@ def test_argument_errors(cuda, V):
         assert s._lib.vof_run(s._ctx, 1, -1) == V.E_INVALID
 
 
+# ---- golden vectors produced by the reference's own kernels -----------------
+def _golden_cases():
+    import json
+
+    from conftest import GOLDEN
+
+    idx = GOLDEN / "index.json"
+    return json.loads(idx.read_text())["cases"] if idx.exists() else []
+
+
+@pytest.mark.parametrize("case", _golden_cases(), ids=lambda c: c["name"])
+def test_golden_vectors(cuda, V, case):
+    """CUDA path vs the stored outputs of voftrial1.cu's kernels: bit-identical
+    to the -fmad=false build, within the case's stated rel-L2 of the FMA build."""
+    from conftest import GOLDEN
+
+    data = np.load(GOLDEN / case["file"])
+    prm = V.default_params(case["nx"], case["ny"], case["nz"], **case["overrides"])
+    inp = {k: data["in_" + k] for k in STATE}
+    got = run_gpu(V, prm, inp, case["istep0"], case["nsteps"], use_graph=True)
+    assert_bitwise(got, {k: data["nofma_" + k] for k in STATE}, STATE, case["name"])
+    for k in STATE:
+        ref = data["fma_" + k].astype(np.float64)
+        g = got[k].astype(np.float64)
+        if k == "p":
+            ref, g = ref[1:-1, 1:-1, 1:-1], g[1:-1, 1:-1, 1:-1]
+            ref, g = ref - ref.mean(), g - g.mean()
+        assert rel_l2(g, ref) <= case["fma_rel_l2"], k
+
+
 # ---- the reference's own kernels (oracle/_ref) -------------------------------
 def _need_ref(orc, variant):
     if not orc.ref_available(variant):
