@@ -11,8 +11,10 @@
 #include <new>
 
 #include "../../include/vof.h"
+#include "jacobi_tb.h"
 #include "plain_step.h"
 #include "reduce.h"
+#include "tma.cuh"
 
 using vof::Geom;
 
@@ -31,6 +33,8 @@ struct vof_ctx {
     double* d_red_scratch;
     double* d_red_result;
     double* h_red_result;       // pinned, for vof_reduce
+    int* d_status;              // device status word written by kernels (DEV_* codes)
+    CUtensorMap maps[4];        // TMA descriptors: p0, p1, p2, rhs
     cudaGraphExec_t graph[3][2];  // [istep % 3][p parity at step start]
     int last_cuda_error;
     size_t bytes;
@@ -94,11 +98,22 @@ void free_ctx(vof_ctx* c) {
         if (c->fields[f]) cudaFree(c->fields[f]);
     if (c->b.p0) cudaFree(c->b.p0);
     if (c->b.p1) cudaFree(c->b.p1);
+    if (c->b.p2) cudaFree(c->b.p2);
     if (c->d_red_scratch) cudaFree(c->d_red_scratch);
     if (c->d_red_result) cudaFree(c->d_red_result);
     if (c->h_red_result) cudaFreeHost(c->h_red_result);
+    if (c->d_status) cudaFree(c->d_status);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     delete c;
+}
+
+// Read (and clear) the device status word after the stream has drained.
+int check_status(vof_ctx* c) {
+    int st = 0;
+    if (cudaMemcpy(&st, c->d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return VOF_E_CUDA;
+    if (st == 0) return VOF_OK;
+    cudaMemset(c->d_status, 0, sizeof(int));
+    return VOF_E_TIMEOUT;
 }
 
 }  // namespace
@@ -118,6 +133,7 @@ const char* vof_error_string(int status) {
         case VOF_E_NONFINITE: return "non-finite value in the state";
         case VOF_E_STATE: return "call not valid in the current state";
         case VOF_E_UNSUPPORTED: return "unsupported mode or feature";
+        case VOF_E_TIMEOUT: return "a device-side wait timed out (result invalid)";
         default: return "unknown status";
     }
 }
@@ -227,9 +243,11 @@ int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
     };
     bool ok = true;
     for (int f = 0; f < VOF_NUM_FIELDS - 1 && ok; ++f) ok = alloc((void**)&c->fields[f], fbytes);
-    ok = ok && alloc((void**)&c->b.p0, fbytes) && alloc((void**)&c->b.p1, fbytes);
+    ok = ok && alloc((void**)&c->b.p0, fbytes) && alloc((void**)&c->b.p1, fbytes) &&
+         alloc((void**)&c->b.p2, fbytes);
     ok = ok && alloc((void**)&c->d_red_scratch, sizeof(double) * vof::RED_SCRATCH_DOUBLES);
     ok = ok && alloc((void**)&c->d_red_result, sizeof(double) * vof::RED_RESULT_DOUBLES);
+    ok = ok && alloc((void**)&c->d_status, sizeof(int));
     if (ok && cudaMallocHost((void**)&c->h_red_result, sizeof(double) * 4) != cudaSuccess) ok = false;
     if (!ok) {
         free_ctx(c);
@@ -243,10 +261,22 @@ int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
     c->b.vs = c->fields[VOF_FIELD_VSTAR - 1];
     c->b.ws = c->fields[VOF_FIELD_WSTAR - 1];
     c->b.rhs = c->fields[VOF_FIELD_RHS - 1];
+    c->b.maps = c->maps;
+    c->b.status = c->d_status;
     c->p_parity = 0;
+    {
+        const float* mapped[4] = {c->b.p0, c->b.p1, c->b.p2, c->b.rhs};
+        for (int q = 0; q < 4; ++q) {
+            if ((e = vof::jacobi_tb_maps(c->g, mapped[q], &c->maps[q])) != cudaSuccess) {
+                c->last_cuda_error = (int)e;
+                free_ctx(c);
+                return VOF_E_UNSUPPORTED;
+            }
+        }
+    }
 
     const int maxn = p->nx > p->ny ? (p->nx > p->nz ? p->nx : p->nz) : (p->ny > p->nz ? p->ny : p->nz);
-    if ((e = vof::plain_configure(maxn)) != cudaSuccess ||
+    if ((e = vof::plain_configure(maxn)) != cudaSuccess || (e = vof::plain_density_pairs(&c->g)) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaStreamSynchronize(c->stream)) != cudaSuccess) {
         c->last_cuda_error = (int)e;
@@ -372,7 +402,8 @@ int vof_sync(vof_ctx* ctx) {
     if (!ctx) return VOF_E_INVALID;
     DeviceGuard dg(ctx->device);
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
-    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    return check_status(ctx);
 }
 
 int vof_reduce_async(vof_ctx* ctx, int what, double* host_out) {

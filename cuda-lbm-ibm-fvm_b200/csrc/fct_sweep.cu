@@ -1,0 +1,370 @@
+// fct_sweep.cu -- one directionally split FCT sweep of the volume fraction
+// (fct_{x,y,z}_sweep_stage1..4, voftrial1.cu:509-905) as a single kernel.
+//
+// Compiled with -fmad=false like plain_step.cu: every expression below keeps
+// the reference's operand order and no multiply-add is contracted.
+//
+// Why the four reference stages collapse into one pass over a grid line.
+// Stage 2 of a sweep zeroes the other direction's antidiffusive fluxes
+// (voftrial1.cu:573-574, 712-713), so the terms they contribute to pp, pm and
+// the stage-4 update vanish (exactly, up to the sign of a zero, which the
+// final clamp01f removes).  What is left couples only cells of the same line
+// along the sweep axis, with a reach of three cells.  The zero-filled buffers
+// the reference never writes (voftrial1.cu:1200-1203) fix the line ends:
+//   Ftd at the two ghost cells is 0, rp and rm at the ghost cells are 0, and
+//   the limiter c of the first face (c[1]) is 0; the wall-face velocities
+//   are 0 after apply_bc_velocity, so the ghost F values enter only as 0*F.
+//
+// Q2 length factors of the reference, per sweep (x | y | z):
+//   stage 1 flux term  (f_l - f_r)*dy*dz/vol | (f_l - f_r)*dy/(dx*dy) | (f_l - f_r)*dy*dx/vol
+//   dv factor          dt*dy*dz              | dt*dx*dz               | dt*dx*dy
+//   limiter q          *dx                   | *dx                    | *dz
+//   stage 4 divisor    /dy                   | /dy                    | /dz
+//
+// Kernel shape.  A block owns a tile of 32 lines (one per lane) over their
+// full length.  The tile's F and face velocity are staged once in shared
+// memory with coalesced loads; then each warp marches one segment of the
+// lines, carrying the stage values of the last few cells in registers, so each
+// cell's fluxes, Ftd, Zalesak ratios and face limiters are computed exactly
+// once (plus a three-cell warm-up at segment starts).  Shared memory is laid
+// out so a warp's 32 lanes (32 lines, same position) hit 32 banks:
+//   x lines: [line][pos] with an odd row pitch;  y/z lines: [pos][line].
+// y/z lines are contiguous across lanes in HBM, so results go straight to
+// global memory; x results are staged and written back row-wise.
+#include <cuda_runtime.h>
+
+#include "fct_sweep.h"
+
+namespace vof {
+
+#if defined(__CUDA_ARCH__) && !defined(VOF_FMAD_FALSE)
+#error "fct_sweep.cu must be compiled with -fmad=false -DVOF_FMAD_FALSE"
+#endif
+
+namespace {
+
+constexpr int LANES = 32;     // lines per tile
+constexpr int WARPS = 8;      // segments per line
+constexpr int THREADS = LANES * WARPS;
+
+__host__ __device__ inline int odd_pitch(int npos) { return npos | 1; }
+
+template <int AXIS>
+struct Sweep {
+    // Per-sweep constants (see the table above) and the IEEE reciprocals of
+    // the constant divisors, for div_rn_pre.
+    float dt, vol, dvfac, hq, h4, t1a, t1b, dxdy;
+    float rvol, rh4, rdxdy;
+    int n;
+
+    __device__ Sweep(const Geom& g) {
+        dt = g.dt;
+        vol = g.dx * g.dy * g.dz;
+        n = AXIS == 0 ? g.nx : (AXIS == 1 ? g.ny : g.nz);
+        dvfac = AXIS == 0 ? g.dt * g.dy * g.dz : (AXIS == 1 ? g.dt * g.dx * g.dz : g.dt * g.dx * g.dy);
+        hq = AXIS == 2 ? g.dz : g.dx;
+        h4 = AXIS == 2 ? g.dz : g.dy;
+        t1a = g.dy;                                    // first factor of the stage-1 flux term
+        t1b = AXIS == 0 ? g.dz : (AXIS == 1 ? 0.0f : g.dx);
+        dxdy = g.dx * g.dy;
+        rvol = __frcp_rn(vol);
+        rh4 = __frcp_rn(h4);
+        rdxdy = __frcp_rn(dxdy);
+    }
+
+    // Stage-1 flux term from the low-order fluxes through the lower (fi) and
+    // upper (fo) faces of a cell.
+    __device__ __forceinline__ float term(float fi, float fo) const {
+        if (AXIS == 1) return div_rn_pre((fi - fo) * t1a, dxdy, rdxdy);
+        return div_rn_pre((fi - fo) * t1a * t1b, vol, rvol);
+    }
+};
+
+// Line accessor: smem values of one lane's line at position q.
+struct LineView {
+    const float* f;
+    const float* v;
+    int qs;  // smem stride between consecutive positions
+    __device__ __forceinline__ float F(int q) const { return f[q * qs]; }
+    __device__ __forceinline__ float V(int q) const { return v[q * qs]; }
+};
+
+// Low-order flux and antidiffusive flux through face fidx (between cells
+// fidx-1 and fidx), as fl_L / fl_H of the reference's stages 1-2.
+__device__ __forceinline__ void face_flux(const LineView& L, int fidx, float dt, float& lo, float& a) {
+    const float uf = L.V(fidx);
+    const float FL = L.F(fidx - 1), FR = L.F(fidx);
+    const float lo_ = (uf >= 0.0f) ? uf * dt * FL : uf * dt * FR;
+    const float hi_ = (uf <= 0.0f) ? uf * dt * FL : uf * dt * FR;
+    lo = lo_;
+    a = hi_ - lo_;
+}
+
+template <int AXIS>
+__device__ __forceinline__ float cell_dv(const Sweep<AXIS>& S, const LineView& L, int c) {
+    return S.vol - S.dvfac * (L.V(c + 1) - L.V(c));
+}
+
+// Stage 1: low-order update of cell c from its face fluxes; rdv = RN(1/dv).
+template <int AXIS>
+__device__ __forceinline__ float ftd_from(const Sweep<AXIS>& S, float Fc, float lo_in, float lo_out, float dv,
+                                         float rdv) {
+    float out = div_rn_pre((Fc + S.term(lo_in, lo_out)) * S.vol, dv, rdv);
+    if (out > 1.0f || out < 0.0f) out = clamp01f(out);
+    return out;
+}
+
+// Stage 2: Zalesak ratios of a cell.
+template <int AXIS>
+__device__ __forceinline__ void limiter(const Sweep<AXIS>& S, float tm, float tc, float tp, float al,
+                                        float ar, float& rp, float& rm) {
+    const float fmx = fmaxf(tc, fmaxf(tm, tp));
+    const float fmn = fminf(tc, fminf(tm, tp));
+    // rp = pp > 0 ? fminf(1, qp/pp) : 0, skipping the division when
+    // qp >= pp (then qp/pp >= 1 and its rounding is >= 1 too).
+    const float pp = fmaxf(0.0f, al) - fminf(0.0f, ar);
+    const float qp = (fmx - tc) * S.hq;
+    rp = 0.0f;
+    if (pp > 0.0f) rp = (qp >= pp) ? 1.0f : fminf(1.0f, qp / pp);
+    const float pm = fmaxf(0.0f, ar) - fminf(0.0f, al);
+    const float qm = (tc - fmn) * S.hq;
+    rm = 0.0f;
+    if (pm > 0.0f) rm = (qm >= pm) ? 1.0f : fminf(1.0f, qm / pm);
+}
+
+// Stage 3: limiter of face f from the ratios of its two cells.
+__device__ __forceinline__ float face_limit(float af, float rp_lo, float rm_lo, float rp_hi, float rm_hi) {
+    return (af >= 0.0f) ? fminf(rp_hi, rm_lo) : fminf(rp_lo, rm_hi);
+}
+
+// ---- from-scratch evaluation (segment warm-up only) -------------------------
+template <int AXIS>
+__device__ float ftd_at(const Sweep<AXIS>& S, const Geom& g, const LineView& L, int c) {
+    if (c < 1 || c > S.n) return 0.0f;
+    float lo_in, lo_out, a;
+    face_flux(L, c, S.dt, lo_in, a);
+    face_flux(L, c + 1, S.dt, lo_out, a);
+    const float dv = cell_dv(S, L, c);
+    return ftd_from(S, L.F(c), lo_in, lo_out, dv, __frcp_rn(dv));
+}
+
+__device__ __forceinline__ float a_at(const LineView& L, int f, int n, float dt) {
+    if (f < 1 || f > n + 1) return 0.0f;
+    float lo, a;
+    face_flux(L, f, dt, lo, a);
+    return a;
+}
+
+template <int AXIS>
+__device__ void ratios_at(const Sweep<AXIS>& S, const Geom& g, const LineView& L, int c, float& rp, float& rm) {
+    if (c < 1 || c > S.n) {
+        rp = 0.0f;
+        rm = 0.0f;
+        return;
+    }
+    limiter(S, ftd_at(S, g, L, c - 1), ftd_at(S, g, L, c), ftd_at(S, g, L, c + 1), a_at(L, c, S.n, S.dt),
+            a_at(L, c + 1, S.n, S.dt), rp, rm);
+}
+
+// Indices whose clamped value is x on an axis of n interior cells: x itself,
+// plus the ghost 0 when x == 1 and the ghost n+1 when x == n.
+__device__ __forceinline__ int mirrors(int x, int n, int* out) {
+    int m = 0;
+    out[m++] = x;
+    if (x == 1) out[m++] = 0;
+    if (x == n) out[m++] = n + 1;
+    return m;
+}
+
+}  // namespace
+
+// ---- one tile ---------------------------------------------------------------
+template <int AXIS, bool FINAL>
+__global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, float* F, const float* __restrict__ vel) {
+    extern __shared__ float smem[];
+    const Sweep<AXIS> S(g);
+    const int n = S.n;
+    const int npos = n + 2;
+    const int na = AXIS == 0 ? g.ny : g.nx;           // lines along a
+    const int nb = AXIS == 2 ? g.ny : g.nz;           // lines along b
+    const int lane = threadIdx.x, warp = threadIdx.y;
+    const int a0 = 1 + blockIdx.x * LANES;            // first line of the tile
+    const int b = 1 + blockIdx.y;
+    const int nl = min(LANES, na - a0 + 1);
+    const int P = odd_pitch(npos);
+
+    // global index of (line a, b; position q)
+    auto gi = [&](int a, int bb, int q) {
+        return AXIS == 0 ? gidx(g, q, a, bb) : (AXIS == 1 ? gidx(g, a, q, bb) : gidx(g, a, bb, q));
+    };
+    // shared index of (line l, position q)
+    const int qs = AXIS == 0 ? 1 : LANES;
+    auto si = [&](int l, int q) { return AXIS == 0 ? l * P + q : q * LANES + l; };
+    const int tile = AXIS == 0 ? LANES * P : npos * LANES;
+    float* sF = smem;
+    float* sV = smem + tile;
+    float* sO = smem + 2 * tile;  // x only: staged results
+
+    // ---- stage the tile (coalesced) ----
+    if (AXIS == 0) {
+        for (int l = warp; l < nl; l += WARPS) {
+            const int base = gi(a0 + l, b, 0);
+            for (int q = lane; q < npos; q += LANES) {
+                sF[l * P + q] = F[base + q];
+                sV[l * P + q] = __ldg(vel + base + q);
+            }
+        }
+    } else {
+        if (lane < nl) {
+            for (int q = warp; q < npos; q += WARPS) {
+                const int gq = gi(a0 + lane, b, q);
+                sF[q * LANES + lane] = F[gq];
+                sV[q * LANES + lane] = __ldg(vel + gq);
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- march one segment of this lane's line ----
+    const int seg = (n + WARPS - 1) / WARPS;
+    const int c0 = 1 + warp * seg;
+    const int c1 = min(n, c0 + seg - 1);
+    const LineView L{sF + si(lane, 0), sV + si(lane, 0), qs};
+    const int a = a0 + lane;
+    const bool live = lane < nl && c0 <= n;
+
+    if (live) {
+        const float dt = S.dt;
+        // state before cell c0
+        float lo2, a0f, a1f, a2f, T0, T1, rp0, rm0, cf0, dv0, dv1, rdv0, rdv1;
+        {
+            float lo_tmp;
+            face_flux(L, c0, dt, lo_tmp, a0f);
+            a1f = a_at(L, c0 + 1, n, dt);
+            a2f = a_at(L, c0 + 2, n, dt);
+            lo2 = 0.0f;
+            if (c0 + 2 <= n + 1) face_flux(L, c0 + 2, dt, lo2, a2f);
+            T0 = ftd_at(S, g, L, c0);
+            T1 = ftd_at(S, g, L, c0 + 1);
+            ratios_at(S, g, L, c0, rp0, rm0);
+            if (c0 == 1) {
+                cf0 = 0.0f;  // c[imin] is never written
+            } else {
+                float rpm, rmm;
+                ratios_at(S, g, L, c0 - 1, rpm, rmm);
+                cf0 = face_limit(a0f, rpm, rmm, rp0, rm0);
+            }
+            dv0 = cell_dv(S, L, c0);
+            dv1 = (c0 + 1 <= n) ? cell_dv(S, L, c0 + 1) : 1.0f;
+            rdv0 = __frcp_rn(dv0);
+            rdv1 = __frcp_rn(dv1);
+        }
+
+        for (int c = c0; c <= c1; ++c) {
+            // face c+3, Ftd(c+2), ratios(c+1), limiter of face c+1, result of cell c
+            float lo3 = 0.0f, a3f = 0.0f;
+            if (c + 3 <= n + 1) face_flux(L, c + 3, dt, lo3, a3f);
+            float T2 = 0.0f, dv2 = 1.0f, rdv2 = 1.0f;
+            if (c + 2 <= n) {
+                dv2 = cell_dv(S, L, c + 2);
+                rdv2 = __frcp_rn(dv2);
+                T2 = ftd_from(S, L.F(c + 2), lo2, lo3, dv2, rdv2);
+            }
+            float rp1 = 0.0f, rm1 = 0.0f;
+            if (c + 1 <= n) limiter(S, T0, T1, T2, a1f, a2f, rp1, rm1);
+            const float cf1 = face_limit(a1f, rp0, rm0, rp1, rm1);
+            float fnew = clamp01f(T0 - div_rn_pre(div_rn_pre(a1f * cf1 - a0f * cf0, S.h4, S.rh4) * S.vol, dv0, rdv0));
+            if (FINAL) fnew = clamp01f(fnew);  // post_process_f_kernel, voftrial1.cu:502-507
+
+            if (AXIS == 0) {
+                sO[lane * P + c] = fnew;
+            } else if (!FINAL) {
+                F[gi(a, b, c)] = fnew;
+            } else {
+                // apply_bc_F (voftrial1.cu:1122-1135) composes to: every ghost
+                // cell takes the value at its clamped interior index.  Write the
+                // interior cell and every ghost that maps onto it.
+                int qv[3], av[3], bv[3];
+                const int nq = mirrors(c, n, qv), nav = mirrors(a, na, av), nbv = mirrors(b, nb, bv);
+                for (int ib = 0; ib < nbv; ++ib)
+                    for (int ia = 0; ia < nav; ++ia)
+                        for (int iq = 0; iq < nq; ++iq) F[gi(av[ia], bv[ib], qv[iq])] = fnew;
+            }
+
+            lo2 = lo3;
+            a0f = a1f;
+            a1f = a2f;
+            a2f = a3f;
+            T0 = T1;
+            T1 = T2;
+            rp0 = rp1;
+            rm0 = rm1;
+            cf0 = cf1;
+            dv0 = dv1;
+            dv1 = dv2;
+            rdv0 = rdv1;
+            rdv1 = rdv2;
+        }
+    }
+
+    if (AXIS == 0) {
+        // ---- write the staged x rows back (coalesced) ----
+        __syncthreads();
+        for (int l = warp; l < nl; l += WARPS) {
+            const int aa = a0 + l;
+            if (!FINAL) {
+                const int base = gi(aa, b, 0);
+                for (int q = 1 + lane; q <= n; q += LANES) F[base + q] = sO[l * P + q];
+            } else {
+                int av[3], bv[3];
+                const int nav = mirrors(aa, na, av), nbv = mirrors(b, nb, bv);
+                for (int ib = 0; ib < nbv; ++ib)
+                    for (int ia = 0; ia < nav; ++ia) {
+                        const int base = gi(av[ia], bv[ib], 0);
+                        for (int q = lane; q <= n + 1; q += LANES)
+                            F[base + q] = sO[l * P + (q < 1 ? 1 : (q > n ? n : q))];
+                    }
+            }
+        }
+    }
+}
+
+size_t fct_smem_bytes(int axis, int n) {
+    const int npos = n + 2;
+    if (axis == 0) return sizeof(float) * 3u * (size_t)LANES * (size_t)odd_pitch(npos);
+    return sizeof(float) * 2u * (size_t)npos * LANES;
+}
+
+template <int AXIS, bool FINAL>
+static cudaError_t launch_axis(const Geom& g, float* F, const float* vel, cudaStream_t s) {
+    const int n = AXIS == 0 ? g.nx : (AXIS == 1 ? g.ny : g.nz);
+    const int na = AXIS == 0 ? g.ny : g.nx;
+    const int nb = AXIS == 2 ? g.ny : g.nz;
+    dim3 grid((na + LANES - 1) / LANES, nb, 1);
+    k_fct<AXIS, FINAL><<<grid, dim3(LANES, WARPS), fct_smem_bytes(AXIS, n), s>>>(g, F, vel);
+    return cudaGetLastError();
+}
+
+cudaError_t fct_launch(const Geom& g, int axis, bool final_sweep, float* F, const float* vel, cudaStream_t s) {
+    if (axis == 0) return final_sweep ? launch_axis<0, true>(g, F, vel, s) : launch_axis<0, false>(g, F, vel, s);
+    if (axis == 1) return final_sweep ? launch_axis<1, true>(g, F, vel, s) : launch_axis<1, false>(g, F, vel, s);
+    return final_sweep ? launch_axis<2, true>(g, F, vel, s) : launch_axis<2, false>(g, F, vel, s);
+}
+
+cudaError_t fct_configure() {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+#define VOF_SET(A, FIN)                                                                      \
+    if ((e = cudaFuncSetAttribute(k_fct<A, FIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                  optin)) != cudaSuccess)                                    \
+        return e;
+    VOF_SET(0, false) VOF_SET(0, true) VOF_SET(1, false) VOF_SET(1, true) VOF_SET(2, false) VOF_SET(2, true)
+#undef VOF_SET
+    return cudaSuccess;
+}
+
+size_t fct_smem_limit() { return 227u * 1024u; }
+
+}  // namespace vof

@@ -1,0 +1,251 @@
+// jacobi_tb.cu -- T Jacobi sweeps of the pressure system per launch
+// (solve_p_jacobi_kernel, voftrial1.cu:401-439, applied T times with the
+// ping-pong of voftrial1.cu:1371-1375), temporally blocked in shared memory.
+//
+// Compiled with -fmad=false: each cell update keeps the reference's
+//     pt = (rhs - ae*pE - aw*pW - an*pN - as*pS - af*pF - ab*pB) / ap
+// with the same operand order, so T blocked sweeps give the same bits as T
+// separate sweeps.  The division uses div_rn_pre with the IEEE reciprocal of
+// ap (a handful of values per launch), which equals the IEEE quotient.
+//
+// Input planes (pressure and rhs) stream into a ring of shared-memory slots
+// through TMA loads issued several planes ahead by one thread and completed
+// on per-slot mbarriers, so HBM latency overlaps the sweeps of earlier planes.
+//
+// 2.5D pipeline.  A block owns BX x BY columns and walks a chunk of z planes.
+// It keeps, for every level t < T, a ring of three planes of an extended tile
+// (BX + 2T) x (BY + 2T) in shared memory.  When plane s of the input (level 0)
+// arrives, level t is computed at plane s - t on the tile shrunk by T - t
+// cells on each side, from level t-1 at planes s-t-1 .. s-t+1; level T, the
+// tile interior, goes to global memory.  Ghost cells (and the never-written
+// ghost planes) are carried unchanged from level to level: the reference
+// never writes pressure ghosts, and they enter interior updates only through
+// zero coefficients.
+#include <cuda_runtime.h>
+
+#include "jacobi_tb.h"
+#include "tma.cuh"
+
+namespace vof {
+
+#if defined(__CUDA_ARCH__) && !defined(VOF_FMAD_FALSE)
+#error "jacobi_tb.cu must be compiled with -fmad=false -DVOF_FMAD_FALSE"
+#endif
+
+// Threads (32, 8).  The tile is BX = BY = 32 - 2(T-1) columns, so every
+// level's rows (BX + 2(T-t) cells wide) fit one warp and each thread updates
+// four rows per level and plane; the extended tile is always 34 x 34 cells.
+constexpr int JB_TX = 32, JB_TY = 8, JB_THREADS = JB_TX * JB_TY, JB_ROWS = 4;
+constexpr int JB_EX = JB_TX + 2, JB_EY = JB_TY * JB_ROWS + 2;
+// TMA box: 40 x 34 x 1 floats from an x origin rounded down to a multiple of
+// 4 elements (16 bytes); a plane slot is padded to a multiple of 128 bytes.
+constexpr int JB_W = 40, JB_PLANE = JB_W * JB_EY, JB_PLANE_PAD = (JB_PLANE * 4 + 127) / 128 * 32;
+constexpr uint32_t JB_BOX_BYTES = JB_PLANE * 4;
+
+template <int T>
+struct JTile {
+    static constexpr int BX = JB_TX - 2 * (T - 1), BY = JB_TY * JB_ROWS - 2 * (T - 1);
+    static constexpr int HOLD = T > 2 ? T : 2;  // steps a plane's slot stays in use
+    static constexpr int SLOTS = HOLD + 3;      // in use + two planes in flight
+    static constexpr size_t SMEM = sizeof(float) * (size_t)(2 * SLOTS + 3 * (T - 1)) * JB_PLANE_PAD +
+                                   sizeof(uint64_t) * SLOTS;
+};
+
+template <int T>
+__global__ void __launch_bounds__(JB_THREADS) k_jacobi_tb(Geom g, const __grid_constant__ CUtensorMap map_p,
+                                                         const __grid_constant__ CUtensorMap map_r,
+                                                         float* __restrict__ pout, int kchunk, int* status) {
+    using Tl = JTile<T>;
+    constexpr int BX = Tl::BX, BY = Tl::BY, SLOTS = Tl::SLOTS, W = JB_W, EX = JB_EX, EY = JB_EY;
+    constexpr int PP = JB_PLANE_PAD;
+    extern __shared__ __align__(128) float smem[];
+    float* in_p = smem;                     // [slot][PP]
+    float* in_r = smem + SLOTS * PP;        // [slot][PP]
+    float* lv = smem + 2 * SLOTS * PP;      // [t-1][plane % 3][PP], t = 1..T-1
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + (2 * SLOTS + 3 * (T - 1)) * PP);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * JB_TX + tx;
+
+    const int x0 = blockIdx.x * BX + 1 - T;    // global i of extended column 0
+    const int xa = x0 - (((x0 % 4) + 4) % 4);  // TMA x origin, multiple of 4
+    const int off = x0 - xa;                   // 0..3
+    const int y0 = blockIdx.y * BY + 1 - T;
+    const int k0 = 1 + blockIdx.z * kchunk;
+    const int k1 = min(g.nz, k0 + kchunk - 1);
+    const int s_lo = max(0, k0 - T), s_end = k1 + T, s_ld = min(g.nz + 1, s_end);
+    // No wall inside the extended tile: every column is interior and every
+    // in-plane coefficient is the full one.
+    const bool open = x0 >= 1 && x0 + EX - 1 <= g.nx && y0 >= 1 && y0 + EY - 1 <= g.ny;
+
+    auto issue = [&](int plane, int sl) {
+        mbar_arrive_expect_tx(&bar[sl], 2 * JB_BOX_BYTES);
+        tma_load_3d(in_p + sl * PP, &map_p, xa, y0, plane, &bar[sl]);
+        tma_load_3d(in_r + sl * PP, &map_r, xa, y0, plane, &bar[sl]);
+    };
+    if (tid == 0) {
+        for (int q = 0; q < SLOTS; ++q) mbar_init(&bar[q], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int q = 0; q < SLOTS && s_lo + q <= s_ld; ++q) issue(s_lo + q, q);
+
+    const float cx = g.dxi * g.dxi, cy = g.dyi * g.dyi, cz = g.dzi * g.dzi;
+    // Diagonal of a column with no in-plane wall: interior planes, first
+    // plane, last plane (reference operand order), and IEEE reciprocals.
+    auto ap_open = [&](int k) {
+        const float af = (k != g.nz) ? cz : 0.0f;
+        const float ab = (k != 1) ? cz : 0.0f;
+        return -(cx + cx + cy + cy + af + ab);
+    };
+    const float apm = ap_open(2), ap1 = ap_open(1), apn = ap_open(g.nz);
+    const float rpm = __frcp_rn(apm), rp1 = __frcp_rn(ap1), rpn = __frcp_rn(apn);
+
+    // slot[d] = ring slot of input plane s - d (d = 0..HOLD+1), kept
+    // incrementally; the first use of every slot has parity 0.
+    int slot[T + 3];
+#pragma unroll
+    for (int d = 0; d < T + 3; ++d) slot[d] = (((s_lo - d - s_lo) % SLOTS) + SLOTS) % SLOTS;
+    uint32_t par_bits = 0;  // bit q: parity of the next wait on slot q
+    int s3 = s_lo % 3;      // s mod 3 for the level rings
+
+    bool ok = true;
+    // Level t is needed at planes k0-(T-t) .. k1+(T-t) and is produced at
+    // step s = plane + t; input planes exist up to the ghost plane nz+1.
+    for (int s = s_lo; s <= s_end; ++s) {
+        if (s <= s_ld) {
+            ok &= mbar_wait(&bar[slot[0]], (par_bits >> slot[0]) & 1u);
+            par_bits ^= 1u << slot[0];
+        }
+#pragma unroll
+        for (int t = 1; t <= T; ++t) {
+            const int q = s - t;  // plane of level t
+            const int lo = k0 - (T - t), hi = k1 + (T - t);
+            if (q >= max(0, lo) && q <= min(g.nz + 1, hi)) {
+                // rings of level t-1 (t >= 2): plane x sits at x % 3
+                const int rq = (s3 - t + 6) % 3, rm = (s3 - t + 5) % 3, rp = (s3 - t + 7) % 3;
+                const float* Pm = (t == 1) ? in_p + slot[2] * PP : lv + ((t - 2) * 3 + rm) * PP;
+                const float* Pc = (t == 1) ? in_p + slot[1] * PP : lv + ((t - 2) * 3 + rq) * PP;
+                const float* Pp = (t == 1) ? in_p + slot[0] * PP : lv + ((t - 2) * 3 + rp) * PP;
+                const float* Rq = in_r + slot[t] * PP;
+                float* Out = lv + ((t < T ? t - 1 : 0) * 3 + rq) * PP;
+                const bool zin = q >= 1 && q <= g.nz;
+                const float af = (q != g.nz) ? cz : 0.0f;
+                const float ab = (q != 1) ? cz : 0.0f;
+                const float apo = (q == 1) ? ap1 : ((q == g.nz) ? apn : apm);
+                const float rapo = (q == 1) ? rp1 : ((q == g.nz) ? rpn : rpm);
+                const int ex = t + tx;
+                const int gi = x0 + ex;
+                if (ex < EX - t) {
+#pragma unroll
+                    for (int r = 0; r < JB_ROWS; ++r) {
+                        const int ey = t + ty + r * JB_TY;
+                        if (ey < EY - t) {
+                            const int c = ey * W + ex + off;
+                            const int gj = y0 + ey;
+                            float val = Pc[c];  // ghosts and cells outside the box carry over
+                            bool upd = false;
+                            if (open) {
+                                if (zin) {
+                                    val = div_rn_pre(Rq[c] - cx * Pc[c + 1] - cx * Pc[c - 1] - cy * Pc[c + W] -
+                                                         cy * Pc[c - W] - af * Pp[c] - ab * Pm[c],
+                                                     apo, rapo);
+                                    upd = true;
+                                }
+                            } else if (zin && gi >= 1 && gi <= g.nx && gj >= 1 && gj <= g.ny) {
+                                const float ae = (gi != g.nx) ? cx : 0.0f;
+                                const float aw = (gi != 1) ? cx : 0.0f;
+                                const float an = (gj != g.ny) ? cy : 0.0f;
+                                const float as = (gj != 1) ? cy : 0.0f;
+                                const float ap = -(ae + aw + an + as + af + ab);
+                                val = div_rn_pre(Rq[c] - ae * Pc[c + 1] - aw * Pc[c - 1] - an * Pc[c + W] -
+                                                     as * Pc[c - W] - af * Pp[c] - ab * Pm[c],
+                                                 ap, __frcp_rn(ap));
+                                upd = true;
+                            }
+                            if (t < T) {
+                                Out[c] = val;
+                            } else if (upd && q >= k0 && q <= k1) {
+                                pout[gidx(g, gi, gj, q)] = val;
+                            }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // The slot of plane s - HOLD is no longer read: refill it.
+        const int freed = s - Tl::HOLD;
+        if (tid == 0 && freed >= s_lo && freed + SLOTS <= s_ld) {
+            fence_proxy_async_smem();
+            issue(freed + SLOTS, slot[Tl::HOLD]);
+        }
+#pragma unroll
+        for (int d = T + 2; d > 0; --d) slot[d] = slot[d - 1];
+        slot[0] = (slot[0] + 1 == SLOTS) ? 0 : slot[0] + 1;
+        s3 = (s3 == 2) ? 0 : s3 + 1;
+    }
+    if (!ok) {
+        // A load that did not land in time may still be in flight: wait
+        // (bounded) for the last planes issued before leaving.
+        for (int pl = max(s_lo, s_ld - SLOTS + 1); pl <= s_ld; ++pl) {
+            const int sl = (pl - s_lo) % SLOTS;
+            mbar_wait(&bar[sl], (par_bits >> sl) & 1u);
+        }
+        atomicOr(status, DEV_TMA_TIMEOUT);
+    }
+    (void)BX;
+    (void)BY;
+}
+
+size_t jacobi_tb_smem_bytes(int T) {
+    switch (T) {
+        case 1: return JTile<1>::SMEM;
+        case 2: return JTile<2>::SMEM;
+        case 3: return JTile<3>::SMEM;
+        case 4: return JTile<4>::SMEM;
+        default: return 0;
+    }
+}
+
+cudaError_t jacobi_tb_configure() {
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_jacobi_tb<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)JTile<1>::SMEM)) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(k_jacobi_tb<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)JTile<2>::SMEM)) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(k_jacobi_tb<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)JTile<3>::SMEM)) != cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute(k_jacobi_tb<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)JTile<4>::SMEM);
+}
+
+cudaError_t jacobi_tb_maps(const Geom& g, const float* field, CUtensorMap* map) {
+    return make_tensor_map_3d(map, field, g.px, g.py, g.nz + 2, JB_W, JB_EY, 1);
+}
+
+template <int T>
+static dim3 tb_grid(const Geom& g, int kchunk) {
+    return dim3((g.nx + JTile<T>::BX - 1) / JTile<T>::BX, (g.ny + JTile<T>::BY - 1) / JTile<T>::BY,
+                (g.nz + kchunk - 1) / kchunk);
+}
+
+cudaError_t jacobi_tb_launch(const Geom& g, int T, const CUtensorMap& map_in, const CUtensorMap& map_rhs,
+                             float* pout, int* status, cudaStream_t s) {
+    // z chunks long enough that the T-plane warm-up at each end is small,
+    // and enough blocks to fill the GPU for a few waves.
+    const int kchunk = g.nz < 16 ? g.nz : 16;
+    const dim3 blk(JB_TX, JB_TY);
+    switch (T) {
+        case 1: k_jacobi_tb<1><<<tb_grid<1>(g, kchunk), blk, JTile<1>::SMEM, s>>>(g, map_in, map_rhs, pout, kchunk, status); break;
+        case 2: k_jacobi_tb<2><<<tb_grid<2>(g, kchunk), blk, JTile<2>::SMEM, s>>>(g, map_in, map_rhs, pout, kchunk, status); break;
+        case 3: k_jacobi_tb<3><<<tb_grid<3>(g, kchunk), blk, JTile<3>::SMEM, s>>>(g, map_in, map_rhs, pout, kchunk, status); break;
+        case 4: k_jacobi_tb<4><<<tb_grid<4>(g, kchunk), blk, JTile<4>::SMEM, s>>>(g, map_in, map_rhs, pout, kchunk, status); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace vof

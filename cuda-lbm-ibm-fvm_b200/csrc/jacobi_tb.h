@@ -1,0 +1,29 @@
+// jacobi_tb.h -- temporally blocked Jacobi sweeps (jacobi_tb.cu).
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "vof_device.cuh"
+
+namespace vof {
+
+// Largest number of sweeps one launch fuses.
+constexpr int JACOBI_TB_MAX = 4;
+
+// Tensor map (TMA descriptor) of one padded field for the sweep kernels.
+cudaError_t jacobi_tb_maps(const Geom& g, const float* field, CUtensorMap* map);
+
+// Enqueue T (1..JACOBI_TB_MAX) Jacobi sweeps reading the pressure field of
+// `map_in` and the rhs of `map_rhs`, writing the interior of `pout` (a
+// different buffer; its ghost cells are left as they are).  A TMA wait that
+// times out sets DEV_TMA_TIMEOUT in *status.
+cudaError_t jacobi_tb_launch(const Geom& g, int T, const CUtensorMap& map_in, const CUtensorMap& map_rhs,
+                             float* pout, int* status, cudaStream_t s);
+
+// Dynamic shared memory of one block for T fused sweeps.
+size_t jacobi_tb_smem_bytes(int T);
+
+// Raise the kernels' dynamic shared-memory ceiling (once per device).
+cudaError_t jacobi_tb_configure();
+
+}  // namespace vof

@@ -1,5 +1,6 @@
 // plain_step.h -- host-side interface of the FP32 drop-in step kernels.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "vof_device.cuh"
@@ -18,17 +19,21 @@ struct PlainBuffers {
     float* rhs;  // rho/dt * div(u*)
     float* p0;   // Jacobi ping-pong pair (DeviceFields::p / ::pt)
     float* p1;
+    float* p2;   // scratch pressure buffer for the blocked sweeps
+    const CUtensorMap* maps;  // TMA descriptors of p0, p1, p2, rhs (in that order)
+    int* status;              // device status word (DEV_* codes, tma.cuh)
 };
 
 // Raise the dynamic shared-memory limit of the FCT kernels for lines of up to
 // max_line interior cells.  Call once per device before the first step.
 cudaError_t plain_configure(int max_line);
 
+// Fill g->rpair / g->qpair (the density pairs of pure cells and dt over
+// them) with device arithmetic.  Call once per context.
+cudaError_t plain_density_pairs(Geom* g);
+
 // True when every FCT line tile of this grid fits in shared memory.
 bool plain_supported(const Geom& g);
-
-// Bytes of dynamic shared memory of one FCT tile for lines of n cells.
-size_t fct_smem_bytes(int n);
 
 // Kernel launches per plain step.
 int plain_kernels_per_step(int jacobi_iters);

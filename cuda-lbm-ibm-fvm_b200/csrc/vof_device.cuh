@@ -21,6 +21,9 @@ struct Geom {
     float dt, dx, dy, dz, dxi, dyi, dzi;
     float rho_l, rho_g, nu_l, nu_g;
     float gx, gy, gz;
+    // 0.5*(rho_a + rho_b) for the pure-phase pairs (gas-gas, liquid-liquid,
+    // gas-liquid) and dt divided by each, formed on the device at set-up.
+    float rpair[3], qpair[3];
 };
 
 __host__ __device__ __forceinline__ int gidx(const Geom& g, int i, int j, int k) {
@@ -43,6 +46,25 @@ __host__ __device__ __forceinline__ float median3f(float a, float b, float c) {
 
 __host__ __device__ __forceinline__ float clamp01f(float v) {
     return median3f(0.0f, 1.0f, v);
+}
+
+// Correctly rounded x / d from a precomputed rd = RN(1/d) (IEEE reciprocal,
+// __frcp_rn), for divisors that are constant or reused across several
+// quotients.  Method: P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990 -- with
+// rd = RN(1/d) and q0 = RN(x*rd) (within one ulp of x/d), the remainder
+// r = x - q0*d is exact in one FMA and q1 = RN(q0 + r*rd) equals RN(x/d),
+// provided nothing underflows or overflows.  Outside the range where that
+// holds (tiny, huge or non-finite operands) the IEEE division is used, and
+// +-0 numerators return x*rd, which carries the IEEE sign of 0/d.
+__device__ __forceinline__ float div_rn_pre(float x, float d, float rd) {
+    const float q0 = __fmul_rn(x, rd);
+    const float r = __fmaf_rn(-q0, d, x);
+    const float q1 = __fmaf_rn(r, rd, q0);
+    const float ax = fabsf(x), aq = fabsf(q0);
+    if (ax >= 0x1p-96f && aq >= 0x1p-96f && aq <= 0x1p+96f) return q1;
+    if (x == 0.0f) return q0;
+    return __fdiv_rn(x, d);
 }
 
 // rho and nu from the volume fraction (voftrial1.cu:95-104), same operand order.

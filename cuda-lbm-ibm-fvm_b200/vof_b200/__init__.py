@@ -27,8 +27,8 @@ LIB_PATH = Path(os.environ.get("VOF_B200_LIB", str(_PKG / "libvof_b200.so")))
 
 # ---- constants mirrored from include/vof.h -------------------------------
 OK = 0
-E_INVALID, E_SIZE, E_NOMEM, E_CUDA, E_NOT_CONVERGED, E_NONFINITE, E_STATE, E_UNSUPPORTED = (
-    -1, -2, -3, -4, -5, -6, -7, -8)
+E_INVALID, E_SIZE, E_NOMEM, E_CUDA, E_NOT_CONVERGED, E_NONFINITE, E_STATE, E_UNSUPPORTED, E_TIMEOUT = (
+    -1, -2, -3, -4, -5, -6, -7, -8, -9)
 MODE_PLAIN, MODE_MIXED, MODE_FP64 = 0, 1, 2
 FIELDS = {"F": 0, "u": 1, "v": 2, "w": 3, "p": 4, "ustar": 5, "vstar": 6, "wstar": 7, "rhs": 8}
 REDUCTIONS = {"volume": 0, "div_l2": 1, "div_max": 2, "pres_resid": 3, "nonfinite": 4,

@@ -30,10 +30,13 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + str(IN
 # source -> extra flags
 SOURCES = {
     "plain_step.cu": ["-fmad=false", "-DVOF_FMAD_FALSE"],
+    "fct_sweep.cu": ["-fmad=false", "-DVOF_FMAD_FALSE"],
+    "jacobi_tb.cu": ["-fmad=false", "-DVOF_FMAD_FALSE"],
+    "tma_host.cu": [],
     "reduce.cu": [],
     "capi.cu": [],
 }
-HEADERS = ["vof_device.cuh", "plain_step.h", "reduce.h"]
+HEADERS = ["vof_device.cuh", "tma.cuh", "plain_step.h", "fct_sweep.h", "jacobi_tb.h", "reduce.h"]
 
 
 def nvcc() -> str:

@@ -41,6 +41,7 @@ extern "C" {
 #define VOF_E_NONFINITE    (-6)  /* watchdog found NaN/Inf in the state            */
 #define VOF_E_STATE        (-7)  /* call not valid in the current context state    */
 #define VOF_E_UNSUPPORTED  (-8)  /* feature not built / mode not available         */
+#define VOF_E_TIMEOUT      (-9)  /* a bounded device-side wait ran out (reported by vof_sync) */
 
 /* ---- solver modes ------------------------------------------------------ */
 #define VOF_MODE_PLAIN  0   /* FP32, jacobi_iters Jacobi sweeps: the drop-in path */
@@ -173,7 +174,11 @@ int vof_step_timed(vof_ctx* ctx, int istep, float* phase_ms, int* launches, int 
 /* Name of phase q of vof_step_timed ("predict", "jacobi", ...), NULL if out of range. */
 const char* vof_phase_name(int phase);
 
-/* Wait for all work enqueued on the context's stream. */
+/*
+ * Wait for all work enqueued on the context's stream.  Also reports
+ * VOF_E_TIMEOUT if a kernel's bounded wait on an asynchronous copy ran out
+ * since the last call (the state is then invalid).
+ */
 int vof_sync(vof_ctx* ctx);
 
 /* Blocking reduction over the current state (VOF_RED_*); result in *out. */

@@ -98,7 +98,7 @@ def test_null_context_calls_return_invalid(V):
 
 def test_error_strings(V):
     lib = V.lib()
-    for code in (0, -1, -2, -3, -4, -5, -6, -7, -8):
+    for code in (0, -1, -2, -3, -4, -5, -6, -7, -8, -9):
         assert lib.vof_error_string(code)
     assert lib.vof_error_string(-99) == b"unknown status"
 

@@ -34,14 +34,16 @@ def run_gpu(V, prm, state, istep0, nsteps, use_graph=False, extras=False):
 
 
 def assert_bitwise(got, want, keys, ctx=""):
+    msgs = []
     for k in keys:
         g, w = got[k], want[k]
         if not np.array_equal(g, w):
             bad = np.argwhere(g != w)
             kk, jj, ii = bad[0]
-            raise AssertionError(
-                f"{ctx} field {k}: {len(bad)} cells differ; first (k,j,i)=({kk},{jj},{ii}) "
-                f"got {g[kk, jj, ii]!r} want {w[kk, jj, ii]!r}")
+            msgs.append(f"field {k}: {len(bad)} cells differ; first (k,j,i)=({kk},{jj},{ii}) "
+                        f"got {g[kk, jj, ii]!r} want {w[kk, jj, ii]!r}")
+    if msgs:
+        raise AssertionError(f"{ctx}: " + " | ".join(msgs))
 
 
 def rel_l2(a, b):
