@@ -303,6 +303,20 @@ cudaError_t plain_density_pairs(Geom* g) {
     return cudaSuccess;
 }
 
+cudaError_t plain_density_pairs_on(Geom* g, float* dev6, cudaStream_t s) {
+    float h[6];
+    k_density_pairs<<<1, 1, 0, s>>>(*g, dev6);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, dev6, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    for (int q = 0; q < 3; ++q) {
+        g->rpair[q] = h[q];
+        g->qpair[q] = h[3 + q];
+    }
+    return cudaSuccess;
+}
+
 bool plain_supported(const Geom& g) {
     return fct_smem_bytes(0, g.nx) <= fct_smem_limit() && fct_smem_bytes(1, g.ny) <= fct_smem_limit() &&
            fct_smem_bytes(2, g.nz) <= fct_smem_limit();

@@ -32,6 +32,10 @@ cudaError_t plain_configure(int max_line);
 // them) with device arithmetic.  Call once per context.
 cudaError_t plain_density_pairs(Geom* g);
 
+// Same, writing the six values through the caller's device scratch `dev6`
+// on stream s (waits for the stream); allocates nothing.
+cudaError_t plain_density_pairs_on(Geom* g, float* dev6, cudaStream_t s);
+
 // True when every FCT line tile of this grid fits in shared memory.
 bool plain_supported(const Geom& g);
 

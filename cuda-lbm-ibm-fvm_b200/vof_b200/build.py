@@ -35,6 +35,7 @@ SOURCES = {
     "tma_host.cu": [],
     "reduce.cu": [],
     "capi.cu": [],
+    "noalloc.cu": [],
 }
 HEADERS = ["vof_device.cuh", "tma.cuh", "plain_step.h", "fct_sweep.h", "jacobi_tb.h", "reduce.h"]
 

@@ -191,6 +191,28 @@ int vof_reduce(vof_ctx* ctx, int what, double* out);
  */
 int vof_reduce_async(vof_ctx* ctx, int what, double* host_out);
 
+/*
+ * One plain step with no allocation at all (no counterpart in the reference).
+ * For callers that must not allocate device memory while they step: programs
+ * whose GPU memory is owned up front by their own pool or allocator, or loops
+ * that cannot afford cudaMalloc's device-wide synchronisation and latency.
+ * The caller owns F, u, v, w, p as device buffers in the reference layout
+ * (nTot floats each) and they are updated in place, with results identical to
+ * a fresh context doing vof_upload + vof_step(istep) + vof_download.
+ * Scratch lives in a fixed device array of VOF_NOALLOC_ARENA_FLOATS floats
+ * (8 MiB, held by every GPU that loads the library until exit) that must hold
+ * 11 padded fields of round_up(nx+2, 32) * (ny+2) * (nz+2) floats: grids up
+ * to about 48^3 fit; larger ones return VOF_E_SIZE without doing anything.
+ * The first call on a device looks up the array's device address (with that
+ * device current); make that first call before any stream capture.  All calls
+ * share the array (each clears what it uses first), so calls that overlap on
+ * the GPU race.  The call waits for `stream` before returning.  Only
+ * VOF_MODE_PLAIN.
+ */
+#define VOF_NOALLOC_ARENA_FLOATS (2u << 20)
+int vof_step_noalloc(const vof_params* p, float* F, float* u, float* v, float* w, float* pres, int istep,
+                     void* stream);
+
 /* cudaError_t of the most recent failing CUDA call in this context (0 if none). */
 int vof_last_cuda_error(const vof_ctx* ctx);
 
