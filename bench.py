@@ -78,6 +78,8 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=10.0,
                     help="target CPU time of the CPU-baseline sample (0 disables)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ext-steps", type=int, default=10,
+                    help="steps of each convergent-mode measurement at the bench size (0 disables)")
     return ap.parse_args(argv)
 
 
@@ -257,6 +259,60 @@ def cpu_baseline(prm, state, seconds: float) -> dict | None:
 
 
 # ---------------------------------------------------------------------------
+# convergent pressure modes (extension): MIXED vs FP64 solver, same tolerance
+# ---------------------------------------------------------------------------
+def measure_convergent(V, n, steps, stream, dev, tol=1e-8):
+    """Time `steps` steps of the MIXED and FP64 modes (3 warm-up steps each) on the
+    workload; each step solves the pressure to ||r|| <= tol ||b||.  The timed
+    region includes the host synchronisations of the convergence checks."""
+    import torch
+
+    out = {}
+    fields = {}
+    state = None
+    for name, mode in (("mixed", V.MODE_MIXED), ("fp64", V.MODE_FP64)):
+        prm = V.default_params(n, gx=0.0, gy=0.0, gz=-9.81, mode=mode, tol=tol, max_outer=200)
+        if state is None:
+            state = workload_state(prm)
+        s = V.Solver(prm, stream=stream.cuda_stream)
+        s.upload_state(**state)
+        for q in range(3):
+            s.step(1 + q)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        outer, rel = [], []
+        e0.record(stream)
+        for q in range(steps):
+            s.step(4 + q)
+            st = s.solver_stats()
+            outer.append(st["outer"])
+            rel.append(st["rel_final"])
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        cells = prm.nx * prm.ny * prm.nz
+        out[name] = {"value": round(cells * steps / (ms / 1e3) / 1e6, 1), "unit": UNIT,
+                     "ms_per_step": round(ms / steps, 4), "vcycles_per_step": round(float(np.mean(outer)), 2),
+                     "max_rel_residual": float(np.max(rel)), "steps": steps,
+                     "inner": "BF16 storage / FP32 math" if name == "mixed" else "FP64"}
+        fields[name] = s.state()
+        s.close()
+    a, b = fields["mixed"], fields["fp64"]
+    diff = {}
+    for k in ("F", "u", "v", "w", "p"):
+        x = a[k].astype(np.float64)
+        y = b[k].astype(np.float64)
+        if k == "p":
+            x, y = x[1:-1, 1:-1, 1:-1], y[1:-1, 1:-1, 1:-1]
+        diff[k] = float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))
+    out["mixed_vs_fp64_rel_l2"] = diff
+    out["speedup_mixed_over_fp64"] = round(out["mixed"]["value"] / out["fp64"]["value"], 3)
+    out["tol"] = tol
+    out["workload"] = f"dam_break_{n}^3, steps 4..{3 + steps} after 3 warm-up steps"
+    return out
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def run_ours(args):
@@ -372,6 +428,11 @@ def run_ours(args):
                "final_volume": float(vols[-1])}
 
     cpu = cpu_baseline(prm, state, args.cpu_seconds) if (rank == 0 and world == 1) else None
+    ext = {}
+    if args.ext_steps > 0 and world == 1:
+        ext["convergent_pressure"] = measure_convergent(V, args.n, args.ext_steps, stream, dev)
+        ext["convergent_pressure"]["speedup_mixed_over_plain"] = round(
+            ext["convergent_pressure"]["mixed"]["value"] / value, 3)
 
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K,
@@ -384,6 +445,7 @@ def run_ours(args):
         "phases_ms": {k: round(v, 5) for k, v in phase_ms.items()},
         "phase_launches": phase_launches,
         "check": {"volume_after": vol, "nonfinite": nonfinite},
+        "extensions": ext,
         "device": props.name,
     }
     solver.close()

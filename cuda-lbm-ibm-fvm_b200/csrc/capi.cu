@@ -12,6 +12,7 @@
 
 #include "../../include/vof.h"
 #include "jacobi_tb.h"
+#include "mg_solve.h"
 #include "plain_step.h"
 #include "reduce.h"
 #include "tma.cuh"
@@ -35,6 +36,11 @@ struct vof_ctx {
     double* h_red_result;       // pinned, for vof_reduce
     int* d_status;              // device status word written by kernels (DEV_* codes)
     CUtensorMap maps[4];        // TMA descriptors: p0, p1, p2, rhs
+    // convergent modes (VOF_MODE_MIXED / VOF_MODE_FP64)
+    int conv;                   // nonzero in those modes
+    double* p64;                // FP64 pressure (padded layout); p0 holds its FP32 copy
+    vof::MgSolver mg;
+    vof::MgStats stats;         // of the last pressure solve
     cudaGraphExec_t graph[3][2];  // [istep % 3][p parity at step start]
     int last_cuda_error;
     size_t bytes;
@@ -79,6 +85,8 @@ int validate(const vof_params* p) {
     if (p->jacobi_iters < 0 || p->jacobi_iters > 100000) return VOF_E_INVALID;
     if (p->mode != VOF_MODE_PLAIN && p->mode != VOF_MODE_MIXED && p->mode != VOF_MODE_FP64)
         return VOF_E_INVALID;
+    if (p->mode != VOF_MODE_PLAIN && (!(p->tol > 0.0) || p->max_outer < 1 || p->max_outer > 100000))
+        return VOF_E_INVALID;
     return VOF_OK;
 }
 
@@ -103,6 +111,15 @@ void free_ctx(vof_ctx* c) {
     if (c->d_red_result) cudaFree(c->d_red_result);
     if (c->h_red_result) cudaFreeHost(c->h_red_result);
     if (c->d_status) cudaFree(c->d_status);
+    if (c->p64) cudaFree(c->p64);
+    for (int l = 0; l < c->mg.nlev; ++l) {
+        if (c->mg.lv[l].e0) cudaFree(c->mg.lv[l].e0);
+        if (c->mg.lv[l].e1) cudaFree(c->mg.lv[l].e1);
+        if (c->mg.lv[l].b) cudaFree(c->mg.lv[l].b);
+    }
+    if (c->mg.d_partial) cudaFree(c->mg.d_partial);
+    if (c->mg.d_result) cudaFree(c->mg.d_result);
+    if (c->mg.h_result) cudaFreeHost(c->mg.h_result);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     delete c;
 }
@@ -114,6 +131,19 @@ int check_status(vof_ctx* c) {
     if (st == 0) return VOF_OK;
     cudaMemset(c->d_status, 0, sizeof(int));
     return VOF_E_TIMEOUT;
+}
+
+// One step of a convergent mode: predictor and rhs, the multigrid-accelerated
+// FP64 defect correction for the pressure, correction and the FCT sweeps.
+int conv_step(vof_ctx* c, int istep, cudaEvent_t* ev) {
+    cudaError_t e = vof::plain_front(c->g, c->b, c->stream, ev);
+    if (e != cudaSuccess) return fail_cuda(c, e);
+    e = vof::mg_solve(c->g, c->mg, c->b.rhs, c->p64, c->b.p0, c->prm.tol, c->prm.max_outer, &c->stats, c->stream);
+    const bool not_conv = (e == cudaErrorNotReady);
+    if (e != cudaSuccess && !not_conv) return fail_cuda(c, e);
+    e = vof::plain_back(c->g, c->b, istep, c->b.p0, c->stream, ev);
+    if (e != cudaSuccess) return fail_cuda(c, e);
+    return not_conv ? VOF_E_NOT_CONVERGED : VOF_OK;
 }
 
 }  // namespace
@@ -192,7 +222,6 @@ int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
     *out = nullptr;
     int st = validate(p);
     if (st != VOF_OK) return st;
-    if (p->mode != VOF_MODE_PLAIN) return VOF_E_UNSUPPORTED;
 
     vof_ctx* c = new (std::nothrow) vof_ctx;
     if (!c) return VOF_E_NOMEM;
@@ -248,6 +277,20 @@ int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
     ok = ok && alloc((void**)&c->d_red_scratch, sizeof(double) * vof::RED_SCRATCH_DOUBLES);
     ok = ok && alloc((void**)&c->d_red_result, sizeof(double) * vof::RED_RESULT_DOUBLES);
     ok = ok && alloc((void**)&c->d_status, sizeof(int));
+    c->conv = (p->mode != VOF_MODE_PLAIN);
+    if (ok && c->conv) {
+        c->mg.mode = (p->mode == VOF_MODE_MIXED) ? vof::MG_MIXED : vof::MG_FP64;
+        c->mg.nlev = vof::mg_plan(g, c->mg.lv, vof::MG_MAX_LEVELS);
+        const size_t vb = vof::mg_storage_bytes(c->mg.mode);
+        ok = alloc((void**)&c->p64, c->elems * sizeof(double));
+        for (int l = 0; l < c->mg.nlev && ok; ++l) {
+            const size_t nb = (size_t)c->mg.lv[l].ncell * vb;
+            ok = alloc(&c->mg.lv[l].e0, nb) && alloc(&c->mg.lv[l].e1, nb) && alloc(&c->mg.lv[l].b, nb);
+        }
+        ok = ok && alloc((void**)&c->mg.d_partial, sizeof(double) * vof::MG_PARTIAL_DOUBLES);
+        ok = ok && alloc((void**)&c->mg.d_result, sizeof(double) * 8);
+        if (ok && cudaMallocHost((void**)&c->mg.h_result, sizeof(double) * 2) != cudaSuccess) ok = false;
+    }
     if (ok && cudaMallocHost((void**)&c->h_red_result, sizeof(double) * 4) != cudaSuccess) ok = false;
     if (!ok) {
         free_ctx(c);
@@ -277,6 +320,7 @@ int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
 
     const int maxn = p->nx > p->ny ? (p->nx > p->nz ? p->nx : p->nz) : (p->ny > p->nz ? p->ny : p->nz);
     if ((e = vof::plain_configure(maxn)) != cudaSuccess || (e = vof::plain_density_pairs(&c->g)) != cudaSuccess ||
+        (c->conv && (e = vof::mg_configure(c->mg)) != cudaSuccess) ||
         (e = cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaStreamSynchronize(c->stream)) != cudaSuccess) {
         c->last_cuda_error = (int)e;
@@ -311,6 +355,7 @@ int vof_upload(vof_ctx* ctx, int field, const float* src, int src_is_device) {
                                       (size_t)(g.ny + 2) * (g.nz + 2),
                                       src_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                       ctx->stream);
+    if (e == cudaSuccess && ctx->conv && field == VOF_FIELD_P) e = vof::mg_widen(g, dst, ctx->p64, ctx->stream);
     return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
 }
 
@@ -332,6 +377,7 @@ int vof_download(vof_ctx* ctx, int field, float* dst, int dst_is_device) {
 int vof_step(vof_ctx* ctx, int istep) {
     if (!ctx) return VOF_E_INVALID;
     DeviceGuard dg(ctx->device);
+    if (ctx->conv) return conv_step(ctx, istep, nullptr);
     cudaError_t e = vof::plain_step(ctx->g, ctx->b, istep, ctx->prm.jacobi_iters, &ctx->p_parity,
                                     ctx->stream);
     return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
@@ -340,6 +386,13 @@ int vof_step(vof_ctx* ctx, int istep) {
 int vof_run(vof_ctx* ctx, int istep0, int nsteps) {
     if (!ctx || nsteps < 0) return VOF_E_INVALID;
     DeviceGuard dg(ctx->device);
+    if (ctx->conv) {  // data-dependent solver loop: plain launches, no graphs
+        for (int s = 0; s < nsteps; ++s) {
+            const int st = conv_step(ctx, istep0 + s, nullptr);
+            if (st != VOF_OK) return st;
+        }
+        return VOF_OK;
+    }
     for (int s = 0; s < nsteps; ++s) {
         const int istep = istep0 + s;
         const int r = ((istep % 3) + 3) % 3;
@@ -377,19 +430,27 @@ int vof_step_timed(vof_ctx* ctx, int istep, float* phase_ms, int* launches, int 
     cudaEvent_t ev[vof::PLAIN_PHASES + 1] = {};
     cudaError_t e = cudaSuccess;
     for (int q = 0; q <= vof::PLAIN_PHASES && e == cudaSuccess; ++q) e = cudaEventCreate(&ev[q]);
-    if (e == cudaSuccess)
+    int conv_status = VOF_OK;
+    if (e == cudaSuccess && ctx->conv) {
+        conv_status = conv_step(ctx, istep, ev);
+        if (conv_status == VOF_E_CUDA) e = (cudaError_t)ctx->last_cuda_error;
+    } else if (e == cudaSuccess) {
         e = vof::plain_step(ctx->g, ctx->b, istep, ctx->prm.jacobi_iters, &ctx->p_parity, ctx->stream, ev);
+    }
     if (e == cudaSuccess) e = cudaEventSynchronize(ev[vof::PLAIN_PHASES]);
     const int n = nphase < VOF_PHASES ? nphase : VOF_PHASES;
     for (int q = 0; q < n && e == cudaSuccess; ++q) {
         float ms = 0.0f;
         e = cudaEventElapsedTime(&ms, ev[q], ev[q + 1]);
         if (phase_ms) phase_ms[q] = ms;
-        if (launches) launches[q] = vof::plain_phase_launches(q, ctx->prm.jacobi_iters);
+        if (launches)
+            launches[q] = (ctx->conv && q == vof::PHASE_JACOBI) ? ctx->stats.launches
+                                                                : vof::plain_phase_launches(q, ctx->prm.jacobi_iters);
     }
     for (int q = 0; q <= vof::PLAIN_PHASES; ++q)
         if (ev[q]) cudaEventDestroy(ev[q]);
     if (e != cudaSuccess) return fail_cuda(ctx, e);
+    if (conv_status != VOF_OK) return conv_status;
     return n;
 }
 
@@ -435,10 +496,20 @@ int vof_reduce(vof_ctx* ctx, int what, double* out) {
     return VOF_OK;
 }
 
+int vof_solver_stats(const vof_ctx* ctx, int* outer, double* rel_initial, double* rel_final) {
+    if (!ctx) return VOF_E_INVALID;
+    if (!ctx->conv) return VOF_E_STATE;
+    if (outer) *outer = ctx->stats.outer;
+    if (rel_initial) *rel_initial = ctx->stats.rel_initial;
+    if (rel_final) *rel_final = ctx->stats.rel_final;
+    return VOF_OK;
+}
+
 int vof_last_cuda_error(const vof_ctx* ctx) { return ctx ? ctx->last_cuda_error : 0; }
 
 int vof_kernels_per_step(const vof_ctx* ctx) {
     if (!ctx) return VOF_E_INVALID;
+    if (ctx->conv) return 2 + ctx->stats.launches + 4;  // the last step's count
     return vof::plain_kernels_per_step(ctx->prm.jacobi_iters);
 }
 

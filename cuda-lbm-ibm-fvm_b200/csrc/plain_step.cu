@@ -370,22 +370,53 @@ static void column_launch(const Geom& g, dim3& grid, int& kchunk) {
     grid = dim3(bx, by, (g.nz + kchunk - 1) / kchunk);
 }
 
-cudaError_t plain_step(const Geom& g, const PlainBuffers& b, int istep, int jacobi_iters,
-                       int* p_parity, cudaStream_t s, cudaEvent_t* ev) {
+// ev (optional, PLAIN_PHASES+1 events): ev[0] before the step, ev[q+1]
+// after phase q (predict, rhs, pressure, correct, sweep 1, sweep 2, sweep 3).
+static inline cudaError_t mark(cudaEvent_t* ev, int q, cudaStream_t s) {
+    return ev ? cudaEventRecord(ev[q], s) : cudaSuccess;
+}
+
+cudaError_t plain_front(const Geom& g, const PlainBuffers& b, cudaStream_t s, cudaEvent_t* ev) {
     const dim3 blk(TX, TY, 1);
     dim3 grid;
     int kchunk = 1;
     column_launch(g, grid, kchunk);
     cudaError_t e;
-    // ev (optional, PLAIN_PHASES+1 events): ev[0] before the step, ev[q+1]
-    // after phase q (predict, rhs, jacobi, correct, sweep 1, sweep 2, sweep 3).
-    auto mark = [&](int q) -> cudaError_t { return ev ? cudaEventRecord(ev[q], s) : cudaSuccess; };
-
-    if ((e = mark(0)) != cudaSuccess) return e;
+    if ((e = mark(ev, 0, s)) != cudaSuccess) return e;
     k_predict<<<grid, blk, 0, s>>>(g, b.F, b.u, b.v, b.w, b.us, b.vs, b.ws, kchunk);
-    if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(1)) != cudaSuccess) return e;
+    if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(ev, 1, s)) != cudaSuccess) return e;
     k_rhs<<<grid, blk, 0, s>>>(g, b.F, b.us, b.vs, b.ws, b.rhs, kchunk);
-    if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(2)) != cudaSuccess) return e;
+    if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(ev, 2, s)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+cudaError_t plain_back(const Geom& g, const PlainBuffers& b, int istep, const float* p, cudaStream_t s,
+                       cudaEvent_t* ev) {
+    cudaError_t e;
+    if ((e = mark(ev, 3, s)) != cudaSuccess) return e;
+    {
+        const dim3 cb(32, 4, 2);
+        const dim3 cg((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + 1) / 2);
+        k_correct<<<cg, cb, 0, s>>>(g, b.F, b.us, b.vs, b.ws, p, b.u, b.v, b.w);
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(ev, 4, s)) != cudaSuccess) return e;
+
+    // Sweep order by istep % 3 (voftrial1.cu:1384-1396).
+    const int r = ((istep % 3) + 3) % 3;
+    static const int order[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
+    for (int q = 0; q < 3; ++q) {
+        const int axis = order[r][q];
+        const float* vel = axis == 0 ? b.u : (axis == 1 ? b.v : b.w);
+        if ((e = fct_launch(g, axis, q == 2, b.F, vel, s)) != cudaSuccess || (e = mark(ev, 5 + q, s)) != cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t plain_step(const Geom& g, const PlainBuffers& b, int istep, int jacobi_iters,
+                       int* p_parity, cudaStream_t s, cudaEvent_t* ev) {
+    cudaError_t e = plain_front(g, b, s, ev);
+    if (e != cudaSuccess) return e;
 
     // Jacobi (voftrial1.cu:1371-1375): JACOBI_T sweeps per launch.  The
     // reference ping-pongs p <-> pt once per sweep, so after N sweeps its
@@ -414,25 +445,7 @@ cudaError_t plain_step(const Geom& g, const PlainBuffers& b, int istep, int jaco
         }
     }
     *p_parity = dst;
-    if ((e = mark(3)) != cudaSuccess) return e;
-
-    {
-        const dim3 cb(32, 4, 2);
-        const dim3 cg((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + 1) / 2);
-        k_correct<<<cg, cb, 0, s>>>(g, b.F, b.us, b.vs, b.ws, pbuf[dst], b.u, b.v, b.w);
-    }
-    if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(4)) != cudaSuccess) return e;
-
-    // Sweep order by istep % 3 (voftrial1.cu:1384-1396).
-    const int r = ((istep % 3) + 3) % 3;
-    static const int order[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
-    for (int q = 0; q < 3; ++q) {
-        const int axis = order[r][q];
-        const float* vel = axis == 0 ? b.u : (axis == 1 ? b.v : b.w);
-        if ((e = fct_launch(g, axis, q == 2, b.F, vel, s)) != cudaSuccess || (e = mark(5 + q)) != cudaSuccess)
-            return e;
-    }
-    return cudaSuccess;
+    return plain_back(g, b, istep, pbuf[dst], s, ev);
 }
 
 int plain_phase_launches(int phase, int jacobi_iters) {

@@ -60,6 +60,13 @@ enum {
 cudaError_t plain_step(const Geom& g, const PlainBuffers& b, int istep, int jacobi_iters,
                        int* p_parity, cudaStream_t s, cudaEvent_t* ev = nullptr);
 
+// The two halves around the pressure solve: predictor + rhs, and velocity
+// correction (with pressure p) + the three FCT sweeps.  plain_step is
+// plain_front, the Jacobi sweeps, plain_back.
+cudaError_t plain_front(const Geom& g, const PlainBuffers& b, cudaStream_t s, cudaEvent_t* ev = nullptr);
+cudaError_t plain_back(const Geom& g, const PlainBuffers& b, int istep, const float* p, cudaStream_t s,
+                       cudaEvent_t* ev = nullptr);
+
 // Kernel launches of one phase.
 int plain_phase_launches(int phase, int jacobi_iters);
 

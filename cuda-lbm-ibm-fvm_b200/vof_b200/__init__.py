@@ -108,6 +108,8 @@ def _declare(lib):
         "vof_device_bytes": (C.c_size_t, [vp]),
         "vof_step_timed": (C.c_int, [vp, C.c_int, P(C.c_float), P(C.c_int), C.c_int]),
         "vof_phase_name": (C.c_char_p, [C.c_int]),
+        "vof_solver_stats": (C.c_int, [vp, P(C.c_int), P(C.c_double), P(C.c_double)]),
+        "vof_step_noalloc": (C.c_int, [P(Params), vp, vp, vp, vp, vp, C.c_int, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -134,7 +136,7 @@ def exported_symbols():
             "vof_create", "vof_destroy", "vof_get_params", "vof_upload", "vof_download",
             "vof_step", "vof_run", "vof_sync", "vof_reduce", "vof_reduce_async",
             "vof_last_cuda_error", "vof_kernels_per_step", "vof_device_bytes",
-            "vof_step_timed", "vof_phase_name"]
+            "vof_step_timed", "vof_phase_name", "vof_solver_stats", "vof_step_noalloc"]
 
 
 def default_params(nx: int, ny: int | None = None, nz: int | None = None, **overrides) -> Params:
@@ -257,6 +259,12 @@ class Solver:
         if st < 0:
             self._check(st, "vof_step_timed")
         return {self._lib.vof_phase_name(q).decode(): (ms[q], la[q]) for q in range(st)}
+
+    def solver_stats(self) -> dict:
+        """Convergent modes: {'outer', 'rel_initial', 'rel_final'} of the last solve."""
+        o, a, b = C.c_int(), C.c_double(), C.c_double()
+        self._check(self._lib.vof_solver_stats(self._ctx, C.byref(o), C.byref(a), C.byref(b)), "vof_solver_stats")
+        return {"outer": o.value, "rel_initial": a.value, "rel_final": b.value}
 
     @property
     def kernels_per_step(self) -> int:

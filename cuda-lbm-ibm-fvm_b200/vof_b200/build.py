@@ -33,11 +33,12 @@ SOURCES = {
     "fct_sweep.cu": ["-fmad=false", "-DVOF_FMAD_FALSE"],
     "jacobi_tb.cu": ["-fmad=false", "-DVOF_FMAD_FALSE"],
     "tma_host.cu": [],
+    "mg_solve.cu": [],
     "reduce.cu": [],
     "capi.cu": [],
     "noalloc.cu": [],
 }
-HEADERS = ["vof_device.cuh", "tma.cuh", "plain_step.h", "fct_sweep.h", "jacobi_tb.h", "reduce.h"]
+HEADERS = ["vof_device.cuh", "tma.cuh", "plain_step.h", "fct_sweep.h", "jacobi_tb.h", "mg_solve.h", "reduce.h"]
 
 
 def nvcc() -> str:

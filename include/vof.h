@@ -213,6 +213,14 @@ int vof_reduce_async(vof_ctx* ctx, int what, double* host_out);
 int vof_step_noalloc(const vof_params* p, float* F, float* u, float* v, float* w, float* pres, int istep,
                      void* stream);
 
+/*
+ * Convergent modes (VOF_MODE_MIXED, VOF_MODE_FP64; no counterpart in the
+ * reference): V-cycles done by the last pressure solve and its relative
+ * residual ||b - A p|| / ||b|| (FP64, b = rhs - mean) at entry and at exit.
+ * VOF_E_STATE in VOF_MODE_PLAIN.
+ */
+int vof_solver_stats(const vof_ctx* ctx, int* outer, double* rel_initial, double* rel_final);
+
 /* cudaError_t of the most recent failing CUDA call in this context (0 if none). */
 int vof_last_cuda_error(const vof_ctx* ctx);
 

@@ -61,6 +61,9 @@ def oracle_lib():
             fn.restype = C.c_int
             fn.argtypes = [C.POINTER(Params)] + [C.POINTER(T)] * 5 + [C.c_int, C.c_int] + \
                 [C.POINTER(T)] * 4 + [C.c_int]
+        lib.oracle_run_conv_f64.restype = C.c_int
+        lib.oracle_run_conv_f64.argtypes = [C.POINTER(Params)] + [C.POINTER(C.c_double)] * 5 + \
+            [C.c_int, C.c_int, C.c_double, C.c_int]
         lib.oracle_clamp01f.restype = C.c_float
         lib.oracle_clamp01f.argtypes = [C.c_float]
         lib.oracle_clamp01d.restype = C.c_double
@@ -93,6 +96,16 @@ def run_f32(prm, state, istep0: int, nsteps: int, nthreads: int = 0, extras: boo
 def run_f64(prm, state, istep0: int, nsteps: int, nthreads: int = 0, extras: bool = False) -> dict:
     """nsteps reference steps in FP64 on a copy of `state` (promoted to float64)."""
     return _run(oracle_lib().oracle_run_f64, C.c_double, np.float64, prm, state, istep0, nsteps, nthreads, extras)
+
+
+def run_conv_f64(prm, state, istep0: int, nsteps: int, tol: float = 1e-12, nthreads: int = 0) -> dict:
+    """FP64 steps with the pressure solved to ||r|| <= tol ||b|| (CG), mean(p) = 0."""
+    st = {k: np.ascontiguousarray(state[k], dtype=np.float64).copy() for k in STATE}
+    rc = oracle_lib().oracle_run_conv_f64(C.byref(prm), *(_ptr(st[k], C.c_double) for k in STATE), istep0,
+                                          nsteps, float(tol), int(nthreads))
+    if rc != 0:
+        raise RuntimeError(f"oracle conv run failed: {rc}")
+    return st
 
 
 def clamp01f(x: float) -> float:

@@ -415,15 +415,97 @@ struct Oracle {
                 }
     }
 
+    // Convergent pressure solve (extension; no reference counterpart):
+    // A p = rhs - mean(rhs) with the Jacobi sweep's Neumann operator, by
+    // conjugate gradients on -A from the current p, to ||r|| <= tol ||b||,
+    // then the gauge mean(p) = 0.  Returns the final relative residual.
+    double conv_tol = 0.0;  // > 0 selects the convergent solve
+    int conv_iters = 0;
+    void apply_negA(const std::vector<double>& x, std::vector<double>& y) {
+        const double cx = (double)P.dxi * P.dxi, cyy = (double)P.dyi * P.dyi, cz = (double)P.dzi * P.dzi;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+        for (int k = 1; k <= P.nz; ++k)
+            for (int j = 1; j <= P.ny; ++j)
+                for (int i = 1; i <= P.nx; ++i) {
+                    const size_t c = id(i, j, k);
+                    const double xc = x[c];
+                    double s = 0;
+                    if (i != P.nx) s += cx * (x[id(i + 1, j, k)] - xc);
+                    if (i != 1) s += cx * (x[id(i - 1, j, k)] - xc);
+                    if (j != P.ny) s += cyy * (x[id(i, j + 1, k)] - xc);
+                    if (j != 1) s += cyy * (x[id(i, j - 1, k)] - xc);
+                    if (k != P.nz) s += cz * (x[id(i, j, k + 1)] - xc);
+                    if (k != 1) s += cz * (x[id(i, j, k - 1)] - xc);
+                    y[c] = -s;
+                }
+    }
+    double dot_in(const std::vector<double>& a, const std::vector<double>& b) {
+        double s = 0;
+#pragma omp parallel for num_threads(nthreads) schedule(static) reduction(+ : s)
+        for (int k = 1; k <= P.nz; ++k)
+            for (int j = 1; j <= P.ny; ++j)
+                for (int i = 1; i <= P.nx; ++i) s += a[id(i, j, k)] * b[id(i, j, k)];
+        return s;
+    }
+    double solve_conv() {
+        const size_t n = N;
+        std::vector<double> x(n, 0.0), b(n, 0.0), r(n, 0.0), d(n, 0.0), q(n, 0.0);
+        double mean = 0;
+        for (int k = 1; k <= P.nz; ++k)
+            for (int j = 1; j <= P.ny; ++j)
+                for (int i = 1; i <= P.nx; ++i) {
+                    x[id(i, j, k)] = (double)p[id(i, j, k)];
+                    b[id(i, j, k)] = (double)rhs_at(i, j, k);
+                    mean += b[id(i, j, k)];
+                }
+        const double ncell = (double)P.nx * P.ny * P.nz;
+        mean /= ncell;
+        for (int k = 1; k <= P.nz; ++k)
+            for (int j = 1; j <= P.ny; ++j)
+                for (int i = 1; i <= P.nx; ++i) b[id(i, j, k)] = -(b[id(i, j, k)] - mean);  // system -A x = -b
+        apply_negA(x, q);
+        for (size_t t = 0; t < n; ++t) r[t] = b[t] - q[t];
+        const double bn = std::sqrt(dot_in(b, b));
+        double rr = dot_in(r, r);
+        d = r;
+        int it = 0;
+        while (bn > 0 && std::sqrt(rr) > conv_tol * bn && it < 20000) {
+            apply_negA(d, q);
+            const double al = rr / dot_in(d, q);
+            for (size_t t = 0; t < n; ++t) {
+                x[t] += al * d[t];
+                r[t] -= al * q[t];
+            }
+            const double rr2 = dot_in(r, r);
+            for (size_t t = 0; t < n; ++t) d[t] = r[t] + (rr2 / rr) * d[t];
+            rr = rr2;
+            ++it;
+        }
+        conv_iters = it;
+        double pm = 0;
+        for (int k = 1; k <= P.nz; ++k)
+            for (int j = 1; j <= P.ny; ++j)
+                for (int i = 1; i <= P.nx; ++i) pm += x[id(i, j, k)];
+        pm /= ncell;
+        for (int k = 1; k <= P.nz; ++k)
+            for (int j = 1; j <= P.ny; ++j)
+                for (int i = 1; i <= P.nx; ++i) p[id(i, j, k)] = (T)(x[id(i, j, k)] - pm);
+        return bn > 0 ? std::sqrt(rr) / bn : 0.0;
+    }
+
     // One time step, voftrial1.cu:1364-1401.
     void step(int istep) {
         cal_nu_rho();
         advect_u();
         advect_v();
         advect_w();
-        for (int it = 0; it < P.jacobi_iters; ++it) {
-            jacobi_sweep(p, pt);
-            std::swap(p, pt);
+        if (conv_tol > 0) {
+            solve_conv();
+        } else {
+            for (int it = 0; it < P.jacobi_iters; ++it) {
+                jacobi_sweep(p, pt);
+                std::swap(p, pt);
+            }
         }
         update_uvw();
         bc_velocity();
@@ -445,11 +527,12 @@ struct Oracle {
 
 template <typename T>
 int run(const vof_params* prm, T* F, T* u, T* v, T* w, T* p, int istep0, int nsteps, T* us_out,
-        T* vs_out, T* ws_out, T* rhs_out, int nthreads) {
+        T* vs_out, T* ws_out, T* rhs_out, int nthreads, double conv_tol = 0.0) {
     if (!prm || !F || !u || !v || !w || !p || nsteps < 0) return VOF_E_INVALID;
     if (prm->nx < 1 || prm->ny < 1 || prm->nz < 1) return VOF_E_SIZE;
     if (nthreads <= 0) nthreads = omp_get_max_threads();
     Oracle<T> o(make_prm(prm, T(0)), nthreads);
+    o.conv_tol = conv_tol;
     const size_t n = o.N;
     std::copy(F, F + n, o.F.begin());
     std::copy(u, u + n, o.u.begin());
@@ -488,6 +571,15 @@ int oracle_run_f32(const vof_params* prm, float* F, float* u, float* v, float* w
 int oracle_run_f64(const vof_params* prm, double* F, double* u, double* v, double* w, double* p, int istep0,
                    int nsteps, double* us, double* vs, double* ws, double* rhs, int nthreads) {
     return run<double>(prm, F, u, v, w, p, istep0, nsteps, us, vs, ws, rhs, nthreads);
+}
+
+// FP64 steps with the convergent pressure solve (CG to ||r|| <= tol ||b||,
+// gauge mean(p) = 0) in place of the Jacobi sweeps: the FP64 oracle of
+// VOF_MODE_MIXED / VOF_MODE_FP64.
+int oracle_run_conv_f64(const vof_params* prm, double* F, double* u, double* v, double* w, double* p, int istep0,
+                        int nsteps, double tol, int nthreads) {
+    if (!(tol > 0)) return VOF_E_INVALID;
+    return run<double>(prm, F, u, v, w, p, istep0, nsteps, nullptr, nullptr, nullptr, nullptr, nthreads, tol);
 }
 
 // clamp01f of the reference on one value, in float and in double.
