@@ -112,14 +112,7 @@ void free_ctx(vof_ctx* c) {
     if (c->h_red_result) cudaFreeHost(c->h_red_result);
     if (c->d_status) cudaFree(c->d_status);
     if (c->p64) cudaFree(c->p64);
-    for (int l = 0; l < c->mg.nlev; ++l) {
-        if (c->mg.lv[l].e0) cudaFree(c->mg.lv[l].e0);
-        if (c->mg.lv[l].e1) cudaFree(c->mg.lv[l].e1);
-        if (c->mg.lv[l].b) cudaFree(c->mg.lv[l].b);
-    }
-    if (c->mg.d_partial) cudaFree(c->mg.d_partial);
-    if (c->mg.d_result) cudaFree(c->mg.d_result);
-    if (c->mg.h_result) cudaFreeHost(c->mg.h_result);
+    vof::mg_destroy(&c->mg);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     delete c;
 }
@@ -138,7 +131,8 @@ int check_status(vof_ctx* c) {
 int conv_step(vof_ctx* c, int istep, cudaEvent_t* ev) {
     cudaError_t e = vof::plain_front(c->g, c->b, c->stream, ev);
     if (e != cudaSuccess) return fail_cuda(c, e);
-    e = vof::mg_solve(c->g, c->mg, c->b.rhs, c->p64, c->b.p0, c->prm.tol, c->prm.max_outer, &c->stats, c->stream);
+    e = vof::mg_solve(c->g, c->mg, c->b.rhs, c->p64, c->b.p0, c->prm.tol, c->prm.max_outer, &c->stats, c->stream,
+                       c->cap_stream);
     const bool not_conv = (e == cudaErrorNotReady);
     if (e != cudaSuccess && !not_conv) return fail_cuda(c, e);
     e = vof::plain_back(c->g, c->b, istep, c->b.p0, c->stream, ev);
@@ -279,17 +273,10 @@ int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
     ok = ok && alloc((void**)&c->d_status, sizeof(int));
     c->conv = (p->mode != VOF_MODE_PLAIN);
     if (ok && c->conv) {
-        c->mg.mode = (p->mode == VOF_MODE_MIXED) ? vof::MG_MIXED : vof::MG_FP64;
-        c->mg.nlev = vof::mg_plan(g, c->mg.lv, vof::MG_MAX_LEVELS);
-        const size_t vb = vof::mg_storage_bytes(c->mg.mode);
         ok = alloc((void**)&c->p64, c->elems * sizeof(double));
-        for (int l = 0; l < c->mg.nlev && ok; ++l) {
-            const size_t nb = (size_t)c->mg.lv[l].ncell * vb;
-            ok = alloc(&c->mg.lv[l].e0, nb) && alloc(&c->mg.lv[l].e1, nb) && alloc(&c->mg.lv[l].b, nb);
-        }
-        ok = ok && alloc((void**)&c->mg.d_partial, sizeof(double) * vof::MG_PARTIAL_DOUBLES);
-        ok = ok && alloc((void**)&c->mg.d_result, sizeof(double) * 8);
-        if (ok && cudaMallocHost((void**)&c->mg.h_result, sizeof(double) * 2) != cudaSuccess) ok = false;
+        if (ok && vof::mg_create(g, p->mode == VOF_MODE_MIXED ? vof::MG_MIXED : vof::MG_FP64, &c->mg, c->stream,
+                                 &c->bytes) != cudaSuccess)
+            ok = false;
     }
     if (ok && cudaMallocHost((void**)&c->h_red_result, sizeof(double) * 4) != cudaSuccess) ok = false;
     if (!ok) {
@@ -320,7 +307,6 @@ int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
 
     const int maxn = p->nx > p->ny ? (p->nx > p->nz ? p->nx : p->nz) : (p->ny > p->nz ? p->ny : p->nz);
     if ((e = vof::plain_configure(maxn)) != cudaSuccess || (e = vof::plain_density_pairs(&c->g)) != cudaSuccess ||
-        (c->conv && (e = vof::mg_configure(c->mg)) != cudaSuccess) ||
         (e = cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaStreamSynchronize(c->stream)) != cudaSuccess) {
         c->last_cuda_error = (int)e;
@@ -355,7 +341,7 @@ int vof_upload(vof_ctx* ctx, int field, const float* src, int src_is_device) {
                                       (size_t)(g.ny + 2) * (g.nz + 2),
                                       src_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                       ctx->stream);
-    if (e == cudaSuccess && ctx->conv && field == VOF_FIELD_P) e = vof::mg_widen(g, dst, ctx->p64, ctx->stream);
+    if (e == cudaSuccess && ctx->conv && field == VOF_FIELD_P) e = vof::mg_widen(g, ctx->mg, dst, ctx->p64, ctx->stream);
     return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
 }
 

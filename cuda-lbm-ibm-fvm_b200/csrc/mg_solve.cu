@@ -12,16 +12,31 @@
 //   MIXED: every multigrid vector stored in BF16, arithmetic in FP32;
 //   FP64:  the same cycle with FP64 storage and arithmetic (the yardstick).
 // V-cycle: damped Jacobi (omega = 6/7, the Jacobi update of the reference's
-// sweep with damping) as the smoother, 2 pre + 2 post sweeps on large levels
-// and 8 + 8 on levels no wider than 25 cells, averaging restriction,
-// cell-centred multilinear prolongation with zero-gradient ends, coarse
-// operators rediscretised at the coarse spacing.  Each axis is coarsened by
-// its smallest prime factor (2, 3, 5, 7) while at least two cells remain
-// (200 -> 100 -> 50 -> 25 -> 5); the coarsest level gets 100 Jacobi sweeps
-// after removing its mean.
+// sweep with damping) as the smoother, 2 pre + 2 post sweeps on levels wider
+// than 25 cells and 8 + 8 on smaller ones, averaging restriction, cell-centred
+// multilinear prolongation with zero-gradient ends, coarse operators
+// rediscretised at the coarse spacing.  Each axis is coarsened by its
+// smallest prime factor (2, 3, 5, 7) while at least two cells remain
+// (200 -> 100 -> 50 -> 25 -> 5).  The coarsest level is solved exactly with
+// a stored inverse of A + c 11^T (mean-free right-hand side) when it has at
+// most MG_DENSE_MAX cells, otherwise by 100 damped sweeps after removing the
+// mean of its right-hand side.
+//
+// Execution: the large levels run as multi-block kernels (blocks of 32 x 8
+// columns marching kc planes, the z neighbours kept in registers); the first
+// sweep from zero is fused into the kernel producing the level's right-hand
+// side (the FP64 residual, or the restriction), and the last post-sweep of
+// the fine level is fused with p += e.  The deepest levels of at most
+// MG_TAIL_CELLS cells whose vectors fit in shared memory (with the coarse
+// inverse; 5^3 at 200^3) run in one 1024-thread block entirely from shared
+// memory (k_mg_tail), which removes the launch-latency floor of the coarse
+// levels; one outer iteration is a captured CUDA graph.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <utility>
+#include <vector>
 
 #include "mg_solve.h"
 
@@ -32,98 +47,103 @@ struct St;
 template <>
 struct St<__nv_bfloat16> {
     using C = float;
-    __device__ static float ld(const __nv_bfloat16* p, long i) { return __bfloat162float(p[i]); }
-    __device__ static void st(__nv_bfloat16* p, long i, float v) { p[i] = __float2bfloat16_rn(v); }
+    __device__ static float ld(const __nv_bfloat16* p, int i) { return __bfloat162float(p[i]); }
+    __device__ static void st(__nv_bfloat16* p, int i, float v) { p[i] = __float2bfloat16_rn(v); }
+    __device__ static float q(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
 };
 template <>
 struct St<double> {
     using C = double;
-    __device__ static double ld(const double* p, long i) { return p[i]; }
-    __device__ static void st(double* p, long i, double v) { p[i] = v; }
+    __device__ static double ld(const double* p, int i) { return p[i]; }
+    __device__ static void st(double* p, int i, double v) { p[i] = v; }
+    __device__ static double q(double v) { return v; }
 };
 
-constexpr int MG_THREADS = 256;
-constexpr int MG_RED_BLOCKS = 296;
+constexpr int MG_THREADS = MG_BX * MG_BY;
+constexpr int TAIL_THREADS = 1024;
 
-__device__ __forceinline__ long lidx(const MgLevel& L, int i, int j, int k) {
-    return ((long)k * L.ny + j) * L.nx + i;
-}
+__host__ __device__ __forceinline__ int nb_count(int x, int n) { return (x > 0) + (x < n - 1); }
 
-// (A e)_c and the diagonal of A at (i,j,k) of level L.
+// Sigma over the x/y non-wall neighbours of a (e_nb - ec) at compact index c.
 template <typename S, typename C>
-__device__ __forceinline__ void apply_row(const MgLevel& L, const S* e, int i, int j, int k, C& Ae, C& dg) {
+__device__ __forceinline__ C lap_xy(const MgLevel& L, const S* e, int c, int i, int j, C ec) {
     using T = St<S>;
-    const long c = lidx(L, i, j, k);
-    const C ec = T::ld(e, c);
-    const C ax = (C)L.ax, ay = (C)L.ay, az = (C)L.az;
-    C s = 0, d = 0;
-    if (i > 0) { s += ax * ((C)T::ld(e, c - 1) - ec); d -= ax; }
-    if (i < L.nx - 1) { s += ax * ((C)T::ld(e, c + 1) - ec); d -= ax; }
-    if (j > 0) { s += ay * ((C)T::ld(e, c - L.nx) - ec); d -= ay; }
-    if (j < L.ny - 1) { s += ay * ((C)T::ld(e, c + L.nx) - ec); d -= ay; }
-    if (k > 0) { s += az * ((C)T::ld(e, c - (long)L.nx * L.ny) - ec); d -= az; }
-    if (k < L.nz - 1) { s += az * ((C)T::ld(e, c + (long)L.nx * L.ny) - ec); d -= az; }
-    Ae = s;
-    dg = d;
+    const C ax = (C)L.ax, ay = (C)L.ay;
+    C s = 0;
+    if (i > 0) s += ax * ((C)T::ld(e, c - 1) - ec);
+    if (i < L.nx - 1) s += ax * ((C)T::ld(e, c + 1) - ec);
+    if (j > 0) s += ay * ((C)T::ld(e, c - L.nx) - ec);
+    if (j < L.ny - 1) s += ay * ((C)T::ld(e, c + L.nx) - ec);
+    return s;
 }
 
-#define MG_FOR_CELLS(L, i, j, k)                                                                   \
-    for (long t_ = (long)blockIdx.x * blockDim.x + threadIdx.x, n_ = (long)(L).nx * (L).ny * (L).nz; \
-         t_ < n_; t_ += (long)gridDim.x * blockDim.x)                                              \
-        for (int i = (int)(t_ % (L).nx), j = (int)((t_ / (L).nx) % (L).ny),                       \
-                 k = (int)(t_ / ((long)(L).nx * (L).ny)), once_ = 1;                               \
-             once_; once_ = 0)
+template <typename C>
+__device__ __forceinline__ C lap_z(const MgLevel& L, int k, C ec, C em, C ep) {
+    const C az = (C)L.az;
+    C s = 0;
+    if (k > 0) s += az * (em - ec);
+    if (k < L.nz - 1) s += az * (ep - ec);
+    return s;
+}
 
-// Damped Jacobi sweep: eout = ein + w (b - A ein) / diag (ein == nullptr: ein = 0).
+// Damped Jacobi on column (i, j), planes [k0, k1): eout = ein + wd (b - mb - A ein);
+// ein == nullptr means ein = 0.
 template <typename S>
-__global__ void __launch_bounds__(MG_THREADS) k_mg_jacobi(MgLevel L, const S* __restrict__ ein,
-                                                          S* __restrict__ eout, const S* __restrict__ b,
-                                                          double omega) {
+__device__ __forceinline__ void column_sweep(const MgLevel& L, const S* __restrict__ ein, S* __restrict__ eout,
+                                             const S* __restrict__ b, typename St<S>::C mb, int i, int j, int k0,
+                                             int k1) {
     using T = St<S>;
     using C = typename T::C;
-    MG_FOR_CELLS(L, i, j, k) {
-        const long c = lidx(L, i, j, k);
-        C Ae = 0, dg = 0;
+    const int plane = L.nx * L.ny;
+    const int nbxy = nb_count(i, L.nx) * 9 + nb_count(j, L.ny) * 3;
+    int c = (k0 * L.ny + j) * L.nx + i;
+    C em = 0, ec = 0;
+    if (ein) {
+        em = k0 > 0 ? (C)T::ld(ein, c - plane) : (C)0;
+        ec = (C)T::ld(ein, c);
+    }
+    for (int k = k0; k < k1; ++k, c += plane) {
+        C ep = 0, Ae = 0;
         if (ein) {
-            apply_row<S, C>(L, ein, i, j, k, Ae, dg);
-        } else {
-            const C ax = (C)L.ax, ay = (C)L.ay, az = (C)L.az;
-            dg = -(ax * ((i > 0) + (i < L.nx - 1)) + ay * ((j > 0) + (j < L.ny - 1)) + az * ((k > 0) + (k < L.nz - 1)));
+            ep = k + 1 < L.nz ? (C)T::ld(ein, c + plane) : (C)0;
+            Ae = lap_xy<S, C>(L, ein, c, i, j, ec) + lap_z<C>(L, k, ec, em, ep);
         }
-        const C e0 = ein ? (C)T::ld(ein, c) : (C)0;
-        const C r = (C)T::ld(b, c) - Ae;
-        T::st(eout, c, dg != 0 ? e0 + (C)omega * r / dg : e0);
+        T::st(eout, c, ec + (C)L.wd[nbxy + nb_count(k, L.nz)] * ((C)T::ld(b, c) - mb - Ae));
+        em = ec;
+        ec = ep;
     }
 }
 
-// bc = average over the fine cells of each coarse cell of (b - A e).
+// (b - A e) at compact cell (i, j, k), all neighbours loaded.
 template <typename S>
-__global__ void __launch_bounds__(MG_THREADS) k_mg_restrict(MgLevel F, const S* __restrict__ e,
-                                                            const S* __restrict__ b, MgLevel Cl,
-                                                            S* __restrict__ bc) {
+__device__ __forceinline__ typename St<S>::C cell_residual(const MgLevel& L, const S* e, const S* b, int i, int j,
+                                                           int k) {
     using T = St<S>;
     using C = typename T::C;
-    MG_FOR_CELLS(Cl, I, J, K) {
-        C acc = 0;
-        for (int dk = 0; dk < F.rz; ++dk)
-            for (int dj = 0; dj < F.ry; ++dj)
-                for (int di = 0; di < F.rx; ++di) {
-                    const int i = I * F.rx + di, j = J * F.ry + dj, k = K * F.rz + dk;
-                    C Ae, dg;
-                    apply_row<S, C>(F, e, i, j, k, Ae, dg);
-                    acc += (C)T::ld(b, lidx(F, i, j, k)) - Ae;
-                }
-        T::st(bc, lidx(Cl, I, J, K), acc / (C)(F.rx * F.ry * F.rz));
-    }
+    const int plane = L.nx * L.ny;
+    const int c = (k * L.ny + j) * L.nx + i;
+    const C ec = (C)T::ld(e, c);
+    const C em = k > 0 ? (C)T::ld(e, c - plane) : (C)0;
+    const C ep = k < L.nz - 1 ? (C)T::ld(e, c + plane) : (C)0;
+    return (C)T::ld(b, c) - (lap_xy<S, C>(L, e, c, i, j, ec) + lap_z<C>(L, k, ec, em, ep));
 }
 
-// Cell-centred linear interpolation weight along one axis: fine cell x of a
-// level coarsened by r; returns the two coarse indices and the weight of hi.
+// Cell-centred linear interpolation along one axis: fine cell x of a level
+// coarsened by r; the two coarse indices and the weight of hi.
 template <typename C>
 __device__ __forceinline__ void lin1(int x, int r, int nc, int& lo, int& hi, C& t) {
     if (r == 1) {
         lo = hi = x;
         t = 0;
+        return;
+    }
+    if (r == 2) {  // centre offsets -1/4 and +1/4 of a coarse cell
+        const int I = x >> 1;
+        lo = (x & 1) ? I : I - 1;
+        hi = lo + 1;
+        t = (x & 1) ? (C)0.25 : (C)0.75;
+        lo = lo < 0 ? 0 : lo;
+        hi = hi > nc - 1 ? nc - 1 : hi;
         return;
     }
     const int I = x / r, m = x - I * r;
@@ -141,205 +161,405 @@ __device__ __forceinline__ void lin1(int x, int r, int nc, int& lo, int& hi, C& 
     hi = hi > nc - 1 ? nc - 1 : hi;
 }
 
-// e += P ec (multilinear, zero-gradient beyond the coarse ends).
+// e(i,j,k) += (P ec)(i,j,k), multilinear with zero-gradient ends.
 template <typename S>
-__global__ void __launch_bounds__(MG_THREADS) k_mg_prolong(MgLevel F, S* __restrict__ e, MgLevel Cl,
-                                                           const S* __restrict__ ec) {
+__device__ __forceinline__ void prolong_cell(const MgLevel& F, S* e, const MgLevel& Cl, const S* ec, int i, int j,
+                                             int k) {
     using T = St<S>;
     using C = typename T::C;
-    MG_FOR_CELLS(F, i, j, k) {
-        int x0, x1, y0, y1, z0, z1;
-        C tx, ty, tz;
-        lin1<C>(i, F.rx, Cl.nx, x0, x1, tx);
-        lin1<C>(j, F.ry, Cl.ny, y0, y1, ty);
-        lin1<C>(k, F.rz, Cl.nz, z0, z1, tz);
-        auto at = [&](int a, int bb, int cc) { return (C)T::ld(ec, lidx(Cl, a, bb, cc)); };
-        const C c00 = at(x0, y0, z0) * (1 - tx) + at(x1, y0, z0) * tx;
-        const C c10 = at(x0, y1, z0) * (1 - tx) + at(x1, y1, z0) * tx;
-        const C c01 = at(x0, y0, z1) * (1 - tx) + at(x1, y0, z1) * tx;
-        const C c11 = at(x0, y1, z1) * (1 - tx) + at(x1, y1, z1) * tx;
-        const C v = (c00 * (1 - ty) + c10 * ty) * (1 - tz) + (c01 * (1 - ty) + c11 * ty) * tz;
-        const long c = lidx(F, i, j, k);
-        T::st(e, c, (C)T::ld(e, c) + v);
-    }
+    int x0, x1, y0, y1, z0, z1;
+    C tx, ty, tz;
+    lin1<C>(i, F.rx, Cl.nx, x0, x1, tx);
+    lin1<C>(j, F.ry, Cl.ny, y0, y1, ty);
+    lin1<C>(k, F.rz, Cl.nz, z0, z1, tz);
+    const int cp = Cl.nx * Cl.ny;
+    const int r00 = z0 * cp + y0 * Cl.nx, r10 = z0 * cp + y1 * Cl.nx;
+    const int r01 = z1 * cp + y0 * Cl.nx, r11 = z1 * cp + y1 * Cl.nx;
+    const C c00 = (C)T::ld(ec, r00 + x0) * (1 - tx) + (C)T::ld(ec, r00 + x1) * tx;
+    const C c10 = (C)T::ld(ec, r10 + x0) * (1 - tx) + (C)T::ld(ec, r10 + x1) * tx;
+    const C c01 = (C)T::ld(ec, r01 + x0) * (1 - tx) + (C)T::ld(ec, r01 + x1) * tx;
+    const C c11 = (C)T::ld(ec, r11 + x0) * (1 - tx) + (C)T::ld(ec, r11 + x1) * tx;
+    const C v = (c00 * (1 - ty) + c10 * ty) * (1 - tz) + (c01 * (1 - ty) + c11 * ty) * tz;
+    const int c = (k * F.ny + j) * F.nx + i;
+    T::st(e, c, (C)T::ld(e, c) + v);
 }
 
-// Coarsest level, one block: remove the mean of b, then `sweeps` damped
-// Jacobi sweeps from e = 0 in shared memory.
-template <typename S>
-__global__ void __launch_bounds__(MG_THREADS) k_mg_coarsest(MgLevel L, const S* __restrict__ b, S* __restrict__ e,
-                                                            int sweeps, double omega) {
-    using T = St<S>;
-    using C = typename T::C;
-    extern __shared__ __align__(16) unsigned char raw[];
-    C* sb = reinterpret_cast<C*>(raw);
-    C* s0 = sb + L.ncell;
-    C* s1 = s0 + L.ncell;
-    __shared__ double red[MG_THREADS];
-    double acc = 0;
-    for (int c = threadIdx.x; c < L.ncell; c += MG_THREADS) {
-        sb[c] = (C)T::ld(b, c);
-        s0[c] = 0;
-        acc += (double)sb[c];
-    }
-    red[threadIdx.x] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = 0;
-        for (int q = 0; q < MG_THREADS; ++q) s += red[q];
-        red[0] = s / L.ncell;
-    }
-    __syncthreads();
-    const C mean = (C)red[0];
-    for (int c = threadIdx.x; c < L.ncell; c += MG_THREADS) sb[c] -= mean;
-    __syncthreads();
-    const C ax = (C)L.ax, ay = (C)L.ay, az = (C)L.az;
-    for (int sw = 0; sw < sweeps; ++sw) {
-        const C* in = (sw & 1) ? s1 : s0;
-        C* out = (sw & 1) ? s0 : s1;
-        for (int c = threadIdx.x; c < L.ncell; c += MG_THREADS) {
-            const int i = c % L.nx, j = (c / L.nx) % L.ny, k = c / (L.nx * L.ny);
-            const C ev = in[c];
-            C s = 0, d = 0;
-            if (i > 0) { s += ax * (in[c - 1] - ev); d -= ax; }
-            if (i < L.nx - 1) { s += ax * (in[c + 1] - ev); d -= ax; }
-            if (j > 0) { s += ay * (in[c - L.nx] - ev); d -= ay; }
-            if (j < L.ny - 1) { s += ay * (in[c + L.nx] - ev); d -= ay; }
-            if (k > 0) { s += az * (in[c - L.nx * L.ny] - ev); d -= az; }
-            if (k < L.nz - 1) { s += az * (in[c + L.nx * L.ny] - ev); d -= az; }
-            out[c] = d != 0 ? ev + (C)omega * (sb[c] - s) / d : ev;
-        }
-        __syncthreads();
-    }
-    const C* fin = (sweeps & 1) ? s1 : s0;
-    for (int c = threadIdx.x; c < L.ncell; c += MG_THREADS) T::st(e, c, fin[c]);
-}
-
-// ---- fine level, FP64 -------------------------------------------------------
-// Deterministic block reduction of up to 2 doubles into partial[2*block + v].
-__device__ void block_sum2(double a, double b, double* partial) {
-    __shared__ double sh[2][MG_THREADS / 32];
+// ---- reductions ---------------------------------------------------------------
+// Deterministic block sum of two doubles (block size a multiple of 32, up to
+// 1024); every thread gets the totals.
+__device__ __forceinline__ void block_sum2(double& a, double& b) {
+    __shared__ double sh[2][32];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthr = blockDim.x * blockDim.y * blockDim.z;
     for (int o = 16; o > 0; o >>= 1) {
         a += __shfl_down_sync(0xffffffffu, a, o);
         b += __shfl_down_sync(0xffffffffu, b, o);
     }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) {
-        sh[0][wid] = a;
-        sh[1][wid] = b;
+    __syncthreads();  // sh may still be read by a previous call
+    if ((tid & 31) == 0) {
+        sh[0][tid >> 5] = a;
+        sh[1][tid >> 5] = b;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double x = 0, y = 0;
-        for (int q = 0; q < MG_THREADS / 32; ++q) {
-            x += sh[0][q];
-            y += sh[1][q];
-        }
-        partial[2 * blockIdx.x] = x;
-        partial[2 * blockIdx.x + 1] = y;
+    double x = 0, y = 0;
+    for (int q = 0; q < nthr / 32; ++q) {
+        x += sh[0][q];
+        y += sh[1][q];
     }
+    a = x;
+    b = y;
 }
 
-__global__ void __launch_bounds__(MG_THREADS) k_fold2(const double* partial, int nblk, double* out) {
-    __shared__ double sh[2][MG_THREADS];
+__device__ __forceinline__ int block_linear() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
+
+__global__ void __launch_bounds__(MG_THREADS) k_fold2(const double* __restrict__ partial, int nblk,
+                                                      double* __restrict__ out, double* host_out) {
     double a = 0, b = 0;
-    for (int q = threadIdx.x; q < nblk; q += MG_THREADS) {
+    for (int q = threadIdx.x; q < nblk; q += blockDim.x) {
         a += partial[2 * q];
         b += partial[2 * q + 1];
     }
-    sh[0][threadIdx.x] = a;
-    sh[1][threadIdx.x] = b;
-    __syncthreads();
+    block_sum2(a, b);
     if (threadIdx.x == 0) {
-        double x = 0, y = 0;
-        for (int q = 0; q < MG_THREADS; ++q) {
-            x += sh[0][q];
-            y += sh[1][q];
+        out[0] = a;
+        out[1] = b;
+        if (host_out) {
+            host_out[0] = a;
+            host_out[1] = b;
+            __threadfence_system();
         }
-        out[0] = x;
-        out[1] = y;
     }
 }
 
-#define FINE_FOR(g, i, j, k)                                                                   \
-    for (long t_ = (long)blockIdx.x * blockDim.x + threadIdx.x, n_ = (long)(g).nx * (g).ny * (g).nz; \
-         t_ < n_; t_ += (long)gridDim.x * blockDim.x)                                          \
-        for (int i = 1 + (int)(t_ % (g).nx), j = 1 + (int)((t_ / (g).nx) % (g).ny),           \
-                 k = 1 + (int)(t_ / ((long)(g).nx * (g).ny)), once_ = 1;                       \
-             once_; once_ = 0)
+#define LEVEL_TILE(L)                                  \
+    const int i = blockIdx.x * MG_BX + threadIdx.x;    \
+    const int j = blockIdx.y * MG_BY + threadIdx.y;    \
+    const int k0 = blockIdx.z * (L).kc;                \
+    const int k1 = min((L).nz, k0 + (L).kc);           \
+    const bool active = i < (L).nx && j < (L).ny
 
-// Sum of rhs over the interior (for its mean).
-__global__ void __launch_bounds__(MG_THREADS) k_sum_rhs(Geom g, const float* __restrict__ rhs, double* partial) {
-    double a = 0;
-    FINE_FOR(g, i, j, k) a += (double)rhs[gidx(g, i, j, k)];
-    block_sum2(a, 0.0, partial);
+// ---- multi-block level kernels ---------------------------------------------------
+template <typename S>
+__global__ void __launch_bounds__(MG_THREADS) k_mg_jacobi(MgLevel L, const S* __restrict__ ein,
+                                                          S* __restrict__ eout, const S* __restrict__ b,
+                                                          const double* __restrict__ bsum) {
+    using C = typename St<S>::C;
+    LEVEL_TILE(L);
+    if (!active) return;
+    const C mb = bsum ? (C)(bsum[0] / L.ncell) : (C)0;
+    column_sweep<S>(L, ein, eout, b, mb, i, j, k0, k1);
 }
 
-// r = (rhs - mean) - A p64 in FP64; r stored in the inner precision at the
-// fine multigrid level; partial sums of r^2 and b^2.
+// Coarse right-hand side = average of the fine residual over each coarse
+// cell; ec (optional) = the first damped sweep from zero at the coarse level.
 template <typename S>
-__global__ void __launch_bounds__(MG_THREADS) k_residual64(Geom g, const float* __restrict__ rhs,
-                                                           const double* __restrict__ meanp,
-                                                           const double* __restrict__ p, S* __restrict__ r_out,
-                                                           double* partial) {
+__global__ void __launch_bounds__(MG_THREADS) k_mg_restrict(MgLevel F, const S* __restrict__ e,
+                                                            const S* __restrict__ b, MgLevel Cl,
+                                                            S* __restrict__ bc, S* __restrict__ ec) {
     using T = St<S>;
-    const double mean = meanp[0] / ((double)g.nx * g.ny * g.nz);
-    const double ax = (double)g.dxi * g.dxi, ay = (double)g.dyi * g.dyi, az = (double)g.dzi * g.dzi;
+    using C = typename T::C;
+    LEVEL_TILE(Cl);
+    if (!active) return;
+    const C inv = (C)(1.0 / (F.rx * F.ry * F.rz));
+    const int nbxy = nb_count(i, Cl.nx) * 9 + nb_count(j, Cl.ny) * 3;
+    for (int K = k0; K < k1; ++K) {
+        C acc = 0;
+        for (int dk = 0; dk < F.rz; ++dk)
+            for (int dj = 0; dj < F.ry; ++dj)
+                for (int di = 0; di < F.rx; ++di)
+                    acc += cell_residual<S>(F, e, b, i * F.rx + di, j * F.ry + dj, K * F.rz + dk);
+        const C v = acc * inv;
+        const int c = (K * Cl.ny + j) * Cl.nx + i;
+        T::st(bc, c, v);
+        if (ec) T::st(ec, c, (C)Cl.wd[nbxy + nb_count(K, Cl.nz)] * T::q(v));
+    }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(MG_THREADS) k_mg_prolong(MgLevel F, S* __restrict__ e, MgLevel Cl,
+                                                           const S* __restrict__ ec) {
+    LEVEL_TILE(F);
+    if (!active) return;
+    for (int k = k0; k < k1; ++k) prolong_cell<S>(F, e, Cl, ec, i, j, k);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(MG_THREADS) k_level_sum(MgLevel L, const S* __restrict__ b,
+                                                          double* __restrict__ partial) {
+    LEVEL_TILE(L);
+    double a = 0, z = 0;
+    if (active)
+        for (int k = k0; k < k1; ++k) a += (double)St<S>::ld(b, (k * L.ny + j) * L.nx + i);
+    block_sum2(a, z);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        partial[2 * block_linear()] = a;
+        partial[2 * block_linear() + 1] = 0.0;
+    }
+}
+
+// ---- fine level, FP64 (padded layout of the step) ----------------------------------
+__global__ void __launch_bounds__(MG_THREADS) k_sum_rhs(Geom g, MgLevel L0, const float* __restrict__ rhs,
+                                                        double* __restrict__ partial) {
+    LEVEL_TILE(L0);
+    double a = 0, z = 0;
+    if (active)
+        for (int k = k0; k < k1; ++k) a += (double)rhs[gidx(g, i + 1, j + 1, k + 1)];
+    block_sum2(a, z);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        partial[2 * block_linear()] = a;
+        partial[2 * block_linear() + 1] = 0.0;
+    }
+}
+
+// r = (rhs - mean) - A p in FP64, stored as the fine right-hand side b0;
+// e0 (optional) = the first damped sweep from zero; partial sums of r^2, b^2.
+template <typename S>
+__global__ void __launch_bounds__(MG_THREADS) k_resid0(Geom g, MgLevel L0, const float* __restrict__ rhs,
+                                                       const double* __restrict__ sums, const double* __restrict__ p,
+                                                       S* __restrict__ b0, S* __restrict__ e0,
+                                                       double* __restrict__ partial) {
+    using T = St<S>;
+    using C = typename T::C;
+    LEVEL_TILE(L0);
     double rr = 0, bb = 0;
-    FINE_FOR(g, i, j, k) {
-        const int id = gidx(g, i, j, k);
-        const double pc = p[id];
-        double s = 0;
-        if (i > 1) s += ax * (p[id - 1] - pc);
-        if (i < g.nx) s += ax * (p[id + 1] - pc);
-        if (j > 1) s += ay * (p[id - g.px] - pc);
-        if (j < g.ny) s += ay * (p[id + g.px] - pc);
-        if (k > 1) s += az * (p[id - g.plane] - pc);
-        if (k < g.nz) s += az * (p[id + g.plane] - pc);
-        const double b = (double)rhs[id] - mean;
-        const double r = b - s;
-        rr += r * r;
-        bb += b * b;
-        T::st(r_out, ((long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1), (typename T::C)r);
+    if (active) {
+        const double mean = sums[0] / (double)L0.ncell;
+        const double ax = L0.ax, ay = L0.ay, az = L0.az;
+        const int nbxy = nb_count(i, L0.nx) * 9 + nb_count(j, L0.ny) * 3;
+        const int cplane = L0.nx * L0.ny;
+        int id = gidx(g, i + 1, j + 1, k0 + 1);
+        int c = (k0 * L0.ny + j) * L0.nx + i;
+        double pm = k0 > 0 ? p[id - g.plane] : 0.0, pc = p[id];
+        for (int k = k0; k < k1; ++k, id += g.plane, c += cplane) {
+            const double pp = k + 1 < L0.nz ? p[id + g.plane] : 0.0;
+            double s = 0;
+            if (i > 0) s += ax * (p[id - 1] - pc);
+            if (i < L0.nx - 1) s += ax * (p[id + 1] - pc);
+            if (j > 0) s += ay * (p[id - g.px] - pc);
+            if (j < L0.ny - 1) s += ay * (p[id + g.px] - pc);
+            if (k > 0) s += az * (pm - pc);
+            if (k < L0.nz - 1) s += az * (pp - pc);
+            const double b = (double)rhs[id] - mean;
+            const double r = b - s;
+            rr += r * r;
+            bb += b * b;
+            T::st(b0, c, (C)r);
+            if (e0) T::st(e0, c, (C)L0.wd[nbxy + nb_count(k, L0.nz)] * T::q((C)r));
+            pm = pc;
+            pc = pp;
+        }
     }
-    block_sum2(rr, bb, partial);
+    block_sum2(rr, bb);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        partial[2 * block_linear()] = rr;
+        partial[2 * block_linear() + 1] = bb;
+    }
 }
 
-// p64 += e (the inner correction, widened to FP64).
+// Last post-smoothing sweep of the fine level fused with p += e.
 template <typename S>
-__global__ void __launch_bounds__(MG_THREADS) k_update64(Geom g, double* __restrict__ p, const S* __restrict__ e) {
+__global__ void __launch_bounds__(MG_THREADS) k_jac_update(Geom g, MgLevel L0, const S* __restrict__ ein,
+                                                           const S* __restrict__ b, double* __restrict__ p) {
     using T = St<S>;
-    FINE_FOR(g, i, j, k) {
-        const int id = gidx(g, i, j, k);
-        p[id] += (double)T::ld(e, ((long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1));
+    using C = typename T::C;
+    LEVEL_TILE(L0);
+    if (!active) return;
+    const int plane = L0.nx * L0.ny;
+    const int nbxy = nb_count(i, L0.nx) * 9 + nb_count(j, L0.ny) * 3;
+    int c = (k0 * L0.ny + j) * L0.nx + i;
+    int id = gidx(g, i + 1, j + 1, k0 + 1);
+    C em = k0 > 0 ? (C)T::ld(ein, c - plane) : (C)0, ec = (C)T::ld(ein, c);
+    for (int k = k0; k < k1; ++k, c += plane, id += g.plane) {
+        const C ep = k + 1 < L0.nz ? (C)T::ld(ein, c + plane) : (C)0;
+        const C Ae = lap_xy<S, C>(L0, ein, c, i, j, ec) + lap_z<C>(L0, k, ec, em, ep);
+        const C en = ec + (C)L0.wd[nbxy + nb_count(k, L0.nz)] * ((C)T::ld(b, c) - Ae);
+        p[id] += (double)T::q(en);
+        em = ec;
+        ec = ep;
     }
 }
 
-// Sum of p64 over the interior (for the gauge).
-__global__ void __launch_bounds__(MG_THREADS) k_sum_p(Geom g, const double* __restrict__ p, double* partial) {
-    double a = 0;
-    FINE_FOR(g, i, j, k) a += p[gidx(g, i, j, k)];
-    block_sum2(a, 0.0, partial);
+// p += e (the fine level solved entirely by the one-block kernel).
+template <typename S>
+__global__ void __launch_bounds__(MG_THREADS) k_update64(Geom g, MgLevel L0, double* __restrict__ p,
+                                                         const S* __restrict__ e) {
+    LEVEL_TILE(L0);
+    if (!active) return;
+    for (int k = k0; k < k1; ++k) p[gidx(g, i + 1, j + 1, k + 1)] += (double)St<S>::ld(e, (k * L0.ny + j) * L0.nx + i);
 }
 
-// p64 -= mean (gauge mean(p) = 0); p32 = float(p64) on the interior.
-__global__ void __launch_bounds__(MG_THREADS) k_gauge_cast(Geom g, double* __restrict__ p,
+__global__ void __launch_bounds__(MG_THREADS) k_sum_p(Geom g, MgLevel L0, const double* __restrict__ p,
+                                                      double* __restrict__ partial) {
+    LEVEL_TILE(L0);
+    double a = 0, z = 0;
+    if (active)
+        for (int k = k0; k < k1; ++k) a += p[gidx(g, i + 1, j + 1, k + 1)];
+    block_sum2(a, z);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        partial[2 * block_linear()] = a;
+        partial[2 * block_linear() + 1] = 0.0;
+    }
+}
+
+// p -= mean(p) (gauge), p32 = float(p) on the interior.
+__global__ void __launch_bounds__(MG_THREADS) k_gauge_cast(Geom g, MgLevel L0, double* __restrict__ p,
                                                            const double* __restrict__ sump, float* __restrict__ p32) {
-    const double mean = sump[0] / ((double)g.nx * g.ny * g.nz);
-    FINE_FOR(g, i, j, k) {
-        const int id = gidx(g, i, j, k);
+    LEVEL_TILE(L0);
+    if (!active) return;
+    const double mean = sump[0] / (double)L0.ncell;
+    for (int k = k0; k < k1; ++k) {
+        const int id = gidx(g, i + 1, j + 1, k + 1);
         const double v = p[id] - mean;
         p[id] = v;
         p32[id] = (float)v;
     }
 }
 
-// p64 = double(p32) on the interior (after an upload of P).
-__global__ void __launch_bounds__(MG_THREADS) k_widen(Geom g, const float* __restrict__ p32, double* __restrict__ p) {
-    FINE_FOR(g, i, j, k) {
-        const int id = gidx(g, i, j, k);
+__global__ void __launch_bounds__(MG_THREADS) k_widen(Geom g, MgLevel L0, const float* __restrict__ p32,
+                                                      double* __restrict__ p) {
+    LEVEL_TILE(L0);
+    if (!active) return;
+    for (int k = k0; k < k1; ++k) {
+        const int id = gidx(g, i + 1, j + 1, k + 1);
         p[id] = (double)p32[id];
     }
+}
+
+// ---- small levels: one block --------------------------------------------------------
+// Levels lv[0 .. nl-1] (the last is the coarsest) of one V-cycle after b of
+// lv[0] has been written to global memory.  Every vector of these levels
+// (and the dense coarse inverse) lives in shared memory for the whole
+// kernel; b of lv[0] is read from global memory at the start and the final
+// correction of lv[0] written back to `out` at the end.
+template <typename S>
+__device__ void tail_sweep(const MgLevel& L, const S* ein, S* eout, const S* b, typename St<S>::C mb) {
+    for (int j = threadIdx.x >> 5; j < L.ny; j += TAIL_THREADS / 32)
+        for (int i = threadIdx.x & 31; i < L.nx; i += 32) column_sweep<S>(L, ein, eout, b, mb, i, j, 0, L.nz);
+    __syncthreads();
+}
+
+template <typename S>
+__device__ void tail_restrict(const MgLevel& F, const S* e, const S* b, S* scratch, const MgLevel& Cl) {
+    using T = St<S>;
+    using C = typename T::C;
+    for (int c = threadIdx.x; c < F.ncell; c += TAIL_THREADS) {
+        const int i = c % F.nx, j = (c / F.nx) % F.ny, k = c / (F.nx * F.ny);
+        T::st(scratch, c, cell_residual<S>(F, e, b, i, j, k));
+    }
+    __syncthreads();
+    const C inv = (C)(1.0 / (F.rx * F.ry * F.rz));
+    S* bc = static_cast<S*>(Cl.b);
+    for (int c = threadIdx.x; c < Cl.ncell; c += TAIL_THREADS) {
+        const int I = c % Cl.nx, J = (c / Cl.nx) % Cl.ny, K = c / (Cl.nx * Cl.ny);
+        C acc = 0;
+        for (int dk = 0; dk < F.rz; ++dk)
+            for (int dj = 0; dj < F.ry; ++dj) {
+                const int row = ((K * F.rz + dk) * F.ny + J * F.ry + dj) * F.nx + I * F.rx;
+                for (int di = 0; di < F.rx; ++di) acc += (C)T::ld(scratch, row + di);
+            }
+        T::st(bc, c, acc * inv);
+    }
+    __syncthreads();
+}
+
+template <typename S>
+__device__ void tail_prolong(const MgLevel& F, S* e, const MgLevel& Cl, const S* ec) {
+    for (int c = threadIdx.x; c < F.ncell; c += TAIL_THREADS) {
+        const int i = c % F.nx, j = (c / F.nx) % F.ny, k = c / (F.nx * F.ny);
+        prolong_cell<S>(F, e, Cl, ec, i, j, k);
+    }
+    __syncthreads();
+}
+
+template <typename S>
+__device__ typename St<S>::C tail_mean(const MgLevel& L, const S* b) {
+    double a = 0, z = 0;
+    for (int c = threadIdx.x; c < L.ncell; c += TAIL_THREADS) a += (double)St<S>::ld(b, c);
+    block_sum2(a, z);
+    return (typename St<S>::C)(a / L.ncell);
+}
+
+// Bytes of shared memory of one tail vector (16-byte multiple).
+__host__ __device__ __forceinline__ int tail_vec_bytes(int ncell, int elem) { return (ncell * elem + 15) & ~15; }
+
+template <typename S>
+__global__ void __launch_bounds__(TAIL_THREADS) k_mg_tail(const MgLevel* lv, int nl,
+                                                          const typename St<S>::C* cinv_g, S* out) {
+    using T = St<S>;
+    using C = typename T::C;
+    extern __shared__ __align__(16) unsigned char tail_smem[];
+    __shared__ MgLevel sl[MG_MAX_LEVELS];
+    __shared__ int pre_cur[MG_MAX_LEVELS];
+    __shared__ int cinv_off;
+    for (int q = threadIdx.x; q < nl * (int)(sizeof(MgLevel) / sizeof(int)); q += TAIL_THREADS)
+        reinterpret_cast<int*>(sl)[q] = reinterpret_cast<const int*>(lv)[q];
+    __syncthreads();
+    const S* b_g = static_cast<const S*>(sl[0].b);
+    __syncthreads();
+    if (threadIdx.x == 0) {  // re-point every vector into shared memory
+        unsigned char* p = tail_smem;
+        for (int l = 0; l < nl; ++l) {
+            const int vb = tail_vec_bytes(sl[l].ncell, (int)sizeof(S));
+            sl[l].e0 = p;
+            sl[l].e1 = p + vb;
+            sl[l].b = p + 2 * vb;
+            p += 3 * vb;
+        }
+        cinv_off = (int)(p - tail_smem);
+    }
+    __syncthreads();
+    const int last = nl - 1;
+    const int nc = sl[last].ncell;
+    C* cinv = cinv_g ? reinterpret_cast<C*>(tail_smem + cinv_off) : nullptr;
+    {
+        S* b0 = static_cast<S*>(sl[0].b);
+        for (int c = threadIdx.x; c < sl[0].ncell; c += TAIL_THREADS) b0[c] = b_g[c];
+        if (cinv)
+            for (int q = threadIdx.x; q < nc * nc; q += TAIL_THREADS) cinv[q] = cinv_g[q];
+    }
+    __syncthreads();
+    for (int l = 0; l < last; ++l) {
+        const MgLevel& L = sl[l];
+        S* e[2] = {static_cast<S*>(L.e0), static_cast<S*>(L.e1)};
+        const S* b = static_cast<const S*>(L.b);
+        tail_sweep<S>(L, nullptr, e[0], b, (C)0);
+        int cur = 0;
+        for (int q = 1; q < L.nu; ++q, cur ^= 1) tail_sweep<S>(L, e[cur], e[cur ^ 1], b, (C)0);
+        tail_restrict<S>(L, e[cur], b, e[cur ^ 1], sl[l + 1]);
+        if (threadIdx.x == 0) pre_cur[l] = cur;
+    }
+    {
+        const MgLevel& L = sl[last];
+        S* e[2] = {static_cast<S*>(L.e0), static_cast<S*>(L.e1)};
+        const S* b = static_cast<const S*>(L.b);
+        const C mb = tail_mean<S>(L, b);
+        if (cinv) {  // e = (A + c 11^T)^-1 (b - mean b); the inverse is symmetric
+            for (int c = threadIdx.x; c < nc; c += TAIL_THREADS) {
+                C acc = 0;
+                for (int q = 0; q < nc; ++q) acc += cinv[q * nc + c] * ((C)T::ld(b, q) - mb);
+                T::st(e[0], c, acc);
+            }
+            __syncthreads();
+        } else {
+            tail_sweep<S>(L, nullptr, e[0], b, mb);
+            for (int q = 1; q < MG_COARSE_SWEEPS; ++q) tail_sweep<S>(L, e[(q - 1) & 1], e[q & 1], b, mb);
+        }
+    }
+    __syncthreads();
+    for (int l = last - 1; l >= 0; --l) {
+        const MgLevel& L = sl[l];
+        const MgLevel& Cl = sl[l + 1];
+        S* e[2] = {static_cast<S*>(L.e0), static_cast<S*>(L.e1)};
+        const S* b = static_cast<const S*>(L.b);
+        const bool coarse_e0 = (l + 1 == last) && (cinv || !((MG_COARSE_SWEEPS - 1) & 1));
+        const S* ec = static_cast<const S*>(coarse_e0 ? Cl.e0 : Cl.e1);
+        int cur = pre_cur[l];
+        tail_prolong<S>(L, e[cur], Cl, ec);
+        for (int q = 0; q < L.nu; ++q, cur ^= 1) tail_sweep<S>(L, e[cur], e[cur ^ 1], b, (C)0);
+    }
+    const bool fin_e0 = (last == 0) && (cinv || !((MG_COARSE_SWEEPS - 1) & 1));
+    const S* fin = static_cast<const S*>(fin_e0 ? sl[0].e0 : sl[0].e1);
+    for (int c = threadIdx.x; c < sl[0].ncell; c += TAIL_THREADS) out[c] = fin[c];
 }
 
 // ---- host -------------------------------------------------------------------
@@ -350,21 +570,41 @@ static int smallest_factor(int n) {
     return 1;
 }
 
+static void tiling(MgLevel& m) {
+    m.gx = (m.nx + MG_BX - 1) / MG_BX;
+    m.gy = (m.ny + MG_BY - 1) / MG_BY;
+    const int want = 4 * 148 * 8;  // about four waves of 256-thread blocks
+    int zc = (want + m.gx * m.gy - 1) / (m.gx * m.gy);
+    zc = zc < 1 ? 1 : (zc > m.nz ? m.nz : zc);
+    m.kc = (m.nz + zc - 1) / zc;
+    m.gz = (m.nz + m.kc - 1) / m.kc;
+}
+
 int mg_plan(const Geom& g, MgLevel* lv, int max_levels) {
     int n[3] = {g.nx, g.ny, g.nz};
-    double h[3] = {(double)g.dx, (double)g.dy, (double)g.dz};
+    // level 0 uses the coefficients of the FP64 outer operator: (double)(1/h)^2
+    double a[3] = {(double)g.dxi * g.dxi, (double)g.dyi * g.dyi, (double)g.dzi * g.dzi};
     int L = 0;
     while (L < max_levels) {
         MgLevel& m = lv[L];
+        m = MgLevel{};
         m.nx = n[0];
         m.ny = n[1];
         m.nz = n[2];
         m.ncell = n[0] * n[1] * n[2];
-        m.ax = 1.0 / (h[0] * h[0]);
-        m.ay = 1.0 / (h[1] * h[1]);
-        m.az = 1.0 / (h[2] * h[2]);
+        m.ax = a[0];
+        m.ay = a[1];
+        m.az = a[2];
+        for (int x = 0; x < 3; ++x)
+            for (int y = 0; y < 3; ++y)
+                for (int z = 0; z < 3; ++z) {
+                    const double d = a[0] * x + a[1] * y + a[2] * z;
+                    m.wd[x * 9 + y * 3 + z] = d > 0 ? -MG_OMEGA / d : 0.0;
+                }
+        m.nu = (n[0] > 25 || n[1] > 25 || n[2] > 25) ? MG_NU_FINE : MG_NU_COARSE;
+        tiling(m);
         int r[3];
-        for (int a = 0; a < 3; ++a) r[a] = (n[a] > 2) ? smallest_factor(n[a]) : 1;
+        for (int x = 0; x < 3; ++x) r[x] = (n[x] > 2) ? smallest_factor(n[x]) : 1;
         const bool last = (r[0] == 1 && r[1] == 1 && r[2] == 1) || (n[0] <= 3 && n[1] <= 3 && n[2] <= 3) ||
                           L == max_levels - 1;
         m.rx = last ? 1 : r[0];
@@ -372,130 +612,322 @@ int mg_plan(const Geom& g, MgLevel* lv, int max_levels) {
         m.rz = last ? 1 : r[2];
         ++L;
         if (last) break;
-        for (int a = 0; a < 3; ++a) {
-            n[a] /= r[a];
-            h[a] *= r[a];
+        for (int x = 0; x < 3; ++x) {
+            n[x] /= r[x];
+            a[x] /= (double)r[x] * r[x];
         }
     }
     return L;
 }
 
-size_t mg_storage_bytes(int mode) { return mode == MG_MIXED ? 2 : 8; }
-
-// Kernel launches of one V-cycle from level l down (for the launch count).
-static int vcycle_launches(const MgSolver& m, int l) {
-    const MgLevel& L = m.lv[l];
-    if (l == m.nlev - 1) {
-        const size_t smem = 3 * (size_t)L.ncell * (m.mode == MG_MIXED ? sizeof(float) : sizeof(double));
-        return smem <= 200 * 1024 ? 1 : MG_COARSE_SWEEPS;
+// Inverse of A + c 11^T (c = -(ax+ay+az)/n, nonsingular) of level L by
+// Gauss-Jordan elimination with partial pivoting, row-major n x n.
+static bool dense_inverse(const MgLevel& L, std::vector<double>& inv) {
+    const int n = L.ncell;
+    std::vector<double> M((size_t)n * n, 0.0);
+    inv.assign((size_t)n * n, 0.0);
+    const double c = -(L.ax + L.ay + L.az) / n;
+    for (int r = 0; r < n; ++r) {
+        for (int q = 0; q < n; ++q) M[(size_t)r * n + q] = c;
+        inv[(size_t)r * n + r] = 1.0;
+        const int i = r % L.nx, j = (r / L.nx) % L.ny, k = r / (L.nx * L.ny);
+        const int has[6] = {i > 0, i < L.nx - 1, j > 0, j < L.ny - 1, k > 0, k < L.nz - 1};
+        const int off[6] = {-1, 1, -L.nx, L.nx, -L.nx * L.ny, L.nx * L.ny};
+        const double coef[6] = {L.ax, L.ax, L.ay, L.ay, L.az, L.az};
+        for (int q = 0; q < 6; ++q)
+            if (has[q]) {
+                M[(size_t)r * n + r + off[q]] += coef[q];
+                M[(size_t)r * n + r] -= coef[q];
+            }
     }
-    const int nu = (L.nx > 25 || L.ny > 25 || L.nz > 25) ? MG_NU_FINE : MG_NU_COARSE;
-    return 2 * nu + 2 + vcycle_launches(m, l + 1);
-}
-
-template <typename S>
-static cudaError_t vcycle(MgSolver& m, int l, cudaStream_t s) {
-    MgLevel& L = m.lv[l];
-    S* b = static_cast<S*>(L.b);
-    S* e[2] = {static_cast<S*>(L.e0), static_cast<S*>(L.e1)};
-    const int blocks = (int)((L.ncell + MG_THREADS - 1) / MG_THREADS) < 148 * 8
-                           ? (int)((L.ncell + MG_THREADS - 1) / MG_THREADS) : 148 * 8;
-    if (l == m.nlev - 1) {
-        const size_t smem = 3 * (size_t)L.ncell * sizeof(typename St<S>::C);
-        if (smem <= 200 * 1024) {
-            k_mg_coarsest<S><<<1, MG_THREADS, smem, s>>>(L, b, e[0], MG_COARSE_SWEEPS, MG_OMEGA);
-            L.cur = 0;
-            return cudaGetLastError();
+    for (int col = 0; col < n; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < n; ++r)
+            if (fabs(M[(size_t)r * n + col]) > fabs(M[(size_t)piv * n + col])) piv = r;
+        if (M[(size_t)piv * n + col] == 0.0) return false;
+        if (piv != col)
+            for (int q = 0; q < n; ++q) {
+                std::swap(M[(size_t)piv * n + q], M[(size_t)col * n + q]);
+                std::swap(inv[(size_t)piv * n + q], inv[(size_t)col * n + q]);
+            }
+        const double d = 1.0 / M[(size_t)col * n + col];
+        for (int q = 0; q < n; ++q) {
+            M[(size_t)col * n + q] *= d;
+            inv[(size_t)col * n + q] *= d;
         }
-        // large coarsest level: plain sweeps
-        k_mg_jacobi<S><<<blocks, MG_THREADS, 0, s>>>(L, nullptr, e[0], b, MG_OMEGA);
-        for (int q = 1; q < MG_COARSE_SWEEPS; ++q)
-            k_mg_jacobi<S><<<blocks, MG_THREADS, 0, s>>>(L, e[(q - 1) & 1], e[q & 1], b, MG_OMEGA);
-        L.cur = (MG_COARSE_SWEEPS - 1) & 1;
-        return cudaGetLastError();
+        for (int r = 0; r < n; ++r) {
+            if (r == col) continue;
+            const double f = M[(size_t)r * n + col];
+            if (f == 0.0) continue;
+            for (int q = 0; q < n; ++q) {
+                M[(size_t)r * n + q] -= f * M[(size_t)col * n + q];
+                inv[(size_t)r * n + q] -= f * inv[(size_t)col * n + q];
+            }
+        }
     }
-    const int wide = L.nx > 25 || L.ny > 25 || L.nz > 25;
-    const int nu = wide ? MG_NU_FINE : MG_NU_COARSE;
-    int cur = 0;
-    k_mg_jacobi<S><<<blocks, MG_THREADS, 0, s>>>(L, nullptr, e[0], b, MG_OMEGA);
-    for (int q = 1; q < nu; ++q) {
-        k_mg_jacobi<S><<<blocks, MG_THREADS, 0, s>>>(L, e[cur], e[cur ^ 1], b, MG_OMEGA);
-        cur ^= 1;
+    return true;
+}
+
+cudaError_t mg_create(const Geom& g, int mode, MgSolver* m, cudaStream_t s, size_t* bytes) {
+    *m = MgSolver{};
+    m->mode = mode;
+    m->nlev = mg_plan(g, m->lv, MG_MAX_LEVELS);
+    cudaError_t e;
+    const size_t vb = mode == MG_MIXED ? sizeof(__nv_bfloat16) : sizeof(double);
+    const size_t cb = mode == MG_MIXED ? sizeof(float) : sizeof(double);
+    const MgLevel& Lc = m->lv[m->nlev - 1];
+    // The tail: the deepest run of levels (at most MG_TAIL_CELLS cells each)
+    // whose vectors and dense coarse inverse fit in MG_TAIL_SMEM bytes.
+    const bool dense_ok = Lc.ncell <= MG_DENSE_MAX;
+    const size_t inv_bytes = dense_ok ? (size_t)Lc.ncell * Lc.ncell * cb : 0;
+    m->tail = m->nlev;
+    m->tail_smem = 0;
+    {
+        size_t acc = inv_bytes;
+        for (int l = m->nlev - 1; l >= 0; --l) {
+            const size_t lb = 3 * (size_t)tail_vec_bytes(m->lv[l].ncell, (int)vb);
+            if (m->lv[l].ncell > MG_TAIL_CELLS || acc + lb > MG_TAIL_SMEM) break;
+            acc += lb;
+            m->tail = l;
+            m->tail_smem = (int)acc;
+        }
     }
-    MgLevel& Cl = m.lv[l + 1];
-    const int cblocks = (int)((Cl.ncell + MG_THREADS - 1) / MG_THREADS) < 148 * 8
-                            ? (int)((Cl.ncell + MG_THREADS - 1) / MG_THREADS) : 148 * 8;
-    k_mg_restrict<S><<<cblocks, MG_THREADS, 0, s>>>(L, e[cur], b, Cl, static_cast<S*>(Cl.b));
-    cudaError_t err = vcycle<S>(m, l + 1, s);
-    if (err != cudaSuccess) return err;
-    S* ec = static_cast<S*>(Cl.cur ? Cl.e1 : Cl.e0);
-    k_mg_prolong<S><<<blocks, MG_THREADS, 0, s>>>(L, e[cur], Cl, ec);
-    for (int q = 0; q < nu; ++q) {
-        k_mg_jacobi<S><<<blocks, MG_THREADS, 0, s>>>(L, e[cur], e[cur ^ 1], b, MG_OMEGA);
-        cur ^= 1;
+    m->dense = (m->tail < m->nlev) && dense_ok;
+    if (m->tail < m->nlev) {
+        e = mode == MG_MIXED ? cudaFuncSetAttribute(k_mg_tail<__nv_bfloat16>,
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, m->tail_smem)
+                             : cudaFuncSetAttribute(k_mg_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    m->tail_smem);
+        if (e != cudaSuccess) return e;
     }
-    L.cur = cur;
+    auto alloc = [&](void** p, size_t nb) -> cudaError_t {
+        cudaError_t r = cudaMalloc(p, nb);
+        if (r != cudaSuccess) {
+            *p = nullptr;
+            return r;
+        }
+        *bytes += nb;
+        return cudaMemsetAsync(*p, 0, nb, s);
+    };
+    int maxblk = 1;
+    for (int l = 0; l < m->nlev; ++l) {
+        MgLevel& L = m->lv[l];
+        const size_t nb = (size_t)L.ncell * vb;
+        if ((e = alloc(&L.e0, nb)) != cudaSuccess || (e = alloc(&L.e1, nb)) != cudaSuccess ||
+            (e = alloc(&L.b, nb)) != cudaSuccess)
+            return e;
+        const int blk = L.gx * L.gy * L.gz;
+        maxblk = blk > maxblk ? blk : maxblk;
+    }
+    m->nblk = m->lv[0].gx * m->lv[0].gy * m->lv[0].gz;
+    if ((e = alloc((void**)&m->d_partial, sizeof(double) * 2 * maxblk)) != cudaSuccess ||
+        (e = alloc((void**)&m->d_result, sizeof(double) * 8)) != cudaSuccess ||
+        (e = alloc((void**)&m->d_lv, sizeof(MgLevel) * m->nlev)) != cudaSuccess)
+        return e;
+    if ((e = cudaHostAlloc((void**)&m->h_result, sizeof(double) * 2, cudaHostAllocMapped)) != cudaSuccess) {
+        m->h_result = nullptr;
+        return e;
+    }
+    if ((e = cudaHostGetDevicePointer((void**)&m->h_result_dev, m->h_result, 0)) != cudaSuccess) return e;
+    if (m->dense) {
+        std::vector<double> inv;
+        if (!dense_inverse(Lc, inv)) return cudaErrorInvalidValue;
+        if ((e = alloc(&m->d_cinv, inv.size() * cb)) != cudaSuccess) return e;
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+        if (mode == MG_MIXED) {
+            std::vector<float> f(inv.begin(), inv.end());
+            e = cudaMemcpy(m->d_cinv, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice);
+        } else {
+            e = cudaMemcpy(m->d_cinv, inv.data(), inv.size() * sizeof(double), cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) return e;
+    }
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    return cudaMemcpy(m->d_lv, m->lv, sizeof(MgLevel) * m->nlev, cudaMemcpyHostToDevice);
+}
+
+void mg_destroy(MgSolver* m) {
+    for (int l = 0; l < m->nlev; ++l) {
+        if (m->lv[l].e0) cudaFree(m->lv[l].e0);
+        if (m->lv[l].e1) cudaFree(m->lv[l].e1);
+        if (m->lv[l].b) cudaFree(m->lv[l].b);
+    }
+    if (m->d_lv) cudaFree(m->d_lv);
+    if (m->d_cinv) cudaFree(m->d_cinv);
+    if (m->d_partial) cudaFree(m->d_partial);
+    if (m->d_result) cudaFree(m->d_result);
+    if (m->h_result) cudaFreeHost(m->h_result);
+    if (m->iter_graph) cudaGraphExecDestroy(m->iter_graph);
+    *m = MgSolver{};
+}
+
+static dim3 grid_of(const MgLevel& L) { return dim3(L.gx, L.gy, L.gz); }
+static const dim3 kBlock(MG_BX, MG_BY, 1);
+
+// Which buffer holds the final correction of level l after a V-cycle: a
+// smoothed level ends on e1 (first sweep into e0, then nu - 1 + nu more);
+// the coarsest on e0 (dense) or after MG_COARSE_SWEEPS sweeps.
+static void* final_buffer(const MgSolver& m, int l) {
+    const MgLevel& L = m.lv[l];
+    if (l == m.nlev - 1) return (m.dense || !((MG_COARSE_SWEEPS - 1) & 1)) ? L.e0 : L.e1;
+    return L.e1;
+}
+
+// A level above the one-block tail that is smoothed by multi-block kernels.
+static bool multi(const MgSolver& m, int l) { return l < m.tail && l < m.nlev - 1; }
+
+template <typename S>
+static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t s, int& launches) {
+    using C = typename St<S>::C;
+    int pre_cur[MG_MAX_LEVELS] = {};
+    int l = 0;
+    for (; multi(m, l); ++l) {
+        const MgLevel& L = m.lv[l];
+        S* e[2] = {static_cast<S*>(L.e0), static_cast<S*>(L.e1)};
+        const S* b = static_cast<const S*>(L.b);
+        int cur = 0;  // the first sweep was written together with b
+        for (int q = 1; q < L.nu; ++q, cur ^= 1, ++launches)
+            k_mg_jacobi<S><<<grid_of(L), kBlock, 0, s>>>(L, e[cur], e[cur ^ 1], b, nullptr);
+        const MgLevel& Cl = m.lv[l + 1];
+        k_mg_restrict<S><<<grid_of(Cl), kBlock, 0, s>>>(L, e[cur], b, Cl, static_cast<S*>(Cl.b),
+                                                        multi(m, l + 1) ? static_cast<S*>(Cl.e0) : nullptr);
+        ++launches;
+        pre_cur[l] = cur;
+    }
+    if (m.tail < m.nlev) {
+        k_mg_tail<S><<<1, TAIL_THREADS, m.tail_smem, s>>>(m.d_lv + m.tail, m.nlev - m.tail,
+                                                           static_cast<const C*>(m.d_cinv),
+                                                           static_cast<S*>(final_buffer(m, m.tail)));
+        ++launches;
+    } else {  // large coarsest level below no tail: mean-free sweeps from zero
+        const MgLevel& L = m.lv[l];
+        S* e[2] = {static_cast<S*>(L.e0), static_cast<S*>(L.e1)};
+        const S* b = static_cast<const S*>(L.b);
+        k_level_sum<S><<<grid_of(L), kBlock, 0, s>>>(L, b, m.d_partial);
+        k_fold2<<<1, MG_THREADS, 0, s>>>(m.d_partial, L.gx * L.gy * L.gz, m.d_result + 6, nullptr);
+        k_mg_jacobi<S><<<grid_of(L), kBlock, 0, s>>>(L, nullptr, e[0], b, m.d_result + 6);
+        launches += 3;
+        for (int q = 1; q < MG_COARSE_SWEEPS; ++q, ++launches)
+            k_mg_jacobi<S><<<grid_of(L), kBlock, 0, s>>>(L, e[(q - 1) & 1], e[q & 1], b, m.d_result + 6);
+    }
+    for (int lc = l - 1; lc >= 0; --lc) {
+        const MgLevel& L = m.lv[lc];
+        const MgLevel& Cl = m.lv[lc + 1];
+        S* e[2] = {static_cast<S*>(L.e0), static_cast<S*>(L.e1)};
+        const S* b = static_cast<const S*>(L.b);
+        int cur = pre_cur[lc];
+        k_mg_prolong<S><<<grid_of(L), kBlock, 0, s>>>(L, e[cur], Cl, static_cast<const S*>(final_buffer(m, lc + 1)));
+        ++launches;
+        for (int q = 0; q < L.nu; ++q, cur ^= 1, ++launches) {
+            if (lc == 0 && q == L.nu - 1)
+                k_jac_update<S><<<grid_of(L), kBlock, 0, s>>>(g, L, e[cur], b, p64);
+            else
+                k_mg_jacobi<S><<<grid_of(L), kBlock, 0, s>>>(L, e[cur], e[cur ^ 1], b, nullptr);
+        }
+    }
+    if (l == 0) {  // the fine level was solved by the tail or as the coarsest level
+        k_update64<S><<<grid_of(m.lv[0]), kBlock, 0, s>>>(g, m.lv[0], p64, static_cast<const S*>(final_buffer(m, 0)));
+        ++launches;
+    }
     return cudaGetLastError();
 }
 
-cudaError_t mg_configure(const MgSolver& m) {
-    const MgLevel& L = m.lv[m.nlev - 1];
-    const size_t smem = 3 * (size_t)L.ncell * (m.mode == MG_MIXED ? sizeof(float) : sizeof(double));
-    if (smem > 200 * 1024) return cudaSuccess;
-    return m.mode == MG_MIXED
-               ? cudaFuncSetAttribute(k_mg_coarsest<__nv_bfloat16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem)
-               : cudaFuncSetAttribute(k_mg_coarsest<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+cudaError_t mg_widen(const Geom& g, const MgSolver& m, const float* p32, double* p64, cudaStream_t s) {
+    k_widen<<<grid_of(m.lv[0]), kBlock, 0, s>>>(g, m.lv[0], p32, p64);
+    return cudaGetLastError();
 }
 
-cudaError_t mg_widen(const Geom& g, const float* p32, double* p64, cudaStream_t s) {
-    k_widen<<<148 * 8, MG_THREADS, 0, s>>>(g, p32, p64);
+// One outer iteration after the first residual: V-cycle with p += e, then the
+// new residual and its norm (also written to the mapped host copy).
+template <typename S>
+static cudaError_t outer_iteration(const Geom& g, MgSolver& m, const float* rhs, double* p64, cudaStream_t s,
+                                   int& launches) {
+    cudaError_t e = vcycle<S>(g, m, p64, s, launches);
+    if (e != cudaSuccess) return e;
+    const MgLevel& L0 = m.lv[0];
+    k_resid0<S><<<grid_of(L0), kBlock, 0, s>>>(g, L0, rhs, m.d_result + 2, p64, static_cast<S*>(L0.b),
+                                               multi(m, 0) ? static_cast<S*>(L0.e0) : nullptr, m.d_partial);
+    k_fold2<<<1, MG_THREADS, 0, s>>>(m.d_partial, m.nblk, m.d_result, m.h_result_dev);
+    launches += 2;
     return cudaGetLastError();
 }
 
 template <typename S>
-static cudaError_t solve_impl(const Geom& g, MgSolver& m, const float* rhs, double* p64, float* p32,
-                              double tol, int max_outer, MgStats* st, cudaStream_t s) {
-    const int nblk = MG_RED_BLOCKS;
+static cudaError_t capture_iteration(const Geom& g, MgSolver& m, const float* rhs, double* p64, float* p32,
+                                     cudaStream_t cap) {
+    if (m.iter_graph) {
+        cudaGraphExecDestroy(m.iter_graph);
+        m.iter_graph = nullptr;
+    }
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    int launches = 0;
+    const cudaError_t e1 = outer_iteration<S>(g, m, rhs, p64, cap, launches);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(cap, &graph);
+    if (e1 != cudaSuccess || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return e1 != cudaSuccess ? e1 : e;
+    }
+    e = cudaGraphInstantiate(&m.iter_graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        m.iter_graph = nullptr;
+        return e;
+    }
+    m.graph_key[0] = rhs;
+    m.graph_key[1] = p64;
+    m.graph_key[2] = p32;
+    m.graph_launches = launches;
+    return cudaSuccess;
+}
+
+template <typename S>
+static cudaError_t solve_impl(const Geom& g, MgSolver& m, const float* rhs, double* p64, float* p32, double tol,
+                              int max_outer, MgStats* st, cudaStream_t s, cudaStream_t cap) {
+    const MgLevel& L0 = m.lv[0];
+    const dim3 grid = grid_of(L0);
     double* part = m.d_partial;
-    double* res = m.d_result;  // [0..1] fold of the residual, [2..3] sum of rhs, [4..5] sum of p
+    double* res = m.d_result;
     cudaError_t e;
-    k_sum_rhs<<<nblk, MG_THREADS, 0, s>>>(g, rhs, part);
-    k_fold2<<<1, MG_THREADS, 0, s>>>(part, nblk, res + 2);
+    if (!m.iter_graph || m.graph_key[0] != rhs || m.graph_key[1] != p64 || m.graph_key[2] != p32)
+        if ((e = capture_iteration<S>(g, m, rhs, p64, p32, cap)) != cudaSuccess) return e;
+    int launches = 0;
+    k_sum_rhs<<<grid, kBlock, 0, s>>>(g, L0, rhs, part);
+    k_fold2<<<1, MG_THREADS, 0, s>>>(part, m.nblk, res + 2, nullptr);
+    k_resid0<S><<<grid, kBlock, 0, s>>>(g, L0, rhs, res + 2, p64, static_cast<S*>(L0.b),
+                                        multi(m, 0) ? static_cast<S*>(L0.e0) : nullptr, part);
+    k_fold2<<<1, MG_THREADS, 0, s>>>(part, m.nblk, res, m.h_result_dev);
+    launches += 4;
     int it = 0;
     double rel = 0, r0 = -1;
     for (;; ++it) {
-        k_residual64<S><<<nblk, MG_THREADS, 0, s>>>(g, rhs, res + 2, p64, static_cast<S*>(m.lv[0].b), part);
-        k_fold2<<<1, MG_THREADS, 0, s>>>(part, nblk, res);
-        if ((e = cudaMemcpyAsync(m.h_result, res, 2 * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-            return e;
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
         const double rr = m.h_result[0], bb = m.h_result[1];
         rel = bb > 0 ? sqrt(rr / bb) : 0.0;
         if (r0 < 0) r0 = rel;
         if (rel <= tol || it >= max_outer) break;
-        if ((e = vcycle<S>(m, 0, s)) != cudaSuccess) return e;
-        const MgLevel& L0 = m.lv[0];
-        k_update64<S><<<148 * 8, MG_THREADS, 0, s>>>(g, p64, static_cast<const S*>(L0.cur ? L0.e1 : L0.e0));
+        if ((e = cudaGraphLaunch(m.iter_graph, s)) != cudaSuccess) return e;
+        launches += m.graph_launches;
     }
-    // gauge: mean(p) = 0, then the FP32 copy for the velocity correction
-    k_sum_p<<<nblk, MG_THREADS, 0, s>>>(g, p64, part);
-    k_fold2<<<1, MG_THREADS, 0, s>>>(part, nblk, res + 4);
-    k_gauge_cast<<<148 * 8, MG_THREADS, 0, s>>>(g, p64, res + 4, p32);
+    k_sum_p<<<grid, kBlock, 0, s>>>(g, L0, p64, part);
+    k_fold2<<<1, MG_THREADS, 0, s>>>(part, m.nblk, res + 4, nullptr);
+    k_gauge_cast<<<grid, kBlock, 0, s>>>(g, L0, p64, res + 4, p32);
+    launches += 3;
     if (st) {
         st->outer = it;
         st->rel_initial = r0;
         st->rel_final = rel;
-        st->launches = 2 + (it + 1) * 2 + it * (vcycle_launches(m, 0) + 1) + 3;
+        st->launches = launches;
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return rel <= tol ? cudaSuccess : cudaErrorNotReady;
 }
 
 cudaError_t mg_solve(const Geom& g, MgSolver& m, const float* rhs, double* p64, float* p32, double tol,
-                     int max_outer, MgStats* st, cudaStream_t s) {
-    if (m.mode == MG_MIXED) return solve_impl<__nv_bfloat16>(g, m, rhs, p64, p32, tol, max_outer, st, s);
-    return solve_impl<double>(g, m, rhs, p64, p32, tol, max_outer, st, s);
+                     int max_outer, MgStats* st, cudaStream_t s, cudaStream_t cap) {
+    if (m.mode == MG_MIXED) return solve_impl<__nv_bfloat16>(g, m, rhs, p64, p32, tol, max_outer, st, s, cap);
+    return solve_impl<double>(g, m, rhs, p64, p32, tol, max_outer, st, s, cap);
 }
 
 }  // namespace vof

@@ -1,6 +1,7 @@
 // mg_solve.h -- convergent pressure solve of the MIXED / FP64 modes (mg_solve.cu).
 #pragma once
 #include <cuda_runtime.h>
+#include <stddef.h>
 
 #include "vof_device.cuh"
 
@@ -10,29 +11,48 @@ enum { MG_MIXED = 1, MG_FP64 = 2 };  // inner precision: BF16 storage + FP32 mat
 constexpr double MG_OMEGA = 6.0 / 7.0;  // damped-Jacobi weight
 constexpr int MG_NU_FINE = 2;           // pre/post sweeps on levels wider than 25 cells
 constexpr int MG_NU_COARSE = 8;         // pre/post sweeps on the small levels
-constexpr int MG_COARSE_SWEEPS = 100;   // sweeps on the coarsest level
+constexpr int MG_COARSE_SWEEPS = 100;   // sweeps on a coarsest level too large for the dense solve
 constexpr int MG_MAX_LEVELS = 16;
+constexpr int MG_TAIL_CELLS = 4096;     // largest level that may run inside the one-block kernel
+constexpr int MG_TAIL_SMEM = 200 * 1024;  // shared-memory budget of the one-block kernel
+constexpr int MG_DENSE_MAX = 128;       // coarsest levels this small are solved exactly
+constexpr int MG_BX = 32, MG_BY = 8;    // block of the multi-block level kernels
 
-// One multigrid level: compact layout (i fastest, no ghosts), spacing via
-// ax = 1/hx^2 ..., ratio (rx, ry, rz) to the next coarser level.
+// One multigrid level: compact layout (i fastest, no ghosts); A e = sum over
+// the non-wall neighbours of a (e_nb - e_c) with a = ax, ay, az; ratio
+// (rx, ry, rz) to the next coarser level; wd[nbx*9 + nby*3 + nbz] = omega /
+// diag(A) for a cell with nbx, nby, nbz non-wall neighbours along x, y, z
+// (0 where the diagonal is 0).
 struct MgLevel {
-    int nx, ny, nz;
-    long ncell;
+    int nx, ny, nz, ncell;
     double ax, ay, az;
+    double wd[27];
     int rx, ry, rz;
-    void* e0;  // correction, ping-pong pair
+    int nu;                  // pre/post smoothing sweeps
+    int gx, gy, gz, kc;      // launch tiling: grid (gx, gy, gz) of MG_BX x MG_BY blocks, kc planes per block
+    void* e0;                // correction, ping-pong pair
     void* e1;
-    void* b;   // right-hand side of this level
-    int cur;   // which of e0/e1 holds the last result (host side)
+    void* b;                 // right-hand side of this level
 };
 
 struct MgSolver {
-    int mode;  // MG_MIXED or MG_FP64
+    int mode;        // MG_MIXED or MG_FP64
     int nlev;
+    int tail;        // first level handled by the one-block kernel (nlev: none)
+    int dense;       // the coarsest level is solved with the stored inverse
+    int tail_smem;   // dynamic shared memory of the one-block kernel
     MgLevel lv[MG_MAX_LEVELS];
-    double* d_partial;  // reduction partials
-    double* d_result;   // 8 doubles
-    double* h_result;   // pinned, 2 doubles
+    MgLevel* d_lv;   // device copy of lv (read by the one-block kernel)
+    void* d_cinv;    // dense inverse of the coarsest operator (C type), or null
+    double* d_partial;  // reduction partials, 2 per block of the largest tiling
+    int nblk;           // blocks of the fine tiling
+    double* d_result;   // [0..1] residual sums, [2..3] sum of rhs, [4..5] sum of p, [6..7] coarse mean
+    double* h_result;   // mapped pinned host copy of the residual sums (2 doubles)
+    double* h_result_dev;  // its device alias
+    // One outer iteration (V-cycle, p += e, new residual) captured once as a graph.
+    cudaGraphExec_t iter_graph;
+    const void* graph_key[3];  // rhs, p64, p32 the graph was captured with
+    int graph_launches;        // kernels in it
 };
 
 struct MgStats {
@@ -42,24 +62,24 @@ struct MgStats {
     int launches;        // kernel launches of the last solve
 };
 
-constexpr int MG_PARTIAL_DOUBLES = 2 * 296;
-
-// Fill the level geometry of the hierarchy for grid g; returns the level count.
+// Level geometry of the hierarchy for grid g (no allocation); returns the level count.
 int mg_plan(const Geom& g, MgLevel* lv, int max_levels);
 
-// Bytes of one stored value for the mode.
-size_t mg_storage_bytes(int mode);
-
-// Shared-memory attribute of the coarsest-level kernel (once per solver).
-cudaError_t mg_configure(const MgSolver& m);
+// Plan and allocate the solver for grid g (zeroed buffers, the dense coarse
+// inverse, the device level table); bytes += device bytes allocated.
+cudaError_t mg_create(const Geom& g, int mode, MgSolver* m, cudaStream_t s, size_t* bytes);
+void mg_destroy(MgSolver* m);
 
 // Solve A p = rhs - mean(rhs) to ||r|| <= tol ||b|| (FP64 defect correction,
-// warm start from p64, gauge mean(p) = 0), then p32 = float(p64).  Waits for
-// the stream at every outer iteration.  cudaErrorNotReady: max_outer reached.
+// warm start from p64, gauge mean(p) = 0), then p32 = float(p64).  Each outer
+// iteration is one launch of a CUDA graph (captured on `cap`, a stream of the
+// same device that is not the legacy default stream, at the first call);
+// waits for stream s at every outer iteration.  cudaErrorNotReady: max_outer
+// reached.
 cudaError_t mg_solve(const Geom& g, MgSolver& m, const float* rhs, double* p64, float* p32, double tol,
-                     int max_outer, MgStats* st, cudaStream_t s);
+                     int max_outer, MgStats* st, cudaStream_t s, cudaStream_t cap);
 
 // p64 = double(p32) on the interior (after the pressure field is uploaded).
-cudaError_t mg_widen(const Geom& g, const float* p32, double* p64, cudaStream_t s);
+cudaError_t mg_widen(const Geom& g, const MgSolver& m, const float* p32, double* p64, cudaStream_t s);
 
 }  // namespace vof

@@ -64,6 +64,37 @@ def test_random_state_odd_factor_grids(cuda, V, orc, shape):
         assert rel_l2(got[k], ref[k]) <= 1e-4, (k, rel_l2(got[k], ref[k]))
 
 
+@pytest.mark.parametrize("mode", ["MODE_MIXED", "MODE_FP64"])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (60, 48, 40)])
+def test_multi_block_levels_vs_fp64_oracle(cuda, V, orc, mode, shape):
+    """Grids whose fine levels are smoothed by the multi-block kernels, with
+    the fused residual / first sweep and last sweep / update kernels."""
+    prm = V.default_params(*shape, dt=2e-4, mode=getattr(V, mode), tol=1e-8, max_outer=100)
+    state = ic.random_state(prm, seed=3, vel_scale=0.5)
+    got, stats = run_mode(V, prm, state, 1, 3)
+    assert all(s["rel_final"] <= 1e-8 for s in stats), stats
+    assert all(s["outer"] <= 25 for s in stats), stats
+    ref = orc.run_conv_f64(prm, state, 1, 3, tol=1e-12)
+    assert rel_l2(got["F"], ref["F"]) <= 1e-5
+    for k in ("u", "v", "w"):
+        assert rel_l2(got[k], ref[k]) <= 1e-4, (k, rel_l2(got[k], ref[k]))
+    assert rel_l2(got["p"], ref["p"], interior=True) <= 1e-5
+
+
+def test_large_prime_grid_without_coarsening(cuda, V, orc):
+    """37^3 has no factor to coarsen by and is too large for the one-block
+    kernel: the level is smoothed by mean-free damped sweeps only (slow but
+    convergent)."""
+    prm = V.default_params(37, 37, 37, dt=2e-4, mode=V.MODE_MIXED, tol=1e-6, max_outer=400)
+    state = ic.random_state(prm, seed=8, vel_scale=0.5)
+    got, stats = run_mode(V, prm, state, 1, 1)
+    assert stats[0]["rel_final"] <= 1e-6, stats
+    ref = orc.run_conv_f64(prm, state, 1, 1, tol=1e-12)
+    assert rel_l2(got["F"], ref["F"]) <= 1e-5
+    for k in ("u", "v", "w"):
+        assert rel_l2(got[k], ref[k]) <= 1e-3, (k, rel_l2(got[k], ref[k]))
+
+
 def test_mixed_and_fp64_modes_agree(cuda, V):
     prm_m = V.default_params(24, 24, 24, dt=1e-4, mode=V.MODE_MIXED, tol=1e-10, max_outer=80)
     prm_d = V.default_params(24, 24, 24, dt=1e-4, mode=V.MODE_FP64, tol=1e-10, max_outer=80)
