@@ -11,16 +11,17 @@
 // in the inner precision and p += e in FP64.  The inner solve:
 //   MIXED: every multigrid vector stored in BF16, arithmetic in FP32;
 //   FP64:  the same cycle with FP64 storage and arithmetic (the yardstick).
-// V-cycle: damped Jacobi (omega = 6/7, the Jacobi update of the reference's
-// sweep with damping) as the smoother, 2 pre + 2 post sweeps on levels wider
-// than 25 cells and 8 + 8 on smaller ones, averaging restriction, cell-centred
+// V-cycle: Chebyshev-accelerated Jacobi (the Jacobi update of the reference's
+// sweep inside the Chebyshev three-term recurrence) as the smoother, degree 3
+// before and after on levels wider than 25 cells (eigenvalues of D^-1 A in
+// [1/3, 2]) and degree 8 on smaller ones ([1/15, 2]), averaging restriction, cell-centred
 // multilinear prolongation with zero-gradient ends, coarse operators
 // rediscretised at the coarse spacing.  Each axis is coarsened by its
 // smallest prime factor (2, 3, 5, 7) while at least two cells remain
 // (200 -> 100 -> 50 -> 25 -> 5).  The coarsest level is solved exactly with
 // a stored inverse of A + c 11^T (mean-free right-hand side) when it has at
-// most MG_DENSE_MAX cells, otherwise by 100 damped sweeps after removing the
-// mean of its right-hand side.
+// most MG_DENSE_MAX cells, otherwise by 100 damped Jacobi sweeps (omega =
+// 6/7) after removing the mean of its right-hand side.
 //
 // Execution: the large levels run as multi-block kernels (blocks of 32 x 8
 // columns marching kc planes, the z neighbours kept in registers); the first
@@ -86,12 +87,14 @@ __device__ __forceinline__ C lap_z(const MgLevel& L, int k, C ec, C em, C ep) {
     return s;
 }
 
-// Damped Jacobi on column (i, j), planes [k0, k1): eout = ein + wd (b - mb - A ein);
-// ein == nullptr means ein = 0.
+// One smoothing step on column (i, j), planes [k0, k1):
+//   eout = ein + alpha (ein - xprev) + beta D^-1 (b - mb - A ein),
+// xprev = the value eout holds on entry (read_prev) or 0; ein == nullptr
+// means ein = 0.
 template <typename S>
 __device__ __forceinline__ void column_sweep(const MgLevel& L, const S* __restrict__ ein, S* __restrict__ eout,
-                                             const S* __restrict__ b, typename St<S>::C mb, int i, int j, int k0,
-                                             int k1) {
+                                             const S* __restrict__ b, typename St<S>::C mb, typename St<S>::C alpha,
+                                             typename St<S>::C beta, bool read_prev, int i, int j, int k0, int k1) {
     using T = St<S>;
     using C = typename T::C;
     const int plane = L.nx * L.ny;
@@ -108,7 +111,8 @@ __device__ __forceinline__ void column_sweep(const MgLevel& L, const S* __restri
             ep = k + 1 < L.nz ? (C)T::ld(ein, c + plane) : (C)0;
             Ae = lap_xy<S, C>(L, ein, c, i, j, ec) + lap_z<C>(L, k, ec, em, ep);
         }
-        T::st(eout, c, ec + (C)L.wd[nbxy + nb_count(k, L.nz)] * ((C)T::ld(b, c) - mb - Ae));
+        const C xp = read_prev ? (C)T::ld(eout, c) : (C)0;
+        T::st(eout, c, ec + alpha * (ec - xp) + beta * (C)L.idg[nbxy + nb_count(k, L.nz)] * ((C)T::ld(b, c) - mb - Ae));
         em = ec;
         ec = ep;
     }
@@ -240,18 +244,19 @@ __global__ void __launch_bounds__(MG_THREADS) k_fold2(const double* __restrict__
 
 // ---- multi-block level kernels ---------------------------------------------------
 template <typename S>
-__global__ void __launch_bounds__(MG_THREADS) k_mg_jacobi(MgLevel L, const S* __restrict__ ein,
+__global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(MgLevel L, const S* __restrict__ ein,
                                                           S* __restrict__ eout, const S* __restrict__ b,
-                                                          const double* __restrict__ bsum) {
+                                                          const double* __restrict__ bsum, double alpha, double beta,
+                                                          int read_prev) {
     using C = typename St<S>::C;
     LEVEL_TILE(L);
     if (!active) return;
     const C mb = bsum ? (C)(bsum[0] / L.ncell) : (C)0;
-    column_sweep<S>(L, ein, eout, b, mb, i, j, k0, k1);
+    column_sweep<S>(L, ein, eout, b, mb, (C)alpha, (C)beta, read_prev != 0, i, j, k0, k1);
 }
 
 // Coarse right-hand side = average of the fine residual over each coarse
-// cell; ec (optional) = the first damped sweep from zero at the coarse level.
+// cell; ec (optional) = the first smoothing step from zero at the coarse level.
 template <typename S>
 __global__ void __launch_bounds__(MG_THREADS) k_mg_restrict(MgLevel F, const S* __restrict__ e,
                                                             const S* __restrict__ b, MgLevel Cl,
@@ -271,7 +276,39 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_restrict(MgLevel F, const S* 
         const C v = acc * inv;
         const int c = (K * Cl.ny + j) * Cl.nx + i;
         T::st(bc, c, v);
-        if (ec) T::st(ec, c, (C)Cl.wd[nbxy + nb_count(K, Cl.nz)] * T::q(v));
+        if (ec) T::st(ec, c, (C)Cl.cb[0] * (C)Cl.idg[nbxy + nb_count(K, Cl.nz)] * T::q(v));
+    }
+}
+
+// The same for coarsening ratios above 8 cells per coarse cell (3, 5, 7 along
+// an axis): one block of RW_THREADS per coarse cell sums its fine residuals.
+constexpr int RW_THREADS = 128;
+template <typename S>
+__global__ void __launch_bounds__(RW_THREADS) k_mg_restrict_wide(MgLevel F, const S* __restrict__ e,
+                                                                 const S* __restrict__ b, MgLevel Cl,
+                                                                 S* __restrict__ bc, S* __restrict__ ec) {
+    using T = St<S>;
+    using C = typename T::C;
+    __shared__ C part[RW_THREADS / 32];
+    const int c = blockIdx.x;
+    const int I = c % Cl.nx, J = (c / Cl.nx) % Cl.ny, K = c / (Cl.nx * Cl.ny);
+    const int nf = F.rx * F.ry * F.rz;
+    C acc = 0;
+    for (int t = threadIdx.x; t < nf; t += RW_THREADS) {
+        const int di = t % F.rx, dj = (t / F.rx) % F.ry, dk = t / (F.rx * F.ry);
+        acc += cell_residual<S>(F, e, b, I * F.rx + di, J * F.ry + dj, K * F.rz + dk);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        C sum = 0;
+        for (int q = 0; q < RW_THREADS / 32; ++q) sum += part[q];
+        const C v = sum * (C)(1.0 / nf);
+        T::st(bc, c, v);
+        if (ec)
+            T::st(ec, c, (C)Cl.cb[0] * (C)Cl.idg[nb_count(I, Cl.nx) * 9 + nb_count(J, Cl.ny) * 3 + nb_count(K, Cl.nz)] *
+                             T::q(v));
     }
 }
 
@@ -312,7 +349,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_sum_rhs(Geom g, MgLevel L0, cons
 }
 
 // r = (rhs - mean) - A p in FP64, stored as the fine right-hand side b0;
-// e0 (optional) = the first damped sweep from zero; partial sums of r^2, b^2.
+// e0 (optional) = the first smoothing step from zero; partial sums of r^2, b^2.
 template <typename S>
 __global__ void __launch_bounds__(MG_THREADS) k_resid0(Geom g, MgLevel L0, const float* __restrict__ rhs,
                                                        const double* __restrict__ sums, const double* __restrict__ p,
@@ -344,7 +381,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_resid0(Geom g, MgLevel L0, const
             rr += r * r;
             bb += b * b;
             T::st(b0, c, (C)r);
-            if (e0) T::st(e0, c, (C)L0.wd[nbxy + nb_count(k, L0.nz)] * T::q((C)r));
+            if (e0) T::st(e0, c, (C)L0.cb[0] * (C)L0.idg[nbxy + nb_count(k, L0.nz)] * T::q((C)r));
             pm = pc;
             pc = pp;
         }
@@ -356,10 +393,13 @@ __global__ void __launch_bounds__(MG_THREADS) k_resid0(Geom g, MgLevel L0, const
     }
 }
 
-// Last post-smoothing sweep of the fine level fused with p += e.
+// Last post-smoothing step of the fine level fused with p += e (xprev read
+// from `prev` when read_prev).
 template <typename S>
-__global__ void __launch_bounds__(MG_THREADS) k_jac_update(Geom g, MgLevel L0, const S* __restrict__ ein,
-                                                           const S* __restrict__ b, double* __restrict__ p) {
+__global__ void __launch_bounds__(MG_THREADS) k_smooth_update(Geom g, MgLevel L0, const S* __restrict__ ein,
+                                                              const S* __restrict__ prev, const S* __restrict__ b,
+                                                              double* __restrict__ p, double alpha, double beta,
+                                                              int read_prev) {
     using T = St<S>;
     using C = typename T::C;
     LEVEL_TILE(L0);
@@ -372,7 +412,8 @@ __global__ void __launch_bounds__(MG_THREADS) k_jac_update(Geom g, MgLevel L0, c
     for (int k = k0; k < k1; ++k, c += plane, id += g.plane) {
         const C ep = k + 1 < L0.nz ? (C)T::ld(ein, c + plane) : (C)0;
         const C Ae = lap_xy<S, C>(L0, ein, c, i, j, ec) + lap_z<C>(L0, k, ec, em, ep);
-        const C en = ec + (C)L0.wd[nbxy + nb_count(k, L0.nz)] * ((C)T::ld(b, c) - Ae);
+        const C xp = read_prev ? (C)T::ld(prev, c) : (C)0;
+        const C en = ec + (C)alpha * (ec - xp) + (C)beta * (C)L0.idg[nbxy + nb_count(k, L0.nz)] * ((C)T::ld(b, c) - Ae);
         p[id] += (double)T::q(en);
         em = ec;
         ec = ep;
@@ -432,9 +473,11 @@ __global__ void __launch_bounds__(MG_THREADS) k_widen(Geom g, MgLevel L0, const 
 // kernel; b of lv[0] is read from global memory at the start and the final
 // correction of lv[0] written back to `out` at the end.
 template <typename S>
-__device__ void tail_sweep(const MgLevel& L, const S* ein, S* eout, const S* b, typename St<S>::C mb) {
+__device__ void tail_sweep(const MgLevel& L, const S* ein, S* eout, const S* b, typename St<S>::C mb,
+                           typename St<S>::C alpha, typename St<S>::C beta, bool read_prev) {
     for (int j = threadIdx.x >> 5; j < L.ny; j += TAIL_THREADS / 32)
-        for (int i = threadIdx.x & 31; i < L.nx; i += 32) column_sweep<S>(L, ein, eout, b, mb, i, j, 0, L.nz);
+        for (int i = threadIdx.x & 31; i < L.nx; i += 32)
+            column_sweep<S>(L, ein, eout, b, mb, alpha, beta, read_prev, i, j, 0, L.nz);
     __syncthreads();
 }
 
@@ -522,9 +565,10 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_mg_tail(const MgLevel* lv, int
         const MgLevel& L = sl[l];
         S* e[2] = {static_cast<S*>(L.e0), static_cast<S*>(L.e1)};
         const S* b = static_cast<const S*>(L.b);
-        tail_sweep<S>(L, nullptr, e[0], b, (C)0);
+        tail_sweep<S>(L, nullptr, e[0], b, (C)0, (C)0, (C)L.cb[0], false);
         int cur = 0;
-        for (int q = 1; q < L.nu; ++q, cur ^= 1) tail_sweep<S>(L, e[cur], e[cur ^ 1], b, (C)0);
+        for (int q = 1; q < L.nu; ++q, cur ^= 1)
+            tail_sweep<S>(L, e[cur], e[cur ^ 1], b, (C)0, (C)L.ca[q], (C)L.cb[q], q >= 2);
         tail_restrict<S>(L, e[cur], b, e[cur ^ 1], sl[l + 1]);
         if (threadIdx.x == 0) pre_cur[l] = cur;
     }
@@ -541,8 +585,9 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_mg_tail(const MgLevel* lv, int
             }
             __syncthreads();
         } else {
-            tail_sweep<S>(L, nullptr, e[0], b, mb);
-            for (int q = 1; q < MG_COARSE_SWEEPS; ++q) tail_sweep<S>(L, e[(q - 1) & 1], e[q & 1], b, mb);
+            tail_sweep<S>(L, nullptr, e[0], b, mb, (C)0, (C)MG_OMEGA, false);
+            for (int q = 1; q < MG_COARSE_SWEEPS; ++q)
+                tail_sweep<S>(L, e[(q - 1) & 1], e[q & 1], b, mb, (C)0, (C)MG_OMEGA, false);
         }
     }
     __syncthreads();
@@ -555,7 +600,8 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_mg_tail(const MgLevel* lv, int
         const S* ec = static_cast<const S*>(coarse_e0 ? Cl.e0 : Cl.e1);
         int cur = pre_cur[l];
         tail_prolong<S>(L, e[cur], Cl, ec);
-        for (int q = 0; q < L.nu; ++q, cur ^= 1) tail_sweep<S>(L, e[cur], e[cur ^ 1], b, (C)0);
+        for (int q = 0; q < L.nu; ++q, cur ^= 1)
+            tail_sweep<S>(L, e[cur], e[cur ^ 1], b, (C)0, (C)L.ca[q], (C)L.cb[q], q >= 1);
     }
     const bool fin_e0 = (last == 0) && (cinv || !((MG_COARSE_SWEEPS - 1) & 1));
     const S* fin = static_cast<const S*>(fin_e0 ? sl[0].e0 : sl[0].e1);
@@ -580,6 +626,21 @@ static void tiling(MgLevel& m) {
     m.gz = (m.nz + m.kc - 1) / m.kc;
 }
 
+// Coefficients of the Chebyshev smoother of degree nu on [lo, hi] in the
+// two-term form x_{q+1} = x_q + ca[q] (x_q - x_{q-1}) + cb[q] D^-1 r_q.
+static void chebyshev(int nu, double lo, double hi, double* ca, double* cb) {
+    const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    ca[0] = 0.0;
+    cb[0] = 1.0 / theta;
+    for (int q = 1; q < nu; ++q) {
+        const double rn = 1.0 / (2.0 * sigma - rho);
+        ca[q] = rn * rho;
+        cb[q] = 2.0 * rn / delta;
+        rho = rn;
+    }
+}
+
 int mg_plan(const Geom& g, MgLevel* lv, int max_levels) {
     int n[3] = {g.nx, g.ny, g.nz};
     // level 0 uses the coefficients of the FP64 outer operator: (double)(1/h)^2
@@ -599,9 +660,11 @@ int mg_plan(const Geom& g, MgLevel* lv, int max_levels) {
             for (int y = 0; y < 3; ++y)
                 for (int z = 0; z < 3; ++z) {
                     const double d = a[0] * x + a[1] * y + a[2] * z;
-                    m.wd[x * 9 + y * 3 + z] = d > 0 ? -MG_OMEGA / d : 0.0;
+                    m.idg[x * 9 + y * 3 + z] = d > 0 ? -1.0 / d : 0.0;
                 }
-        m.nu = (n[0] > 25 || n[1] > 25 || n[2] > 25) ? MG_NU_FINE : MG_NU_COARSE;
+        const bool wide = n[0] > 25 || n[1] > 25 || n[2] > 25;
+        m.nu = wide ? MG_NU_FINE : MG_NU_COARSE;
+        chebyshev(m.nu, MG_CHEB_HI / (wide ? MG_RATIO_FINE : MG_RATIO_COARSE), MG_CHEB_HI, m.ca, m.cb);
         tiling(m);
         int r[3];
         for (int x = 0; x < 3; ++x) r[x] = (n[x] > 2) ? smallest_factor(n[x]) : 1;
@@ -765,7 +828,7 @@ static dim3 grid_of(const MgLevel& L) { return dim3(L.gx, L.gy, L.gz); }
 static const dim3 kBlock(MG_BX, MG_BY, 1);
 
 // Which buffer holds the final correction of level l after a V-cycle: a
-// smoothed level ends on e1 (first sweep into e0, then nu - 1 + nu more);
+// smoothed level ends on e1 (first step into e0, then nu - 1 + nu more);
 // the coarsest on e0 (dense) or after MG_COARSE_SWEEPS sweeps.
 static void* final_buffer(const MgSolver& m, int l) {
     const MgLevel& L = m.lv[l];
@@ -785,12 +848,15 @@ static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t 
         const MgLevel& L = m.lv[l];
         S* e[2] = {static_cast<S*>(L.e0), static_cast<S*>(L.e1)};
         const S* b = static_cast<const S*>(L.b);
-        int cur = 0;  // the first sweep was written together with b
+        int cur = 0;  // the first step (from zero) was written together with b
         for (int q = 1; q < L.nu; ++q, cur ^= 1, ++launches)
-            k_mg_jacobi<S><<<grid_of(L), kBlock, 0, s>>>(L, e[cur], e[cur ^ 1], b, nullptr);
+            k_mg_smooth<S><<<grid_of(L), kBlock, 0, s>>>(L, e[cur], e[cur ^ 1], b, nullptr, L.ca[q], L.cb[q], q >= 2);
         const MgLevel& Cl = m.lv[l + 1];
-        k_mg_restrict<S><<<grid_of(Cl), kBlock, 0, s>>>(L, e[cur], b, Cl, static_cast<S*>(Cl.b),
-                                                        multi(m, l + 1) ? static_cast<S*>(Cl.e0) : nullptr);
+        S* ec = multi(m, l + 1) ? static_cast<S*>(Cl.e0) : nullptr;
+        if (L.rx * L.ry * L.rz > 8)
+            k_mg_restrict_wide<S><<<Cl.ncell, RW_THREADS, 0, s>>>(L, e[cur], b, Cl, static_cast<S*>(Cl.b), ec);
+        else
+            k_mg_restrict<S><<<grid_of(Cl), kBlock, 0, s>>>(L, e[cur], b, Cl, static_cast<S*>(Cl.b), ec);
         ++launches;
         pre_cur[l] = cur;
     }
@@ -805,10 +871,11 @@ static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t 
         const S* b = static_cast<const S*>(L.b);
         k_level_sum<S><<<grid_of(L), kBlock, 0, s>>>(L, b, m.d_partial);
         k_fold2<<<1, MG_THREADS, 0, s>>>(m.d_partial, L.gx * L.gy * L.gz, m.d_result + 6, nullptr);
-        k_mg_jacobi<S><<<grid_of(L), kBlock, 0, s>>>(L, nullptr, e[0], b, m.d_result + 6);
+        k_mg_smooth<S><<<grid_of(L), kBlock, 0, s>>>(L, nullptr, e[0], b, m.d_result + 6, 0.0, MG_OMEGA, 0);
         launches += 3;
         for (int q = 1; q < MG_COARSE_SWEEPS; ++q, ++launches)
-            k_mg_jacobi<S><<<grid_of(L), kBlock, 0, s>>>(L, e[(q - 1) & 1], e[q & 1], b, m.d_result + 6);
+            k_mg_smooth<S><<<grid_of(L), kBlock, 0, s>>>(L, e[(q - 1) & 1], e[q & 1], b, m.d_result + 6, 0.0,
+                                                         MG_OMEGA, 0);
     }
     for (int lc = l - 1; lc >= 0; --lc) {
         const MgLevel& L = m.lv[lc];
@@ -820,9 +887,11 @@ static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t 
         ++launches;
         for (int q = 0; q < L.nu; ++q, cur ^= 1, ++launches) {
             if (lc == 0 && q == L.nu - 1)
-                k_jac_update<S><<<grid_of(L), kBlock, 0, s>>>(g, L, e[cur], b, p64);
+                k_smooth_update<S><<<grid_of(L), kBlock, 0, s>>>(g, L, e[cur], e[cur ^ 1], b, p64, L.ca[q], L.cb[q],
+                                                                 q >= 1);
             else
-                k_mg_jacobi<S><<<grid_of(L), kBlock, 0, s>>>(L, e[cur], e[cur ^ 1], b, nullptr);
+                k_mg_smooth<S><<<grid_of(L), kBlock, 0, s>>>(L, e[cur], e[cur ^ 1], b, nullptr, L.ca[q], L.cb[q],
+                                                             q >= 1);
         }
     }
     if (l == 0) {  // the fine level was solved by the tail or as the coarsest level

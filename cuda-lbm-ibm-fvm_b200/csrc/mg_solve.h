@@ -8,9 +8,15 @@
 namespace vof {
 
 enum { MG_MIXED = 1, MG_FP64 = 2 };  // inner precision: BF16 storage + FP32 math, or FP64
-constexpr double MG_OMEGA = 6.0 / 7.0;  // damped-Jacobi weight
-constexpr int MG_NU_FINE = 2;           // pre/post sweeps on levels wider than 25 cells
-constexpr int MG_NU_COARSE = 8;         // pre/post sweeps on the small levels
+constexpr double MG_OMEGA = 6.0 / 7.0;  // damped-Jacobi weight (coarsest level without the dense solve)
+// Smoother: Chebyshev-accelerated Jacobi of degree nu on the eigenvalues of
+// D^-1 A in [MG_CHEB_HI / ratio, MG_CHEB_HI] (D^-1 A has its spectrum in [0, 2]).
+constexpr double MG_CHEB_HI = 2.0;
+constexpr int MG_NU_FINE = 3;           // pre/post degree on levels wider than 25 cells
+constexpr double MG_RATIO_FINE = 6.0;   // eigenvalue ratio they damp (the 2x-coarsening high modes)
+constexpr int MG_NU_COARSE = 8;         // pre/post degree on the small levels
+constexpr double MG_RATIO_COARSE = 30.0;  // wider: these levels may coarsen by 3, 5 or 7
+constexpr int MG_MAX_NU = 8;
 constexpr int MG_COARSE_SWEEPS = 100;   // sweeps on a coarsest level too large for the dense solve
 constexpr int MG_MAX_LEVELS = 16;
 constexpr int MG_TAIL_CELLS = 4096;     // largest level that may run inside the one-block kernel
@@ -20,15 +26,17 @@ constexpr int MG_BX = 32, MG_BY = 8;    // block of the multi-block level kernel
 
 // One multigrid level: compact layout (i fastest, no ghosts); A e = sum over
 // the non-wall neighbours of a (e_nb - e_c) with a = ax, ay, az; ratio
-// (rx, ry, rz) to the next coarser level; wd[nbx*9 + nby*3 + nbz] = omega /
-// diag(A) for a cell with nbx, nby, nbz non-wall neighbours along x, y, z
-// (0 where the diagonal is 0).
+// (rx, ry, rz) to the next coarser level; idg[nbx*9 + nby*3 + nbz] =
+// 1 / diag(A) for a cell with nbx, nby, nbz non-wall neighbours along x, y, z
+// (0 where the diagonal is 0).  Smoothing step q (x_0 the start):
+//   x_{q+1} = x_q + ca[q] (x_q - x_{q-1}) + cb[q] D^-1 (b - A x_q).
 struct MgLevel {
     int nx, ny, nz, ncell;
     double ax, ay, az;
-    double wd[27];
+    double idg[27];
+    double ca[MG_MAX_NU], cb[MG_MAX_NU];
     int rx, ry, rz;
-    int nu;                  // pre/post smoothing sweeps
+    int nu;                  // pre/post smoothing degree
     int gx, gy, gz, kc;      // launch tiling: grid (gx, gy, gz) of MG_BX x MG_BY blocks, kc planes per block
     void* e0;                // correction, ping-pong pair
     void* e1;
