@@ -5,6 +5,9 @@ Imported by tests/, __graft_entry__.smoke() and bench.py (CPU-baseline leg and
 
   * ``run_f32`` / ``run_f64``: the CPU restatement of the reference step
     (vof_oracle.cpp), FP32 without FMA contraction, or FP64.
+  * ``run_conv_f64``: FP64 steps with the pressure solved to a tolerance (CG).
+  * ``adjoint`` / ``SwitchTape``: the host adjoint of the step (vof_adjoint.cpp)
+    and the switch-frozen forward that checks it by finite differences.
   * ``ref_run`` / ``ref_time``: the reference's own kernels (voftrial1.cu
     compiled with ref_harness.cu into oracle/_ref/); GPU only.
 """
@@ -64,6 +67,23 @@ def oracle_lib():
         lib.oracle_run_conv_f64.restype = C.c_int
         lib.oracle_run_conv_f64.argtypes = [C.POINTER(Params)] + [C.POINTER(C.c_double)] * 5 + \
             [C.c_int, C.c_int, C.c_double, C.c_int]
+        D = C.POINTER(C.c_double)
+        for name, T in (("oracle_adjoint_f32", C.c_float), ("oracle_adjoint_f64", C.c_double)):
+            fn = getattr(lib, name)
+            fn.restype = C.c_int
+            fn.argtypes = [C.POINTER(Params)] + [C.POINTER(T)] * 5 + [C.c_int, C.c_int, D] + [D] * 7 + [C.c_int]
+        lib.oracle_tangent_f64.restype = C.c_int
+        lib.oracle_tangent_f64.argtypes = [C.POINTER(Params)] + [D] * 11 + [C.c_int, C.c_int, D, D, D, C.c_int]
+        lib.oracle_tape_new.restype = C.c_void_p
+        lib.oracle_tape_new.argtypes = []
+        lib.oracle_tape_free.restype = None
+        lib.oracle_tape_free.argtypes = [C.c_void_p]
+        lib.oracle_tape_size.restype = C.c_longlong
+        lib.oracle_tape_size.argtypes = [C.c_void_p]
+        for name, T in (("oracle_tape_run_f32", C.c_float), ("oracle_tape_run_f64", C.c_double)):
+            fn = getattr(lib, name)
+            fn.restype = C.c_int
+            fn.argtypes = [C.c_void_p, C.c_int, C.POINTER(Params)] + [C.POINTER(T)] * 5 + [C.c_int, C.c_int, D, D]
         lib.oracle_clamp01f.restype = C.c_float
         lib.oracle_clamp01f.argtypes = [C.c_float]
         lib.oracle_clamp01d.restype = C.c_double
@@ -106,6 +126,96 @@ def run_conv_f64(prm, state, istep0: int, nsteps: int, tol: float = 1e-12, nthre
     if rc != 0:
         raise RuntimeError(f"oracle conv run failed: {rc}")
     return st
+
+
+def _box(box):
+    b = np.asarray(box if box is not None else (-1e300, 1e300) * 3, dtype=np.float64)
+    assert b.shape == (6,)
+    return b
+
+
+def adjoint(prm, state, istep0: int, nsteps: int, box, precision: str = "f32", nthreads: int = 0) -> dict:
+    """Host adjoint of L = sum over `box` (x0, x1, y0, y1, z0, z1; strict bounds
+    on cell centres) of F dV after nsteps steps: dL/d(F, u, v, w, p) of the
+    initial state (float64, reference layout) as "lF", "lu", ..., dL/dg as
+    "grad_g" and the loss as "loss".  The forward runs in FP32 ("f32", the
+    CUDA plain path's arithmetic) or FP64 ("f64")."""
+    T, dt = (C.c_float, np.float32) if precision == "f32" else (C.c_double, np.float64)
+    fn = oracle_lib().oracle_adjoint_f32 if precision == "f32" else oracle_lib().oracle_adjoint_f64
+    st = {k: np.ascontiguousarray(state[k], dtype=dt) for k in STATE}
+    out = {k: np.zeros(prm.shape, dtype=np.float64) for k in ("lF", "lu", "lv", "lw", "lp")}
+    g = np.zeros(3)
+    loss = np.zeros(1)
+    b = _box(box)
+    D = C.POINTER(C.c_double)
+    rc = fn(C.byref(prm), *(_ptr(st[k], T) for k in STATE), istep0, nsteps, _ptr(b, C.c_double),
+            *(_ptr(out[k], C.c_double) for k in ("lF", "lu", "lv", "lw", "lp")), _ptr(g, C.c_double),
+            _ptr(loss, C.c_double), int(nthreads))
+    if rc != 0:
+        raise RuntimeError(f"oracle adjoint failed: {rc}")
+    out["grad_g"] = g
+    out["loss"] = float(loss[0])
+    return out
+
+
+def tangent(prm, state, direction: dict, istep0: int, nsteps: int, box, dg=None, nthreads: int = 0):
+    """(loss, dloss): the FP64 box loss and its derivative along `direction`
+    (arrays for any of F, u, v, w, p) and dg (body force), by the dual-number
+    tangent of the FP64 step with the adjoint's switch convention."""
+    st = {k: np.ascontiguousarray(state[k], dtype=np.float64) for k in STATE}
+    dd = {k: (np.ascontiguousarray(direction[k], dtype=np.float64) if k in direction else None) for k in STATE}
+    g = None if dg is None else np.ascontiguousarray(dg, dtype=np.float64)
+    loss, dloss = np.zeros(1), np.zeros(1)
+    b = _box(box)
+    rc = oracle_lib().oracle_tangent_f64(C.byref(prm), *(_ptr(st[k], C.c_double) for k in STATE),
+                                         *(_ptr(dd[k], C.c_double) for k in STATE), _ptr(g, C.c_double), istep0,
+                                         nsteps, _ptr(b, C.c_double), _ptr(loss, C.c_double),
+                                         _ptr(dloss, C.c_double), int(nthreads))
+    if rc != 0:
+        raise RuntimeError(f"oracle tangent failed: {rc}")
+    return float(loss[0]), float(dloss[0])
+
+
+class SwitchTape:
+    """The switches of one forward run: record() runs the base point and keeps
+    every non-smooth choice; replay() runs another state with those choices
+    frozen (the base point's piecewise-smooth map).  Both return the final
+    state and the box loss."""
+
+    def __init__(self, prm, istep0: int, nsteps: int, box, precision: str = "f64"):
+        self.prm, self.istep0, self.nsteps, self.box = prm, istep0, nsteps, _box(box)
+        self.T, self.dt = (C.c_float, np.float32) if precision == "f32" else (C.c_double, np.float64)
+        self.fn = oracle_lib().oracle_tape_run_f32 if precision == "f32" else oracle_lib().oracle_tape_run_f64
+        self.h = oracle_lib().oracle_tape_new()
+
+    def _run(self, state, replay):
+        st = {k: np.ascontiguousarray(state[k], dtype=self.dt).copy() for k in STATE}
+        loss = np.zeros(1)
+        rc = self.fn(self.h, int(replay), C.byref(self.prm), *(_ptr(st[k], self.T) for k in STATE), self.istep0,
+                     self.nsteps, _ptr(self.box, C.c_double), _ptr(loss, C.c_double))
+        if rc != 0:
+            raise RuntimeError(f"tape run failed: {rc} (replay={replay})")
+        return st, float(loss[0])
+
+    def record(self, state):
+        return self._run(state, False)
+
+    def replay(self, state):
+        return self._run(state, True)
+
+    def size(self) -> int:
+        return int(oracle_lib().oracle_tape_size(self.h))
+
+    def close(self):
+        if self.h:
+            oracle_lib().oracle_tape_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def clamp01f(x: float) -> float:
