@@ -1,0 +1,943 @@
+// adjoint.cu -- reverse mode of the plain step on the device (extension; the
+// reference has no adjoint).  Compiled with -fmad=false: the FP32 forward
+// values recomputed here (FCT stages, advecting velocities, clamps) are the
+// forward's own bits, so every switch of the reverse pass is the one the
+// forward took.  Adjoint fields are FP64.
+//
+// Derivative conventions (the same as the host adjoint in the oracle): a
+// branch differentiates the side it took; fmaxf / fminf differentiate the
+// argument they returned, the first on a tie; clamp01f has derivative 1 on
+// [0, 1] and 0 outside.
+//
+// Per reversed step (voftrial1.cu:1364-1401 backwards):
+//   recompute: predictor + rhs, the Jacobi sweeps, the velocity correction,
+//     F before sweeps 2 and 3 (the forward's own kernels);
+//   F boundary copies (voftrial1.cu:1053-1135) reversed;
+//   each FCT sweep reversed (voftrial1.cu:509-905): its stages recomputed
+//     cell by cell, then four gather kernels (limiter and stage 4, stage 2's
+//     extrema, the face fluxes and velocities, F) -- no atomics;
+//   velocity boundary copies (voftrial1.cu:959-1051) reversed;
+//   velocity correction (voftrial1.cu:441-493) reversed (atomics into the
+//     pressure and density adjoints);
+//   Jacobi sweeps transposed (voftrial1.cu:401-439): mu = lambda / ap,
+//     lrhs += mu, lambda' = -N mu, one gather kernel per sweep;
+//   rhs (voftrial1.cu:418-422) reversed, gather;
+//   advection (voftrial1.cu:230-399) reversed (atomics), dL/dg per block;
+//   rho and nu (voftrial1.cu:95-104) reversed.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include <new>
+
+#include "adjoint.h"
+#include "fct_sweep.h"
+#include "jacobi_tb.h"
+
+namespace vof {
+
+namespace {
+
+struct Range {
+    int i0, i1, j0, j1, k0, k1;  // inclusive
+};
+
+constexpr int AB_X = 32, AB_Y = 4, AB_Z = 2;
+
+inline dim3 grid_of(const Range& r) {
+    return dim3((r.i1 - r.i0 + AB_X) / AB_X, (r.j1 - r.j0 + AB_Y) / AB_Y, (r.k1 - r.k0 + AB_Z) / AB_Z);
+}
+const dim3 kBlk(AB_X, AB_Y, AB_Z);
+
+#define RANGE_CELL(R)                                              \
+    const int i = (R).i0 + blockIdx.x * blockDim.x + threadIdx.x; \
+    const int j = (R).j0 + blockIdx.y * blockDim.y + threadIdx.y; \
+    const int k = (R).k0 + blockIdx.z * blockDim.z + threadIdx.z; \
+    if (i > (R).i1 || j > (R).j1 || k > (R).k1) return
+
+inline Range interior(const Geom& g) { return {1, g.nx, 1, g.ny, 1, g.nz}; }
+
+// The sweep axis DIR: unit offset, position along it, line length.
+template <int DIR>
+__device__ __forceinline__ int sstride(const Geom& g) {
+    return DIR == 0 ? 1 : (DIR == 1 ? g.px : g.plane);
+}
+template <int DIR>
+__device__ __forceinline__ int spos(int i, int j, int k) {
+    return DIR == 0 ? i : (DIR == 1 ? j : k);
+}
+template <int DIR>
+__device__ __forceinline__ int slen(const Geom& g) {
+    return DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
+}
+template <int DIR>
+__device__ __forceinline__ float dvfac_of(const Geom& g) {
+    return DIR == 0 ? g.dt * g.dy * g.dz : (DIR == 1 ? g.dt * g.dx * g.dz : g.dt * g.dx * g.dy);
+}
+__device__ __forceinline__ float lowflux(const Geom& g, const float* vel, const float* F, int f, int cm, int cp) {
+    const float uf = vel[f];
+    return (uf >= 0.0f) ? uf * g.dt * F[cm] : uf * g.dt * F[cp];
+}
+__device__ __forceinline__ float highflux(const Geom& g, const float* vel, const float* F, int f, int cm, int cp) {
+    const float uf = vel[f];
+    return (uf <= 0.0f) ? uf * g.dt * F[cm] : uf * g.dt * F[cp];
+}
+
+// ---- FCT stages, cell by cell (the expressions of fct_x/y/z_sweep_stage1..3) -----
+template <int DIR>
+__global__ void __launch_bounds__(256) k_fs1(Geom g, Range R, const float* __restrict__ F,
+                                             const float* __restrict__ vel, float* __restrict__ Ftd) {
+    RANGE_CELL(R);
+    const int s = sstride<DIR>(g), c = gidx(g, i, j, k);
+    const float vol = g.dx * g.dy * g.dz;
+    const float dv = vol - dvfac_of<DIR>(g) * (vel[c + s] - vel[c]);
+    const float f_in = lowflux(g, vel, F, c, c - s, c);
+    const float f_out = lowflux(g, vel, F, c + s, c, c + s);
+    float term;
+    if (DIR == 0) term = (f_in - f_out) * g.dy * g.dz / vol;
+    else if (DIR == 1) term = (f_in - f_out) * g.dy / (g.dx * g.dy);
+    else term = (f_in - f_out) * g.dy * g.dx / vol;
+    float out = (F[c] + term) * vol / dv;
+    if (out > 1.0f || out < 0.0f) out = clamp01f(out);
+    Ftd[c] = out;
+}
+
+// A at the lower face of every cell (and the upper face of the last), rp, rm.
+template <int DIR>
+__global__ void __launch_bounds__(256) k_fs2(Geom g, Range R, const float* __restrict__ F,
+                                             const float* __restrict__ vel, const float* __restrict__ Ftd,
+                                             float* __restrict__ A, float* __restrict__ rp, float* __restrict__ rm) {
+    RANGE_CELL(R);
+    const int s = sstride<DIR>(g), c = gidx(g, i, j, k);
+    const float a1 = highflux(g, vel, F, c + s, c, c + s) - lowflux(g, vel, F, c + s, c, c + s);
+    const float a0 = highflux(g, vel, F, c, c - s, c) - lowflux(g, vel, F, c, c - s, c);
+    A[c] = a0;
+    if (spos<DIR>(i, j, k) == slen<DIR>(g)) A[c + s] = a1;
+    const float pp = fmaxf(0.0f, a0) - fminf(0.0f, a1);
+    const float pm = fmaxf(0.0f, a1) - fminf(0.0f, a0);
+    const float fmx = fmaxf(Ftd[c], fmaxf(Ftd[c - s], Ftd[c + s]));
+    const float fmn = fminf(Ftd[c], fminf(Ftd[c - s], Ftd[c + s]));
+    const float hq = DIR == 2 ? g.dz : g.dx;
+    const float qp = (fmx - Ftd[c]) * hq;
+    rp[c] = (pp > 0.0f) ? fminf(1.0f, qp / pp) : 0.0f;
+    const float qm = (Ftd[c] - fmn) * hq;
+    rm[c] = (pm > 0.0f) ? fminf(1.0f, qm / pm) : 0.0f;
+}
+
+// The limiter at the upper face of every cell; 0 at the first face (never
+// written by the reference's stage 3).
+template <int DIR>
+__global__ void __launch_bounds__(256) k_fs3(Geom g, Range R, const float* __restrict__ A,
+                                             const float* __restrict__ rp, const float* __restrict__ rm,
+                                             float* __restrict__ C) {
+    RANGE_CELL(R);
+    const int s = sstride<DIR>(g), c = gidx(g, i, j, k);
+    C[c + s] = (A[c + s] >= 0.0f) ? fminf(rp[c + s], rm[c]) : fminf(rp[c], rm[c + s]);
+    if (spos<DIR>(i, j, k) == 1) C[c] = 0.0f;
+}
+
+// Stage 4 of cell c: the adjoint of its input (g4 = lF * clamp derivative),
+// lX = adjoint of X = (A1 C1 - A0 C0) / K4, and X itself.
+struct S4 {
+    double g4, lX, X, dv;
+};
+template <int DIR>
+__device__ __forceinline__ S4 stage4(const Geom& g, const float* vel, const float* Ftd, const float* A,
+                                     const float* C, const double* lF, int c) {
+    const int s = sstride<DIR>(g);
+    const float vol = g.dx * g.dy * g.dz;
+    const float dv = vol - dvfac_of<DIR>(g) * (vel[c + s] - vel[c]);
+    const float K4 = DIR == 2 ? g.dz : g.dy;
+    const float out = Ftd[c] - ((A[c + s] * C[c + s] - A[c] * C[c]) / K4) * vol / dv;
+    S4 r;
+    r.g4 = (out >= 0.0f && out <= 1.0f) ? lF[c] : 0.0;
+    r.dv = (double)dv;
+    r.X = ((double)A[c + s] * C[c + s] - (double)A[c] * C[c]) / (double)K4;
+    r.lX = -r.g4 * (double)vol / r.dv;
+    return r;
+}
+
+// Adjoint, part 1 (per interior cell): stage 4, the limiter (stage 3) and the
+// limiter ratios (stage 2).  Stores lX, the stage-4 part of ldv, the
+// extremum adjoints with the cells they selected, lpp / lpm and lown = the
+// direct adjoint of Ftd[c].
+template <int DIR>
+__global__ void __launch_bounds__(256) k_as3(Geom g, Range R, const float* __restrict__ vel,
+                                             const float* __restrict__ Ftd, const float* __restrict__ A,
+                                             const float* __restrict__ C, const float* __restrict__ rp,
+                                             const float* __restrict__ rm, const double* __restrict__ lF,
+                                             double* __restrict__ lX, double* __restrict__ ldv,
+                                             double* __restrict__ lmx, double* __restrict__ lmn,
+                                             double* __restrict__ lpp, double* __restrict__ lpm,
+                                             double* __restrict__ lown, unsigned char* __restrict__ sel) {
+    RANGE_CELL(R);
+    const int s = sstride<DIR>(g), c = gidx(g, i, j, k);
+    const int pos = spos<DIR>(i, j, k), n = slen<DIR>(g);
+    const S4 me = stage4<DIR>(g, vel, Ftd, A, C, lF, c);
+    const double lXm = pos >= 2 ? stage4<DIR>(g, vel, Ftd, A, C, lF, c - s).lX : 0.0;
+    const double lXp = pos <= n - 1 ? stage4<DIR>(g, vel, Ftd, A, C, lF, c + s).lX : 0.0;
+    const double K4 = DIR == 2 ? (double)g.dz : (double)g.dy;
+    lX[c] = me.lX;
+    ldv[c] = me.g4 * me.X * (double)(g.dx * g.dy * g.dz) / (me.dv * me.dv);
+    // limiter: faces c (lower) and c + s (upper)
+    const double lC_hi = (me.lX - lXp) * (double)A[c + s] / K4;
+    const double lC_lo = pos >= 2 ? (lXm - me.lX) * (double)A[c] / K4 : 0.0;
+    double lrp = 0.0, lrm = 0.0;
+    if (pos >= 2) {
+        if (A[c] >= 0.0f) {
+            if (rp[c] <= rm[c - s]) lrp += lC_lo;
+        } else {
+            if (!(rp[c - s] <= rm[c])) lrm += lC_lo;
+        }
+    }
+    if (A[c + s] >= 0.0f) {
+        if (!(rp[c + s] <= rm[c])) lrm += lC_hi;
+    } else {
+        if (rp[c] <= rm[c + s]) lrp += lC_hi;
+    }
+    // limiter ratios
+    const float a0 = A[c], a1 = A[c + s];
+    const float pp = fmaxf(0.0f, a0) - fminf(0.0f, a1);
+    const float pm = fmaxf(0.0f, a1) - fminf(0.0f, a0);
+    const float fc = Ftd[c], fl = Ftd[c - s], fh = Ftd[c + s];
+    const float fmx = fmaxf(fc, fmaxf(fl, fh));
+    const float fmn = fminf(fc, fminf(fl, fh));
+    const float hqf = DIR == 2 ? g.dz : g.dx;
+    const double hq = (double)hqf;
+    const float qp = (fmx - fc) * hqf, qm = (fc - fmn) * hqf;
+    double lqp = 0.0, lqm = 0.0, dpp = 0.0, dpm = 0.0;
+    if (lrp != 0.0 && pp > 0.0f && qp / pp < 1.0f) {
+        lqp = lrp / (double)pp;
+        dpp = -lrp * (double)qp / ((double)pp * pp);
+    }
+    if (lrm != 0.0 && pm > 0.0f && qm / pm < 1.0f) {
+        lqm = lrm / (double)pm;
+        dpm = -lrm * (double)qm / ((double)pm * pm);
+    }
+    const int in_mx = (fl >= fh) ? 0 : 2;  // 0: c - s, 1: c, 2: c + s
+    const int smx = (fc >= (in_mx == 0 ? fl : fh)) ? 1 : in_mx;
+    const int in_mn = (fl <= fh) ? 0 : 2;
+    const int smn = (fc <= (in_mn == 0 ? fl : fh)) ? 1 : in_mn;
+    lmx[c] = lqp * hq;
+    lmn[c] = -lqm * hq;
+    sel[c] = (unsigned char)(smx | (smn << 2));
+    lpp[c] = dpp;
+    lpm[c] = dpm;
+    lown[c] = me.g4 - lqp * hq + lqm * hq;
+}
+
+// Adjoint, part 2 (per interior cell): the full adjoint of Ftd[c] (own terms
+// and the neighbours' extrema that selected c), then stage 1: lterm = the
+// adjoint of the stage-1 flux difference (and of F[c] through it), ldv total.
+template <int DIR>
+__global__ void __launch_bounds__(256) k_as2(Geom g, Range R, const float* __restrict__ F,
+                                             const float* __restrict__ vel, const double* __restrict__ lmx,
+                                             const double* __restrict__ lmn, const unsigned char* __restrict__ sel,
+                                             const double* __restrict__ lown, double* __restrict__ ldv,
+                                             double* __restrict__ lterm) {
+    RANGE_CELL(R);
+    const int s = sstride<DIR>(g), c = gidx(g, i, j, k);
+    const int pos = spos<DIR>(i, j, k), n = slen<DIR>(g);
+    double lFtd = lown[c];
+    for (int d = -1; d <= 1; ++d) {
+        if (pos + d < 1 || pos + d > n) continue;
+        const int e = c + d * s;
+        const int sb = sel[e];
+        const int want = 1 - d;  // e's slot (0, 1, 2 = e - s, e, e + s) that is c
+        if ((sb & 3) == want) lFtd += lmx[e];
+        if ((sb >> 2) == want) lFtd += lmn[e];
+    }
+    const float vol = g.dx * g.dy * g.dz;
+    const float dv = vol - dvfac_of<DIR>(g) * (vel[c + s] - vel[c]);
+    const float f_in = lowflux(g, vel, F, c, c - s, c);
+    const float f_out = lowflux(g, vel, F, c + s, c, c + s);
+    float term;
+    if (DIR == 0) term = (f_in - f_out) * g.dy * g.dz / vol;
+    else if (DIR == 1) term = (f_in - f_out) * g.dy / (g.dx * g.dy);
+    else term = (f_in - f_out) * g.dy * g.dx / vol;
+    const float out = (F[c] + term) * vol / dv;
+    const double h = (out > 1.0f || out < 0.0f) ? 0.0 : lFtd;
+    const double dvd = (double)dv, vold = (double)vol;
+    lterm[c] = h * vold / dvd;
+    ldv[c] -= h * ((double)F[c] + (double)term) * vold / (dvd * dvd);
+}
+
+// Adjoint, part 3 (per face: positions 1 .. n+1 along the axis, the face
+// being the lower face of cell f): the low-order flux LF_f and the
+// antidiffusive flux A_f, and the face velocity.
+template <int DIR>
+__global__ void __launch_bounds__(256) k_as1(Geom g, Range R, const float* __restrict__ F,
+                                             const float* __restrict__ vel, const float* __restrict__ A,
+                                             const float* __restrict__ C, const double* __restrict__ lX,
+                                             const double* __restrict__ lpp, const double* __restrict__ lpm,
+                                             const double* __restrict__ ldv, const double* __restrict__ lterm,
+                                             double* __restrict__ lLF, double* __restrict__ lA,
+                                             double* __restrict__ lvel) {
+    RANGE_CELL(R);
+    const int s = sstride<DIR>(g), f = gidx(g, i, j, k);
+    const int pos = spos<DIR>(i, j, k), n = slen<DIR>(g);
+    const bool lo = pos >= 2, hi = pos <= n;  // cells f - s and f are interior
+    const double vol = (double)(g.dx * g.dy * g.dz);
+    const double K1 = DIR == 0 ? (double)g.dy * g.dz / vol
+                               : (DIR == 1 ? (double)g.dy / ((double)g.dx * g.dy) : (double)g.dy * g.dx / vol);
+    const double K4 = DIR == 2 ? (double)g.dz : (double)g.dy;
+    const double dt = (double)g.dt;
+    const float a = A[f];
+    const double l_LF = K1 * ((hi ? lterm[f] : 0.0) - (lo ? lterm[f - s] : 0.0));
+    double l_A = ((lo ? lX[f - s] : 0.0) - (hi ? lX[f] : 0.0)) * (double)C[f] / K4;
+    if (hi) l_A += (a > 0.0f ? lpp[f] : 0.0) - (a < 0.0f ? lpm[f] : 0.0);
+    if (lo) l_A += -(a < 0.0f ? lpp[f - s] : 0.0) + (a > 0.0f ? lpm[f - s] : 0.0);
+    const float uf = vel[f];
+    const int hs = (uf <= 0.0f) ? f - s : f;
+    const int ls = (uf >= 0.0f) ? f - s : f;
+    lvel[f] += l_LF * dt * (double)F[ls] + l_A * dt * ((double)F[hs] - (double)F[ls]) +
+               (double)dvfac_of<DIR>(g) * ((hi ? ldv[f] : 0.0) - (lo ? ldv[f - s] : 0.0));
+    lLF[f] = l_LF;
+    lA[f] = l_A;
+}
+
+// Adjoint, part 4 (per cell: positions 0 .. n+1 along the axis): the adjoint
+// of the sweep's input F (the ghosts keep theirs: the sweep does not write them).
+template <int DIR>
+__global__ void __launch_bounds__(256) k_as0(Geom g, Range R, const float* __restrict__ vel,
+                                             const double* __restrict__ lterm, const double* __restrict__ lLF,
+                                             const double* __restrict__ lA, double* __restrict__ lF) {
+    RANGE_CELL(R);
+    const int s = sstride<DIR>(g), c = gidx(g, i, j, k);
+    const int pos = spos<DIR>(i, j, k), n = slen<DIR>(g);
+    const double dt = (double)g.dt;
+    double acc = (pos >= 1 && pos <= n) ? lterm[c] : lF[c];
+    if (pos >= 1) {  // face c: cell c is its upper cell
+        const float uf = vel[c];
+        const double w = (double)uf * dt;
+        if (uf < 0.0f) acc += lLF[c] * w;                          // lowflux took F[c]
+        acc += lA[c] * w * ((uf > 0.0f ? 1.0 : 0.0) - (uf < 0.0f ? 1.0 : 0.0));
+    }
+    if (pos <= n) {  // face c + s: cell c is its lower cell
+        const float uf = vel[c + s];
+        const double w = (double)uf * dt;
+        if (uf >= 0.0f) acc += lLF[c + s] * w;
+        acc += lA[c + s] * w * ((uf <= 0.0f ? 1.0 : 0.0) - (uf >= 0.0f ? 1.0 : 0.0));
+    }
+    lF[c] = acc;
+}
+
+// ---- boundary copies, reversed ---------------------------------------------------
+__global__ void k_adj_bcF_z(Geom g, double* __restrict__ l) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nx + 1 || j > g.ny + 1) return;
+    const int a = gidx(g, i, j, 0), b = gidx(g, i, j, 1), c = gidx(g, i, j, g.nz), d = gidx(g, i, j, g.nz + 1);
+    l[b] += l[a];
+    l[a] = 0.0;
+    l[c] += l[d];
+    l[d] = 0.0;
+}
+__global__ void k_adj_bcF_x(Geom g, double* __restrict__ l) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j > g.ny + 1 || k > g.nz + 1) return;
+    const int a = gidx(g, 0, j, k), b = gidx(g, 1, j, k), c = gidx(g, g.nx, j, k), d = gidx(g, g.nx + 1, j, k);
+    l[b] += l[a];
+    l[a] = 0.0;
+    l[c] += l[d];
+    l[d] = 0.0;
+}
+__global__ void k_adj_bcF_y(Geom g, double* __restrict__ l) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nx + 1 || k > g.nz + 1) return;
+    const int a = gidx(g, i, 0, k), b = gidx(g, i, 1, k), c = gidx(g, i, g.ny, k), d = gidx(g, i, g.ny + 1, k);
+    l[b] += l[a];
+    l[a] = 0.0;
+    l[c] += l[d];
+    l[d] = 0.0;
+}
+
+__device__ __forceinline__ void mv(double* l, int dst, int src) {
+    l[src] += l[dst];
+    l[dst] = 0.0;
+}
+// set_bc_vel_k: u, v copied into the k ghosts, w zero at k = 1 and nz + 1.
+__global__ void k_adj_bcv_z(Geom g, double* __restrict__ lu, double* __restrict__ lv, double* __restrict__ lw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nx + 1 || j > g.ny + 1) return;
+    const int k0 = gidx(g, i, j, 0), k1 = gidx(g, i, j, 1), kn = gidx(g, i, j, g.nz), kf = gidx(g, i, j, g.nz + 1);
+    mv(lu, k0, k1);
+    mv(lv, k0, k1);
+    lw[k1] = 0.0;
+    mv(lu, kf, kn);
+    mv(lv, kf, kn);
+    lw[kf] = 0.0;
+}
+// set_bc_vel_i: u zero at i = 1 and nx + 1, v, w copied into the i ghosts.
+__global__ void k_adj_bcv_x(Geom g, double* __restrict__ lu, double* __restrict__ lv, double* __restrict__ lw) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j > g.ny + 1 || k > g.nz + 1) return;
+    const int i0 = gidx(g, 0, j, k), i1 = gidx(g, 1, j, k), in = gidx(g, g.nx, j, k), ir = gidx(g, g.nx + 1, j, k);
+    lu[i1] = 0.0;
+    mv(lv, i0, i1);
+    mv(lw, i0, i1);
+    lu[ir] = 0.0;
+    mv(lv, ir, in);
+    mv(lw, ir, in);
+}
+// set_bc_vel_j: v zero at j = 1 and ny + 1, u, w copied into the j ghosts.
+__global__ void k_adj_bcv_y(Geom g, double* __restrict__ lu, double* __restrict__ lv, double* __restrict__ lw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i > g.nx + 1 || k > g.nz + 1) return;
+    const int j0 = gidx(g, i, 0, k), j1 = gidx(g, i, 1, k), jn = gidx(g, i, g.ny, k), jt = gidx(g, i, g.ny + 1, k);
+    mv(lu, j0, j1);
+    lv[j1] = 0.0;
+    mv(lw, j0, j1);
+    mv(lu, jt, jn);
+    lv[jt] = 0.0;
+    mv(lw, jt, jn);
+}
+
+// ---- velocity correction, reversed ----------------------------------------------
+__global__ void __launch_bounds__(256) k_adj_update(Geom g, Range R, const float* __restrict__ F,
+                                                    const float* __restrict__ p, double* __restrict__ lu,
+                                                    double* __restrict__ lv, double* __restrict__ lw,
+                                                    double* __restrict__ lus, double* __restrict__ lvs,
+                                                    double* __restrict__ lws, double* __restrict__ lp,
+                                                    double* __restrict__ lrho) {
+    RANGE_CELL(R);
+    const int c = gidx(g, i, j, k);
+    const int pos[3] = {i, j, k}, st[3] = {1, g.px, g.plane};
+    const double hinv[3] = {(double)g.dxi, (double)g.dyi, (double)g.dzi};
+    double* lvel[3] = {lu, lv, lw};
+    double* lvs_[3] = {lus, lvs, lws};
+    const float rho_c = rho_of(g, F[c]);
+    const double dt = (double)g.dt;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (pos[a] < 2) continue;
+        const int m = c - st[a];
+        const double gv = lvel[a][c];
+        lvel[a][c] = 0.0;
+        lvs_[a][c] = gv;
+        if (gv == 0.0) continue;
+        const float r = 0.5f * (rho_c + rho_of(g, F[m]));
+        const double rd = (double)r;
+        const double coef = dt / rd * hinv[a];
+        atomicAdd(lp + c, -gv * coef);
+        atomicAdd(lp + m, gv * coef);
+        const double lr = gv * dt * ((double)p[c] - (double)p[m]) * hinv[a] / (rd * rd);
+        atomicAdd(lrho + c, 0.5 * lr);
+        atomicAdd(lrho + m, 0.5 * lr);
+    }
+}
+
+// ---- Jacobi, transposed -----------------------------------------------------------
+__device__ __forceinline__ float ap_of(const Geom& g, int i, int j, int k) {
+    const float cx = g.dxi * g.dxi, cy = g.dyi * g.dyi, cz = g.dzi * g.dzi;
+    const float ae = (i != g.nx) ? cx : 0.0f, aw = (i != 1) ? cx : 0.0f;
+    const float an = (j != g.ny) ? cy : 0.0f, as = (j != 1) ? cy : 0.0f;
+    const float af = (k != g.nz) ? cz : 0.0f, ab = (k != 1) ? cz : 0.0f;
+    return -(ae + aw + an + as + af + ab);
+}
+__global__ void __launch_bounds__(256) k_adj_jacobi(Geom g, Range R, const double* __restrict__ lin,
+                                                    double* __restrict__ lout, double* __restrict__ lrhs,
+                                                    int first) {
+    RANGE_CELL(R);
+    const int c = gidx(g, i, j, k);
+    const double mu = lin[c] / (double)ap_of(g, i, j, k);
+    lrhs[c] = first ? mu : lrhs[c] + mu;
+    const double cxx = (double)(g.dxi * g.dxi), cyy = (double)(g.dyi * g.dyi), czz = (double)(g.dzi * g.dzi);
+    double s = 0.0;
+    if (i != g.nx) s += cxx * (lin[c + 1] / (double)ap_of(g, i + 1, j, k));
+    if (i != 1) s += cxx * (lin[c - 1] / (double)ap_of(g, i - 1, j, k));
+    if (j != g.ny) s += cyy * (lin[c + g.px] / (double)ap_of(g, i, j + 1, k));
+    if (j != 1) s += cyy * (lin[c - g.px] / (double)ap_of(g, i, j - 1, k));
+    if (k != g.nz) s += czz * (lin[c + g.plane] / (double)ap_of(g, i, j, k + 1));
+    if (k != 1) s += czz * (lin[c - g.plane] / (double)ap_of(g, i, j, k - 1));
+    lout[c] = -s;
+}
+
+// ---- rhs = rho/dt div(u*), reversed (gather over the cells sharing a face) -------
+__global__ void __launch_bounds__(256) k_adj_rhs(Geom g, Range R, const float* __restrict__ F,
+                                                 const float* __restrict__ us, const float* __restrict__ vs,
+                                                 const float* __restrict__ ws, const double* __restrict__ lrhs,
+                                                 double* __restrict__ lus, double* __restrict__ lvs,
+                                                 double* __restrict__ lws, double* __restrict__ lrho) {
+    RANGE_CELL(R);
+    const int c = gidx(g, i, j, k), sy = g.px, sz = g.plane;
+    const double dt = (double)g.dt, dxi = (double)g.dxi, dyi = (double)g.dyi, dzi = (double)g.dzi;
+    const double gr = lrhs[c];
+    const double div = ((double)us[c + 1] - us[c]) * dxi + ((double)vs[c + sy] - vs[c]) * dyi +
+                       ((double)ws[c + sz] - ws[c]) * dzi;
+    lrho[c] += gr * div / dt;
+    const double kk = gr * (double)rho_of(g, F[c]) / dt;
+    const double kx = i >= 2 ? lrhs[c - 1] * (double)rho_of(g, F[c - 1]) / dt : 0.0;
+    const double ky = j >= 2 ? lrhs[c - sy] * (double)rho_of(g, F[c - sy]) / dt : 0.0;
+    const double kz = k >= 2 ? lrhs[c - sz] * (double)rho_of(g, F[c - sz]) / dt : 0.0;
+    lus[c] += (kx - kk) * dxi;
+    lvs[c] += (ky - kk) * dyi;
+    lws[c] += (kz - kk) * dzi;
+}
+
+// ---- advection, reversed (scatter with FP64 atomics) --------------------------------
+// One momentum component q at face c: q* = q + dt (visc + adv + g_q),
+// adv = -a dq/dx - b dq/dy - cc dq/dz, upwinded by the signs of a, b, cc;
+// (a, b, cc) are q itself along its own axis and 4-point averages otherwise.
+template <int COMP>
+__device__ __forceinline__ double adj_momentum(const Geom& g, int c, int i, int j, int k, const float* u,
+                                               const float* v, const float* w, double G, double nuc, double* lu,
+                                               double* lv, double* lw, double& lnu) {
+    const int sx = 1, sy = g.px, sz = g.plane;
+    const float* q = COMP == 0 ? u : (COMP == 1 ? v : w);
+    double* lq = COMP == 0 ? lu : (COMP == 1 ? lv : lw);
+    int ia[4], ib[4];
+    float a, b, cc;
+    double *la, *lb;
+    if (COMP == 0) {
+        ia[0] = c - sx; ia[1] = c - sx + sy; ia[2] = c; ia[3] = c + sy;
+        ib[0] = c - sx; ib[1] = c - sx + sz; ib[2] = c; ib[3] = c + sz;
+        a = q[c];
+        b = 0.25f * (v[ia[0]] + v[ia[1]] + v[ia[2]] + v[ia[3]]);
+        cc = 0.25f * (w[ib[0]] + w[ib[1]] + w[ib[2]] + w[ib[3]]);
+        la = lv;
+        lb = lw;
+    } else if (COMP == 1) {
+        ia[0] = c - sy; ia[1] = c; ia[2] = c + sx - sy; ia[3] = c + sx;
+        ib[0] = c - sy + sz; ib[1] = c - sy; ib[2] = c; ib[3] = c + sz;
+        a = 0.25f * (u[ia[0]] + u[ia[1]] + u[ia[2]] + u[ia[3]]);
+        b = q[c];
+        cc = 0.25f * (w[ib[0]] + w[ib[1]] + w[ib[2]] + w[ib[3]]);
+        la = lu;
+        lb = lw;
+    } else {
+        ia[0] = c + sx - sz; ia[1] = c - sz; ia[2] = c + sx; ia[3] = c;
+        ib[0] = c + sy - sz; ib[1] = c - sz; ib[2] = c; ib[3] = c + sy;
+        a = 0.25f * (u[ia[0]] + u[ia[1]] + u[ia[2]] + u[ia[3]]);
+        b = 0.25f * (v[ib[0]] + v[ib[1]] + v[ib[2]] + v[ib[3]]);
+        cc = q[c];
+        la = lu;
+        lb = lv;
+    }
+    const double hx = (double)g.dxi, hy = (double)g.dyi, hz = (double)g.dzi;
+    const double hx2 = hx * hx, hy2 = hy * hy, hz2 = hz * hz;
+    const double qc = q[c], qxm = q[c - sx], qxp = q[c + sx], qym = q[c - sy], qyp = q[c + sy], qzm = q[c - sz],
+                 qzp = q[c + sz];
+    const bool ux = a > 0.0f, uy = b > 0.0f, uz = cc > 0.0f;
+    const double dqdx = ux ? (qc - qxm) * hx : (qxp - qc) * hx;
+    const double dqdy = uy ? (qc - qym) * hy : (qyp - qc) * hy;
+    const double dqdz = uz ? (qc - qzm) * hz : (qzp - qc) * hz;
+    const double Gd = G * (double)g.dt;
+    lnu += Gd * ((qxm - 2.0 * qc + qxp) * hx2 + (qym - 2.0 * qc + qyp) * hy2 + (qzm - 2.0 * qc + qzp) * hz2);
+    double own = G - Gd * nuc * 2.0 * (hx2 + hy2 + hz2);
+    atomicAdd(lq + c - sx, Gd * nuc * hx2);
+    atomicAdd(lq + c + sx, Gd * nuc * hx2);
+    atomicAdd(lq + c - sy, Gd * nuc * hy2);
+    atomicAdd(lq + c + sy, Gd * nuc * hy2);
+    atomicAdd(lq + c - sz, Gd * nuc * hz2);
+    atomicAdd(lq + c + sz, Gd * nuc * hz2);
+    const double ga = -Gd * (double)a, gb = -Gd * (double)b, gc = -Gd * (double)cc;
+    if (ux) { own += ga * hx; atomicAdd(lq + c - sx, -ga * hx); }
+    else { atomicAdd(lq + c + sx, ga * hx); own -= ga * hx; }
+    if (uy) { own += gb * hy; atomicAdd(lq + c - sy, -gb * hy); }
+    else { atomicAdd(lq + c + sy, gb * hy); own -= gb * hy; }
+    if (uz) { own += gc * hz; atomicAdd(lq + c - sz, -gc * hz); }
+    else { atomicAdd(lq + c + sz, gc * hz); own -= gc * hz; }
+    const double l_a = -Gd * dqdx, l_b = -Gd * dqdy, l_c = -Gd * dqdz;
+    if (COMP == 0) {
+        own += l_a;
+        for (int t = 0; t < 4; ++t) { atomicAdd(la + ia[t], 0.25 * l_b); atomicAdd(lb + ib[t], 0.25 * l_c); }
+    } else if (COMP == 1) {
+        own += l_b;
+        for (int t = 0; t < 4; ++t) { atomicAdd(la + ia[t], 0.25 * l_a); atomicAdd(lb + ib[t], 0.25 * l_c); }
+    } else {
+        own += l_c;
+        for (int t = 0; t < 4; ++t) { atomicAdd(la + ia[t], 0.25 * l_a); atomicAdd(lb + ib[t], 0.25 * l_b); }
+    }
+    atomicAdd(lq + c, own);
+    return Gd;
+}
+
+__global__ void __launch_bounds__(256) k_adj_advect(Geom g, Range R, const float* __restrict__ F,
+                                                    const float* __restrict__ u, const float* __restrict__ v,
+                                                    const float* __restrict__ w, const double* __restrict__ lus,
+                                                    const double* __restrict__ lvs, const double* __restrict__ lws,
+                                                    double* lu, double* lv, double* lw, double* __restrict__ lnu,
+                                                    double* __restrict__ partial) {
+    const int i = R.i0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = R.j0 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = R.k0 + blockIdx.z * blockDim.z + threadIdx.z;
+    double gsum[3] = {0.0, 0.0, 0.0};
+    if (i <= R.i1 && j <= R.j1 && k <= R.k1) {
+        const int c = gidx(g, i, j, k);
+        const double nuc = (double)nu_of(g, F[c]);
+        double lnc = 0.0;
+        if (i >= 2 && lus[c] != 0.0) gsum[0] = adj_momentum<0>(g, c, i, j, k, u, v, w, lus[c], nuc, lu, lv, lw, lnc);
+        if (j >= 2 && lvs[c] != 0.0) gsum[1] = adj_momentum<1>(g, c, i, j, k, u, v, w, lvs[c], nuc, lu, lv, lw, lnc);
+        if (k >= 2 && lws[c] != 0.0) gsum[2] = adj_momentum<2>(g, c, i, j, k, u, v, w, lws[c], nuc, lu, lv, lw, lnc);
+        lnu[c] = lnc;
+    }
+    // deterministic block sums of dL/dg
+    __shared__ double sh[3][8];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    for (int q = 0; q < 3; ++q)
+        for (int o = 16; o > 0; o >>= 1) gsum[q] += __shfl_down_sync(0xffffffffu, gsum[q], o);
+    if ((tid & 31) == 0)
+        for (int q = 0; q < 3; ++q) sh[q][tid >> 5] = gsum[q];
+    __syncthreads();
+    if (tid == 0) {
+        const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+        for (int q = 0; q < 3; ++q) {
+            double t = 0.0;
+            for (int wv = 0; wv < 8; ++wv) t += sh[q][wv];
+            partial[3 * blk + q] = t;
+        }
+    }
+}
+
+// sums[q] += Sigma_b partial[3 b + q] (q < ncomp), in a fixed order.
+__global__ void k_fold_add(const double* __restrict__ partial, int nblk, int ncomp, double* sums) {
+    __shared__ double sh[3][256];
+    for (int q = 0; q < ncomp; ++q) {
+        double t = 0.0;
+        for (int b = threadIdx.x; b < nblk; b += blockDim.x) t += partial[ncomp * b + q];
+        sh[q][threadIdx.x] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int q = 0; q < ncomp; ++q) {
+            double t = 0.0;
+            for (int b = 0; b < (int)blockDim.x; ++b) t += sh[q][b];
+            sums[q] += t;
+        }
+}
+
+// ---- rho and nu, reversed --------------------------------------------------------
+__global__ void __launch_bounds__(256) k_adj_rho_nu(Geom g, Range R, const float* __restrict__ F,
+                                                    double* __restrict__ lrho, double* __restrict__ lnu,
+                                                    double* __restrict__ lF) {
+    RANGE_CELL(R);
+    const int c = gidx(g, i, j, k);
+    const double lr = lrho[c], ln = lnu[c];
+    lrho[c] = 0.0;
+    lnu[c] = 0.0;
+    if (lr == 0.0 && ln == 0.0) return;
+    const float f = F[c];
+    if (!(f >= 0.0f && f <= 1.0f)) return;
+    lF[c] += lr * ((double)g.rho_l - (double)g.rho_g) + ln * ((double)g.nu_l - (double)g.nu_g);
+}
+
+// ---- the loss: L = Sigma over the box of F dV; lF = dV there ----------------------------
+__device__ __forceinline__ bool in_box(const Geom& g, const double* b, int i, int j, int k) {
+    const double xc = (i - 0.5) * (double)g.dx, yc = (j - 0.5) * (double)g.dy, zc = (k - 0.5) * (double)g.dz;
+    return xc > b[0] && xc < b[1] && yc > b[2] && yc < b[3] && zc > b[4] && zc < b[5];
+}
+struct Box6 {
+    double b[6];
+};
+__global__ void __launch_bounds__(256) k_seed(Geom g, Range R, Box6 box, const float* __restrict__ F,
+                                              double* __restrict__ lF, double* __restrict__ partial) {
+    const int i = R.i0 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = R.j0 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = R.k0 + blockIdx.z * blockDim.z + threadIdx.z;
+    const double dV = (double)g.dx * (double)g.dy * (double)g.dz;
+    double acc = 0.0;
+    if (i <= R.i1 && j <= R.j1 && k <= R.k1) {
+        const int c = gidx(g, i, j, k);
+        const bool inside = i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz && in_box(g, box.b, i, j, k);
+        lF[c] = inside ? dV : 0.0;
+        if (inside) acc = (double)F[c] * dV;
+    }
+    __shared__ double sh[8];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((tid & 31) == 0) sh[tid >> 5] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int wv = 0; wv < 8; ++wv) t += sh[wv];
+        partial[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = t;
+    }
+}
+
+// ---- host -------------------------------------------------------------------------
+inline Range axis_range(const Geom& g, int dir, int lo, int hi_extra) {
+    Range r = interior(g);
+    if (dir == 0) { r.i0 = lo; r.i1 = g.nx + hi_extra; }
+    else if (dir == 1) { r.j0 = lo; r.j1 = g.ny + hi_extra; }
+    else { r.k0 = lo; r.k1 = g.nz + hi_extra; }
+    return r;
+}
+
+template <int DIR>
+cudaError_t sweep_adjoint(AdjEngine& e, const float* Fs, const float* vel, double* lvel, cudaStream_t s) {
+    const Geom& g = e.g;
+    const Range I = interior(g);
+    const dim3 gi = grid_of(I);
+    k_fs1<DIR><<<gi, kBlk, 0, s>>>(g, I, Fs, vel, e.Ftd);
+    k_fs2<DIR><<<gi, kBlk, 0, s>>>(g, I, Fs, vel, e.Ftd, e.A, e.rp, e.rm);
+    k_fs3<DIR><<<gi, kBlk, 0, s>>>(g, I, e.A, e.rp, e.rm, e.C);
+    k_as3<DIR><<<gi, kBlk, 0, s>>>(g, I, vel, e.Ftd, e.A, e.C, e.rp, e.rm, e.lF, e.lX, e.ldv, e.lmx, e.lmn, e.lpp,
+                                   e.lpm, e.lown, e.sel);
+    k_as2<DIR><<<gi, kBlk, 0, s>>>(g, I, Fs, vel, e.lmx, e.lmn, e.sel, e.lown, e.ldv, e.lterm);
+    const Range Rf = axis_range(g, DIR, 1, 1);
+    k_as1<DIR><<<grid_of(Rf), kBlk, 0, s>>>(g, Rf, Fs, vel, e.A, e.C, e.lX, e.lpp, e.lpm, e.ldv, e.lterm, e.lLF,
+                                             e.lA, lvel);
+    const Range Rc = axis_range(g, DIR, 0, 1);
+    k_as0<DIR><<<grid_of(Rc), kBlk, 0, s>>>(g, Rc, vel, e.lterm, e.lLF, e.lA, e.lF);
+    return cudaGetLastError();
+}
+
+cudaError_t copy_field(float* dst, const float* src, size_t elems, cudaStream_t s) {
+    return cudaMemcpyAsync(dst, src, elems * sizeof(float), cudaMemcpyDeviceToDevice, s);
+}
+
+cudaError_t load_state(AdjEngine& e, const AdjState& x, cudaStream_t s) {
+    float* dst[5] = {e.wb.F, e.wb.u, e.wb.v, e.wb.w, e.wb.p0};
+    cudaError_t r;
+    for (int q = 0; q < 5; ++q)
+        if ((r = copy_field(dst[q], x.f[q], e.elems, s)) != cudaSuccess) return r;
+    return cudaSuccess;
+}
+
+// One reversed step from its start state x.
+cudaError_t adjoint_step(AdjEngine& e, const AdjState& x, int istep, cudaStream_t s) {
+    const Geom& g = e.g;
+    cudaError_t r;
+    // recompute
+    if ((r = load_state(e, x, s)) != cudaSuccess) return r;
+    if ((r = plain_front(g, e.wb, s)) != cudaSuccess) return r;
+    int par = 0;
+    if ((r = plain_pressure(g, e.wb, e.jacobi_iters, &par, s)) != cudaSuccess) return r;
+    const float* pafter = par ? e.wb.p1 : e.wb.p0;
+    if ((r = plain_correct(g, e.wb, pafter, s)) != cudaSuccess) return r;
+    const int rr = ((istep % 3) + 3) % 3;
+    static const int order[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
+    const int* dirs = order[rr];
+    const float* velof[3] = {e.wb.u, e.wb.v, e.wb.w};
+    double* lvelof[3] = {e.lu, e.lv, e.lw};
+    if ((r = copy_field(e.Fin1, x.f[0], e.elems, s)) != cudaSuccess ||
+        (r = fct_launch(g, dirs[0], false, e.Fin1, velof[dirs[0]], s)) != cudaSuccess ||
+        (r = copy_field(e.Fin2, e.Fin1, e.elems, s)) != cudaSuccess ||
+        (r = fct_launch(g, dirs[1], false, e.Fin2, velof[dirs[1]], s)) != cudaSuccess)
+        return r;
+    // F boundary copies
+    {
+        const dim3 b(16, 16);
+        k_adj_bcF_z<<<dim3((g.nx + 2 + 15) / 16, (g.ny + 2 + 15) / 16), b, 0, s>>>(g, e.lF);
+        k_adj_bcF_x<<<dim3((g.ny + 2 + 15) / 16, (g.nz + 2 + 15) / 16), b, 0, s>>>(g, e.lF);
+        k_adj_bcF_y<<<dim3((g.nx + 2 + 15) / 16, (g.nz + 2 + 15) / 16), b, 0, s>>>(g, e.lF);
+    }
+    // the three sweeps, last first
+    const float* Fsw[3] = {x.f[0], e.Fin1, e.Fin2};
+    for (int q = 2; q >= 0; --q) {
+        const int d = dirs[q];
+        r = d == 0 ? sweep_adjoint<0>(e, Fsw[q], velof[0], lvelof[0], s)
+                   : (d == 1 ? sweep_adjoint<1>(e, Fsw[q], velof[1], lvelof[1], s)
+                             : sweep_adjoint<2>(e, Fsw[q], velof[2], lvelof[2], s));
+        if (r != cudaSuccess) return r;
+    }
+    // velocity boundary copies, then the correction
+    {
+        const dim3 b(16, 16);
+        k_adj_bcv_z<<<dim3((g.nx + 2 + 15) / 16, (g.ny + 2 + 15) / 16), b, 0, s>>>(g, e.lu, e.lv, e.lw);
+        k_adj_bcv_x<<<dim3((g.ny + 2 + 15) / 16, (g.nz + 2 + 15) / 16), b, 0, s>>>(g, e.lu, e.lv, e.lw);
+        k_adj_bcv_y<<<dim3((g.nx + 2 + 15) / 16, (g.nz + 2 + 15) / 16), b, 0, s>>>(g, e.lu, e.lv, e.lw);
+    }
+    const Range I = interior(g);
+    const dim3 gi = grid_of(I);
+    k_adj_update<<<gi, kBlk, 0, s>>>(g, I, x.f[0], pafter, e.lu, e.lv, e.lw, e.lus, e.lvs, e.lws, e.lp[e.lp_cur],
+                                     e.lrho);
+    // Jacobi transposed, rhs
+    for (int it = 0; it < e.jacobi_iters; ++it) {
+        k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.lp[e.lp_cur], e.lp[e.lp_cur ^ 1], e.lrhs, it == 0);
+        e.lp_cur ^= 1;
+    }
+    if (e.jacobi_iters > 0)
+        k_adj_rhs<<<gi, kBlk, 0, s>>>(g, I, x.f[0], e.wb.us, e.wb.vs, e.wb.ws, e.lrhs, e.lus, e.lvs, e.lws, e.lrho);
+    // advection, then rho and nu
+    k_adj_advect<<<gi, kBlk, 0, s>>>(g, I, x.f[0], x.f[1], x.f[2], x.f[3], e.lus, e.lvs, e.lws, e.lu, e.lv, e.lw,
+                                     e.lnu, e.d_partial);
+    k_fold_add<<<1, 256, 0, s>>>(e.d_partial, (int)(gi.x * gi.y * gi.z), 3, e.d_sums);
+    k_adj_rho_nu<<<gi, kBlk, 0, s>>>(g, I, x.f[0], e.lrho, e.lnu, e.lF);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int adj_kernels_per_step(const AdjEngine& e) {
+    // recompute: front 2, pressure (Jacobi launches), correct 1, two sweeps;
+    // adjoint: 3 + 3 x 7 + 3 + 1 + iters + 1 + 1 + 1 + 1
+    return 2 + plain_phase_launches(PHASE_JACOBI, e.jacobi_iters) + 1 + 2 + 3 + 21 + 3 + 1 + e.jacobi_iters +
+           (e.jacobi_iters > 0 ? 1 : 0) + 3;
+}
+
+cudaError_t adj_create(const Geom& g, int jacobi_iters, AdjEngine* e, cudaStream_t s) {
+    *e = AdjEngine{};
+    e->g = g;
+    e->jacobi_iters = jacobi_iters;
+    e->elems = (size_t)g.plane * (g.nz + 2);
+    cudaError_t r;
+    auto alloc = [&](void** p, size_t nb) -> cudaError_t {
+        cudaError_t q = cudaMalloc(p, nb);
+        if (q != cudaSuccess) {
+            *p = nullptr;
+            return q;
+        }
+        e->bytes += nb;
+        return cudaMemsetAsync(*p, 0, nb, s);
+    };
+    const size_t fb = e->elems * sizeof(float), db = e->elems * sizeof(double);
+    float** f32[] = {&e->wb.F, &e->wb.u, &e->wb.v, &e->wb.w, &e->wb.us, &e->wb.vs, &e->wb.ws, &e->wb.rhs, &e->wb.p0,
+                     &e->wb.p1, &e->wb.p2, &e->Fin1, &e->Fin2, &e->Ftd, &e->A, &e->C, &e->rp, &e->rm};
+    for (float** p : f32)
+        if ((r = alloc((void**)p, fb)) != cudaSuccess) return r;
+    double** f64[] = {&e->lF, &e->lu, &e->lv, &e->lw, &e->lp[0], &e->lp[1], &e->lus, &e->lvs, &e->lws, &e->lrhs,
+                      &e->lrho, &e->lnu, &e->lX, &e->lown, &e->lmx, &e->lmn, &e->lpp, &e->lpm, &e->ldv, &e->lterm,
+                      &e->lLF, &e->lA};
+    for (double** p : f64)
+        if ((r = alloc((void**)p, db)) != cudaSuccess) return r;
+    if ((r = alloc((void**)&e->sel, e->elems)) != cudaSuccess) return r;
+    if ((r = alloc((void**)&e->status, sizeof(int))) != cudaSuccess) return r;
+    const dim3 gi = grid_of(interior(g));
+    e->npartial = (int)(gi.x * gi.y * gi.z);
+    const Range full{0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1};
+    const dim3 gf = grid_of(full);
+    const int nseed = (int)(gf.x * gf.y * gf.z);
+    const int np = 3 * e->npartial > nseed ? 3 * e->npartial : nseed;
+    if ((r = alloc((void**)&e->d_partial, sizeof(double) * np)) != cudaSuccess) return r;
+    if ((r = alloc((void**)&e->d_sums, sizeof(double) * 4)) != cudaSuccess) return r;
+    if ((r = cudaMallocHost((void**)&e->h_sums, sizeof(double) * 4)) != cudaSuccess) {
+        e->h_sums = nullptr;
+        return r;
+    }
+    const float* mapped[4] = {e->wb.p0, e->wb.p1, e->wb.p2, e->wb.rhs};
+    for (int q = 0; q < 4; ++q)
+        if ((r = jacobi_tb_maps(g, mapped[q], &e->maps[q])) != cudaSuccess) return r;
+    e->wb.maps = e->maps;
+    e->wb.status = e->status;
+    return cudaStreamSynchronize(s);
+}
+
+static void free_states(AdjState* st, int n) {
+    if (!st) return;
+    for (int m = 0; m < n; ++m)
+        for (int q = 0; q < 5; ++q)
+            if (st[m].f[q]) cudaFree(st[m].f[q]);
+    delete[] st;
+}
+
+void adj_destroy(AdjEngine* e) {
+    free_states(e->cp, e->ncp);
+    free_states(e->seg, e->every);
+    float* f32[] = {e->wb.F, e->wb.u, e->wb.v, e->wb.w, e->wb.us, e->wb.vs, e->wb.ws, e->wb.rhs, e->wb.p0,
+                    e->wb.p1, e->wb.p2, e->Fin1, e->Fin2, e->Ftd, e->A, e->C, e->rp, e->rm};
+    for (float* p : f32)
+        if (p) cudaFree(p);
+    double* f64[] = {e->lF, e->lu, e->lv, e->lw, e->lp[0], e->lp[1], e->lus, e->lvs, e->lws, e->lrhs, e->lrho,
+                     e->lnu, e->lX, e->lown, e->lmx, e->lmn, e->lpp, e->lpm, e->ldv, e->lterm, e->lLF, e->lA,
+                     e->d_partial, e->d_sums};
+    for (double* p : f64)
+        if (p) cudaFree(p);
+    if (e->sel) cudaFree(e->sel);
+    if (e->status) cudaFree(e->status);
+    if (e->h_sums) cudaFreeHost(e->h_sums);
+    *e = AdjEngine{};
+}
+
+static cudaError_t alloc_states(AdjState*& st, int n, size_t elems, size_t* bytes) {
+    st = new (std::nothrow) AdjState[n];
+    if (!st) return cudaErrorMemoryAllocation;
+    for (int m = 0; m < n; ++m)
+        for (int q = 0; q < 5; ++q) st[m].f[q] = nullptr;
+    for (int m = 0; m < n; ++m)
+        for (int q = 0; q < 5; ++q) {
+            cudaError_t r = cudaMalloc((void**)&st[m].f[q], elems * sizeof(float));
+            if (r != cudaSuccess) {
+                st[m].f[q] = nullptr;
+                return r;
+            }
+            *bytes += elems * sizeof(float);
+        }
+    return cudaSuccess;
+}
+
+cudaError_t adj_tape(AdjEngine* e, int istep0, int nsteps, int every, cudaStream_t s) {
+    if (every <= 0) {
+        every = 1;
+        while ((long long)every * every < nsteps) ++every;
+    }
+    if (every > nsteps) every = nsteps > 0 ? nsteps : 1;
+    const int ncp = nsteps > 0 ? (nsteps + every - 1) / every : 0;
+    if (e->cp && (ncp != e->ncp || every != e->every)) {
+        free_states(e->cp, e->ncp);
+        free_states(e->seg, e->every);
+        e->cp = e->seg = nullptr;
+        e->ncp = 0;
+    }
+    cudaError_t r;
+    if (!e->cp && ncp > 0) {
+        e->ncp = ncp;
+        e->every = every;
+        if ((r = alloc_states(e->cp, ncp, e->elems, &e->bytes)) != cudaSuccess) return r;
+        if ((r = alloc_states(e->seg, every, e->elems, &e->bytes)) != cudaSuccess) return r;
+    }
+    e->istep0 = istep0;
+    e->nsteps = nsteps;
+    e->every = every;
+    e->recorded = false;
+    (void)s;
+    return cudaSuccess;
+}
+
+cudaError_t adj_save(AdjEngine* e, int m, const AdjState& x, cudaStream_t s) {
+    if (m < 0 || m >= e->ncp) return cudaErrorInvalidValue;
+    cudaError_t r;
+    for (int q = 0; q < 5; ++q)
+        if ((r = copy_field(e->cp[m].f[q], x.f[q], e->elems, s)) != cudaSuccess) return r;
+    return cudaSuccess;
+}
+
+cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6], double* loss, double grad_g[3],
+                         cudaStream_t s) {
+    const Geom& g = e->g;
+    cudaError_t r;
+    // seed and loss
+    double* zero[] = {e->lu, e->lv, e->lw, e->lp[0], e->lp[1], e->lrho, e->lnu};
+    for (double* p : zero)
+        if ((r = cudaMemsetAsync(p, 0, e->elems * sizeof(double), s)) != cudaSuccess) return r;
+    if ((r = cudaMemsetAsync(e->d_sums, 0, 4 * sizeof(double), s)) != cudaSuccess) return r;
+    e->lp_cur = 0;
+    {
+        const Range full{0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1};
+        const dim3 gf = grid_of(full);
+        Box6 b;
+        for (int q = 0; q < 6; ++q) b.b[q] = box[q];
+        k_seed<<<gf, kBlk, 0, s>>>(g, full, b, fin.f[0], e->lF, e->d_partial);
+        k_fold_add<<<1, 256, 0, s>>>(e->d_partial, (int)(gf.x * gf.y * gf.z), 1, e->d_sums + 3);
+        if ((r = cudaGetLastError()) != cudaSuccess) return r;
+    }
+    // segments, last first
+    for (int m = e->ncp - 1; m >= 0; --m) {
+        const int first = m * e->every;
+        const int count = (e->nsteps - first) < e->every ? (e->nsteps - first) : e->every;
+        // the segment's states: checkpoint m, then count - 1 steps with the engine's buffers
+        for (int q = 0; q < 5; ++q)
+            if ((r = copy_field(e->seg[0].f[q], e->cp[m].f[q], e->elems, s)) != cudaSuccess) return r;
+        if (count > 1) {
+            if ((r = load_state(*e, e->seg[0], s)) != cudaSuccess) return r;
+            int par = 0;
+            for (int q = 1; q < count; ++q) {
+                if ((r = plain_step(g, e->wb, e->istep0 + first + q - 1, e->jacobi_iters, &par, s)) != cudaSuccess)
+                    return r;
+                const float* src[5] = {e->wb.F, e->wb.u, e->wb.v, e->wb.w, par ? e->wb.p1 : e->wb.p0};
+                for (int t = 0; t < 5; ++t)
+                    if ((r = copy_field(e->seg[q].f[t], src[t], e->elems, s)) != cudaSuccess) return r;
+            }
+        }
+        for (int q = count - 1; q >= 0; --q)
+            if ((r = adjoint_step(*e, e->seg[q], e->istep0 + first + q, s)) != cudaSuccess) return r;
+    }
+    if ((r = cudaMemcpyAsync(e->h_sums, e->d_sums, 4 * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return r;
+    if ((r = cudaStreamSynchronize(s)) != cudaSuccess) return r;
+    if (grad_g)
+        for (int q = 0; q < 3; ++q) grad_g[q] = e->h_sums[q];
+    if (loss) *loss = e->h_sums[3];
+    return cudaSuccess;
+}
+
+}  // namespace vof

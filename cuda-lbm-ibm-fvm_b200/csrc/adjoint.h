@@ -1,0 +1,71 @@
+// adjoint.h -- the adjoint of the plain step on the device (adjoint.cu).
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "plain_step.h"
+#include "vof_device.cuh"
+
+namespace vof {
+
+// One state of the step: F, u, v, w, p in the padded layout (FP32).
+struct AdjState {
+    float* f[5];
+};
+
+// The device side of vof_forward_record / vof_backward.  Forward: the
+// context's own steps, with the state copied to a checkpoint every `every`
+// steps.  Backward: per segment (last first), the segment's states are
+// recomputed from its checkpoint with the engine's own buffers, then the
+// steps are reversed one by one, each recomputing its intermediates (rho,
+// u*, the pressure after the sweeps, the corrected velocity, F before each
+// FCT sweep) in FP32 -- bit for bit the forward's values -- and applying the
+// transposed kernels to FP64 adjoint fields.
+struct AdjEngine {
+    Geom g;
+    int jacobi_iters;
+    size_t elems;           // padded elements per field
+    // forward tape
+    int istep0, nsteps, every, ncp;
+    AdjState* cp;            // ncp checkpoints (host array of device states)
+    AdjState* seg;           // every segment states
+    bool recorded;
+    // recompute buffers (FP32)
+    PlainBuffers wb;
+    CUtensorMap maps[4];
+    int* status;
+    float *Fin1, *Fin2, *Ftd, *A, *C, *rp, *rm;
+    // adjoint fields (FP64)
+    double *lF, *lu, *lv, *lw, *lp[2], *lus, *lvs, *lws, *lrhs, *lrho, *lnu;
+    double *lX, *lown, *lmx, *lmn, *lpp, *lpm, *ldv, *lterm, *lLF, *lA;
+    unsigned char* sel;
+    int lp_cur;             // which lp buffer holds the pressure adjoint
+    double* d_partial;      // block partials (body force, loss)
+    int npartial;
+    double* d_sums;         // [0..2] dL/dg, [3] loss
+    double* h_sums;         // pinned copy
+    size_t bytes;
+};
+
+// Allocate the engine for grid g (no tape yet).  Buffers are zeroed.
+cudaError_t adj_create(const Geom& g, int jacobi_iters, AdjEngine* e, cudaStream_t s);
+void adj_destroy(AdjEngine* e);
+
+// (Re)allocate the tape for nsteps steps from istep0 with a checkpoint every
+// `every` steps (0: ceil(sqrt(nsteps))).
+cudaError_t adj_tape(AdjEngine* e, int istep0, int nsteps, int every, cudaStream_t s);
+
+// Copy the state x into checkpoint m.
+cudaError_t adj_save(AdjEngine* e, int m, const AdjState& x, cudaStream_t s);
+
+// Reverse the recorded run: L = sum over the box of F dV of the final state
+// `fin`; afterwards lF, lu, lv, lw, lp[lp_cur] hold dL/d(initial state) and
+// d_sums[0..3] dL/dg and L.  Waits for stream s.
+cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6], double* loss, double grad_g[3],
+                         cudaStream_t s);
+
+// Kernel launches of one reversed step (recompute and adjoint).
+int adj_kernels_per_step(const AdjEngine& e);
+
+}  // namespace vof

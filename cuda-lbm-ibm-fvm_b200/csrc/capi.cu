@@ -12,6 +12,7 @@
 
 #include "../../include/vof.h"
 #include "jacobi_tb.h"
+#include "adjoint.h"
 #include "mg_solve.h"
 #include "plain_step.h"
 #include "reduce.h"
@@ -41,6 +42,7 @@ struct vof_ctx {
     double* p64;                // FP64 pressure (padded layout); p0 holds its FP32 copy
     vof::MgSolver mg;
     vof::MgStats stats;         // of the last pressure solve
+    vof::AdjEngine* adj;        // adjoint engine (vof_forward_record / vof_backward), or null
     cudaGraphExec_t graph[3][2];  // [istep % 3][p parity at step start]
     int last_cuda_error;
     size_t bytes;
@@ -113,6 +115,10 @@ void free_ctx(vof_ctx* c) {
     if (c->d_status) cudaFree(c->d_status);
     if (c->p64) cudaFree(c->p64);
     vof::mg_destroy(&c->mg);
+    if (c->adj) {
+        vof::adj_destroy(c->adj);
+        delete c->adj;
+    }
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     delete c;
 }
@@ -491,6 +497,77 @@ int vof_solver_stats(const vof_ctx* ctx, int* outer, double* rel_initial, double
     return VOF_OK;
 }
 
+int vof_forward_record(vof_ctx* ctx, int istep0, int nsteps, int checkpoint_every) {
+    if (!ctx || nsteps < 1 || checkpoint_every < 0) return VOF_E_INVALID;
+    if (ctx->conv) return VOF_E_UNSUPPORTED;
+    DeviceGuard dg(ctx->device);
+    cudaError_t e;
+    if (!ctx->adj) {
+        ctx->adj = new (std::nothrow) vof::AdjEngine();
+        if (!ctx->adj) return VOF_E_NOMEM;
+        e = vof::adj_create(ctx->g, ctx->prm.jacobi_iters, ctx->adj, ctx->stream);
+        if (e != cudaSuccess) {
+            vof::adj_destroy(ctx->adj);
+            delete ctx->adj;
+            ctx->adj = nullptr;
+            return e == cudaErrorMemoryAllocation ? VOF_E_NOMEM : fail_cuda(ctx, e);
+        }
+    }
+    vof::AdjEngine* A = ctx->adj;
+    if ((e = vof::adj_tape(A, istep0, nsteps, checkpoint_every, ctx->stream)) != cudaSuccess)
+        return e == cudaErrorMemoryAllocation ? VOF_E_NOMEM : fail_cuda(ctx, e);
+    for (int n = 0; n < nsteps; ++n) {
+        if (n % A->every == 0) {
+            vof::AdjState x;
+            for (int q = 0; q < 5; ++q) x.f[q] = field_ptr(ctx, q);
+            if ((e = vof::adj_save(A, n / A->every, x, ctx->stream)) != cudaSuccess) return fail_cuda(ctx, e);
+        }
+        e = vof::plain_step(ctx->g, ctx->b, istep0 + n, ctx->prm.jacobi_iters, &ctx->p_parity, ctx->stream);
+        if (e != cudaSuccess) return fail_cuda(ctx, e);
+    }
+    const int st = vof_sync(ctx);
+    if (st != VOF_OK) return st;
+    A->recorded = true;
+    return VOF_OK;
+}
+
+int vof_backward(vof_ctx* ctx, const double* box, double* loss, double* grad_g) {
+    if (!ctx || !box) return VOF_E_INVALID;
+    if (!ctx->adj || !ctx->adj->recorded) return VOF_E_STATE;
+    DeviceGuard dg(ctx->device);
+    vof::AdjState fin;
+    for (int q = 0; q < 5; ++q) fin.f[q] = field_ptr(ctx, q);
+    cudaError_t e = vof::adj_backward(ctx->adj, fin, box, loss, grad_g, ctx->stream);
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    int st = 0;
+    if (cudaMemcpy(&st, ctx->adj->status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return VOF_E_CUDA;
+    if (st != 0) {
+        cudaMemset(ctx->adj->status, 0, sizeof(int));
+        return VOF_E_TIMEOUT;
+    }
+    return VOF_OK;
+}
+
+int vof_adjoint_download(vof_ctx* ctx, int field, double* dst) {
+    if (!ctx || !dst || field < VOF_FIELD_F || field > VOF_FIELD_P) return VOF_E_INVALID;
+    if (!ctx->adj || !ctx->adj->recorded) return VOF_E_STATE;
+    DeviceGuard dg(ctx->device);
+    const vof::AdjEngine* A = ctx->adj;
+    const double* src[5] = {A->lF, A->lu, A->lv, A->lw, A->lp[A->lp_cur]};
+    const Geom& g = ctx->g;
+    const size_t w = (size_t)(g.nx + 2) * sizeof(double);
+    cudaError_t e = cudaMemcpy2DAsync(dst, w, src[field], (size_t)g.px * sizeof(double), w,
+                                      (size_t)(g.ny + 2) * (g.nz + 2), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
+}
+
+int vof_adjoint_kernels_per_step(const vof_ctx* ctx) {
+    if (!ctx) return VOF_E_INVALID;
+    if (!ctx->adj) return VOF_E_STATE;
+    return vof::adj_kernels_per_step(*ctx->adj);
+}
+
 int vof_last_cuda_error(const vof_ctx* ctx) { return ctx ? ctx->last_cuda_error : 0; }
 
 int vof_kernels_per_step(const vof_ctx* ctx) {
@@ -499,6 +576,6 @@ int vof_kernels_per_step(const vof_ctx* ctx) {
     return vof::plain_kernels_per_step(ctx->prm.jacobi_iters);
 }
 
-size_t vof_device_bytes(const vof_ctx* ctx) { return ctx ? ctx->bytes : 0; }
+size_t vof_device_bytes(const vof_ctx* ctx) { return ctx ? ctx->bytes + (ctx->adj ? ctx->adj->bytes : 0) : 0; }
 
 }  // extern "C"

@@ -390,16 +390,18 @@ cudaError_t plain_front(const Geom& g, const PlainBuffers& b, cudaStream_t s, cu
     return cudaSuccess;
 }
 
+cudaError_t plain_correct(const Geom& g, const PlainBuffers& b, const float* p, cudaStream_t s) {
+    const dim3 cb(32, 4, 2);
+    const dim3 cg((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + 1) / 2);
+    k_correct<<<cg, cb, 0, s>>>(g, b.F, b.us, b.vs, b.ws, p, b.u, b.v, b.w);
+    return cudaGetLastError();
+}
+
 cudaError_t plain_back(const Geom& g, const PlainBuffers& b, int istep, const float* p, cudaStream_t s,
                        cudaEvent_t* ev) {
     cudaError_t e;
     if ((e = mark(ev, 3, s)) != cudaSuccess) return e;
-    {
-        const dim3 cb(32, 4, 2);
-        const dim3 cg((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + 1) / 2);
-        k_correct<<<cg, cb, 0, s>>>(g, b.F, b.us, b.vs, b.ws, p, b.u, b.v, b.w);
-    }
-    if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(ev, 4, s)) != cudaSuccess) return e;
+    if ((e = plain_correct(g, b, p, s)) != cudaSuccess || (e = mark(ev, 4, s)) != cudaSuccess) return e;
 
     // Sweep order by istep % 3 (voftrial1.cu:1384-1396).
     const int r = ((istep % 3) + 3) % 3;
@@ -413,11 +415,8 @@ cudaError_t plain_back(const Geom& g, const PlainBuffers& b, int istep, const fl
     return cudaSuccess;
 }
 
-cudaError_t plain_step(const Geom& g, const PlainBuffers& b, int istep, int jacobi_iters,
-                       int* p_parity, cudaStream_t s, cudaEvent_t* ev) {
-    cudaError_t e = plain_front(g, b, s, ev);
-    if (e != cudaSuccess) return e;
-
+cudaError_t plain_pressure(const Geom& g, const PlainBuffers& b, int jacobi_iters, int* p_parity, cudaStream_t s) {
+    cudaError_t e;
     // Jacobi (voftrial1.cu:1371-1375): JACOBI_T sweeps per launch.  The
     // reference ping-pongs p <-> pt once per sweep, so after N sweeps its
     // pressure sits in the buffer it started in when N is even and in the
@@ -445,7 +444,16 @@ cudaError_t plain_step(const Geom& g, const PlainBuffers& b, int istep, int jaco
         }
     }
     *p_parity = dst;
-    return plain_back(g, b, istep, pbuf[dst], s, ev);
+    return cudaSuccess;
+}
+
+cudaError_t plain_step(const Geom& g, const PlainBuffers& b, int istep, int jacobi_iters,
+                       int* p_parity, cudaStream_t s, cudaEvent_t* ev) {
+    cudaError_t e = plain_front(g, b, s, ev);
+    if (e != cudaSuccess) return e;
+    if ((e = plain_pressure(g, b, jacobi_iters, p_parity, s)) != cudaSuccess) return e;
+    float* pbuf[3] = {b.p0, b.p1, b.p2};
+    return plain_back(g, b, istep, pbuf[*p_parity], s, ev);
 }
 
 int plain_phase_launches(int phase, int jacobi_iters) {

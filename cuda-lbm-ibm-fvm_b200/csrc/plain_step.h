@@ -67,6 +67,12 @@ cudaError_t plain_front(const Geom& g, const PlainBuffers& b, cudaStream_t s, cu
 cudaError_t plain_back(const Geom& g, const PlainBuffers& b, int istep, const float* p, cudaStream_t s,
                        cudaEvent_t* ev = nullptr);
 
+// The pieces of plain_step: the Jacobi sweeps from the pressure in buffer
+// p0/p1 selected by *p_parity (updated to the buffer holding the result), and
+// the velocity correction with its boundary conditions.
+cudaError_t plain_pressure(const Geom& g, const PlainBuffers& b, int jacobi_iters, int* p_parity, cudaStream_t s);
+cudaError_t plain_correct(const Geom& g, const PlainBuffers& b, const float* p, cudaStream_t s);
+
 // Kernel launches of one phase.
 int plain_phase_launches(int phase, int jacobi_iters);
 

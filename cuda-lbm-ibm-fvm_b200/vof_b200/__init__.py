@@ -110,6 +110,10 @@ def _declare(lib):
         "vof_phase_name": (C.c_char_p, [C.c_int]),
         "vof_solver_stats": (C.c_int, [vp, P(C.c_int), P(C.c_double), P(C.c_double)]),
         "vof_step_noalloc": (C.c_int, [P(Params), vp, vp, vp, vp, vp, C.c_int, vp]),
+        "vof_forward_record": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
+        "vof_backward": (C.c_int, [vp, P(C.c_double), P(C.c_double), P(C.c_double)]),
+        "vof_adjoint_download": (C.c_int, [vp, C.c_int, vp]),
+        "vof_adjoint_kernels_per_step": (C.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -136,7 +140,8 @@ def exported_symbols():
             "vof_create", "vof_destroy", "vof_get_params", "vof_upload", "vof_download",
             "vof_step", "vof_run", "vof_sync", "vof_reduce", "vof_reduce_async",
             "vof_last_cuda_error", "vof_kernels_per_step", "vof_device_bytes",
-            "vof_step_timed", "vof_phase_name", "vof_solver_stats", "vof_step_noalloc"]
+            "vof_step_timed", "vof_phase_name", "vof_solver_stats", "vof_step_noalloc",
+            "vof_forward_record", "vof_backward", "vof_adjoint_download", "vof_adjoint_kernels_per_step"]
 
 
 def default_params(nx: int, ny: int | None = None, nz: int | None = None, **overrides) -> Params:
@@ -265,6 +270,33 @@ class Solver:
         o, a, b = C.c_int(), C.c_double(), C.c_double()
         self._check(self._lib.vof_solver_stats(self._ctx, C.byref(o), C.byref(a), C.byref(b)), "vof_solver_stats")
         return {"outer": o.value, "rel_initial": a.value, "rel_final": b.value}
+
+    # ---- adjoint ----------------------------------------------------------
+    def forward_record(self, istep0: int, nsteps: int, checkpoint_every: int = 0):
+        """nsteps plain steps from istep0, with checkpoints for backward()."""
+        self._check(self._lib.vof_forward_record(self._ctx, istep0, nsteps, checkpoint_every), "vof_forward_record")
+
+    def backward(self, box) -> dict:
+        """Reverse pass of the recorded run for L = sum over `box` (x0, x1, y0,
+        y1, z0, z1; strict bounds on cell centres) of F dV: {'loss', 'grad_g'}."""
+        b = np.ascontiguousarray(box, dtype=np.float64)
+        if b.shape != (6,):
+            raise ValueError("box must be (x0, x1, y0, y1, z0, z1)")
+        loss = C.c_double()
+        g = np.zeros(3)
+        self._check(self._lib.vof_backward(self._ctx, b.ctypes.data_as(C.POINTER(C.c_double)), C.byref(loss),
+                                           g.ctypes.data_as(C.POINTER(C.c_double))), "vof_backward")
+        return {"loss": loss.value, "grad_g": g}
+
+    def adjoint(self, field) -> np.ndarray:
+        """dL/d(field) of the recorded run's initial state (float64, reference layout)."""
+        out = np.empty(self.prm.shape, dtype=np.float64)
+        self._check(self._lib.vof_adjoint_download(self._ctx, self._fid(field), out.ctypes.data), "vof_adjoint_download")
+        return out
+
+    @property
+    def adjoint_kernels_per_step(self) -> int:
+        return self._lib.vof_adjoint_kernels_per_step(self._ctx)
 
     @property
     def kernels_per_step(self) -> int:

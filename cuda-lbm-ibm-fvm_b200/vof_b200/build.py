@@ -4,7 +4,8 @@ The shared library is written next to this file, inside the source tree, so it
 travels with the repository to the machine that runs it.  Object files go to
 ``cuda-lbm-ibm-fvm_b200/_build``.
 
-``plain_step.cu`` is compiled with ``-fmad=false``: the FP32 drop-in step keeps
+``plain_step.cu`` (and the other FP32 step sources, and ``adjoint.cu``, which
+recomputes the step's values) are compiled with ``-fmad=false``: the FP32 drop-in step keeps
 the reference's per-point expressions without FMA contraction, which makes it
 bit-identical to the CPU restatement (oracle/) and to the reference's kernels
 compiled the same way.
@@ -32,13 +33,14 @@ SOURCES = {
     "plain_step.cu": ["-fmad=false", "-DVOF_FMAD_FALSE"],
     "fct_sweep.cu": ["-fmad=false", "-DVOF_FMAD_FALSE"],
     "jacobi_tb.cu": ["-fmad=false", "-DVOF_FMAD_FALSE"],
+    "adjoint.cu": ["-fmad=false", "-DVOF_FMAD_FALSE"],
     "tma_host.cu": [],
     "mg_solve.cu": [],
     "reduce.cu": [],
     "capi.cu": [],
     "noalloc.cu": [],
 }
-HEADERS = ["vof_device.cuh", "tma.cuh", "plain_step.h", "fct_sweep.h", "jacobi_tb.h", "mg_solve.h", "reduce.h"]
+HEADERS = ["vof_device.cuh", "tma.cuh", "plain_step.h", "fct_sweep.h", "jacobi_tb.h", "mg_solve.h", "reduce.h", "adjoint.h"]
 
 
 def nvcc() -> str:

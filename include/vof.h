@@ -221,6 +221,37 @@ int vof_step_noalloc(const vof_params* p, float* F, float* u, float* v, float* w
  */
 int vof_solver_stats(const vof_ctx* ctx, int* outer, double* rel_initial, double* rel_final);
 
+/* ---- adjoint (extension; the reference has no adjoint) ----------------------
+ * Gradient of L = sum of F dV over the interior cells whose centre lies
+ * strictly inside box = {x0, x1, y0, y1, z0, z1} after a recorded run, with
+ * respect to the run's initial state and the body force.  Derivative
+ * conventions at the step's non-smooth points: a branch (upwinding, the FCT
+ * flux direction) differentiates the side the forward took, fmaxf / fminf the
+ * argument returned (the first on a tie), a clamp to [0, 1] has derivative 1
+ * on [0, 1] and 0 outside.  The forward is the plain FP32 step, the adjoint
+ * fields are FP64.
+ *
+ * vof_forward_record: nsteps plain steps from istep0 on the context's state
+ * (like vof_run), storing a device checkpoint of the state every
+ * checkpoint_every steps (0: ceil(sqrt(nsteps))).  VOF_MODE_PLAIN only
+ * (VOF_E_UNSUPPORTED otherwise).  Device memory: ceil(nsteps/every) + every
+ * states of five fields, plus the engine's work fields (allocated once).
+ *
+ * vof_backward: the reverse pass of the recorded run from the context's
+ * current (final) state; *loss = L, grad_g = dL/d(gx, gy, gz).  Recomputes
+ * each segment from its checkpoint and each step from its start state.
+ * VOF_E_STATE without a recorded run.
+ *
+ * vof_adjoint_download: dL/d(field) of the initial state (field F, U, V, W or
+ * P), FP64, reference layout, to host memory; valid after vof_backward.
+ */
+int vof_forward_record(vof_ctx* ctx, int istep0, int nsteps, int checkpoint_every);
+int vof_backward(vof_ctx* ctx, const double* box, double* loss, double* grad_g);
+int vof_adjoint_download(vof_ctx* ctx, int field, double* dst);
+/* Kernel launches of one reversed step (recompute included); VOF_E_STATE
+ * before the first vof_forward_record. */
+int vof_adjoint_kernels_per_step(const vof_ctx* ctx);
+
 /* cudaError_t of the most recent failing CUDA call in this context (0 if none). */
 int vof_last_cuda_error(const vof_ctx* ctx);
 
