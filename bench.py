@@ -80,6 +80,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ext-steps", type=int, default=10,
                     help="steps of each convergent-mode measurement at the bench size (0 disables)")
+    ap.add_argument("--adj-steps", type=int, default=400,
+                    help="steps of the adjoint measurement at 64^3 (the bench size runs 1/8 of them; 0 disables)")
     return ap.parse_args(argv)
 
 
@@ -313,6 +315,70 @@ def measure_convergent(V, n, steps, stream, dev, tol=1e-8):
 
 
 # ---------------------------------------------------------------------------
+# adjoint (extension): gradient of a box loss w.r.t. the initial velocity
+# perturbation and the body force; time of the reverse pass vs the forward
+# ---------------------------------------------------------------------------
+def measure_adjoint(V, n, steps, every, stream, dev, dense=False):
+    """dam break n^3 with N(0, (1e-3)^2) perturbations of u, v, w on interior
+    faces (splitmix64 seed 3), loss = sum of F dV over cells with centre
+    x > 0.06 and z < 0.02; forward = `steps` plain steps through captured
+    graphs, record = the same steps with a checkpoint every `every` steps,
+    backward = the reverse pass (segment recompute + per-step recompute +
+    FP64 adjoint kernels).  CUDA events on the library's stream.  dense: the
+    loss box is the whole domain (every adjoint field dense; at 4e-6 s x 400
+    steps no liquid reaches the x > 0.06, z < 0.02 box, whose loss and
+    adjoint are then 0 almost everywhere)."""
+    import torch
+
+    from vof_b200 import ic
+
+    prm = V.default_params(n, gx=0.0, gy=0.0, gz=-9.81)
+    st = ic.rest_state(prm, ic.dam_break(prm))
+    lo = {"u": (1, 1, 2), "v": (1, 2, 1), "w": (2, 1, 1)}
+    for q, k in enumerate(("u", "v", "w")):
+        a = lo[k]
+        shape = (prm.nz + 1 - a[0], prm.ny + 1 - a[1], prm.nx + 1 - a[2])
+        st[k][a[0]:prm.nz + 1, a[1]:prm.ny + 1, a[2]:prm.nx + 1] += (
+            1e-3 * ic.normal(3 * 1000 + q, int(np.prod(shape))).reshape(shape)).astype(np.float32)
+    box = (0.06, 1e300, -1e300, 1e300, -1e300, 0.02) if not dense else (-1e300, 1e300) * 3
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    with V.Solver(prm, stream=stream.cuda_stream) as s:
+        s.upload_state(**st)
+        s.run(1, 3)  # graphs captured
+        s.upload_state(**st)
+        fwd_ms, _ = timed(lambda: s.run(1, steps))
+        s.upload_state(**st)
+        s.forward_record(1, min(steps, 3), every)  # engine allocated outside the timed region
+        s.upload_state(**st)
+        rec_ms, _ = timed(lambda: s.forward_record(1, steps, every))
+        bwd_ms, r = timed(lambda: s.backward(box))
+        lu = s.adjoint("u")
+        kps = s.adjoint_kernels_per_step
+        nbytes = s.device_bytes
+    return {"workload": f"dam_break_{n}^3 + N(0,1e-3^2) interior-face velocity perturbation (seed 3), "
+                        f"{steps} steps, loss = sum F dV over " + ("the whole domain" if dense else "x>0.06, z<0.02"),
+            "steps": steps, "checkpoint_every": every if every > 0 else int(np.ceil(np.sqrt(steps))),
+            "forward_ms_per_step": round(fwd_ms / steps, 4),
+            "record_ms_per_step": round(rec_ms / steps, 4),
+            "backward_ms_per_step": round(bwd_ms / steps, 4),
+            "backward_over_forward": round(bwd_ms / fwd_ms, 3),
+            "record_plus_backward_over_forward": round((rec_ms + bwd_ms) / fwd_ms, 3),
+            "loss": r["loss"], "dL_dg": [float(x) for x in r["grad_g"]],
+            "dL_du_norm": float(np.linalg.norm(lu)),
+            "kernels_per_reversed_step": kps, "device_bytes": int(nbytes),
+            "precision": "FP32 forward (bit-identical to the plain step), FP64 adjoint fields"}
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def run_ours(args):
@@ -433,6 +499,10 @@ def run_ours(args):
         ext["convergent_pressure"] = measure_convergent(V, args.n, args.ext_steps, stream, dev)
         ext["convergent_pressure"]["speedup_mixed_over_plain"] = round(
             ext["convergent_pressure"]["mixed"]["value"] / value, 3)
+    if args.adj_steps > 0 and world == 1:
+        ext["adjoint"] = [measure_adjoint(V, 64, args.adj_steps, 20, stream, dev),
+                          measure_adjoint(V, 64, args.adj_steps, 20, stream, dev, dense=True),
+                          measure_adjoint(V, args.n, max(1, args.adj_steps // 8), 0, stream, dev, dense=True)]
 
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K,

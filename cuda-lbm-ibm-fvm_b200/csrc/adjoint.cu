@@ -14,8 +14,9 @@
 //     F before sweeps 2 and 3 (the forward's own kernels);
 //   F boundary copies (voftrial1.cu:1053-1135) reversed;
 //   each FCT sweep reversed (voftrial1.cu:509-905): its stages recomputed
-//     cell by cell, then four gather kernels (limiter and stage 4, stage 2's
-//     extrema, the face fluxes and velocities, F) -- no atomics;
+//     cell by cell, then five gather kernels (stage 4; the limiter and
+//     stage 2's ratios; stage 2's extrema and stage 1; the face fluxes and
+//     velocities; F) -- no atomics;
 //   velocity boundary copies (voftrial1.cu:959-1051) reversed;
 //   velocity correction (voftrial1.cu:441-493) reversed (atomics into the
 //     pressure and density adjoints);
@@ -135,83 +136,88 @@ __global__ void __launch_bounds__(256) k_fs3(Geom g, Range R, const float* __res
     if (spos<DIR>(i, j, k) == 1) C[c] = 0.0f;
 }
 
-// Stage 4 of cell c: the adjoint of its input (g4 = lF * clamp derivative),
-// lX = adjoint of X = (A1 C1 - A0 C0) / K4, and X itself.
-struct S4 {
-    double g4, lX, X, dv;
-};
+// Adjoint, part 0 (per interior cell): stage 4.  out = Ftd - X vol / dv,
+// X = (A1 C1 - A0 C0) / K4, F = clamp01f(out): g4 = lF * (clamp derivative)
+// is the adjoint of Ftd through stage 4; lX = -g4 vol / dv the adjoint of X;
+// ldv (stage-4 part) = g4 X vol / dv^2.
 template <int DIR>
-__device__ __forceinline__ S4 stage4(const Geom& g, const float* vel, const float* Ftd, const float* A,
-                                     const float* C, const double* lF, int c) {
-    const int s = sstride<DIR>(g);
+__global__ void __launch_bounds__(256) k_as4(Geom g, Range R, const float* __restrict__ vel,
+                                             const float* __restrict__ Ftd, const float* __restrict__ A,
+                                             const float* __restrict__ C, const double* __restrict__ lF,
+                                             double* __restrict__ lX, double* __restrict__ ldv,
+                                             double* __restrict__ lown) {
+    RANGE_CELL(R);
+    const int s = sstride<DIR>(g), c = gidx(g, i, j, k);
     const float vol = g.dx * g.dy * g.dz;
     const float dv = vol - dvfac_of<DIR>(g) * (vel[c + s] - vel[c]);
     const float K4 = DIR == 2 ? g.dz : g.dy;
-    const float out = Ftd[c] - ((A[c + s] * C[c + s] - A[c] * C[c]) / K4) * vol / dv;
-    S4 r;
-    r.g4 = (out >= 0.0f && out <= 1.0f) ? lF[c] : 0.0;
-    r.dv = (double)dv;
-    r.X = ((double)A[c + s] * C[c + s] - (double)A[c] * C[c]) / (double)K4;
-    r.lX = -r.g4 * (double)vol / r.dv;
-    return r;
+    const float a0 = A[c], a1 = A[c + s], c0 = C[c], c1 = C[c + s];
+    const float out = Ftd[c] - ((a1 * c1 - a0 * c0) / K4) * vol / dv;
+    const double g4 = (out >= 0.0f && out <= 1.0f) ? lF[c] : 0.0;
+    const double idv = 1.0 / (double)dv, vold = (double)vol;
+    const double X = ((double)a1 * c1 - (double)a0 * c0) / (double)K4;
+    lX[c] = -g4 * vold * idv;
+    ldv[c] = g4 * X * vold * idv * idv;
+    lown[c] = g4;
 }
 
-// Adjoint, part 1 (per interior cell): stage 4, the limiter (stage 3) and the
-// limiter ratios (stage 2).  Stores lX, the stage-4 part of ldv, the
-// extremum adjoints with the cells they selected, lpp / lpm and lown = the
-// direct adjoint of Ftd[c].
+// Adjoint, part 1 (per interior cell): the limiter (stage 3) and the limiter
+// ratios (stage 2).  Stores the extremum adjoints with the cells they
+// selected, lpp / lpm, and adds the direct stage-2 terms to lown (the
+// adjoint of Ftd[c] from its own cell).
 template <int DIR>
-__global__ void __launch_bounds__(256) k_as3(Geom g, Range R, const float* __restrict__ vel,
-                                             const float* __restrict__ Ftd, const float* __restrict__ A,
-                                             const float* __restrict__ C, const float* __restrict__ rp,
-                                             const float* __restrict__ rm, const double* __restrict__ lF,
-                                             double* __restrict__ lX, double* __restrict__ ldv,
+__global__ void __launch_bounds__(256) k_as3(Geom g, Range R, const float* __restrict__ Ftd,
+                                             const float* __restrict__ A, const float* __restrict__ rp,
+                                             const float* __restrict__ rm, const double* __restrict__ lX,
                                              double* __restrict__ lmx, double* __restrict__ lmn,
                                              double* __restrict__ lpp, double* __restrict__ lpm,
                                              double* __restrict__ lown, unsigned char* __restrict__ sel) {
     RANGE_CELL(R);
     const int s = sstride<DIR>(g), c = gidx(g, i, j, k);
     const int pos = spos<DIR>(i, j, k), n = slen<DIR>(g);
-    const S4 me = stage4<DIR>(g, vel, Ftd, A, C, lF, c);
-    const double lXm = pos >= 2 ? stage4<DIR>(g, vel, Ftd, A, C, lF, c - s).lX : 0.0;
-    const double lXp = pos <= n - 1 ? stage4<DIR>(g, vel, Ftd, A, C, lF, c + s).lX : 0.0;
-    const double K4 = DIR == 2 ? (double)g.dz : (double)g.dy;
-    lX[c] = me.lX;
-    ldv[c] = me.g4 * me.X * (double)(g.dx * g.dy * g.dz) / (me.dv * me.dv);
+    const double iK4 = 1.0 / (DIR == 2 ? (double)g.dz : (double)g.dy);
+    const double lXc = lX[c];
+    const double lXm = pos >= 2 ? lX[c - s] : 0.0;
+    const double lXp = pos <= n - 1 ? lX[c + s] : 0.0;
+    const float a0 = A[c], a1 = A[c + s];
     // limiter: faces c (lower) and c + s (upper)
-    const double lC_hi = (me.lX - lXp) * (double)A[c + s] / K4;
-    const double lC_lo = pos >= 2 ? (lXm - me.lX) * (double)A[c] / K4 : 0.0;
+    const double lC_hi = (lXc - lXp) * (double)a1 * iK4;
+    const double lC_lo = pos >= 2 ? (lXm - lXc) * (double)a0 * iK4 : 0.0;
     double lrp = 0.0, lrm = 0.0;
     if (pos >= 2) {
-        if (A[c] >= 0.0f) {
+        if (a0 >= 0.0f) {
             if (rp[c] <= rm[c - s]) lrp += lC_lo;
         } else {
             if (!(rp[c - s] <= rm[c])) lrm += lC_lo;
         }
     }
-    if (A[c + s] >= 0.0f) {
+    if (a1 >= 0.0f) {
         if (!(rp[c + s] <= rm[c])) lrm += lC_hi;
     } else {
         if (rp[c] <= rm[c + s]) lrp += lC_hi;
     }
     // limiter ratios
-    const float a0 = A[c], a1 = A[c + s];
     const float pp = fmaxf(0.0f, a0) - fminf(0.0f, a1);
     const float pm = fmaxf(0.0f, a1) - fminf(0.0f, a0);
     const float fc = Ftd[c], fl = Ftd[c - s], fh = Ftd[c + s];
-    const float fmx = fmaxf(fc, fmaxf(fl, fh));
-    const float fmn = fminf(fc, fminf(fl, fh));
     const float hqf = DIR == 2 ? g.dz : g.dx;
     const double hq = (double)hqf;
-    const float qp = (fmx - fc) * hqf, qm = (fc - fmn) * hqf;
     double lqp = 0.0, lqm = 0.0, dpp = 0.0, dpm = 0.0;
-    if (lrp != 0.0 && pp > 0.0f && qp / pp < 1.0f) {
-        lqp = lrp / (double)pp;
-        dpp = -lrp * (double)qp / ((double)pp * pp);
+    if (lrp != 0.0) {
+        const float qp = (fmaxf(fc, fmaxf(fl, fh)) - fc) * hqf;
+        if (pp > 0.0f && qp / pp < 1.0f) {
+            const double ip = 1.0 / (double)pp;
+            lqp = lrp * ip;
+            dpp = -lqp * (double)qp * ip;
+        }
     }
-    if (lrm != 0.0 && pm > 0.0f && qm / pm < 1.0f) {
-        lqm = lrm / (double)pm;
-        dpm = -lrm * (double)qm / ((double)pm * pm);
+    if (lrm != 0.0) {
+        const float qm = (fc - fminf(fc, fminf(fl, fh))) * hqf;
+        if (pm > 0.0f && qm / pm < 1.0f) {
+            const double ip = 1.0 / (double)pm;
+            lqm = lrm * ip;
+            dpm = -lqm * (double)qm * ip;
+        }
     }
     const int in_mx = (fl >= fh) ? 0 : 2;  // 0: c - s, 1: c, 2: c + s
     const int smx = (fc >= (in_mx == 0 ? fl : fh)) ? 1 : in_mx;
@@ -222,7 +228,7 @@ __global__ void __launch_bounds__(256) k_as3(Geom g, Range R, const float* __res
     sel[c] = (unsigned char)(smx | (smn << 2));
     lpp[c] = dpp;
     lpm[c] = dpm;
-    lown[c] = me.g4 - lqp * hq + lqm * hq;
+    lown[c] += -lqp * hq + lqm * hq;
 }
 
 // Adjoint, part 2 (per interior cell): the full adjoint of Ftd[c] (own terms
@@ -391,83 +397,114 @@ __global__ void k_adj_bcv_y(Geom g, double* __restrict__ lu, double* __restrict_
     mv(lw, jt, jn);
 }
 
-// ---- velocity correction, reversed ----------------------------------------------
+// ---- velocity correction, reversed (gather over the six faces of a cell) -----------
+// Face q along axis a (its cells q - st and q): u_q = u*_q - dt/r (p_q - p_{q-st}) h^-1,
+// r = (rho_q + rho_{q-st}) / 2.  Cell c collects, from its lower faces (q = c)
+// and upper faces (q = c + st), the adjoints of p_c and rho_c; the face
+// adjoint itself moves to lus / lvs / lws (the zeroing of lu / lv / lw at the
+// updated faces happens in k_adj_rhs, after every cell has read them).
 __global__ void __launch_bounds__(256) k_adj_update(Geom g, Range R, const float* __restrict__ F,
-                                                    const float* __restrict__ p, double* __restrict__ lu,
-                                                    double* __restrict__ lv, double* __restrict__ lw,
+                                                    const float* __restrict__ p, const double* __restrict__ lu,
+                                                    const double* __restrict__ lv, const double* __restrict__ lw,
                                                     double* __restrict__ lus, double* __restrict__ lvs,
                                                     double* __restrict__ lws, double* __restrict__ lp,
                                                     double* __restrict__ lrho) {
     RANGE_CELL(R);
     const int c = gidx(g, i, j, k);
-    const int pos[3] = {i, j, k}, st[3] = {1, g.px, g.plane};
+    const int pos[3] = {i, j, k}, len[3] = {g.nx, g.ny, g.nz}, st[3] = {1, g.px, g.plane};
     const double hinv[3] = {(double)g.dxi, (double)g.dyi, (double)g.dzi};
-    double* lvel[3] = {lu, lv, lw};
+    const double* lvel[3] = {lu, lv, lw};
     double* lvs_[3] = {lus, lvs, lws};
     const float rho_c = rho_of(g, F[c]);
-    const double dt = (double)g.dt;
+    const double dt = (double)g.dt, pc = (double)p[c];
+    double lpc = 0.0, lrc = 0.0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        if (pos[a] < 2) continue;
-        const int m = c - st[a];
-        const double gv = lvel[a][c];
-        lvel[a][c] = 0.0;
-        lvs_[a][c] = gv;
-        if (gv == 0.0) continue;
-        const float r = 0.5f * (rho_c + rho_of(g, F[m]));
-        const double rd = (double)r;
-        const double coef = dt / rd * hinv[a];
-        atomicAdd(lp + c, -gv * coef);
-        atomicAdd(lp + m, gv * coef);
-        const double lr = gv * dt * ((double)p[c] - (double)p[m]) * hinv[a] / (rd * rd);
-        atomicAdd(lrho + c, 0.5 * lr);
-        atomicAdd(lrho + m, 0.5 * lr);
+        if (pos[a] >= 2) {  // lower face: c is its upper cell
+            const int m = c - st[a];
+            const double gv = lvel[a][c];
+            lvs_[a][c] = gv;
+            if (gv != 0.0) {
+                const double ir = 1.0 / (double)(0.5f * (rho_c + rho_of(g, F[m])));
+                lpc -= gv * dt * ir * hinv[a];
+                lrc += 0.5 * gv * dt * (pc - (double)p[m]) * hinv[a] * ir * ir;
+            }
+        }
+        if (pos[a] + 1 <= len[a]) {  // upper face: c is its lower cell
+            const int q = c + st[a];
+            const double gv = lvel[a][q];
+            if (gv != 0.0) {
+                const double ir = 1.0 / (double)(0.5f * (rho_of(g, F[q]) + rho_c));
+                lpc += gv * dt * ir * hinv[a];
+                lrc += 0.5 * gv * dt * ((double)p[q] - pc) * hinv[a] * ir * ir;
+            }
+        }
     }
+    lp[c] += lpc;
+    lrho[c] = lrc;
 }
 
-// ---- Jacobi, transposed -----------------------------------------------------------
-__device__ __forceinline__ float ap_of(const Geom& g, int i, int j, int k) {
-    const float cx = g.dxi * g.dxi, cy = g.dyi * g.dyi, cz = g.dzi * g.dzi;
-    const float ae = (i != g.nx) ? cx : 0.0f, aw = (i != 1) ? cx : 0.0f;
-    const float an = (j != g.ny) ? cy : 0.0f, as = (j != 1) ? cy : 0.0f;
-    const float af = (k != g.nz) ? cz : 0.0f, ab = (k != 1) ? cz : 0.0f;
-    return -(ae + aw + an + as + af + ab);
+// ---- Jacobi, transposed, on mu = lambda / ap --------------------------------------
+// Forward sweep: p' = (rhs - N p) / ap.  Reverse: mu_k = lambda_k / ap,
+// lrhs += mu_k, lambda_{k-1} = -N mu_k; carried as mu: mu_{k-1} = -N mu_k / ap.
+// inv_ap[flags] = 1 / ap (FP32 ap of the forward, in its order) for the six
+// wall flags (i==1, i==nx, j==1, j==ny, k==1, k==nz) of a cell.
+__device__ __forceinline__ int wall_flags(const Geom& g, int i, int j, int k) {
+    return (i == 1) | ((i == g.nx) << 1) | ((j == 1) << 2) | ((j == g.ny) << 3) | ((k == 1) << 4) |
+           ((k == g.nz) << 5);
 }
-__global__ void __launch_bounds__(256) k_adj_jacobi(Geom g, Range R, const double* __restrict__ lin,
-                                                    double* __restrict__ lout, double* __restrict__ lrhs,
-                                                    int first) {
-    RANGE_CELL(R);
-    const int c = gidx(g, i, j, k);
-    const double mu = lin[c] / (double)ap_of(g, i, j, k);
-    lrhs[c] = first ? mu : lrhs[c] + mu;
+__device__ __forceinline__ double neg_N(const Geom& g, const double* mu, int c, int i, int j, int k) {
     const double cxx = (double)(g.dxi * g.dxi), cyy = (double)(g.dyi * g.dyi), czz = (double)(g.dzi * g.dzi);
     double s = 0.0;
-    if (i != g.nx) s += cxx * (lin[c + 1] / (double)ap_of(g, i + 1, j, k));
-    if (i != 1) s += cxx * (lin[c - 1] / (double)ap_of(g, i - 1, j, k));
-    if (j != g.ny) s += cyy * (lin[c + g.px] / (double)ap_of(g, i, j + 1, k));
-    if (j != 1) s += cyy * (lin[c - g.px] / (double)ap_of(g, i, j - 1, k));
-    if (k != g.nz) s += czz * (lin[c + g.plane] / (double)ap_of(g, i, j, k + 1));
-    if (k != 1) s += czz * (lin[c - g.plane] / (double)ap_of(g, i, j, k - 1));
-    lout[c] = -s;
+    if (i != g.nx) s += cxx * mu[c + 1];
+    if (i != 1) s += cxx * mu[c - 1];
+    if (j != g.ny) s += cyy * mu[c + g.px];
+    if (j != 1) s += cyy * mu[c - g.px];
+    if (k != g.nz) s += czz * mu[c + g.plane];
+    if (k != 1) s += czz * mu[c - g.plane];
+    return -s;
+}
+// mode 0: mu = lin / ap, lrhs = mu;  1: mu = -N lin / ap, lrhs += mu;  2: out = -N lin.
+__global__ void __launch_bounds__(256) k_adj_jacobi(Geom g, Range R, InvAp ia, const double* __restrict__ lin,
+                                                    double* __restrict__ lout, double* __restrict__ lrhs, int mode) {
+    RANGE_CELL(R);
+    const int c = gidx(g, i, j, k);
+    if (mode == 2) {
+        lout[c] = neg_N(g, lin, c, i, j, k);
+        return;
+    }
+    const double inv = ia.v[wall_flags(g, i, j, k)];
+    const double mu = (mode == 0 ? lin[c] : neg_N(g, lin, c, i, j, k)) * inv;
+    lout[c] = mu;
+    lrhs[c] = mode == 0 ? mu : lrhs[c] + mu;
 }
 
 // ---- rhs = rho/dt div(u*), reversed (gather over the cells sharing a face) -------
+// Also zeroes lu / lv / lw at the faces the correction overwrote (their
+// adjoints moved to lus / lvs / lws in k_adj_update).  has_rhs = 0: no
+// Jacobi sweeps, so no rhs adjoint.
 __global__ void __launch_bounds__(256) k_adj_rhs(Geom g, Range R, const float* __restrict__ F,
                                                  const float* __restrict__ us, const float* __restrict__ vs,
                                                  const float* __restrict__ ws, const double* __restrict__ lrhs,
                                                  double* __restrict__ lus, double* __restrict__ lvs,
-                                                 double* __restrict__ lws, double* __restrict__ lrho) {
+                                                 double* __restrict__ lws, double* __restrict__ lrho,
+                                                 double* __restrict__ lu, double* __restrict__ lv,
+                                                 double* __restrict__ lw, int has_rhs) {
     RANGE_CELL(R);
     const int c = gidx(g, i, j, k), sy = g.px, sz = g.plane;
-    const double dt = (double)g.dt, dxi = (double)g.dxi, dyi = (double)g.dyi, dzi = (double)g.dzi;
+    if (i >= 2) lu[c] = 0.0;
+    if (j >= 2) lv[c] = 0.0;
+    if (k >= 2) lw[c] = 0.0;
+    if (!has_rhs) return;
+    const double idt = 1.0 / (double)g.dt, dxi = (double)g.dxi, dyi = (double)g.dyi, dzi = (double)g.dzi;
     const double gr = lrhs[c];
     const double div = ((double)us[c + 1] - us[c]) * dxi + ((double)vs[c + sy] - vs[c]) * dyi +
                        ((double)ws[c + sz] - ws[c]) * dzi;
-    lrho[c] += gr * div / dt;
-    const double kk = gr * (double)rho_of(g, F[c]) / dt;
-    const double kx = i >= 2 ? lrhs[c - 1] * (double)rho_of(g, F[c - 1]) / dt : 0.0;
-    const double ky = j >= 2 ? lrhs[c - sy] * (double)rho_of(g, F[c - sy]) / dt : 0.0;
-    const double kz = k >= 2 ? lrhs[c - sz] * (double)rho_of(g, F[c - sz]) / dt : 0.0;
+    lrho[c] += gr * div * idt;
+    const double kk = gr * (double)rho_of(g, F[c]) * idt;
+    const double kx = i >= 2 ? lrhs[c - 1] * (double)rho_of(g, F[c - 1]) * idt : 0.0;
+    const double ky = j >= 2 ? lrhs[c - sy] * (double)rho_of(g, F[c - sy]) * idt : 0.0;
+    const double kz = k >= 2 ? lrhs[c - sz] * (double)rho_of(g, F[c - sz]) * idt : 0.0;
     lus[c] += (kx - kk) * dxi;
     lvs[c] += (ky - kk) * dyi;
     lws[c] += (kz - kk) * dzi;
@@ -551,11 +588,16 @@ __device__ __forceinline__ double adj_momentum(const Geom& g, int c, int i, int 
     return Gd;
 }
 
+// Also the adjoint of rho and nu (cal_nu_rho_kernel, voftrial1.cu:95-104): with
+// lrho complete (correction and rhs) and lnu from the three momentum
+// equations of this cell, lF[c] += (lrho drho/dF + lnu dnu/dF).  dL/dg: each
+// block adds its sums to its own slot of `partial` (summed once at the end).
 __global__ void __launch_bounds__(256) k_adj_advect(Geom g, Range R, const float* __restrict__ F,
                                                     const float* __restrict__ u, const float* __restrict__ v,
                                                     const float* __restrict__ w, const double* __restrict__ lus,
                                                     const double* __restrict__ lvs, const double* __restrict__ lws,
-                                                    double* lu, double* lv, double* lw, double* __restrict__ lnu,
+                                                    double* lu, double* lv, double* lw,
+                                                    const double* __restrict__ lrho, double* __restrict__ lF,
                                                     double* __restrict__ partial) {
     const int i = R.i0 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = R.j0 + blockIdx.y * blockDim.y + threadIdx.y;
@@ -563,12 +605,15 @@ __global__ void __launch_bounds__(256) k_adj_advect(Geom g, Range R, const float
     double gsum[3] = {0.0, 0.0, 0.0};
     if (i <= R.i1 && j <= R.j1 && k <= R.k1) {
         const int c = gidx(g, i, j, k);
-        const double nuc = (double)nu_of(g, F[c]);
+        const float Fc = F[c];
+        const double nuc = (double)nu_of(g, Fc);
         double lnc = 0.0;
         if (i >= 2 && lus[c] != 0.0) gsum[0] = adj_momentum<0>(g, c, i, j, k, u, v, w, lus[c], nuc, lu, lv, lw, lnc);
         if (j >= 2 && lvs[c] != 0.0) gsum[1] = adj_momentum<1>(g, c, i, j, k, u, v, w, lvs[c], nuc, lu, lv, lw, lnc);
         if (k >= 2 && lws[c] != 0.0) gsum[2] = adj_momentum<2>(g, c, i, j, k, u, v, w, lws[c], nuc, lu, lv, lw, lnc);
-        lnu[c] = lnc;
+        const double lr = lrho[c];
+        if ((lr != 0.0 || lnc != 0.0) && Fc >= 0.0f && Fc <= 1.0f)
+            lF[c] += lr * ((double)g.rho_l - (double)g.rho_g) + lnc * ((double)g.nu_l - (double)g.nu_g);
     }
     // deterministic block sums of dL/dg
     __shared__ double sh[3][8];
@@ -583,12 +628,13 @@ __global__ void __launch_bounds__(256) k_adj_advect(Geom g, Range R, const float
         for (int q = 0; q < 3; ++q) {
             double t = 0.0;
             for (int wv = 0; wv < 8; ++wv) t += sh[q][wv];
-            partial[3 * blk + q] = t;
+            partial[3 * blk + q] += t;
         }
     }
 }
 
-// sums[q] += Sigma_b partial[3 b + q] (q < ncomp), in a fixed order.
+// sums[q] += Sigma_b partial[ncomp b + q] (q < ncomp), in a fixed order:
+// each of the 256 threads sums a strided subset, then thread 0 the 256 results.
 __global__ void k_fold_add(const double* __restrict__ partial, int nblk, int ncomp, double* sums) {
     __shared__ double sh[3][256];
     for (int q = 0; q < ncomp; ++q) {
@@ -603,21 +649,6 @@ __global__ void k_fold_add(const double* __restrict__ partial, int nblk, int nco
             for (int b = 0; b < (int)blockDim.x; ++b) t += sh[q][b];
             sums[q] += t;
         }
-}
-
-// ---- rho and nu, reversed --------------------------------------------------------
-__global__ void __launch_bounds__(256) k_adj_rho_nu(Geom g, Range R, const float* __restrict__ F,
-                                                    double* __restrict__ lrho, double* __restrict__ lnu,
-                                                    double* __restrict__ lF) {
-    RANGE_CELL(R);
-    const int c = gidx(g, i, j, k);
-    const double lr = lrho[c], ln = lnu[c];
-    lrho[c] = 0.0;
-    lnu[c] = 0.0;
-    if (lr == 0.0 && ln == 0.0) return;
-    const float f = F[c];
-    if (!(f >= 0.0f && f <= 1.0f)) return;
-    lF[c] += lr * ((double)g.rho_l - (double)g.rho_g) + ln * ((double)g.nu_l - (double)g.nu_g);
 }
 
 // ---- the loss: L = Sigma over the box of F dV; lF = dV there ----------------------------
@@ -670,8 +701,8 @@ cudaError_t sweep_adjoint(AdjEngine& e, const float* Fs, const float* vel, doubl
     k_fs1<DIR><<<gi, kBlk, 0, s>>>(g, I, Fs, vel, e.Ftd);
     k_fs2<DIR><<<gi, kBlk, 0, s>>>(g, I, Fs, vel, e.Ftd, e.A, e.rp, e.rm);
     k_fs3<DIR><<<gi, kBlk, 0, s>>>(g, I, e.A, e.rp, e.rm, e.C);
-    k_as3<DIR><<<gi, kBlk, 0, s>>>(g, I, vel, e.Ftd, e.A, e.C, e.rp, e.rm, e.lF, e.lX, e.ldv, e.lmx, e.lmn, e.lpp,
-                                   e.lpm, e.lown, e.sel);
+    k_as4<DIR><<<gi, kBlk, 0, s>>>(g, I, vel, e.Ftd, e.A, e.C, e.lF, e.lX, e.ldv, e.lown);
+    k_as3<DIR><<<gi, kBlk, 0, s>>>(g, I, e.Ftd, e.A, e.rp, e.rm, e.lX, e.lmx, e.lmn, e.lpp, e.lpm, e.lown, e.sel);
     k_as2<DIR><<<gi, kBlk, 0, s>>>(g, I, Fs, vel, e.lmx, e.lmn, e.sel, e.lown, e.ldv, e.lterm);
     const Range Rf = axis_range(g, DIR, 1, 1);
     k_as1<DIR><<<grid_of(Rf), kBlk, 0, s>>>(g, Rf, Fs, vel, e.A, e.C, e.lX, e.lpp, e.lpm, e.ldv, e.lterm, e.lLF,
@@ -741,18 +772,22 @@ cudaError_t adjoint_step(AdjEngine& e, const AdjState& x, int istep, cudaStream_
     const dim3 gi = grid_of(I);
     k_adj_update<<<gi, kBlk, 0, s>>>(g, I, x.f[0], pafter, e.lu, e.lv, e.lw, e.lus, e.lvs, e.lws, e.lp[e.lp_cur],
                                      e.lrho);
-    // Jacobi transposed, rhs
-    for (int it = 0; it < e.jacobi_iters; ++it) {
-        k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.lp[e.lp_cur], e.lp[e.lp_cur ^ 1], e.lrhs, it == 0);
+    // Jacobi transposed (on mu = lambda / ap), then rhs
+    if (e.jacobi_iters > 0) {
+        k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.inv_ap, e.lp[e.lp_cur], e.lp[e.lp_cur ^ 1], e.lrhs, 0);
+        e.lp_cur ^= 1;
+        for (int it = 1; it < e.jacobi_iters; ++it) {
+            k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.inv_ap, e.lp[e.lp_cur], e.lp[e.lp_cur ^ 1], e.lrhs, 1);
+            e.lp_cur ^= 1;
+        }
+        k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.inv_ap, e.lp[e.lp_cur], e.lp[e.lp_cur ^ 1], e.lrhs, 2);
         e.lp_cur ^= 1;
     }
-    if (e.jacobi_iters > 0)
-        k_adj_rhs<<<gi, kBlk, 0, s>>>(g, I, x.f[0], e.wb.us, e.wb.vs, e.wb.ws, e.lrhs, e.lus, e.lvs, e.lws, e.lrho);
-    // advection, then rho and nu
+    k_adj_rhs<<<gi, kBlk, 0, s>>>(g, I, x.f[0], e.wb.us, e.wb.vs, e.wb.ws, e.lrhs, e.lus, e.lvs, e.lws, e.lrho, e.lu,
+                                  e.lv, e.lw, e.jacobi_iters > 0);
+    // advection with rho and nu
     k_adj_advect<<<gi, kBlk, 0, s>>>(g, I, x.f[0], x.f[1], x.f[2], x.f[3], e.lus, e.lvs, e.lws, e.lu, e.lv, e.lw,
-                                     e.lnu, e.d_partial);
-    k_fold_add<<<1, 256, 0, s>>>(e.d_partial, (int)(gi.x * gi.y * gi.z), 3, e.d_sums);
-    k_adj_rho_nu<<<gi, kBlk, 0, s>>>(g, I, x.f[0], e.lrho, e.lnu, e.lF);
+                                     e.lrho, e.lF, e.d_partial);
     return cudaGetLastError();
 }
 
@@ -760,9 +795,10 @@ cudaError_t adjoint_step(AdjEngine& e, const AdjState& x, int istep, cudaStream_
 
 int adj_kernels_per_step(const AdjEngine& e) {
     // recompute: front 2, pressure (Jacobi launches), correct 1, two sweeps;
-    // adjoint: 3 + 3 x 7 + 3 + 1 + iters + 1 + 1 + 1 + 1
-    return 2 + plain_phase_launches(PHASE_JACOBI, e.jacobi_iters) + 1 + 2 + 3 + 21 + 3 + 1 + e.jacobi_iters +
-           (e.jacobi_iters > 0 ? 1 : 0) + 3;
+    // adjoint: F copies 3, sweeps 3 x 8, velocity copies 3, correction 1,
+    // Jacobi iters + 1 (none without sweeps), rhs 1, advection 1
+    return 2 + plain_phase_launches(PHASE_JACOBI, e.jacobi_iters) + 1 + 2 + 3 + 24 + 3 + 1 +
+           (e.jacobi_iters > 0 ? e.jacobi_iters + 1 : 0) + 1 + 1;
 }
 
 cudaError_t adj_create(const Geom& g, int jacobi_iters, AdjEngine* e, cudaStream_t s) {
@@ -803,6 +839,15 @@ cudaError_t adj_create(const Geom& g, int jacobi_iters, AdjEngine* e, cudaStream
     if ((r = cudaMallocHost((void**)&e->h_sums, sizeof(double) * 4)) != cudaSuccess) {
         e->h_sums = nullptr;
         return r;
+    }
+    // 1 / ap for the 64 wall-flag combinations (the forward's FP32 ap, in its order)
+    for (int f = 0; f < 64; ++f) {
+        const float cx = g.dxi * g.dxi, cy = g.dyi * g.dyi, cz = g.dzi * g.dzi;
+        const bool i1 = f & 1, inx = f & 2, j1 = f & 4, jny = f & 8, k1 = f & 16, knz = f & 32;
+        const float ae = inx ? 0.0f : cx, aw = i1 ? 0.0f : cx, an = jny ? 0.0f : cy, as = j1 ? 0.0f : cy;
+        const float af = knz ? 0.0f : cz, ab = k1 ? 0.0f : cz;
+        const float ap = -(ae + aw + an + as + af + ab);
+        e->inv_ap.v[f] = ap != 0.0f ? 1.0 / (double)ap : 0.0;
     }
     const float* mapped[4] = {e->wb.p0, e->wb.p1, e->wb.p2, e->wb.rhs};
     for (int q = 0; q < 4; ++q)
@@ -896,7 +941,7 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
     const Geom& g = e->g;
     cudaError_t r;
     // seed and loss
-    double* zero[] = {e->lu, e->lv, e->lw, e->lp[0], e->lp[1], e->lrho, e->lnu};
+    double* zero[] = {e->lu, e->lv, e->lw, e->lp[0], e->lp[1], e->lrho};
     for (double* p : zero)
         if ((r = cudaMemsetAsync(p, 0, e->elems * sizeof(double), s)) != cudaSuccess) return r;
     if ((r = cudaMemsetAsync(e->d_sums, 0, 4 * sizeof(double), s)) != cudaSuccess) return r;
@@ -909,6 +954,7 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
         k_seed<<<gf, kBlk, 0, s>>>(g, full, b, fin.f[0], e->lF, e->d_partial);
         k_fold_add<<<1, 256, 0, s>>>(e->d_partial, (int)(gf.x * gf.y * gf.z), 1, e->d_sums + 3);
         if ((r = cudaGetLastError()) != cudaSuccess) return r;
+        if ((r = cudaMemsetAsync(e->d_partial, 0, sizeof(double) * 3 * e->npartial, s)) != cudaSuccess) return r;
     }
     // segments, last first
     for (int m = e->ncp - 1; m >= 0; --m) {
@@ -931,6 +977,8 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
         for (int q = count - 1; q >= 0; --q)
             if ((r = adjoint_step(*e, e->seg[q], e->istep0 + first + q, s)) != cudaSuccess) return r;
     }
+    k_fold_add<<<1, 256, 0, s>>>(e->d_partial, e->npartial, 3, e->d_sums);
+    if ((r = cudaGetLastError()) != cudaSuccess) return r;
     if ((r = cudaMemcpyAsync(e->h_sums, e->d_sums, 4 * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
         return r;
     if ((r = cudaStreamSynchronize(s)) != cudaSuccess) return r;

@@ -9,6 +9,12 @@
 
 namespace vof {
 
+// 1 / ap of the Jacobi sweep for the 64 combinations of a cell's six wall
+// flags (i == 1, i == nx, j == 1, j == ny, k == 1, k == nz; bit 0 .. 5).
+struct InvAp {
+    double v[64];
+};
+
 // One state of the step: F, u, v, w, p in the padded layout (FP32).
 struct AdjState {
     float* f[5];
@@ -41,6 +47,7 @@ struct AdjEngine {
     double *lX, *lown, *lmx, *lmn, *lpp, *lpm, *ldv, *lterm, *lLF, *lA;
     unsigned char* sel;
     int lp_cur;             // which lp buffer holds the pressure adjoint
+    InvAp inv_ap;
     double* d_partial;      // block partials (body force, loss)
     int npartial;
     double* d_sums;         // [0..2] dL/dg, [3] loss
