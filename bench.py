@@ -61,7 +61,7 @@ ALG_BYTES = {
     "sweep3": 12,
 }
 KERNEL_NAMES = {
-    "predict": "k_predict", "rhs": "k_rhs", "jacobi": "k_jacobi", "correct": "k_correct",
+    "predict": "k_predict", "rhs": "k_rhs", "jacobi": "k_jacobi_tb", "correct": "k_correct",
     "sweep1": "k_fct", "sweep2": "k_fct", "sweep3": "k_fct",
 }
 STEP_MODEL_BYTES = 188  # B per cell-step of the fused plain path (10 sweeps, FP32)
