@@ -232,9 +232,15 @@ def barrier(world: int, device=None):
 # CPU baseline
 # ---------------------------------------------------------------------------
 def cpu_baseline(prm, state, seconds: float) -> dict | None:
+    """The FP64 CPU restatement (oracle) on the host: all cores on a bounded
+    sample of the workload (steps after one warm-up step, about `seconds`),
+    one core on one step, and the 32^3 dam break (200 steps) on all cores."""
     if seconds <= 0:
         return None
     from oracle import oracle as orc
+
+    import vof_b200 as V
+    from vof_b200 import ic
 
     cores = os.cpu_count() or 1
     cells = prm.nx * prm.ny * prm.nz
@@ -245,8 +251,16 @@ def cpu_baseline(prm, state, seconds: float) -> dict | None:
     per = max(t1 - t0, 1e-6)
     n = int(min(20, max(1, round(seconds / per))))
     t0 = time.perf_counter()
-    orc.run_f64(prm, st, 2, n, nthreads=cores)
+    st = orc.run_f64(prm, st, 2, n, nthreads=cores)
     el = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    orc.run_f64(prm, st, 2 + n, 1, nthreads=1)
+    el1 = time.perf_counter() - t0
+    small = V.default_params(32, gx=0.0, gy=0.0, gz=-9.81)
+    s_state = ic.rest_state(small, ic.dam_break(small))
+    t0 = time.perf_counter()
+    orc.run_f64(small, s_state, 1, 200, nthreads=cores)
+    el32 = time.perf_counter() - t0
     cpu = "unknown"
     try:
         for ln in open("/proc/cpuinfo"):
@@ -256,8 +270,11 @@ def cpu_baseline(prm, state, seconds: float) -> dict | None:
     except Exception:
         pass
     return {"value": cells * n / el / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"FP64 CPU restatement (oracle/vof_oracle.cpp, OpenMP {cores} threads, {cpu}): "
-                      f"steps 2..{n + 1} of the {prm.nx}^3 workload after 1 warm-up step, {el:.2f} s"}
+            "sample": f"FP64 CPU restatement (oracle/vof_oracle.cpp, OpenMP {cores} threads = nproc, {cpu}): "
+                      f"steps 2..{n + 1} of the {prm.nx}^3 workload after 1 warm-up step, {el:.2f} s",
+            "single_thread_value": cells / el1 / 1e6,
+            "dam_break_32_200_steps": {"value": 32 ** 3 * 200 / el32 / 1e6, "seconds": round(el32, 3),
+                                       "cores": cores}}
 
 
 # ---------------------------------------------------------------------------
@@ -367,6 +384,8 @@ def measure_adjoint(V, n, steps, every, stream, dev, dense=False):
     return {"workload": f"dam_break_{n}^3 + N(0,1e-3^2) interior-face velocity perturbation (seed 3), "
                         f"{steps} steps, loss = sum F dV over " + ("the whole domain" if dense else "x>0.06, z<0.02"),
             "steps": steps, "checkpoint_every": every if every > 0 else int(np.ceil(np.sqrt(steps))),
+            "forward_mcell_s": round(prm.nx * prm.ny * prm.nz * steps / fwd_ms / 1e3, 1),
+            "backward_mcell_s": round(prm.nx * prm.ny * prm.nz * steps / bwd_ms / 1e3, 1),
             "forward_ms_per_step": round(fwd_ms / steps, 4),
             "record_ms_per_step": round(rec_ms / steps, 4),
             "backward_ms_per_step": round(bwd_ms / steps, 4),
@@ -454,9 +473,11 @@ def run_ours(args):
                 "phase": dom, "alg_bytes_per_cell": ALG_BYTES[dom], "units_per_launch": cells,
                 "launch_ms": round(per_launch_s * 1e3, 5), "peak_source": peak_src}
     step_ms = ms_max / K
+    step_gbs = STEP_MODEL_BYTES * cells / (step_ms / 1e3) / 1e9
     step_roofline = {"model_bytes_per_cell_step": STEP_MODEL_BYTES,
-                     "achieved_gbs": round(STEP_MODEL_BYTES * cells / (step_ms / 1e3) / 1e9, 1),
-                     "frac_of_peak": round(STEP_MODEL_BYTES * cells / (step_ms / 1e3) / 1e9 / peak, 4)}
+                     "achieved_gbs": round(step_gbs, 1),
+                     "frac_of_peak": round(step_gbs / peak, 4), "peak_gbs": peak,
+                     "frac_of_nominal_8tbs": round(step_gbs / 8000.0, 4)}
 
     # e2e through the public API with host buffers
     e2e = None
