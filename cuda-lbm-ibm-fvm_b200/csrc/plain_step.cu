@@ -417,6 +417,7 @@ cudaError_t plain_back(const Geom& g, const PlainBuffers& b, int istep, const fl
 
 cudaError_t plain_pressure(const Geom& g, const PlainBuffers& b, int jacobi_iters, int* p_parity, cudaStream_t s) {
     cudaError_t e;
+
     // Jacobi (voftrial1.cu:1371-1375): JACOBI_T sweeps per launch.  The
     // reference ping-pongs p <-> pt once per sweep, so after N sweeps its
     // pressure sits in the buffer it started in when N is even and in the

@@ -57,28 +57,32 @@ def _stale(target: Path, deps) -> bool:
     return any(Path(d).stat().st_mtime > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile every CUDA source for sm_100a and link libvof_b200.so."""
-    BUILD_DIR.mkdir(parents=True, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, extra=(), lib_path: Path | None = None,
+          build_dir: Path | None = None) -> Path:
+    """Compile every CUDA source for sm_100a and link libvof_b200.so (or
+    lib_path, with `extra` nvcc flags on every source, objects in build_dir)."""
+    lib_out = LIB_PATH if lib_path is None else Path(lib_path)
+    bdir = BUILD_DIR if build_dir is None else Path(build_dir)
+    bdir.mkdir(parents=True, exist_ok=True)
     headers = [SRC_DIR / h for h in HEADERS] + [INCLUDE_DIR / "vof.h"]
     objs = []
-    for src, extra in SOURCES.items():
+    for src, flags in SOURCES.items():
         s = SRC_DIR / src
-        o = BUILD_DIR / (src + ".o")
+        o = bdir / (src + ".o")
         objs.append(o)
         if force or _stale(o, [s, *headers, Path(__file__)]):
-            cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", str(s), "-o", str(o)]
+            cmd = [nvcc(), *ARCH, *COMMON, *flags, *extra, "-c", str(s), "-o", str(o)]
             if verbose:
                 print(" ".join(cmd), file=sys.stderr)
             subprocess.run(cmd, check=True)
-    if force or _stale(LIB_PATH, objs):
-        tmp = LIB_PATH.with_suffix(".so.tmp")
+    if force or _stale(lib_out, objs):
+        tmp = lib_out.with_suffix(".so.tmp")
         cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *map(str, objs), "-o", str(tmp)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
-        os.replace(tmp, LIB_PATH)
-    return LIB_PATH
+        os.replace(tmp, lib_out)
+    return lib_out
 
 
 if __name__ == "__main__":
