@@ -255,6 +255,68 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(MgLevel L, const S* __
     column_sweep<S>(L, ein, eout, b, mb, (C)alpha, (C)beta, read_prev != 0, i, j, k0, k1);
 }
 
+// The same step for BF16 levels of even width, two cells of a row per thread
+// (bf16x2 loads and stores; the x neighbours of a pair come from the
+// neighbouring lanes).  Same arithmetic, same order as column_sweep.
+__device__ __forceinline__ float2 ld2(const __nv_bfloat16* p, int i) {
+    return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p + i));
+}
+__global__ void __launch_bounds__(MG_THREADS) k_mg_smooth2(MgLevel L, const __nv_bfloat16* __restrict__ ein,
+                                                           __nv_bfloat16* __restrict__ eout,
+                                                           const __nv_bfloat16* __restrict__ b, double alpha_d,
+                                                           double beta_d, int read_prev) {
+    const int pi = blockIdx.x * MG_BX + threadIdx.x;  // pair index along x
+    const int i0 = 2 * pi;
+    const int j = blockIdx.y * MG_BY + threadIdx.y;
+    const int k0 = blockIdx.z * L.kc;
+    const int k1 = min(L.nz, k0 + L.kc);
+    const bool act = i0 < L.nx && j < L.ny;
+    const int ic = act ? i0 : 0, jc = j < L.ny ? j : 0;  // inactive lanes read a valid pair
+    const int plane = L.nx * L.ny;
+    const float alpha = (float)alpha_d, beta = (float)beta_d;
+    const float ax = (float)L.ax, ay = (float)L.ay, az = (float)L.az;
+    const int nby = nb_count(jc, L.ny) * 3;
+    const int nb0 = nb_count(ic, L.nx) * 9 + nby, nb1 = nb_count(ic + 1, L.nx) * 9 + nby;
+    int c = (k0 * L.ny + jc) * L.nx + ic;
+    float2 em = k0 > 0 ? ld2(ein, c - plane) : make_float2(0.0f, 0.0f);
+    float2 ec = ld2(ein, c);
+    for (int k = k0; k < k1; ++k, c += plane) {
+        const float2 ep = k + 1 < L.nz ? ld2(ein, c + plane) : make_float2(0.0f, 0.0f);
+        float w = __shfl_up_sync(0xffffffffu, ec.y, 1);    // e(i0 - 1)
+        float e2 = __shfl_down_sync(0xffffffffu, ec.x, 1); // e(i0 + 2)
+        if (threadIdx.x == 0 && ic > 0) w = __bfloat162float(ein[c - 1]);
+        if (threadIdx.x == MG_BX - 1 && ic + 2 < L.nx) e2 = __bfloat162float(ein[c + 2]);
+        const float2 sv = jc > 0 ? ld2(ein, c - L.nx) : make_float2(0.0f, 0.0f);
+        const float2 nv = jc < L.ny - 1 ? ld2(ein, c + L.nx) : make_float2(0.0f, 0.0f);
+        const float2 bv = ld2(b, c);
+        const float2 xp = read_prev ? ld2(eout, c) : make_float2(0.0f, 0.0f);
+        // cell i0: x- (if i0 > 0), x+ (= i0 + 1, always inside: nx even)
+        float s0 = 0.0f;
+        if (ic > 0) s0 += ax * (w - ec.x);
+        s0 += ax * (ec.y - ec.x);
+        if (jc > 0) s0 += ay * (sv.x - ec.x);
+        if (jc < L.ny - 1) s0 += ay * (nv.x - ec.x);
+        float z0 = 0.0f;
+        if (k > 0) z0 += az * (em.x - ec.x);
+        if (k < L.nz - 1) z0 += az * (ep.x - ec.x);
+        // cell i0 + 1: x- (= i0, always), x+ (if i0 + 2 < nx)
+        float s1 = 0.0f;
+        s1 += ax * (ec.x - ec.y);
+        if (ic + 2 < L.nx) s1 += ax * (e2 - ec.y);
+        if (jc > 0) s1 += ay * (sv.y - ec.y);
+        if (jc < L.ny - 1) s1 += ay * (nv.y - ec.y);
+        float z1 = 0.0f;
+        if (k > 0) z1 += az * (em.y - ec.y);
+        if (k < L.nz - 1) z1 += az * (ep.y - ec.y);
+        const int nbz = nb_count(k, L.nz);
+        const float o0 = ec.x + alpha * (ec.x - xp.x) + beta * (float)L.idg[nb0 + nbz] * (bv.x - 0.0f - (s0 + z0));
+        const float o1 = ec.y + alpha * (ec.y - xp.y) + beta * (float)L.idg[nb1 + nbz] * (bv.y - 0.0f - (s1 + z1));
+        if (act) *reinterpret_cast<__nv_bfloat162*>(eout + c) = __floats2bfloat162_rn(o0, o1);
+        em = ec;
+        ec = ep;
+    }
+}
+
 // Coarse right-hand side = average of the fine residual over each coarse
 // cell; ec (optional) = the first smoothing step from zero at the coarse level.
 template <typename S>
@@ -836,6 +898,21 @@ static void* final_buffer(const MgSolver& m, int l) {
     return L.e1;
 }
 
+// One smoothing step of a multi-block level: the paired BF16 kernel on levels
+// of even width, the generic one otherwise.
+template <typename S>
+static void smooth(const MgLevel& L, const S* ein, S* eout, const S* b, double ca, double cb, bool read_prev,
+                   cudaStream_t s) {
+    if constexpr (sizeof(S) == 2) {
+        if ((L.nx & 1) == 0) {
+            const dim3 g2((L.nx / 2 + MG_BX - 1) / MG_BX, L.gy, L.gz);
+            k_mg_smooth2<<<g2, kBlock, 0, s>>>(L, ein, eout, b, ca, cb, read_prev ? 1 : 0);
+            return;
+        }
+    }
+    k_mg_smooth<S><<<grid_of(L), kBlock, 0, s>>>(L, ein, eout, b, nullptr, ca, cb, read_prev);
+}
+
 // A level above the one-block tail that is smoothed by multi-block kernels.
 static bool multi(const MgSolver& m, int l) { return l < m.tail && l < m.nlev - 1; }
 
@@ -850,7 +927,7 @@ static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t 
         const S* b = static_cast<const S*>(L.b);
         int cur = 0;  // the first step (from zero) was written together with b
         for (int q = 1; q < L.nu; ++q, cur ^= 1, ++launches)
-            k_mg_smooth<S><<<grid_of(L), kBlock, 0, s>>>(L, e[cur], e[cur ^ 1], b, nullptr, L.ca[q], L.cb[q], q >= 2);
+            smooth<S>(L, e[cur], e[cur ^ 1], b, L.ca[q], L.cb[q], q >= 2, s);
         const MgLevel& Cl = m.lv[l + 1];
         S* ec = multi(m, l + 1) ? static_cast<S*>(Cl.e0) : nullptr;
         if (L.rx * L.ry * L.rz > 8)
@@ -890,8 +967,7 @@ static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t 
                 k_smooth_update<S><<<grid_of(L), kBlock, 0, s>>>(g, L, e[cur], e[cur ^ 1], b, p64, L.ca[q], L.cb[q],
                                                                  q >= 1);
             else
-                k_mg_smooth<S><<<grid_of(L), kBlock, 0, s>>>(L, e[cur], e[cur ^ 1], b, nullptr, L.ca[q], L.cb[q],
-                                                             q >= 1);
+                smooth<S>(L, e[cur], e[cur ^ 1], b, L.ca[q], L.cb[q], q >= 1, s);
         }
     }
     if (l == 0) {  // the fine level was solved by the tail or as the coarsest level
