@@ -327,6 +327,280 @@ __global__ void __launch_bounds__(256) k_as0(Geom g, Range R, const float* __res
     lF[c] = acc;
 }
 
+// ---- the whole sweep adjoint in one kernel, LPB lines per block in shared memory ----
+// The same quantities as k_fs1..3 and k_as4..0, staged per line in shared
+// memory (positions 0 .. n+1 of LPB lines), one phase per __syncthreads: load,
+// the three forward stages (the forward's expressions), stage 4's adjoint,
+// the limiter and stage 2's ratios, stage 2's extrema and stage 1, the faces,
+// F.  Global traffic: F, vel and lF read once, lF and lvel written once.
+// Thread mapping: DIR 0 (x lines): a line's positions run over consecutive
+// threads (coalesced along x); DIR 1/2: LPB x-adjacent lines per block, the
+// line index fastest (LPB consecutive floats per position).
+constexpr int FA_THREADS = 256;
+__host__ __device__ __forceinline__ size_t fa_smem_bytes(int lpb, int n) {
+    const size_t m = (size_t)lpb * (n + 2);
+    return m * (7 * sizeof(double) + 7 * sizeof(float) + 1);
+}
+template <int DIR, int LPB>
+__global__ void __launch_bounds__(FA_THREADS) k_fct_adjoint(Geom g, const float* __restrict__ Fg,
+                                                            const float* __restrict__ velg, double* __restrict__ lFg,
+                                                            double* __restrict__ lvelg) {
+    extern __shared__ __align__(16) unsigned char fa_smem[];
+    const int n = slen<DIR>(g), N2 = n + 2, M = LPB * N2;
+    double* sLX = reinterpret_cast<double*>(fa_smem);
+    double* sLdv = sLX + M;
+    double* sLmx = sLdv + M;   // later: the adjoint of the low-order flux at each face
+    double* sLmn = sLmx + M;   // later: the adjoint of A at each face
+    double* sLpp = sLmn + M;
+    double* sLpm = sLpp + M;
+    double* sLown = sLpm + M;  // later (P6, in place): lterm
+    double* sLterm = sLown;
+    float* sF = reinterpret_cast<float*>(sLown + M);
+    float* sV = sF + M;
+    float* sFtd = sV + M;
+    float* sA = sFtd + M;
+    float* sRp = sA + M;
+    float* sRm = sRp + M;
+    float* sC = sRm + M;
+    unsigned char* sSel = reinterpret_cast<unsigned char*>(sC + M);
+
+    constexpr int TPL = FA_THREADS / LPB;  // threads per line
+    const int tid = threadIdx.x;
+    const int l = DIR == 0 ? tid / TPL : tid % LPB;
+    const int p0 = DIR == 0 ? tid % TPL : tid / LPB;
+    // this thread's line: global base (position 0) and stride along the axis
+    int base, gs;
+    bool act;
+    if (DIR == 0) {
+        const int j = 1 + blockIdx.x * LPB + l, k = 1 + blockIdx.y;
+        act = j <= g.ny;
+        base = gidx(g, 0, act ? j : 1, k);
+        gs = 1;
+    } else if (DIR == 1) {
+        const int i = 1 + blockIdx.x * LPB + l, k = 1 + blockIdx.y;
+        act = i <= g.nx;
+        base = gidx(g, act ? i : 1, 0, k);
+        gs = g.px;
+    } else {
+        const int i = 1 + blockIdx.x * LPB + l, j = 1 + blockIdx.y;
+        act = i <= g.nx;
+        base = gidx(g, act ? i : 1, j, 0);
+        gs = g.plane;
+    }
+    auto si = [&](int q) { return DIR == 0 ? l * N2 + q : q * LPB + l; };
+    const float vol = g.dx * g.dy * g.dz;
+    const float dvfac = dvfac_of<DIR>(g);
+    const float K4 = DIR == 2 ? g.dz : g.dy;
+    const float hqf = DIR == 2 ? g.dz : g.dx;
+    const double vold = (double)vol, dt = (double)g.dt, iK4 = 1.0 / (double)K4, hq = (double)hqf;
+    const double K1 = DIR == 0 ? (double)g.dy * g.dz / vold
+                               : (DIR == 1 ? (double)g.dy / ((double)g.dx * g.dy) : (double)g.dy * g.dx / vold);
+
+    // P0: load
+    if (act)
+        for (int q = p0; q < N2; q += TPL) {
+            const int c = base + q * gs;
+            sF[si(q)] = Fg[c];
+            sV[si(q)] = q >= 1 ? velg[c] : 0.0f;
+        }
+    __syncthreads();
+    // P1: stage 1 (Ftd; 0 at the ghosts)
+    if (act)
+        for (int q = p0; q < N2; q += TPL) {
+            if (q == 0 || q == n + 1) {
+                sFtd[si(q)] = 0.0f;
+                continue;
+            }
+            const float vl = sV[si(q)], vh = sV[si(q + 1)];
+            const float dv = vol - dvfac * (vh - vl);
+            const float f_in = (vl >= 0.0f) ? vl * g.dt * sF[si(q - 1)] : vl * g.dt * sF[si(q)];
+            const float f_out = (vh >= 0.0f) ? vh * g.dt * sF[si(q)] : vh * g.dt * sF[si(q + 1)];
+            float term;
+            if (DIR == 0) term = (f_in - f_out) * g.dy * g.dz / vol;
+            else if (DIR == 1) term = (f_in - f_out) * g.dy / (g.dx * g.dy);
+            else term = (f_in - f_out) * g.dy * g.dx / vol;
+            float out = (sF[si(q)] + term) * vol / dv;
+            if (out > 1.0f || out < 0.0f) out = clamp01f(out);
+            sFtd[si(q)] = out;
+        }
+    __syncthreads();
+    // P2: stage 2 (A at the lower face of every cell and the last upper face; rp, rm)
+    if (act)
+        for (int q = p0; q < N2; q += TPL) {
+            if (q == 0 || q == n + 1) {
+                sRp[si(q)] = 0.0f;
+                sRm[si(q)] = 0.0f;
+                continue;
+            }
+            const float vl = sV[si(q)], vh = sV[si(q + 1)];
+            const float Fm = sF[si(q - 1)], Fc = sF[si(q)], Fp = sF[si(q + 1)];
+            const float a1 = ((vh <= 0.0f) ? vh * g.dt * Fc : vh * g.dt * Fp) -
+                             ((vh >= 0.0f) ? vh * g.dt * Fc : vh * g.dt * Fp);
+            const float a0 = ((vl <= 0.0f) ? vl * g.dt * Fm : vl * g.dt * Fc) -
+                             ((vl >= 0.0f) ? vl * g.dt * Fm : vl * g.dt * Fc);
+            sA[si(q)] = a0;
+            if (q == n) sA[si(q + 1)] = a1;
+            const float pp = fmaxf(0.0f, a0) - fminf(0.0f, a1);
+            const float pm = fmaxf(0.0f, a1) - fminf(0.0f, a0);
+            const float fc = sFtd[si(q)], fl = sFtd[si(q - 1)], fh = sFtd[si(q + 1)];
+            const float fmx = fmaxf(fc, fmaxf(fl, fh));
+            const float fmn = fminf(fc, fminf(fl, fh));
+            const float qp = (fmx - fc) * hqf;
+            sRp[si(q)] = (pp > 0.0f) ? fminf(1.0f, qp / pp) : 0.0f;
+            const float qm = (fc - fmn) * hqf;
+            sRm[si(q)] = (pm > 0.0f) ? fminf(1.0f, qm / pm) : 0.0f;
+        }
+    __syncthreads();
+    // P3: stage 3 (C at the upper face of every cell; 0 at the first face)
+    if (act)
+        for (int q = p0; q < N2; q += TPL) {
+            if (q == 0 || q == n + 1) continue;
+            const int f = q + 1;
+            sC[si(f)] = (sA[si(f)] >= 0.0f) ? fminf(sRp[si(f)], sRm[si(q)]) : fminf(sRp[si(q)], sRm[si(f)]);
+            if (q == 1) sC[si(1)] = 0.0f;
+        }
+    __syncthreads();
+    // P4: stage 4 reversed: g4, lX, the stage-4 part of ldv
+    if (act)
+        for (int q = p0; q < N2; q += TPL) {
+            if (q == 0 || q == n + 1) {
+                sLX[si(q)] = 0.0;
+                continue;
+            }
+            const float dv = vol - dvfac * (sV[si(q + 1)] - sV[si(q)]);
+            const float a0 = sA[si(q)], a1 = sA[si(q + 1)], c0 = sC[si(q)], c1 = sC[si(q + 1)];
+            const float out = sFtd[si(q)] - ((a1 * c1 - a0 * c0) / K4) * vol / dv;
+            const double g4 = (out >= 0.0f && out <= 1.0f) ? lFg[base + q * gs] : 0.0;
+            const double idv = 1.0 / (double)dv;
+            const double X = ((double)a1 * c1 - (double)a0 * c0) * iK4;
+            sLX[si(q)] = -g4 * vold * idv;
+            sLdv[si(q)] = g4 * X * vold * idv * idv;
+            sLown[si(q)] = g4;
+        }
+    __syncthreads();
+    // P5: limiter (stage 3) and limiter ratios (stage 2) reversed
+    if (act)
+        for (int q = p0; q < N2; q += TPL) {
+            if (q == 0 || q == n + 1) continue;
+            const double lXc = sLX[si(q)], lXm = sLX[si(q - 1)], lXp = sLX[si(q + 1)];
+            const float a0 = sA[si(q)], a1 = sA[si(q + 1)];
+            const double lC_hi = (lXc - lXp) * (double)a1 * iK4;
+            const double lC_lo = q >= 2 ? (lXm - lXc) * (double)a0 * iK4 : 0.0;
+            double lrp = 0.0, lrm = 0.0;
+            if (q >= 2) {
+                if (a0 >= 0.0f) {
+                    if (sRp[si(q)] <= sRm[si(q - 1)]) lrp += lC_lo;
+                } else {
+                    if (!(sRp[si(q - 1)] <= sRm[si(q)])) lrm += lC_lo;
+                }
+            }
+            if (a1 >= 0.0f) {
+                if (!(sRp[si(q + 1)] <= sRm[si(q)])) lrm += lC_hi;
+            } else {
+                if (sRp[si(q)] <= sRm[si(q + 1)]) lrp += lC_hi;
+            }
+            const float pp = fmaxf(0.0f, a0) - fminf(0.0f, a1);
+            const float pm = fmaxf(0.0f, a1) - fminf(0.0f, a0);
+            const float fc = sFtd[si(q)], fl = sFtd[si(q - 1)], fh = sFtd[si(q + 1)];
+            double lqp = 0.0, lqm = 0.0, dpp = 0.0, dpm = 0.0;
+            if (lrp != 0.0) {
+                const float qp = (fmaxf(fc, fmaxf(fl, fh)) - fc) * hqf;
+                if (pp > 0.0f && qp / pp < 1.0f) {
+                    const double ip = 1.0 / (double)pp;
+                    lqp = lrp * ip;
+                    dpp = -lqp * (double)qp * ip;
+                }
+            }
+            if (lrm != 0.0) {
+                const float qm = (fc - fminf(fc, fminf(fl, fh))) * hqf;
+                if (pm > 0.0f && qm / pm < 1.0f) {
+                    const double ip = 1.0 / (double)pm;
+                    lqm = lrm * ip;
+                    dpm = -lqm * (double)qm * ip;
+                }
+            }
+            const int in_mx = (fl >= fh) ? 0 : 2;
+            const int smx = (fc >= (in_mx == 0 ? fl : fh)) ? 1 : in_mx;
+            const int in_mn = (fl <= fh) ? 0 : 2;
+            const int smn = (fc <= (in_mn == 0 ? fl : fh)) ? 1 : in_mn;
+            sLmx[si(q)] = lqp * hq;
+            sLmn[si(q)] = -lqm * hq;
+            sSel[si(q)] = (unsigned char)(smx | (smn << 2));
+            sLpp[si(q)] = dpp;
+            sLpm[si(q)] = dpm;
+            sLown[si(q)] += -lqp * hq + lqm * hq;
+        }
+    __syncthreads();
+    // P6: the adjoint of Ftd (own terms and the neighbours' extrema), stage 1 reversed
+    if (act)
+        for (int q = p0; q < N2; q += TPL) {
+            if (q == 0 || q == n + 1) {
+                sLterm[si(q)] = 0.0;  // (sLown of a ghost is never read)
+                continue;
+            }
+            double lFtd = sLown[si(q)];
+            for (int d = -1; d <= 1; ++d) {
+                const int e = q + d;
+                if (e < 1 || e > n) continue;
+                const int sb = sSel[si(e)];
+                const int want = 1 - d;
+                if ((sb & 3) == want) lFtd += sLmx[si(e)];
+                if ((sb >> 2) == want) lFtd += sLmn[si(e)];
+            }
+            const float vl = sV[si(q)], vh = sV[si(q + 1)];
+            const float dv = vol - dvfac * (vh - vl);
+            const float f_in = (vl >= 0.0f) ? vl * g.dt * sF[si(q - 1)] : vl * g.dt * sF[si(q)];
+            const float f_out = (vh >= 0.0f) ? vh * g.dt * sF[si(q)] : vh * g.dt * sF[si(q + 1)];
+            float term;
+            if (DIR == 0) term = (f_in - f_out) * g.dy * g.dz / vol;
+            else if (DIR == 1) term = (f_in - f_out) * g.dy / (g.dx * g.dy);
+            else term = (f_in - f_out) * g.dy * g.dx / vol;
+            const float out = (sF[si(q)] + term) * vol / dv;
+            const double h = (out > 1.0f || out < 0.0f) ? 0.0 : lFtd;
+            const double dvd = (double)dv;
+            sLterm[si(q)] = h * vold / dvd;
+            sLdv[si(q)] -= h * ((double)sF[si(q)] + (double)term) * vold / (dvd * dvd);
+        }
+    __syncthreads();
+    // P7: faces 1 .. n+1 (the lower face of position q): LF and A reversed, the face velocity
+    if (act)
+        for (int q = p0; q < N2; q += TPL) {
+            if (q == 0) continue;
+            const bool lo = q >= 2, hi = q <= n;
+            const float a = sA[si(q)];
+            const double l_LF = K1 * ((hi ? sLterm[si(q)] : 0.0) - (lo ? sLterm[si(q - 1)] : 0.0));
+            double l_A = ((lo ? sLX[si(q - 1)] : 0.0) - (hi ? sLX[si(q)] : 0.0)) * (double)sC[si(q)] * iK4;
+            if (hi) l_A += (a > 0.0f ? sLpp[si(q)] : 0.0) - (a < 0.0f ? sLpm[si(q)] : 0.0);
+            if (lo) l_A += -(a < 0.0f ? sLpp[si(q - 1)] : 0.0) + (a > 0.0f ? sLpm[si(q - 1)] : 0.0);
+            const float uf = sV[si(q)];
+            const float Fh = (uf <= 0.0f) ? sF[si(q - 1)] : sF[si(q)];
+            const float Fl = (uf >= 0.0f) ? sF[si(q - 1)] : sF[si(q)];
+            lvelg[base + q * gs] += l_LF * dt * (double)Fl + l_A * dt * ((double)Fh - (double)Fl) +
+                                    (double)dvfac * ((hi ? sLdv[si(q)] : 0.0) - (lo ? sLdv[si(q - 1)] : 0.0));
+            sLmx[si(q)] = l_LF;  // the extremum adjoints were last read in P6
+            sLmn[si(q)] = l_A;
+        }
+    __syncthreads();
+    // P8: the adjoint of the sweep's input F (ghosts keep theirs)
+    if (act)
+        for (int q = p0; q < N2; q += TPL) {
+            double acc = (q >= 1 && q <= n) ? sLterm[si(q)] : lFg[base + q * gs];
+            if (q >= 1) {  // face q: this cell is its upper cell
+                const float uf = sV[si(q)];
+                const double w = (double)uf * dt;
+                if (uf < 0.0f) acc += sLmx[si(q)] * w;
+                acc += sLmn[si(q)] * w * ((uf > 0.0f ? 1.0 : 0.0) - (uf < 0.0f ? 1.0 : 0.0));
+            }
+            if (q <= n) {  // face q + 1: this cell is its lower cell
+                const float uf = sV[si(q + 1)];
+                const double w = (double)uf * dt;
+                if (uf >= 0.0f) acc += sLmx[si(q + 1)] * w;
+                acc += sLmn[si(q + 1)] * w * ((uf <= 0.0f ? 1.0 : 0.0) - (uf >= 0.0f ? 1.0 : 0.0));
+            }
+            lFg[base + q * gs] = acc;
+        }
+}
+
 // ---- boundary copies, reversed ---------------------------------------------------
 __global__ void k_adj_bcF_z(Geom g, double* __restrict__ l) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -693,9 +967,46 @@ inline Range axis_range(const Geom& g, int dir, int lo, int hi_extra) {
     return r;
 }
 
+template <int DIR, int LPB>
+cudaError_t launch_fct_adjoint(const Geom& g, const float* Fs, const float* vel, double* lF, double* lvel,
+                               cudaStream_t s) {
+    const int n = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
+    const size_t smem = fa_smem_bytes(LPB, n);
+    cudaError_t r = cudaFuncSetAttribute(k_fct_adjoint<DIR, LPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (r != cudaSuccess) return r;
+    dim3 grid;
+    if (DIR == 0) grid = dim3((g.ny + LPB - 1) / LPB, g.nz);
+    else if (DIR == 1) grid = dim3((g.nx + LPB - 1) / LPB, g.nz);
+    else grid = dim3((g.nx + LPB - 1) / LPB, g.ny);
+    k_fct_adjoint<DIR, LPB><<<grid, FA_THREADS, smem, s>>>(g, Fs, vel, lF, lvel);
+    return cudaGetLastError();
+}
+
+// Largest shared memory one block may take.
+size_t fa_smem_limit() {
+    static size_t lim = 0;
+    if (!lim) {
+        int dev = 0, v = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess)
+            lim = (size_t)v;
+    }
+    return lim;
+}
+
 template <int DIR>
 cudaError_t sweep_adjoint(AdjEngine& e, const float* Fs, const float* vel, double* lvel, cudaStream_t s) {
     const Geom& g = e.g;
+    {  // one fused kernel when a block of lines fits in shared memory
+        const int n = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
+        // the most lines per block with at least two blocks per SM, else the most that fit
+        const size_t lim = fa_smem_limit(), two = lim / 2 - 1024;
+        if (fa_smem_bytes(8, n) <= two) return launch_fct_adjoint<DIR, 8>(g, Fs, vel, e.lF, lvel, s);
+        if (fa_smem_bytes(4, n) <= two) return launch_fct_adjoint<DIR, 4>(g, Fs, vel, e.lF, lvel, s);
+        if (fa_smem_bytes(2, n) <= two) return launch_fct_adjoint<DIR, 2>(g, Fs, vel, e.lF, lvel, s);
+        if (fa_smem_bytes(2, n) <= lim) return launch_fct_adjoint<DIR, 2>(g, Fs, vel, e.lF, lvel, s);
+    }
     const Range I = interior(g);
     const dim3 gi = grid_of(I);
     k_fs1<DIR><<<gi, kBlk, 0, s>>>(g, I, Fs, vel, e.Ftd);
