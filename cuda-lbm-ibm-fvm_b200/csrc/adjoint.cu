@@ -1032,7 +1032,24 @@ cudaError_t load_state(AdjEngine& e, const AdjState& x, cudaStream_t s) {
     cudaError_t r;
     for (int q = 0; q < 5; ++q)
         if ((r = copy_field(dst[q], x.f[q], e.elems, s)) != cudaSuccess) return r;
+    if (e.conv)
+        return cudaMemcpyAsync(e.p64, x.p64, e.elems * sizeof(double), cudaMemcpyDeviceToDevice, s);
     return cudaSuccess;
+}
+
+// The pressure of the step whose predictor and rhs are in e.wb: the plain
+// Jacobi sweeps, or the convergent solve warm-started from e.p64 (the same
+// call the forward made, so the same bits).  Returns the FP32 pressure.
+cudaError_t step_pressure(AdjEngine& e, const float** pafter, cudaStream_t s) {
+    if (e.conv) {
+        cudaError_t r = mg_solve(e.g, e.mg_fwd, e.wb.rhs, e.p64, e.wb.p0, e.tol, e.max_outer, nullptr, s, e.cap);
+        *pafter = e.wb.p0;
+        return r == cudaErrorNotReady ? cudaSuccess : r;  // the forward took the same unconverged iterate
+    }
+    int par = 0;
+    cudaError_t r = plain_pressure(e.g, e.wb, e.jacobi_iters, &par, s);
+    *pafter = par ? e.wb.p1 : e.wb.p0;
+    return r;
 }
 
 // One reversed step from its start state x.
@@ -1042,9 +1059,8 @@ cudaError_t adjoint_step(AdjEngine& e, const AdjState& x, int istep, cudaStream_
     // recompute
     if ((r = load_state(e, x, s)) != cudaSuccess) return r;
     if ((r = plain_front(g, e.wb, s)) != cudaSuccess) return r;
-    int par = 0;
-    if ((r = plain_pressure(g, e.wb, e.jacobi_iters, &par, s)) != cudaSuccess) return r;
-    const float* pafter = par ? e.wb.p1 : e.wb.p0;
+    const float* pafter = nullptr;
+    if ((r = step_pressure(e, &pafter, s)) != cudaSuccess) return r;
     if ((r = plain_correct(g, e.wb, pafter, s)) != cudaSuccess) return r;
     const int rr = ((istep % 3) + 3) % 3;
     static const int order[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
@@ -1083,8 +1099,15 @@ cudaError_t adjoint_step(AdjEngine& e, const AdjState& x, int istep, cudaStream_
     const dim3 gi = grid_of(I);
     k_adj_update<<<gi, kBlk, 0, s>>>(g, I, x.f[0], pafter, e.lu, e.lv, e.lw, e.lus, e.lvs, e.lws, e.lp[e.lp_cur],
                                      e.lrho);
-    // Jacobi transposed (on mu = lambda / ap), then rhs
-    if (e.jacobi_iters > 0) {
+    // the pressure solve reversed: convergent modes -- lrhs = the mean-free
+    // solution of A mu = lp - mean(lp) (warm start: the previous step's), and
+    // the state pressure (only a warm start) gets no adjoint; plain -- the
+    // Jacobi sweeps transposed (on mu = lambda / ap)
+    if (e.conv) {
+        r = mg_solve64(g, e.mg_adj, e.lp[e.lp_cur], e.lrhs, e.tol, e.max_outer, nullptr, s, e.cap);
+        if (r != cudaSuccess) return r;
+        if ((r = cudaMemsetAsync(e.lp[e.lp_cur], 0, e.elems * sizeof(double), s)) != cudaSuccess) return r;
+    } else if (e.jacobi_iters > 0) {
         k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.inv_ap, e.lp[e.lp_cur], e.lp[e.lp_cur ^ 1], e.lrhs, 0);
         e.lp_cur ^= 1;
         for (int it = 1; it < e.jacobi_iters; ++it) {
@@ -1095,7 +1118,7 @@ cudaError_t adjoint_step(AdjEngine& e, const AdjState& x, int istep, cudaStream_
         e.lp_cur ^= 1;
     }
     k_adj_rhs<<<gi, kBlk, 0, s>>>(g, I, x.f[0], e.wb.us, e.wb.vs, e.wb.ws, e.lrhs, e.lus, e.lvs, e.lws, e.lrho, e.lu,
-                                  e.lv, e.lw, e.jacobi_iters > 0);
+                                  e.lv, e.lw, e.conv || e.jacobi_iters > 0);
     // advection with rho and nu
     k_adj_advect<<<gi, kBlk, 0, s>>>(g, I, x.f[0], x.f[1], x.f[2], x.f[3], e.lus, e.lvs, e.lws, e.lu, e.lv, e.lw,
                                      e.lrho, e.lF, e.d_partial);
@@ -1112,10 +1135,14 @@ int adj_kernels_per_step(const AdjEngine& e) {
            (e.jacobi_iters > 0 ? e.jacobi_iters + 1 : 0) + 1 + 1;
 }
 
-cudaError_t adj_create(const Geom& g, int jacobi_iters, AdjEngine* e, cudaStream_t s) {
+cudaError_t adj_create(const Geom& g, int jacobi_iters, int mg_mode, double tol, int max_outer, AdjEngine* e,
+                       cudaStream_t s) {
     *e = AdjEngine{};
     e->g = g;
     e->jacobi_iters = jacobi_iters;
+    e->conv = mg_mode != 0;
+    e->tol = tol;
+    e->max_outer = max_outer;
     e->elems = (size_t)g.plane * (g.nz + 2);
     cudaError_t r;
     auto alloc = [&](void** p, size_t nb) -> cudaError_t {
@@ -1163,6 +1190,15 @@ cudaError_t adj_create(const Geom& g, int jacobi_iters, AdjEngine* e, cudaStream
     const float* mapped[4] = {e->wb.p0, e->wb.p1, e->wb.p2, e->wb.rhs};
     for (int q = 0; q < 4; ++q)
         if ((r = jacobi_tb_maps(g, mapped[q], &e->maps[q])) != cudaSuccess) return r;
+    if (e->conv) {
+        if ((r = alloc((void**)&e->p64, db)) != cudaSuccess) return r;
+        if ((r = mg_create(g, mg_mode, &e->mg_fwd, s, &e->bytes)) != cudaSuccess) return r;
+        if ((r = mg_create(g, mg_mode, &e->mg_adj, s, &e->bytes)) != cudaSuccess) return r;
+        if ((r = cudaStreamCreateWithFlags(&e->cap, cudaStreamNonBlocking)) != cudaSuccess) {
+            e->cap = nullptr;
+            return r;
+        }
+    }
     e->wb.maps = e->maps;
     e->wb.status = e->status;
     return cudaStreamSynchronize(s);
@@ -1170,9 +1206,11 @@ cudaError_t adj_create(const Geom& g, int jacobi_iters, AdjEngine* e, cudaStream
 
 static void free_states(AdjState* st, int n) {
     if (!st) return;
-    for (int m = 0; m < n; ++m)
+    for (int m = 0; m < n; ++m) {
         for (int q = 0; q < 5; ++q)
             if (st[m].f[q]) cudaFree(st[m].f[q]);
+        if (st[m].p64) cudaFree(st[m].p64);
+    }
     delete[] st;
 }
 
@@ -1190,16 +1228,24 @@ void adj_destroy(AdjEngine* e) {
         if (p) cudaFree(p);
     if (e->sel) cudaFree(e->sel);
     if (e->status) cudaFree(e->status);
+    if (e->p64) cudaFree(e->p64);
+    if (e->conv) {
+        mg_destroy(&e->mg_fwd);
+        mg_destroy(&e->mg_adj);
+    }
+    if (e->cap) cudaStreamDestroy(e->cap);
     if (e->h_sums) cudaFreeHost(e->h_sums);
     *e = AdjEngine{};
 }
 
-static cudaError_t alloc_states(AdjState*& st, int n, size_t elems, size_t* bytes) {
+static cudaError_t alloc_states(AdjState*& st, int n, size_t elems, bool with_p64, size_t* bytes) {
     st = new (std::nothrow) AdjState[n];
     if (!st) return cudaErrorMemoryAllocation;
-    for (int m = 0; m < n; ++m)
+    for (int m = 0; m < n; ++m) {
         for (int q = 0; q < 5; ++q) st[m].f[q] = nullptr;
-    for (int m = 0; m < n; ++m)
+        st[m].p64 = nullptr;
+    }
+    for (int m = 0; m < n; ++m) {
         for (int q = 0; q < 5; ++q) {
             cudaError_t r = cudaMalloc((void**)&st[m].f[q], elems * sizeof(float));
             if (r != cudaSuccess) {
@@ -1208,6 +1254,15 @@ static cudaError_t alloc_states(AdjState*& st, int n, size_t elems, size_t* byte
             }
             *bytes += elems * sizeof(float);
         }
+        if (with_p64) {
+            cudaError_t r = cudaMalloc((void**)&st[m].p64, elems * sizeof(double));
+            if (r != cudaSuccess) {
+                st[m].p64 = nullptr;
+                return r;
+            }
+            *bytes += elems * sizeof(double);
+        }
+    }
     return cudaSuccess;
 }
 
@@ -1228,8 +1283,8 @@ cudaError_t adj_tape(AdjEngine* e, int istep0, int nsteps, int every, cudaStream
     if (!e->cp && ncp > 0) {
         e->ncp = ncp;
         e->every = every;
-        if ((r = alloc_states(e->cp, ncp, e->elems, &e->bytes)) != cudaSuccess) return r;
-        if ((r = alloc_states(e->seg, every, e->elems, &e->bytes)) != cudaSuccess) return r;
+        if ((r = alloc_states(e->cp, ncp, e->elems, e->conv, &e->bytes)) != cudaSuccess) return r;
+        if ((r = alloc_states(e->seg, every, e->elems, e->conv, &e->bytes)) != cudaSuccess) return r;
     }
     e->istep0 = istep0;
     e->nsteps = nsteps;
@@ -1244,6 +1299,8 @@ cudaError_t adj_save(AdjEngine* e, int m, const AdjState& x, cudaStream_t s) {
     cudaError_t r;
     for (int q = 0; q < 5; ++q)
         if ((r = copy_field(e->cp[m].f[q], x.f[q], e->elems, s)) != cudaSuccess) return r;
+    if (e->conv)
+        return cudaMemcpyAsync(e->cp[m].p64, x.p64, e->elems * sizeof(double), cudaMemcpyDeviceToDevice, s);
     return cudaSuccess;
 }
 
@@ -1252,7 +1309,7 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
     const Geom& g = e->g;
     cudaError_t r;
     // seed and loss
-    double* zero[] = {e->lu, e->lv, e->lw, e->lp[0], e->lp[1], e->lrho};
+    double* zero[] = {e->lu, e->lv, e->lw, e->lp[0], e->lp[1], e->lrho, e->lrhs};
     for (double* p : zero)
         if ((r = cudaMemsetAsync(p, 0, e->elems * sizeof(double), s)) != cudaSuccess) return r;
     if ((r = cudaMemsetAsync(e->d_sums, 0, 4 * sizeof(double), s)) != cudaSuccess) return r;
@@ -1274,15 +1331,28 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
         // the segment's states: checkpoint m, then count - 1 steps with the engine's buffers
         for (int q = 0; q < 5; ++q)
             if ((r = copy_field(e->seg[0].f[q], e->cp[m].f[q], e->elems, s)) != cudaSuccess) return r;
+        if (e->conv && (r = cudaMemcpyAsync(e->seg[0].p64, e->cp[m].p64, e->elems * sizeof(double),
+                                            cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+            return r;
         if (count > 1) {
             if ((r = load_state(*e, e->seg[0], s)) != cudaSuccess) return r;
             int par = 0;
             for (int q = 1; q < count; ++q) {
-                if ((r = plain_step(g, e->wb, e->istep0 + first + q - 1, e->jacobi_iters, &par, s)) != cudaSuccess)
+                const int istep = e->istep0 + first + q - 1;
+                if (e->conv) {
+                    const float* pa = nullptr;
+                    if ((r = plain_front(g, e->wb, s)) != cudaSuccess || (r = step_pressure(*e, &pa, s)) != cudaSuccess ||
+                        (r = plain_back(g, e->wb, istep, pa, s)) != cudaSuccess)
+                        return r;
+                } else if ((r = plain_step(g, e->wb, istep, e->jacobi_iters, &par, s)) != cudaSuccess) {
                     return r;
+                }
                 const float* src[5] = {e->wb.F, e->wb.u, e->wb.v, e->wb.w, par ? e->wb.p1 : e->wb.p0};
                 for (int t = 0; t < 5; ++t)
                     if ((r = copy_field(e->seg[q].f[t], src[t], e->elems, s)) != cudaSuccess) return r;
+                if (e->conv && (r = cudaMemcpyAsync(e->seg[q].p64, e->p64, e->elems * sizeof(double),
+                                                    cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+                    return r;
             }
         }
         for (int q = count - 1; q >= 0; --q)

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+#include "mg_solve.h"
 #include "plain_step.h"
 #include "vof_device.cuh"
 
@@ -15,9 +16,11 @@ struct InvAp {
     double v[64];
 };
 
-// One state of the step: F, u, v, w, p in the padded layout (FP32).
+// One state of the step: F, u, v, w, p in the padded layout (FP32), and in
+// the convergent modes the FP64 pressure the next solve starts from.
 struct AdjState {
     float* f[5];
+    double* p64;
 };
 
 // The device side of vof_forward_record / vof_backward.  Forward: the
@@ -31,6 +34,14 @@ struct AdjState {
 struct AdjEngine {
     Geom g;
     int jacobi_iters;
+    // convergent modes: the pressure is the solve of the mean-free system
+    // (to tol), whose adjoint is the same solve on the pressure's adjoint
+    int conv;
+    double tol;
+    int max_outer;
+    MgSolver mg_fwd, mg_adj;   // forward recompute; adjoint solve
+    double* p64;               // FP64 pressure of the recompute
+    cudaStream_t cap;          // capture stream of the solvers' graphs
     size_t elems;           // padded elements per field
     // forward tape
     int istep0, nsteps, every, ncp;
@@ -56,7 +67,10 @@ struct AdjEngine {
 };
 
 // Allocate the engine for grid g (no tape yet).  Buffers are zeroed.
-cudaError_t adj_create(const Geom& g, int jacobi_iters, AdjEngine* e, cudaStream_t s);
+// mg_mode: 0 for the plain step (jacobi_iters sweeps), MG_MIXED or MG_FP64
+// for the convergent solve to tol with at most max_outer V-cycles.
+cudaError_t adj_create(const Geom& g, int jacobi_iters, int mg_mode, double tol, int max_outer, AdjEngine* e,
+                       cudaStream_t s);
 void adj_destroy(AdjEngine* e);
 
 // (Re)allocate the tape for nsteps steps from istep0 with a checkpoint every

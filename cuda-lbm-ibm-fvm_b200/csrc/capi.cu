@@ -499,13 +499,13 @@ int vof_solver_stats(const vof_ctx* ctx, int* outer, double* rel_initial, double
 
 int vof_forward_record(vof_ctx* ctx, int istep0, int nsteps, int checkpoint_every) {
     if (!ctx || nsteps < 1 || checkpoint_every < 0) return VOF_E_INVALID;
-    if (ctx->conv) return VOF_E_UNSUPPORTED;
     DeviceGuard dg(ctx->device);
     cudaError_t e;
     if (!ctx->adj) {
         ctx->adj = new (std::nothrow) vof::AdjEngine();
         if (!ctx->adj) return VOF_E_NOMEM;
-        e = vof::adj_create(ctx->g, ctx->prm.jacobi_iters, ctx->adj, ctx->stream);
+        e = vof::adj_create(ctx->g, ctx->prm.jacobi_iters, ctx->conv ? ctx->mg.mode : 0, ctx->prm.tol,
+                            ctx->prm.max_outer, ctx->adj, ctx->stream);
         if (e != cudaSuccess) {
             vof::adj_destroy(ctx->adj);
             delete ctx->adj;
@@ -516,19 +516,27 @@ int vof_forward_record(vof_ctx* ctx, int istep0, int nsteps, int checkpoint_ever
     vof::AdjEngine* A = ctx->adj;
     if ((e = vof::adj_tape(A, istep0, nsteps, checkpoint_every, ctx->stream)) != cudaSuccess)
         return e == cudaErrorMemoryAllocation ? VOF_E_NOMEM : fail_cuda(ctx, e);
+    int not_conv = 0;
     for (int n = 0; n < nsteps; ++n) {
         if (n % A->every == 0) {
             vof::AdjState x;
             for (int q = 0; q < 5; ++q) x.f[q] = field_ptr(ctx, q);
+            x.p64 = ctx->conv ? ctx->p64 : nullptr;
             if ((e = vof::adj_save(A, n / A->every, x, ctx->stream)) != cudaSuccess) return fail_cuda(ctx, e);
         }
-        e = vof::plain_step(ctx->g, ctx->b, istep0 + n, ctx->prm.jacobi_iters, &ctx->p_parity, ctx->stream);
-        if (e != cudaSuccess) return fail_cuda(ctx, e);
+        if (ctx->conv) {
+            const int st = conv_step(ctx, istep0 + n, nullptr);
+            if (st == VOF_E_NOT_CONVERGED) not_conv = 1;
+            else if (st != VOF_OK) return st;
+        } else {
+            e = vof::plain_step(ctx->g, ctx->b, istep0 + n, ctx->prm.jacobi_iters, &ctx->p_parity, ctx->stream);
+            if (e != cudaSuccess) return fail_cuda(ctx, e);
+        }
     }
     const int st = vof_sync(ctx);
     if (st != VOF_OK) return st;
     A->recorded = true;
-    return VOF_OK;
+    return not_conv ? VOF_E_NOT_CONVERGED : VOF_OK;
 }
 
 int vof_backward(vof_ctx* ctx, const double* box, double* loss, double* grad_g) {
@@ -537,7 +545,9 @@ int vof_backward(vof_ctx* ctx, const double* box, double* loss, double* grad_g) 
     DeviceGuard dg(ctx->device);
     vof::AdjState fin;
     for (int q = 0; q < 5; ++q) fin.f[q] = field_ptr(ctx, q);
+    fin.p64 = ctx->conv ? ctx->p64 : nullptr;
     cudaError_t e = vof::adj_backward(ctx->adj, fin, box, loss, grad_g, ctx->stream);
+    if (e == cudaErrorNotReady) return VOF_E_NOT_CONVERGED;
     if (e != cudaSuccess) return fail_cuda(ctx, e);
     int st = 0;
     if (cudaMemcpy(&st, ctx->adj->status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return VOF_E_CUDA;

@@ -397,7 +397,8 @@ __global__ void __launch_bounds__(MG_THREADS) k_level_sum(MgLevel L, const S* __
 }
 
 // ---- fine level, FP64 (padded layout of the step) ----------------------------------
-__global__ void __launch_bounds__(MG_THREADS) k_sum_rhs(Geom g, MgLevel L0, const float* __restrict__ rhs,
+template <typename R>
+__global__ void __launch_bounds__(MG_THREADS) k_sum_rhs(Geom g, MgLevel L0, const R* __restrict__ rhs,
                                                         double* __restrict__ partial) {
     LEVEL_TILE(L0);
     double a = 0, z = 0;
@@ -412,8 +413,8 @@ __global__ void __launch_bounds__(MG_THREADS) k_sum_rhs(Geom g, MgLevel L0, cons
 
 // r = (rhs - mean) - A p in FP64, stored as the fine right-hand side b0;
 // e0 (optional) = the first smoothing step from zero; partial sums of r^2, b^2.
-template <typename S>
-__global__ void __launch_bounds__(MG_THREADS) k_resid0(Geom g, MgLevel L0, const float* __restrict__ rhs,
+template <typename S, typename R>
+__global__ void __launch_bounds__(MG_THREADS) k_resid0(Geom g, MgLevel L0, const R* __restrict__ rhs,
                                                        const double* __restrict__ sums, const double* __restrict__ p,
                                                        S* __restrict__ b0, S* __restrict__ e0,
                                                        double* __restrict__ partial) {
@@ -514,7 +515,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_gauge_cast(Geom g, MgLevel L0, d
         const int id = gidx(g, i + 1, j + 1, k + 1);
         const double v = p[id] - mean;
         p[id] = v;
-        p32[id] = (float)v;
+        if (p32) p32[id] = (float)v;
     }
 }
 
@@ -984,21 +985,21 @@ cudaError_t mg_widen(const Geom& g, const MgSolver& m, const float* p32, double*
 
 // One outer iteration after the first residual: V-cycle with p += e, then the
 // new residual and its norm (also written to the mapped host copy).
-template <typename S>
-static cudaError_t outer_iteration(const Geom& g, MgSolver& m, const float* rhs, double* p64, cudaStream_t s,
+template <typename S, typename R>
+static cudaError_t outer_iteration(const Geom& g, MgSolver& m, const R* rhs, double* p64, cudaStream_t s,
                                    int& launches) {
     cudaError_t e = vcycle<S>(g, m, p64, s, launches);
     if (e != cudaSuccess) return e;
     const MgLevel& L0 = m.lv[0];
-    k_resid0<S><<<grid_of(L0), kBlock, 0, s>>>(g, L0, rhs, m.d_result + 2, p64, static_cast<S*>(L0.b),
+    k_resid0<S, R><<<grid_of(L0), kBlock, 0, s>>>(g, L0, rhs, m.d_result + 2, p64, static_cast<S*>(L0.b),
                                                multi(m, 0) ? static_cast<S*>(L0.e0) : nullptr, m.d_partial);
     k_fold2<<<1, MG_THREADS, 0, s>>>(m.d_partial, m.nblk, m.d_result, m.h_result_dev);
     launches += 2;
     return cudaGetLastError();
 }
 
-template <typename S>
-static cudaError_t capture_iteration(const Geom& g, MgSolver& m, const float* rhs, double* p64, float* p32,
+template <typename S, typename R>
+static cudaError_t capture_iteration(const Geom& g, MgSolver& m, const R* rhs, double* p64, float* p32,
                                      cudaStream_t cap) {
     if (m.iter_graph) {
         cudaGraphExecDestroy(m.iter_graph);
@@ -1007,7 +1008,7 @@ static cudaError_t capture_iteration(const Geom& g, MgSolver& m, const float* rh
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return e;
     int launches = 0;
-    const cudaError_t e1 = outer_iteration<S>(g, m, rhs, p64, cap, launches);
+    const cudaError_t e1 = outer_iteration<S, R>(g, m, rhs, p64, cap, launches);
     cudaGraph_t graph = nullptr;
     e = cudaStreamEndCapture(cap, &graph);
     if (e1 != cudaSuccess || e != cudaSuccess) {
@@ -1027,8 +1028,8 @@ static cudaError_t capture_iteration(const Geom& g, MgSolver& m, const float* rh
     return cudaSuccess;
 }
 
-template <typename S>
-static cudaError_t solve_impl(const Geom& g, MgSolver& m, const float* rhs, double* p64, float* p32, double tol,
+template <typename S, typename R>
+static cudaError_t solve_impl(const Geom& g, MgSolver& m, const R* rhs, double* p64, float* p32, double tol,
                               int max_outer, MgStats* st, cudaStream_t s, cudaStream_t cap) {
     const MgLevel& L0 = m.lv[0];
     const dim3 grid = grid_of(L0);
@@ -1036,11 +1037,11 @@ static cudaError_t solve_impl(const Geom& g, MgSolver& m, const float* rhs, doub
     double* res = m.d_result;
     cudaError_t e;
     if (!m.iter_graph || m.graph_key[0] != rhs || m.graph_key[1] != p64 || m.graph_key[2] != p32)
-        if ((e = capture_iteration<S>(g, m, rhs, p64, p32, cap)) != cudaSuccess) return e;
+        if ((e = capture_iteration<S, R>(g, m, rhs, p64, p32, cap)) != cudaSuccess) return e;
     int launches = 0;
-    k_sum_rhs<<<grid, kBlock, 0, s>>>(g, L0, rhs, part);
+    k_sum_rhs<R><<<grid, kBlock, 0, s>>>(g, L0, rhs, part);
     k_fold2<<<1, MG_THREADS, 0, s>>>(part, m.nblk, res + 2, nullptr);
-    k_resid0<S><<<grid, kBlock, 0, s>>>(g, L0, rhs, res + 2, p64, static_cast<S*>(L0.b),
+    k_resid0<S, R><<<grid, kBlock, 0, s>>>(g, L0, rhs, res + 2, p64, static_cast<S*>(L0.b),
                                         multi(m, 0) ? static_cast<S*>(L0.e0) : nullptr, part);
     k_fold2<<<1, MG_THREADS, 0, s>>>(part, m.nblk, res, m.h_result_dev);
     launches += 4;
@@ -1071,8 +1072,16 @@ static cudaError_t solve_impl(const Geom& g, MgSolver& m, const float* rhs, doub
 
 cudaError_t mg_solve(const Geom& g, MgSolver& m, const float* rhs, double* p64, float* p32, double tol,
                      int max_outer, MgStats* st, cudaStream_t s, cudaStream_t cap) {
-    if (m.mode == MG_MIXED) return solve_impl<__nv_bfloat16>(g, m, rhs, p64, p32, tol, max_outer, st, s, cap);
-    return solve_impl<double>(g, m, rhs, p64, p32, tol, max_outer, st, s, cap);
+    if (m.mode == MG_MIXED)
+        return solve_impl<__nv_bfloat16, float>(g, m, rhs, p64, p32, tol, max_outer, st, s, cap);
+    return solve_impl<double, float>(g, m, rhs, p64, p32, tol, max_outer, st, s, cap);
+}
+
+cudaError_t mg_solve64(const Geom& g, MgSolver& m, const double* rhs, double* p64, double tol, int max_outer,
+                       MgStats* st, cudaStream_t s, cudaStream_t cap) {
+    if (m.mode == MG_MIXED)
+        return solve_impl<__nv_bfloat16, double>(g, m, rhs, p64, nullptr, tol, max_outer, st, s, cap);
+    return solve_impl<double, double>(g, m, rhs, p64, nullptr, tol, max_outer, st, s, cap);
 }
 
 }  // namespace vof

@@ -87,6 +87,11 @@ void mg_destroy(MgSolver* m);
 cudaError_t mg_solve(const Geom& g, MgSolver& m, const float* rhs, double* p64, float* p32, double tol,
                      int max_outer, MgStats* st, cudaStream_t s, cudaStream_t cap);
 
+// The same solve for an FP64 right-hand side (padded layout; its interior is
+// read), with no FP32 copy of the solution (the adjoint of the pressure solve).
+cudaError_t mg_solve64(const Geom& g, MgSolver& m, const double* rhs, double* p64, double tol, int max_outer,
+                       MgStats* st, cudaStream_t s, cudaStream_t cap);
+
 // p64 = double(p32) on the interior (after the pressure field is uploaded).
 cudaError_t mg_widen(const Geom& g, const MgSolver& m, const float* p32, double* p64, cudaStream_t s);
 

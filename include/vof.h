@@ -231,11 +231,14 @@ int vof_solver_stats(const vof_ctx* ctx, int* outer, double* rel_initial, double
  * on [0, 1] and 0 outside.  The forward is the plain FP32 step, the adjoint
  * fields are FP64.
  *
- * vof_forward_record: nsteps plain steps from istep0 on the context's state
- * (like vof_run), storing a device checkpoint of the state every
- * checkpoint_every steps (0: ceil(sqrt(nsteps))).  VOF_MODE_PLAIN only
- * (VOF_E_UNSUPPORTED otherwise).  Device memory: ceil(nsteps/every) + every
- * states of five fields, plus the engine's work fields (allocated once).
+ * vof_forward_record: nsteps steps from istep0 on the context's state (like
+ * vof_run), storing a device checkpoint of the state every checkpoint_every
+ * steps (0: ceil(sqrt(nsteps))).  Device memory: ceil(nsteps/every) + every
+ * states of five fields (and the FP64 pressure in the convergent modes), plus
+ * the engine's work fields (allocated once).  In VOF_MODE_MIXED / FP64 the
+ * pressure is taken as the exact solution of the mean-free system (its
+ * adjoint is the same solve on the pressure's adjoint, to prm.tol; the state
+ * pressure, only a warm start, gets a zero adjoint).
  *
  * vof_backward: the reverse pass of the recorded run from the context's
  * current (final) state; *loss = L, grad_g = dL/d(gx, gy, gz).  Recomputes

@@ -72,6 +72,11 @@ def oracle_lib():
             fn = getattr(lib, name)
             fn.restype = C.c_int
             fn.argtypes = [C.POINTER(Params)] + [C.POINTER(T)] * 5 + [C.c_int, C.c_int, D] + [D] * 7 + [C.c_int]
+        for name, T in (("oracle_adjoint_conv_f32", C.c_float), ("oracle_adjoint_conv_f64", C.c_double)):
+            fn = getattr(lib, name)
+            fn.restype = C.c_int
+            fn.argtypes = [C.POINTER(Params)] + [C.POINTER(T)] * 5 + [C.c_int, C.c_int, D] + [D] * 7 + \
+                [C.c_double, C.c_int]
         lib.oracle_tangent_f64.restype = C.c_int
         lib.oracle_tangent_f64.argtypes = [C.POINTER(Params)] + [D] * 11 + [C.c_int, C.c_int, D, D, D, C.c_int]
         lib.oracle_tape_new.restype = C.c_void_p
@@ -134,14 +139,20 @@ def _box(box):
     return b
 
 
-def adjoint(prm, state, istep0: int, nsteps: int, box, precision: str = "f32", nthreads: int = 0) -> dict:
+def adjoint(prm, state, istep0: int, nsteps: int, box, precision: str = "f32", nthreads: int = 0,
+            conv_tol: float = 0.0) -> dict:
     """Host adjoint of L = sum over `box` (x0, x1, y0, y1, z0, z1; strict bounds
     on cell centres) of F dV after nsteps steps: dL/d(F, u, v, w, p) of the
     initial state (float64, reference layout) as "lF", "lu", ..., dL/dg as
     "grad_g" and the loss as "loss".  The forward runs in FP32 ("f32", the
-    CUDA plain path's arithmetic) or FP64 ("f64")."""
+    CUDA plain path's arithmetic) or FP64 ("f64"); conv_tol > 0 solves every
+    step's pressure to that tolerance instead of the Jacobi sweeps."""
     T, dt = (C.c_float, np.float32) if precision == "f32" else (C.c_double, np.float64)
-    fn = oracle_lib().oracle_adjoint_f32 if precision == "f32" else oracle_lib().oracle_adjoint_f64
+    if conv_tol > 0:
+        base = oracle_lib().oracle_adjoint_conv_f32 if precision == "f32" else oracle_lib().oracle_adjoint_conv_f64
+        fn = lambda *a: base(*a[:-1], float(conv_tol), a[-1])  # noqa: E731
+    else:
+        fn = oracle_lib().oracle_adjoint_f32 if precision == "f32" else oracle_lib().oracle_adjoint_f64
     st = {k: np.ascontiguousarray(state[k], dtype=dt) for k in STATE}
     out = {k: np.zeros(prm.shape, dtype=np.float64) for k in ("lF", "lu", "lv", "lw", "lp")}
     g = np.zeros(3)

@@ -70,6 +70,7 @@ struct Adjoint {
     std::vector<double> lus, lvs, lws, lrho, lnu, lrhs, lq, lFn;
     std::vector<double> lFtd, lA, lC, lrp, lrm, ldv;  // of one sweep
     double lg[3] = {0, 0, 0};
+    double conv_tol = 0.0;  // > 0: the pressure is the convergent solve (oracle_core.h solve_conv)
     // forward values of the step being reversed
     std::vector<T> rho, nu, us, vs, ws, pafter, u1, v1, w1, Fin[3], Fstart, ustart, vstart, wstart;
 
@@ -100,9 +101,14 @@ struct Adjoint {
         us = o.us;
         vs = o.vs;
         ws = o.ws;
-        for (int it = 0; it < o.P.jacobi_iters; ++it) {
-            o.jacobi_sweep(o.p, o.pt);
-            std::swap(o.p, o.pt);
+        if (conv_tol > 0) {
+            o.conv_tol = conv_tol;
+            o.solve_conv();
+        } else {
+            for (int it = 0; it < o.P.jacobi_iters; ++it) {
+                o.jacobi_sweep(o.p, o.pt);
+                std::swap(o.p, o.pt);
+            }
         }
         pafter = o.p;
         o.update_uvw();
@@ -408,6 +414,48 @@ struct Adjoint {
         }
     }
 
+    // ---- the convergent pressure solve, reversed ----------------------------------
+    // p = P A+ Q rhs (Q: remove the mean of rhs, P: gauge mean(p) = 0, A the
+    // symmetric Neumann operator): lrhs = Q A+ P lp, i.e. the mean-free mu
+    // with A mu = lp - mean(lp); the state pressure (a warm start) gets none.
+    void adj_solve() {
+        const int nx = o.P.nx, ny = o.P.ny, nz = o.P.nz;
+        const double ncell = (double)nx * ny * nz;
+        std::vector<double> b(o.N, 0.0), x(o.N, 0.0), r(o.N, 0.0), d(o.N, 0.0), q(o.N, 0.0);
+        double mean = 0;
+        for (int k = 1; k <= nz; ++k)
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i) mean += lp[id(i, j, k)];
+        mean /= ncell;
+        for (int k = 1; k <= nz; ++k)
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i) b[id(i, j, k)] = -(lp[id(i, j, k)] - mean);  // -A x = -b
+        r = b;
+        d = r;
+        const double bn = std::sqrt(o.dot_in(b, b));
+        double rr = o.dot_in(r, r);
+        for (int it = 0; bn > 0 && std::sqrt(rr) > 1e-14 * bn && it < 20000; ++it) {
+            o.apply_negA(d, q);
+            const double al = rr / o.dot_in(d, q);
+            for (size_t t = 0; t < o.N; ++t) {
+                x[t] += al * d[t];
+                r[t] -= al * q[t];
+            }
+            const double rr2 = o.dot_in(r, r);
+            for (size_t t = 0; t < o.N; ++t) d[t] = r[t] + (rr2 / rr) * d[t];
+            rr = rr2;
+        }
+        double xm = 0;
+        for (int k = 1; k <= nz; ++k)
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i) xm += x[id(i, j, k)];
+        xm /= ncell;
+        for (int k = 1; k <= nz; ++k)
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i) lrhs[id(i, j, k)] = x[id(i, j, k)] - xm;
+        std::fill(lp.begin(), lp.end(), 0.0);
+    }
+
     // ---- rhs = rho/dt div(u*) (voftrial1.cu:418-422), reversed ----------------
     void adj_rhs() {
         const double dt = o.P.dt, dxi = o.P.dxi, dyi = o.P.dyi, dzi = o.P.dzi;
@@ -548,7 +596,8 @@ struct Adjoint {
         }
         adj_bc_velocity();
         adj_update();
-        adj_jacobi();
+        if (conv_tol > 0) adj_solve();
+        else adj_jacobi();
         adj_rhs();
         adj_advect_comp(0);
         adj_advect_comp(1);
@@ -560,12 +609,13 @@ struct Adjoint {
 template <typename T>
 int adjoint_run(const vof_params* prm, const T* F, const T* u, const T* v, const T* w, const T* p, int istep0,
                 int nsteps, const double* box, double* lF, double* lu, double* lv, double* lw, double* lp,
-                double* grad_g, double* loss, int nthreads) {
+                double* grad_g, double* loss, int nthreads, double conv_tol = 0.0) {
     if (!prm || !F || !u || !v || !w || !p || !box || nsteps < 0) return VOF_E_INVALID;
     if (prm->nx < 1 || prm->ny < 1 || prm->nz < 1) return VOF_E_SIZE;
     if (nthreads <= 0) nthreads = omp_get_max_threads();
     const Box b{box[0], box[1], box[2], box[3], box[4], box[5]};
     Adjoint<T> A(make_prm(prm, T(0)), nthreads);
+    A.conv_tol = conv_tol;
     Oracle<T>& o = A.o;
     const size_t n = o.N;
     std::vector<State<T>> states((size_t)nsteps);
@@ -573,6 +623,7 @@ int adjoint_run(const vof_params* prm, const T* F, const T* u, const T* v, const
                  std::vector<T>(w, w + n), std::vector<T>(p, p + n)};
     {
         Oracle<T> fw(make_prm(prm, T(0)), nthreads);
+        fw.conv_tol = conv_tol;
         fw.F = cur.F;
         fw.u = cur.u;
         fw.v = cur.v;
@@ -734,6 +785,26 @@ int oracle_tangent_f64(const vof_params* prm, const double* F, const double* u, 
     const double* x0[5] = {F, u, v, w, p};
     const double* dx0[5] = {dF, du, dv, dw, dp};
     return tangent_run(prm, x0, dx0, dg, istep0, nsteps, box, loss, dloss, nthreads);
+}
+
+// The same with the convergent pressure solve (CG to ||r|| <= tol ||b||, mean
+// zero) in every step: the host adjoint of VOF_MODE_MIXED / VOF_MODE_FP64.
+int oracle_adjoint_conv_f32(const vof_params* prm, const float* F, const float* u, const float* v, const float* w,
+                            const float* p, int istep0, int nsteps, const double* box, double* lF, double* lu,
+                            double* lv, double* lw, double* lp, double* grad_g, double* loss, double tol,
+                            int nthreads) {
+    if (!(tol > 0)) return VOF_E_INVALID;
+    return adjoint_run<float>(prm, F, u, v, w, p, istep0, nsteps, box, lF, lu, lv, lw, lp, grad_g, loss, nthreads,
+                              tol);
+}
+
+int oracle_adjoint_conv_f64(const vof_params* prm, const double* F, const double* u, const double* v,
+                            const double* w, const double* p, int istep0, int nsteps, const double* box, double* lF,
+                            double* lu, double* lv, double* lw, double* lp, double* grad_g, double* loss, double tol,
+                            int nthreads) {
+    if (!(tol > 0)) return VOF_E_INVALID;
+    return adjoint_run<double>(prm, F, u, v, w, p, istep0, nsteps, box, lF, lu, lv, lw, lp, grad_g, loss, nthreads,
+                               tol);
 }
 
 void* oracle_tape_new(void) { return new Tape(); }

@@ -131,3 +131,25 @@ def test_fp32_and_fp64_trajectories_give_close_gradients(V, orc):
     for k in ("lu", "lv", "lw"):
         assert np.linalg.norm(a[k] - b[k]) <= 1e-3 * np.linalg.norm(b[k]), k
     assert np.allclose(a["grad_g"], b["grad_g"], rtol=1e-3)
+
+
+def test_convergent_solve_adjoint_against_finite_differences(V, orc):
+    """With the pressure solved to 1e-13 every step (the FP64 oracle of the
+    MIXED / FP64 modes), the adjoint's solve step (mean-free solve of A mu =
+    lp - mean(lp)) gives dL/du0, dL/dv0, dL/dw0 that match central
+    differences of that forward; the state pressure gets no adjoint."""
+    prm, st = dam_state(V, 12, 12, 12)
+    box = box_of(prm)
+    steps, eps = 6, 1e-7
+    A = orc.adjoint(prm, st, 1, steps, box, "f64", conv_tol=1e-13)
+    assert np.count_nonzero(A["lp"]) == 0
+    rng = np.random.default_rng(11)
+    for comp in ("u", "v", "w"):
+        d = interior_faces(prm, comp, rng, sigma=1.0)
+        adj = float(np.sum(A["l" + comp] * d))
+        sp, sm = dict(st), dict(st)
+        sp[comp] = st[comp] + eps * d
+        sm[comp] = st[comp] - eps * d
+        fd = (box_loss(prm, orc.run_conv_f64(prm, sp, 1, steps, tol=1e-13)["F"], box) -
+              box_loss(prm, orc.run_conv_f64(prm, sm, 1, steps, tol=1e-13)["F"], box)) / (2 * eps)
+        assert abs(fd - adj) <= 1e-4 * abs(fd), (comp, fd, adj)
