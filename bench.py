@@ -80,6 +80,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ext-steps", type=int, default=10,
                     help="steps of each convergent-mode measurement at the bench size (0 disables)")
+    ap.add_argument("--large-steps", type=int, default=0,
+                    help="steps of the 320^3 mixed-solve + adjoint rollout (0: skip; opt-in)")
     ap.add_argument("--adj-steps", type=int, default=400,
                     help="steps of the adjoint measurement at 64^3 (the bench size runs 1/8 of them; 0 disables)")
     return ap.parse_args(argv)
@@ -405,6 +407,73 @@ def measure_adjoint(V, n, steps, every, stream, dev, dense=False):
 
 
 # ---------------------------------------------------------------------------
+# large rollout (extension, opt-in): 320^3, sinusoidal interface, MIXED
+# pressure solve, adjoint of the box loss with sqrt(N) checkpoints
+# ---------------------------------------------------------------------------
+def measure_large(V, steps, stream, dev, n=320, horizon=5000):
+    """`steps` steps of the 320^3 rollout (h = 0.06 + dx S(x,y)/max|S|,
+    S = sum_{m=1..4} sin(2 pi m x/L + phi_m) sin(2 pi m y/L + psi_m), phases
+    from splitmix64 seed 5), MIXED solve to 1e-8: forward through vof_step,
+    record + reverse pass with checkpoints every ceil(sqrt(steps)) steps; and
+    the device memory the same tape takes for `horizon` steps (computed from
+    the measured per-state and engine sizes)."""
+    import torch
+
+    from vof_b200 import ic
+
+    prm = V.default_params(n, gx=0.0, gy=0.0, gz=-9.81, mode=V.MODE_MIXED, tol=1e-8, max_outer=200)
+    st = ic.rest_state(prm, ic.dam_break(prm, height=ic.sinusoidal_height(prm, seed=5)))
+    box = (0.06, 1e300, -1e300, 1e300, -1e300, 0.02)
+    cells = prm.nx * prm.ny * prm.nz
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    with V.Solver(prm, stream=stream.cuda_stream) as s:
+        base = s.device_bytes
+        s.upload_state(**st)
+        s.step(1)
+        s.upload_state(**st)
+        fwd_ms, _ = timed(lambda: [s.step(1 + q) for q in range(steps)])
+        s.upload_state(**st)
+        s.forward_record(1, steps, 0)  # engine and tape allocated outside the timed region
+        with_tape = s.device_bytes
+        s.upload_state(**st)
+        rec_ms, _ = timed(lambda: s.forward_record(1, steps, 0))
+        bwd_ms, r = timed(lambda: s.backward(box))
+        free, total = torch.cuda.mem_get_info(dev)
+    every = int(np.ceil(np.sqrt(steps)))
+    px = -(-(n + 2) // 32) * 32
+    padded = px * (n + 2) * (n + 2)
+    state_bytes = padded * (5 * 4 + 8)  # five FP32 fields + the FP64 warm start
+    tape_now = (-(-steps // every) + every) * state_bytes
+    engine = with_tape - base - tape_now
+    every_h = int(np.ceil(np.sqrt(horizon)))
+    tape_h = (-(-horizon // every_h) + every_h) * state_bytes
+    return {"workload": f"{n}^3 sinusoidal interface (seed 5), MIXED solve to 1e-8, {steps} steps; "
+                        "loss = sum F dV over x>0.06, z<0.02",
+            "steps": steps, "checkpoint_every": every,
+            "forward_mcell_s": round(cells * steps / fwd_ms / 1e3, 1),
+            "forward_ms_per_step": round(fwd_ms / steps, 3),
+            "record_ms_per_step": round(rec_ms / steps, 3),
+            "backward_ms_per_step": round(bwd_ms / steps, 3),
+            "backward_mcell_s": round(cells * steps / bwd_ms / 1e3, 1),
+            "backward_over_forward": round(bwd_ms / fwd_ms, 3),
+            "device_bytes_solver": int(base), "device_bytes_with_tape": int(with_tape),
+            "device_total_bytes": int(total),
+            "tape_bytes_for_horizon": {"steps": horizon, "checkpoint_every": every_h,
+                                       "bytes": int(tape_h + engine + base),
+                                       "fits": bool(tape_h + engine + base < total)},
+            "loss": r["loss"], "dL_dg": [float(x) for x in r["grad_g"]]}
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def run_ours(args):
@@ -526,6 +595,8 @@ def run_ours(args):
         ext["convergent_pressure"] = measure_convergent(V, args.n, args.ext_steps, stream, dev)
         ext["convergent_pressure"]["speedup_mixed_over_plain"] = round(
             ext["convergent_pressure"]["mixed"]["value"] / value, 3)
+    if args.large_steps > 0 and world == 1:
+        ext["large_mixed_adjoint"] = measure_large(V, args.large_steps, stream, dev)
     if args.adj_steps > 0 and world == 1:
         ext["adjoint"] = [measure_adjoint(V, 64, args.adj_steps, 20, stream, dev),
                           measure_adjoint(V, 64, args.adj_steps, 20, stream, dev, dense=True),
