@@ -1052,26 +1052,81 @@ cudaError_t step_pressure(AdjEngine& e, const float** pafter, cudaStream_t s) {
     return r;
 }
 
-// One reversed step from its start state x.
-cudaError_t adjoint_step(AdjEngine& e, const AdjState& x, int istep, cudaStream_t s) {
+// Sweep axes of step istep, in order (voftrial1.cu:1384-1396).
+inline const int* sweep_order(int istep) {
+    static const int order[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
+    return order[((istep % 3) + 3) % 3];
+}
+
+// What a reversed step reads: the start state, the predictor's output, the
+// pressure after the solve, the corrected velocity and each sweep's input F.
+struct StepData {
+    const float *F, *u, *v, *w;
+    const float *us, *vs, *ws;
+    const float* p;
+    const float* vel[3];
+    const float* Fsw[3];
+};
+
+// The intermediates of step istep recomputed from its start state x with the
+// engine's buffers (the forward's kernels, so the forward's bits).
+cudaError_t recompute_step(AdjEngine& e, const AdjState& x, int istep, StepData* d, cudaStream_t s) {
     const Geom& g = e.g;
     cudaError_t r;
-    // recompute
     if ((r = load_state(e, x, s)) != cudaSuccess) return r;
     if ((r = plain_front(g, e.wb, s)) != cudaSuccess) return r;
     const float* pafter = nullptr;
     if ((r = step_pressure(e, &pafter, s)) != cudaSuccess) return r;
     if ((r = plain_correct(g, e.wb, pafter, s)) != cudaSuccess) return r;
-    const int rr = ((istep % 3) + 3) % 3;
-    static const int order[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
-    const int* dirs = order[rr];
+    const int* dirs = sweep_order(istep);
     const float* velof[3] = {e.wb.u, e.wb.v, e.wb.w};
-    double* lvelof[3] = {e.lu, e.lv, e.lw};
     if ((r = copy_field(e.Fin1, x.f[0], e.elems, s)) != cudaSuccess ||
         (r = fct_launch(g, dirs[0], false, e.Fin1, velof[dirs[0]], s)) != cudaSuccess ||
         (r = copy_field(e.Fin2, e.Fin1, e.elems, s)) != cudaSuccess ||
         (r = fct_launch(g, dirs[1], false, e.Fin2, velof[dirs[1]], s)) != cudaSuccess)
         return r;
+    *d = StepData{x.f[0], x.f[1], x.f[2], x.f[3], e.wb.us, e.wb.vs, e.wb.ws, pafter,
+                  {velof[0], velof[1], velof[2]}, {x.f[0], e.Fin1, e.Fin2}};
+    return cudaSuccess;
+}
+
+// One step of the segment replay on the engine's buffers, keeping its
+// intermediates in mid: the predictor writes mid's u*, v*, w*; F is copied
+// out after the first and the second sweep.  *par: the Jacobi ping-pong
+// parity of the plain step; *pafter: the pressure after the solve.
+cudaError_t replay_step_keep(AdjEngine& e, int istep, const AdjMid& mid, int* par, const float** pafter,
+                             cudaStream_t s) {
+    const Geom& g = e.g;
+    PlainBuffers b = e.wb;
+    b.us = mid.f[0];
+    b.vs = mid.f[1];
+    b.ws = mid.f[2];
+    cudaError_t r;
+    if ((r = plain_front(g, b, s)) != cudaSuccess) return r;
+    if (e.conv) {
+        if ((r = step_pressure(e, pafter, s)) != cudaSuccess) return r;
+    } else {
+        if ((r = plain_pressure(g, b, e.jacobi_iters, par, s)) != cudaSuccess) return r;
+        *pafter = *par ? b.p1 : b.p0;
+    }
+    if ((r = plain_correct(g, b, *pafter, s)) != cudaSuccess) return r;
+    const int* dirs = sweep_order(istep);
+    const float* velof[3] = {b.u, b.v, b.w};
+    if ((r = fct_launch(g, dirs[0], false, b.F, velof[dirs[0]], s)) != cudaSuccess ||
+        (r = copy_field(mid.f[3], b.F, e.elems, s)) != cudaSuccess ||
+        (r = fct_launch(g, dirs[1], false, b.F, velof[dirs[1]], s)) != cudaSuccess ||
+        (r = copy_field(mid.f[4], b.F, e.elems, s)) != cudaSuccess ||
+        (r = fct_launch(g, dirs[2], true, b.F, velof[dirs[2]], s)) != cudaSuccess)
+        return r;
+    return cudaSuccess;
+}
+
+// One reversed step: the adjoint kernels on the step's data d.
+cudaError_t reverse_step(AdjEngine& e, const StepData& d, int istep, cudaStream_t s) {
+    const Geom& g = e.g;
+    cudaError_t r;
+    const int* dirs = sweep_order(istep);
+    double* lvelof[3] = {e.lu, e.lv, e.lw};
     // F boundary copies
     {
         const dim3 b(16, 16);
@@ -1080,12 +1135,11 @@ cudaError_t adjoint_step(AdjEngine& e, const AdjState& x, int istep, cudaStream_
         k_adj_bcF_y<<<dim3((g.nx + 2 + 15) / 16, (g.nz + 2 + 15) / 16), b, 0, s>>>(g, e.lF);
     }
     // the three sweeps, last first
-    const float* Fsw[3] = {x.f[0], e.Fin1, e.Fin2};
     for (int q = 2; q >= 0; --q) {
-        const int d = dirs[q];
-        r = d == 0 ? sweep_adjoint<0>(e, Fsw[q], velof[0], lvelof[0], s)
-                   : (d == 1 ? sweep_adjoint<1>(e, Fsw[q], velof[1], lvelof[1], s)
-                             : sweep_adjoint<2>(e, Fsw[q], velof[2], lvelof[2], s));
+        const int a = dirs[q];
+        r = a == 0 ? sweep_adjoint<0>(e, d.Fsw[q], d.vel[0], lvelof[0], s)
+                   : (a == 1 ? sweep_adjoint<1>(e, d.Fsw[q], d.vel[1], lvelof[1], s)
+                             : sweep_adjoint<2>(e, d.Fsw[q], d.vel[2], lvelof[2], s));
         if (r != cudaSuccess) return r;
     }
     // velocity boundary copies, then the correction
@@ -1097,7 +1151,7 @@ cudaError_t adjoint_step(AdjEngine& e, const AdjState& x, int istep, cudaStream_
     }
     const Range I = interior(g);
     const dim3 gi = grid_of(I);
-    k_adj_update<<<gi, kBlk, 0, s>>>(g, I, x.f[0], pafter, e.lu, e.lv, e.lw, e.lus, e.lvs, e.lws, e.lp[e.lp_cur],
+    k_adj_update<<<gi, kBlk, 0, s>>>(g, I, d.F, d.p, e.lu, e.lv, e.lw, e.lus, e.lvs, e.lws, e.lp[e.lp_cur],
                                      e.lrho);
     // the pressure solve reversed: convergent modes -- lrhs = the mean-free
     // solution of A mu = lp - mean(lp) (warm start: the previous step's), and
@@ -1117,22 +1171,33 @@ cudaError_t adjoint_step(AdjEngine& e, const AdjState& x, int istep, cudaStream_
         k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.inv_ap, e.lp[e.lp_cur], e.lp[e.lp_cur ^ 1], e.lrhs, 2);
         e.lp_cur ^= 1;
     }
-    k_adj_rhs<<<gi, kBlk, 0, s>>>(g, I, x.f[0], e.wb.us, e.wb.vs, e.wb.ws, e.lrhs, e.lus, e.lvs, e.lws, e.lrho, e.lu,
-                                  e.lv, e.lw, e.conv || e.jacobi_iters > 0);
+    k_adj_rhs<<<gi, kBlk, 0, s>>>(g, I, d.F, d.us, d.vs, d.ws, e.lrhs, e.lus, e.lvs, e.lws, e.lrho, e.lu, e.lv, e.lw,
+                                  e.conv || e.jacobi_iters > 0);
     // advection with rho and nu
-    k_adj_advect<<<gi, kBlk, 0, s>>>(g, I, x.f[0], x.f[1], x.f[2], x.f[3], e.lus, e.lvs, e.lws, e.lu, e.lv, e.lw,
-                                     e.lrho, e.lF, e.d_partial);
+    k_adj_advect<<<gi, kBlk, 0, s>>>(g, I, d.F, d.u, d.v, d.w, e.lus, e.lvs, e.lws, e.lu, e.lv, e.lw, e.lrho, e.lF,
+                                     e.d_partial);
     return cudaGetLastError();
 }
 
 }  // namespace
 
 int adj_kernels_per_step(const AdjEngine& e) {
-    // recompute: front 2, pressure (Jacobi launches), correct 1, two sweeps;
-    // adjoint: F copies 3, sweeps 3 x 8, velocity copies 3, correction 1,
-    // Jacobi iters + 1 (none without sweeps), rhs 1, advection 1
-    return 2 + plain_phase_launches(PHASE_JACOBI, e.jacobi_iters) + 1 + 2 + 3 + 24 + 3 + 1 +
-           (e.jacobi_iters > 0 ? e.jacobi_iters + 1 : 0) + 1 + 1;
+    // Per reversed step: the replay's forward step (front 2, pressure,
+    // correction 1, three sweeps), the recomputation when the intermediates
+    // are not kept (front 2, pressure, correction 1, two sweeps), and the
+    // adjoint kernels: F copies 3, the three sweep adjoints (1 launch each when
+    // fused, else 8), velocity copies 3, correction 1, the transposed Jacobi
+    // sweeps (iters + 1), rhs 1, advection 1.  The convergent modes' pressure
+    // solves (multigrid graphs) are not counted.
+    const Geom& g = e.g;
+    const int P = e.conv ? 0 : plain_phase_launches(PHASE_JACOBI, e.jacobi_iters);
+    int sweeps = 0;
+    const int len[3] = {g.nx, g.ny, g.nz};
+    for (int a = 0; a < 3; ++a) sweeps += fa_smem_bytes(2, len[a]) <= fa_smem_limit() ? 1 : 8;
+    const int replay = 2 + P + 1 + 3;
+    const int recompute = e.keep ? 0 : 2 + P + 1 + 2;
+    const int jac = (!e.conv && e.jacobi_iters > 0) ? e.jacobi_iters + 1 : 0;
+    return replay + recompute + 3 + sweeps + 3 + 1 + jac + 1 + 1;
 }
 
 cudaError_t adj_create(const Geom& g, int jacobi_iters, int mg_mode, double tol, int max_outer, AdjEngine* e,
@@ -1214,9 +1279,28 @@ static void free_states(AdjState* st, int n) {
     delete[] st;
 }
 
-void adj_destroy(AdjEngine* e) {
+static void free_mid(AdjMid* m, int n) {
+    if (!m) return;
+    for (int q = 0; q < n; ++q)
+        for (int t = 0; t < 5; ++t)
+            if (m[q].f[t]) cudaFree(m[q].f[t]);
+    delete[] m;
+}
+
+// Free the tape (checkpoints, segment states, intermediates).
+static void free_tape(AdjEngine* e) {
     free_states(e->cp, e->ncp);
     free_states(e->seg, e->every);
+    free_mid(e->mid, e->every);
+    e->cp = e->seg = nullptr;
+    e->mid = nullptr;
+    e->ncp = 0;
+    e->keep = 0;
+    e->tape_bytes = 0;
+}
+
+void adj_destroy(AdjEngine* e) {
+    free_tape(e);
     float* f32[] = {e->wb.F, e->wb.u, e->wb.v, e->wb.w, e->wb.us, e->wb.vs, e->wb.ws, e->wb.rhs, e->wb.p0,
                     e->wb.p1, e->wb.p2, e->Fin1, e->Fin2, e->Ftd, e->A, e->C, e->rp, e->rm};
     for (float* p : f32)
@@ -1238,14 +1322,15 @@ void adj_destroy(AdjEngine* e) {
     *e = AdjEngine{};
 }
 
-static cudaError_t alloc_states(AdjState*& st, int n, size_t elems, bool with_p64, size_t* bytes) {
+// n states; entries below `first` stay unallocated (null).
+static cudaError_t alloc_states(AdjState*& st, int n, int first, size_t elems, bool with_p64, size_t* bytes) {
     st = new (std::nothrow) AdjState[n];
     if (!st) return cudaErrorMemoryAllocation;
     for (int m = 0; m < n; ++m) {
         for (int q = 0; q < 5; ++q) st[m].f[q] = nullptr;
         st[m].p64 = nullptr;
     }
-    for (int m = 0; m < n; ++m) {
+    for (int m = first; m < n; ++m) {
         for (int q = 0; q < 5; ++q) {
             cudaError_t r = cudaMalloc((void**)&st[m].f[q], elems * sizeof(float));
             if (r != cudaSuccess) {
@@ -1266,6 +1351,23 @@ static cudaError_t alloc_states(AdjState*& st, int n, size_t elems, bool with_p6
     return cudaSuccess;
 }
 
+static cudaError_t alloc_mid(AdjMid*& m, int n, size_t elems, size_t* bytes) {
+    m = new (std::nothrow) AdjMid[n];
+    if (!m) return cudaErrorMemoryAllocation;
+    for (int q = 0; q < n; ++q)
+        for (int t = 0; t < 5; ++t) m[q].f[t] = nullptr;
+    for (int q = 0; q < n; ++q)
+        for (int t = 0; t < 5; ++t) {
+            cudaError_t r = cudaMalloc((void**)&m[q].f[t], elems * sizeof(float));
+            if (r != cudaSuccess) {
+                m[q].f[t] = nullptr;
+                return r;
+            }
+            *bytes += elems * sizeof(float);
+        }
+    return cudaSuccess;
+}
+
 cudaError_t adj_tape(AdjEngine* e, int istep0, int nsteps, int every, cudaStream_t s) {
     if (every <= 0) {
         every = 1;
@@ -1273,18 +1375,33 @@ cudaError_t adj_tape(AdjEngine* e, int istep0, int nsteps, int every, cudaStream
     }
     if (every > nsteps) every = nsteps > 0 ? nsteps : 1;
     const int ncp = nsteps > 0 ? (nsteps + every - 1) / every : 0;
-    if (e->cp && (ncp != e->ncp || every != e->every)) {
-        free_states(e->cp, e->ncp);
-        free_states(e->seg, e->every);
-        e->cp = e->seg = nullptr;
-        e->ncp = 0;
+    const size_t fb = e->elems * sizeof(float), db = e->elems * sizeof(double);
+    // keep the intermediates?  (checkpoints + segment states 1.. + intermediates)
+    bool keep = false;
+    if (e->policy == ADJ_STORE_KEEP) {
+        keep = true;
+    } else if (e->policy == ADJ_STORE_AUTO) {
+        size_t fr = 0, tot = 0;
+        const size_t need = (size_t)ncp * (5 * fb + (e->conv ? db : 0)) + (size_t)(every - 1) * 5 * fb +
+                            (size_t)every * 5 * fb;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+            // (the current tape's memory comes back when it is reallocated)
+            keep = need + tot / 32 <= fr + e->tape_bytes;
+        }
     }
+    if (e->cp && (ncp != e->ncp || every != e->every || (int)keep != e->keep)) free_tape(e);
     cudaError_t r;
     if (!e->cp && ncp > 0) {
         e->ncp = ncp;
         e->every = every;
-        if ((r = alloc_states(e->cp, ncp, e->elems, e->conv, &e->bytes)) != cudaSuccess) return r;
-        if ((r = alloc_states(e->seg, every, e->elems, e->conv, &e->bytes)) != cudaSuccess) return r;
+        e->keep = keep;
+        if ((r = alloc_states(e->cp, ncp, 0, e->elems, e->conv, &e->tape_bytes)) != cudaSuccess) return r;
+        // kept tapes: a segment's first state is its checkpoint, and the
+        // replay carries the FP64 warm start itself
+        if ((r = alloc_states(e->seg, every, keep ? 1 : 0, e->elems, e->conv && !keep, &e->tape_bytes)) !=
+            cudaSuccess)
+            return r;
+        if (keep && (r = alloc_mid(e->mid, every, e->elems, &e->tape_bytes)) != cudaSuccess) return r;
     }
     e->istep0 = istep0;
     e->nsteps = nsteps;
@@ -1328,6 +1445,39 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
     for (int m = e->ncp - 1; m >= 0; --m) {
         const int first = m * e->every;
         const int count = (e->nsteps - first) < e->every ? (e->nsteps - first) : e->every;
+        if (e->keep) {
+            // replay every step of the segment from checkpoint m, keeping its
+            // intermediates and the states after steps 0 .. count - 2
+            if ((r = load_state(*e, e->cp[m], s)) != cudaSuccess) return r;
+            int par = 0;
+            const float* pafter[64];
+            const float** pa = count <= 64 ? pafter : new (std::nothrow) const float*[count];
+            if (!pa) return cudaErrorMemoryAllocation;
+            for (int q = 0; q < count && r == cudaSuccess; ++q) {
+                r = replay_step_keep(*e, e->istep0 + first + q, e->mid[q], &par, &pa[q], s);
+                if (r == cudaSuccess && q + 1 < count) {
+                    const float* src[5] = {e->wb.F, e->wb.u, e->wb.v, e->wb.w, pa[q]};
+                    for (int t = 0; t < 5 && r == cudaSuccess; ++t)
+                        r = copy_field(e->seg[q + 1].f[t], src[t], e->elems, s);
+                    pa[q] = e->seg[q + 1].f[4];
+                }
+            }
+            // reverse: step q's next state is seg[q + 1], or the replay's
+            // buffers after the segment's last step
+            for (int q = count - 1; q >= 0 && r == cudaSuccess; --q) {
+                const AdjState& x = q == 0 ? e->cp[m] : e->seg[q];
+                const AdjMid& md = e->mid[q];
+                const float* nu = q + 1 < count ? e->seg[q + 1].f[1] : e->wb.u;
+                const float* nv = q + 1 < count ? e->seg[q + 1].f[2] : e->wb.v;
+                const float* nw = q + 1 < count ? e->seg[q + 1].f[3] : e->wb.w;
+                const StepData d{x.f[0], x.f[1], x.f[2], x.f[3], md.f[0], md.f[1], md.f[2], pa[q],
+                                 {nu, nv, nw}, {x.f[0], md.f[3], md.f[4]}};
+                r = reverse_step(*e, d, e->istep0 + first + q, s);
+            }
+            if (pa != pafter) delete[] pa;
+            if (r != cudaSuccess) return r;
+            continue;
+        }
         // the segment's states: checkpoint m, then count - 1 steps with the engine's buffers
         for (int q = 0; q < 5; ++q)
             if ((r = copy_field(e->seg[0].f[q], e->cp[m].f[q], e->elems, s)) != cudaSuccess) return r;
@@ -1355,8 +1505,12 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
                     return r;
             }
         }
-        for (int q = count - 1; q >= 0; --q)
-            if ((r = adjoint_step(*e, e->seg[q], e->istep0 + first + q, s)) != cudaSuccess) return r;
+        for (int q = count - 1; q >= 0; --q) {
+            StepData d;
+            if ((r = recompute_step(*e, e->seg[q], e->istep0 + first + q, &d, s)) != cudaSuccess ||
+                (r = reverse_step(*e, d, e->istep0 + first + q, s)) != cudaSuccess)
+                return r;
+        }
     }
     k_fold_add<<<1, 256, 0, s>>>(e->d_partial, e->npartial, 3, e->d_sums);
     if ((r = cudaGetLastError()) != cudaSuccess) return r;

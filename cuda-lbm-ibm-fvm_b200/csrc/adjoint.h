@@ -23,14 +23,30 @@ struct AdjState {
     double* p64;
 };
 
+// What the segment replay keeps of each step for the reverse pass: u*, v*,
+// w* (the predictor's output) and F after the first and the second FCT sweep.
+// With these, the start state and the next state (corrected velocity,
+// pressure after the solve), a reversed step needs no recomputation.
+struct AdjMid {
+    float* f[5];
+};
+
+// Where the reverse pass takes a step's intermediates from.
+enum {
+    ADJ_STORE_AUTO = 0,       // kept when they fit in device memory, else recomputed
+    ADJ_STORE_RECOMPUTE = 1,  // always recomputed from the step's start state
+    ADJ_STORE_KEEP = 2        // always kept (allocation failure otherwise)
+};
+
 // The device side of vof_forward_record / vof_backward.  Forward: the
 // context's own steps, with the state copied to a checkpoint every `every`
 // steps.  Backward: per segment (last first), the segment's states are
 // recomputed from its checkpoint with the engine's own buffers, then the
-// steps are reversed one by one, each recomputing its intermediates (rho,
-// u*, the pressure after the sweeps, the corrected velocity, F before each
-// FCT sweep) in FP32 -- bit for bit the forward's values -- and applying the
-// transposed kernels to FP64 adjoint fields.
+// steps are reversed one by one.  A reversed step needs the step's
+// intermediates (u*, the pressure after the sweeps, the corrected velocity,
+// F before each FCT sweep) in FP32, bit for bit the forward's values: kept by
+// the replay (AdjMid, 5 fields per step of a segment) or recomputed from the
+// step's start state.  The transposed kernels then run on FP64 adjoint fields.
 struct AdjEngine {
     Geom g;
     int jacobi_iters;
@@ -46,7 +62,11 @@ struct AdjEngine {
     // forward tape
     int istep0, nsteps, every, ncp;
     AdjState* cp;            // ncp checkpoints (host array of device states)
-    AdjState* seg;           // every segment states
+    AdjState* seg;           // every segment states (kept tapes: entries 1.. only)
+    AdjMid* mid;             // kept tapes: the intermediates of every steps; else null
+    int policy;              // ADJ_STORE_* for the next tape
+    int keep;                // the current tape keeps the intermediates
+    size_t tape_bytes;       // device bytes of the tape
     bool recorded;
     // recompute buffers (FP32)
     PlainBuffers wb;
@@ -74,7 +94,10 @@ cudaError_t adj_create(const Geom& g, int jacobi_iters, int mg_mode, double tol,
 void adj_destroy(AdjEngine* e);
 
 // (Re)allocate the tape for nsteps steps from istep0 with a checkpoint every
-// `every` steps (0: ceil(sqrt(nsteps))).
+// `every` steps (0: ceil(sqrt(nsteps))).  e->policy decides whether the
+// segment replay keeps each step's intermediates; AUTO keeps them when the
+// checkpoints, segment states and intermediates leave 1/32 of the device
+// memory free.
 cudaError_t adj_tape(AdjEngine* e, int istep0, int nsteps, int every, cudaStream_t s);
 
 // Copy the state x into checkpoint m.

@@ -22,6 +22,9 @@ using vof::Geom;
 
 static_assert(sizeof(vof_params) == 136, "vof_params layout is part of the ABI");
 static_assert(VOF_PHASES == vof::PLAIN_PHASES, "phase count");
+static_assert(VOF_ADJ_AUTO == vof::ADJ_STORE_AUTO && VOF_ADJ_RECOMPUTE == vof::ADJ_STORE_RECOMPUTE &&
+                  VOF_ADJ_KEEP == vof::ADJ_STORE_KEEP,
+              "adjoint storage policy codes");
 
 struct vof_ctx {
     vof_params prm;
@@ -43,6 +46,7 @@ struct vof_ctx {
     vof::MgSolver mg;
     vof::MgStats stats;         // of the last pressure solve
     vof::AdjEngine* adj;        // adjoint engine (vof_forward_record / vof_backward), or null
+    int adj_policy;             // VOF_ADJ_* for the next vof_forward_record
     cudaGraphExec_t graph[3][2];  // [istep % 3][p parity at step start]
     int last_cuda_error;
     size_t bytes;
@@ -514,6 +518,7 @@ int vof_forward_record(vof_ctx* ctx, int istep0, int nsteps, int checkpoint_ever
         }
     }
     vof::AdjEngine* A = ctx->adj;
+    A->policy = ctx->adj_policy;
     if ((e = vof::adj_tape(A, istep0, nsteps, checkpoint_every, ctx->stream)) != cudaSuccess)
         return e == cudaErrorMemoryAllocation ? VOF_E_NOMEM : fail_cuda(ctx, e);
     int not_conv = 0;
@@ -578,6 +583,18 @@ int vof_adjoint_kernels_per_step(const vof_ctx* ctx) {
     return vof::adj_kernels_per_step(*ctx->adj);
 }
 
+int vof_adjoint_storage(vof_ctx* ctx, int policy) {
+    if (!ctx || policy < VOF_ADJ_AUTO || policy > VOF_ADJ_KEEP) return VOF_E_INVALID;
+    ctx->adj_policy = policy;
+    return VOF_OK;
+}
+
+int vof_adjoint_keeps(const vof_ctx* ctx) {
+    if (!ctx) return VOF_E_INVALID;
+    if (!ctx->adj || !ctx->adj->cp) return VOF_E_STATE;
+    return ctx->adj->keep ? 1 : 0;
+}
+
 int vof_last_cuda_error(const vof_ctx* ctx) { return ctx ? ctx->last_cuda_error : 0; }
 
 int vof_kernels_per_step(const vof_ctx* ctx) {
@@ -586,6 +603,8 @@ int vof_kernels_per_step(const vof_ctx* ctx) {
     return vof::plain_kernels_per_step(ctx->prm.jacobi_iters);
 }
 
-size_t vof_device_bytes(const vof_ctx* ctx) { return ctx ? ctx->bytes + (ctx->adj ? ctx->adj->bytes : 0) : 0; }
+size_t vof_device_bytes(const vof_ctx* ctx) {
+    return ctx ? ctx->bytes + (ctx->adj ? ctx->adj->bytes + ctx->adj->tape_bytes : 0) : 0;
+}
 
 }  // extern "C"

@@ -30,6 +30,7 @@ OK = 0
 E_INVALID, E_SIZE, E_NOMEM, E_CUDA, E_NOT_CONVERGED, E_NONFINITE, E_STATE, E_UNSUPPORTED, E_TIMEOUT = (
     -1, -2, -3, -4, -5, -6, -7, -8, -9)
 MODE_PLAIN, MODE_MIXED, MODE_FP64 = 0, 1, 2
+ADJ_AUTO, ADJ_RECOMPUTE, ADJ_KEEP = 0, 1, 2
 FIELDS = {"F": 0, "u": 1, "v": 2, "w": 3, "p": 4, "ustar": 5, "vstar": 6, "wstar": 7, "rhs": 8}
 REDUCTIONS = {"volume": 0, "div_l2": 1, "div_max": 2, "pres_resid": 3, "nonfinite": 4,
               "f_min": 5, "f_max": 6}
@@ -114,6 +115,8 @@ def _declare(lib):
         "vof_backward": (C.c_int, [vp, P(C.c_double), P(C.c_double), P(C.c_double)]),
         "vof_adjoint_download": (C.c_int, [vp, C.c_int, vp]),
         "vof_adjoint_kernels_per_step": (C.c_int, [vp]),
+        "vof_adjoint_storage": (C.c_int, [vp, C.c_int]),
+        "vof_adjoint_keeps": (C.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -141,7 +144,8 @@ def exported_symbols():
             "vof_step", "vof_run", "vof_sync", "vof_reduce", "vof_reduce_async",
             "vof_last_cuda_error", "vof_kernels_per_step", "vof_device_bytes",
             "vof_step_timed", "vof_phase_name", "vof_solver_stats", "vof_step_noalloc",
-            "vof_forward_record", "vof_backward", "vof_adjoint_download", "vof_adjoint_kernels_per_step"]
+            "vof_forward_record", "vof_backward", "vof_adjoint_download", "vof_adjoint_kernels_per_step",
+            "vof_adjoint_storage", "vof_adjoint_keeps"]
 
 
 def default_params(nx: int, ny: int | None = None, nz: int | None = None, **overrides) -> Params:
@@ -297,6 +301,18 @@ class Solver:
     @property
     def adjoint_kernels_per_step(self) -> int:
         return self._lib.vof_adjoint_kernels_per_step(self._ctx)
+
+    def adjoint_storage(self, policy: int):
+        """ADJ_AUTO / ADJ_RECOMPUTE / ADJ_KEEP: where the reverse pass takes
+        each step's intermediates from (next forward_record)."""
+        self._check(self._lib.vof_adjoint_storage(self._ctx, policy), "vof_adjoint_storage")
+
+    @property
+    def adjoint_keeps(self) -> bool:
+        """True when the recorded tape keeps the steps' intermediates."""
+        r = self._lib.vof_adjoint_keeps(self._ctx)
+        self._check(min(r, 0), "vof_adjoint_keeps")
+        return r == 1
 
     @property
     def kernels_per_step(self) -> int:

@@ -235,15 +235,19 @@ int vof_solver_stats(const vof_ctx* ctx, int* outer, double* rel_initial, double
  * vof_run), storing a device checkpoint of the state every checkpoint_every
  * steps (0: ceil(sqrt(nsteps))).  Device memory: ceil(nsteps/every) + every
  * states of five fields (and the FP64 pressure in the convergent modes), plus
- * the engine's work fields (allocated once).  In VOF_MODE_MIXED / FP64 the
+ * the engine's work fields (allocated once); with the intermediates kept
+ * (vof_adjoint_storage), every - 1 segment states of five FP32 fields and
+ * every x five FP32 intermediate fields instead of every segment states.  In VOF_MODE_MIXED / FP64 the
  * pressure is taken as the exact solution of the mean-free system (its
  * adjoint is the same solve on the pressure's adjoint, to prm.tol; the state
  * pressure, only a warm start, gets a zero adjoint).
  *
  * vof_backward: the reverse pass of the recorded run from the context's
- * current (final) state; *loss = L, grad_g = dL/d(gx, gy, gz).  Recomputes
- * each segment from its checkpoint and each step from its start state.
- * VOF_E_STATE without a recorded run.
+ * current (final) state; *loss = L, grad_g = dL/d(gx, gy, gz).  Replays each
+ * segment from its checkpoint; a reversed step takes its intermediates (u*,
+ * v*, w*, F between the FCT sweeps) from that replay when they are kept, else
+ * recomputes them from the step's start state.  VOF_E_STATE without a
+ * recorded run.
  *
  * vof_adjoint_download: dL/d(field) of the initial state (field F, U, V, W or
  * P), FP64, reference layout, to host memory; valid after vof_backward.
@@ -251,9 +255,23 @@ int vof_solver_stats(const vof_ctx* ctx, int* outer, double* rel_initial, double
 int vof_forward_record(vof_ctx* ctx, int istep0, int nsteps, int checkpoint_every);
 int vof_backward(vof_ctx* ctx, const double* box, double* loss, double* grad_g);
 int vof_adjoint_download(vof_ctx* ctx, int field, double* dst);
-/* Kernel launches of one reversed step (recompute included); VOF_E_STATE
+/* Kernel launches of one reversed step (segment replay and recompute
+ * included; the convergent modes' multigrid solves not counted); VOF_E_STATE
  * before the first vof_forward_record. */
 int vof_adjoint_kernels_per_step(const vof_ctx* ctx);
+
+/* Where the reverse pass takes each step's intermediates from, for the next
+ * vof_forward_record: VOF_ADJ_AUTO (the default) keeps them when the tape
+ * with them leaves 1/32 of the device memory free, VOF_ADJ_RECOMPUTE always
+ * recomputes them, VOF_ADJ_KEEP always keeps them (VOF_E_NOMEM from
+ * vof_forward_record when they do not fit).  The gradients do not depend on
+ * the choice.  vof_adjoint_keeps: 1 when the recorded tape keeps them, 0 when
+ * it recomputes them, VOF_E_STATE before the first vof_forward_record. */
+#define VOF_ADJ_AUTO      0
+#define VOF_ADJ_RECOMPUTE 1
+#define VOF_ADJ_KEEP      2
+int vof_adjoint_storage(vof_ctx* ctx, int policy);
+int vof_adjoint_keeps(const vof_ctx* ctx);
 
 /* cudaError_t of the most recent failing CUDA call in this context (0 if none). */
 int vof_last_cuda_error(const vof_ctx* ctx);

@@ -30,13 +30,16 @@ def box_of(prm):
     return (0.3 * prm.Lx, 0.6 * prm.Lx, -1e9, 1e9, -1e9, 0.6 * prm.Lz)
 
 
-def gpu_adjoint(V, prm, st, istep0, nsteps, box, every=0):
+def gpu_adjoint(V, prm, st, istep0, nsteps, box, every=0, policy=None):
     with V.Solver(prm) as s:
+        if policy is not None:
+            s.adjoint_storage(policy)
         s.upload_state(**st)
         s.forward_record(istep0, nsteps, every)
         final = s.state()
         r = s.backward(box)
         r.update({k: s.adjoint(f) for k, f in GRADS})
+        r["keeps"] = s.adjoint_keeps
     r["final"] = final
     return r
 
@@ -65,12 +68,36 @@ def test_device_adjoint_matches_host(cuda, V, orc, shape, nsteps, istep0):
     check_against_host(orc, prm, st, istep0, nsteps, box, got)
 
 
+@pytest.mark.parametrize("policy", ["ADJ_KEEP", "ADJ_RECOMPUTE"])
 @pytest.mark.parametrize("every", [1, 3, 4, 0])
-def test_checkpoint_spacing_does_not_change_the_gradient(cuda, V, orc, every):
+def test_checkpoint_spacing_does_not_change_the_gradient(cuda, V, orc, every, policy):
+    """Kept intermediates (from the segment replay) and recomputed ones (from
+    each step's start state) are the forward's bits either way."""
     prm, st = dam_state(V, 14, 12, 10, seed=5)
     box = box_of(prm)
-    got = gpu_adjoint(V, prm, st, 1, 9, box, every=every)
+    got = gpu_adjoint(V, prm, st, 1, 9, box, every=every, policy=getattr(V, policy))
+    assert got["keeps"] == (policy == "ADJ_KEEP")
     check_against_host(orc, prm, st, 1, 9, box, got)
+
+
+def test_storage_policy_auto_keeps_small_tapes(cuda, V):
+    prm, st = dam_state(V, 10, 10, 10)
+    with V.Solver(prm) as s:
+        with pytest.raises(V.VofError) as e:
+            s.adjoint_keeps
+        assert e.value.status == V.E_STATE
+        with pytest.raises(V.VofError) as e:
+            s.adjoint_storage(7)
+        assert e.value.status == V.E_INVALID
+        s.upload_state(**st)
+        s.forward_record(0, 4, 2)
+        assert s.adjoint_keeps
+        b0 = s.device_bytes
+        s.adjoint_storage(V.ADJ_RECOMPUTE)
+        s.upload_state(**st)
+        s.forward_record(0, 4, 2)
+        assert not s.adjoint_keeps
+        assert s.device_bytes < b0  # kept: 5 more fields per segment step, one state fewer
 
 
 @pytest.mark.parametrize("iters", [0, 1, 3])
@@ -108,8 +135,9 @@ def test_state_errors(cuda, V):
         assert e.value.status == V.E_STATE
 
 
+@pytest.mark.parametrize("policy", ["ADJ_KEEP", "ADJ_RECOMPUTE"])
 @pytest.mark.parametrize("mode", ["MODE_MIXED", "MODE_FP64"])
-def test_convergent_mode_adjoint_matches_host(cuda, V, orc, mode):
+def test_convergent_mode_adjoint_matches_host(cuda, V, orc, mode, policy):
     """MIXED / FP64 modes: the pressure is the solve of the mean-free system;
     its adjoint is the same solve on the pressure adjoint (device: the
     multigrid defect correction to 1e-10; host: CG to 1e-12 on the FP32
@@ -118,6 +146,7 @@ def test_convergent_mode_adjoint_matches_host(cuda, V, orc, mode):
     prm, st = dam_state(V, 16, 14, 12, mode=getattr(V, mode), tol=1e-10, max_outer=100)
     box = box_of(prm)
     with V.Solver(prm) as s:
+        s.adjoint_storage(getattr(V, policy))
         s.upload_state(**st)
         s.forward_record(1, 6, 3)
         got = s.backward(box)
