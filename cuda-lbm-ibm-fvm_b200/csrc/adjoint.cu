@@ -31,6 +31,7 @@
 #include <new>
 
 #include "adjoint.h"
+#include "fct_line.cuh"
 #include "fct_sweep.h"
 #include "jacobi_tb.h"
 
@@ -601,6 +602,299 @@ __global__ void __launch_bounds__(FA_THREADS) k_fct_adjoint(Geom g, const float*
         }
 }
 
+// ---- the sweep adjoint as one march along each line, one lane per line ------------
+// A block owns FM_LANES lines (one per lane) and splits each line's positions
+// 0 .. n+1 into WARPS segments, one per warp.  A warp walks its segment once,
+// starting FM_WARM positions early; iteration c evaluates, in registers, the
+// forward and reverse stages at staggered positions, each from values that
+// earlier stages or iterations produced:
+//   s1  face c+6 fluxes, cell c+5 Ftd (stage 1)    s6  cell c+2: limiter ratios reversed
+//   s2  cell c+4 ratios rp, rm (stage 2)           s7  cell c+1: adjoint of Ftd complete, stage 1 reversed
+//   s3  face c+4 limiter C (stage 3)               s8  face c+1: adjoint of its fluxes and its velocity
+//   s4  cell c+3: stage 4 reversed (reads lF)      s9  cell c: adjoint of the sweep's input F
+//   s5  face c+3: the limiter's adjoint, routed to the cell whose ratio it took
+// Adjoint contributions are added where they arise into short windows of
+// accumulators (per cell: lrp, lrm, the adjoint of Ftd, of dv, of the input
+// F; per face: of A).  The forward values are the forward kernel's own
+// expressions (fct_line.cuh), so every switch is the forward's.  The warm-up
+// positions recompute what the previous segment also computes and write
+// nothing; FM_WARM = 12 covers the pipeline's reach (a window entry from
+// before the march start influences outputs at most 11 positions later).
+// lF is updated in place: a warp reads the lF of the cells before its segment
+// during its warm-up and of the three cells after it into registers, then the
+// block synchronises before any warp writes lF.  lvel is read and written only
+// by the warp that owns the face.
+constexpr int FM_LANES = 32, FM_WARM = 12;
+
+template <int DIR>
+struct FmLine {
+    const fct::Sweep<DIR> S;
+    const float* Fl;    // F of the line, position 0
+    const float* Vl;    // face velocity of the line
+    double* lFl;
+    double* lvell;
+    int gs, n, c0, c1;  // stride along the line; the warp's segment [c0, c1]
+    bool live;          // the lane has a line
+    double vold, dt, iK4, hq, K1, dvfac;
+    // forward windows (FP32), positions relative to the iteration's c
+    float F5, V5, lo5;              // F, V and the low-order flux at position c+5
+    float A2, A3, A4, A5;           // antidiffusive flux of faces c+2 .. c+5
+    float T1, T2, T3, T4;           // Ftd of cells c+1 .. c+4
+    float TM1, TM2, TM3, TM4;       // stage-1 flux term of cells c+1 .. c+4
+    unsigned in1;                   // bit q-1: stage 1 of cell c+q was not clamped
+    float dv3, dv4, rdv3, rdv4;     // dv and RN(1/dv) of cells c+3, c+4
+    float rp2, rm2, rp3, rm3;       // ratios of cells c+2, c+3
+    float C3;                       // limiter of face c+3
+    // reverse windows (FP64)
+    double lX2;                     // adjoint of X (stage 4) of cell c+2
+    double LRP2, LRM2;              // adjoint of rp, rm of cell c+2 (face c+2 routed)
+    double LT1, LT2;                // adjoint of Ftd of cells c+1, c+2 (partial)
+    double LA1, LA2;                // adjoint of A of faces c+1, c+2 (partial)
+    double LD1, LD2;                // adjoint of dv of cells c+1, c+2 (partial)
+    double ID1, ID2;                // 1/dv of cells c+1, c+2
+    double ldv0, lterm0;            // final adjoints of dv and of the stage-1 sum of cell c
+    double LF0;                     // adjoint of the input F of cell c (face c added)
+    double tail[3];                 // lF of cells c1+1 .. c1+3
+    float F0;                       // F of cell c
+    // the global loads of the next iteration, issued one iteration early
+    float pF6, pV6, pF1, pV1;       // F, V at position c+6; F, V at position c+1
+    double plf, plv;                // lF of cell c+3 (stage 4), lvel of face c+1
+
+    __device__ FmLine(const Geom& g) : S(g) {}
+
+    __device__ __forceinline__ float ldF(int q) const { return (q >= 0 && q <= n + 1) ? __ldg(Fl + q * gs) : 0.0f; }
+    __device__ __forceinline__ float ldV(int f) const { return (f >= 1 && f <= n + 1) ? __ldg(Vl + f * gs) : 0.0f; }
+    __device__ __forceinline__ bool owned(int q) const { return live && q >= c0 && q <= c1; }
+    // lF of cell e as stage 4 reads it: own and earlier cells from memory, the
+    // three after the segment from the registers loaded before the block barrier
+    __device__ __forceinline__ double lf_at(int e) const {
+        if (!live || e < 1 || e > n || e > c1 + 3) return 0.0;
+        return e <= c1 ? lFl[e * gs] : (e == c1 + 1 ? tail[0] : (e == c1 + 2 ? tail[1] : tail[2]));
+    }
+    __device__ __forceinline__ void prefetch(int c) {
+        pF6 = ldF(c + 6);
+        pV6 = ldV(c + 6);
+        pF1 = ldF(c + 1);
+        pV1 = ldV(c + 1);
+        plf = lf_at(c + 3);
+        plv = owned(c + 1) && c + 1 >= 1 ? lvell[(c + 1) * gs] : 0.0;
+    }
+
+    __device__ void init(int cs) {
+        F5 = ldF(cs + 5);
+        V5 = ldV(cs + 5);
+        lo5 = 0.0f;
+        if (cs + 5 >= 1 && cs + 5 <= n + 1) {
+            float a;
+            fct::flux(V5, ldF(cs + 4), F5, S.dt, lo5, a);
+        }
+        A2 = A3 = A4 = A5 = 0.0f;
+        T1 = T2 = T3 = T4 = 0.0f;
+        TM1 = TM2 = TM3 = TM4 = 0.0f;
+        in1 = 0u;
+        dv3 = dv4 = rdv3 = rdv4 = 1.0f;
+        rp2 = rm2 = rp3 = rm3 = 0.0f;
+        C3 = 0.0f;
+        lX2 = LRP2 = LRM2 = LT1 = LT2 = LA1 = LA2 = LD1 = LD2 = ID1 = ID2 = 0.0;
+        ldv0 = lterm0 = LF0 = 0.0;
+        tail[0] = tail[1] = tail[2] = 0.0;
+        F0 = ldF(cs);
+    }
+
+    __device__ void load_tail() {
+        for (int q = 0; q < 3; ++q) {
+            const int e = c1 + 1 + q;
+            tail[q] = (live && e >= 1 && e <= n) ? lFl[e * gs] : 0.0;
+        }
+    }
+
+    // One iteration; the caller has issued prefetch(c).
+    __device__ __forceinline__ void step(int c) {
+        const float V6 = pV6, F6 = pF6, Fc1 = pF1, Vc1 = pV1;
+        const double lf3 = plf, lv1 = plv;
+        prefetch(c + 1);
+        // s1: face c+6, cell c+5
+        float lo6 = 0.0f, A6 = 0.0f;
+        if (c + 6 >= 1 && c + 6 <= n + 1) fct::flux(V6, F5, F6, S.dt, lo6, A6);
+        float T5 = 0.0f, TM5 = 0.0f, dv5 = 1.0f, rdv5 = 1.0f;
+        bool I5 = false;
+        if (c + 5 >= 1 && c + 5 <= n) {
+            dv5 = S.dv(V5, V6);
+            rdv5 = __frcp_rn(dv5);
+            TM5 = S.term(lo5, lo6);
+            const float o = div_rn_pre((F5 + TM5) * S.vol, dv5, rdv5);  // fct::ftd_from
+            I5 = !(o > 1.0f || o < 0.0f);
+            T5 = I5 ? o : clamp01f(o);
+        }
+        // s2: cell c+4
+        float rp4 = 0.0f, rm4 = 0.0f;
+        if (c + 4 >= 1 && c + 4 <= n) fct::limiter(S, T3, T4, T5, A4, A5, rp4, rm4);
+        // s3: face c+4 (face 1's limiter is never written: 0)
+        const float C4 = (c + 4 >= 2 && c + 4 <= n + 1) ? fct::face_limit(A4, rp3, rm3, rp4, rm4) : 0.0f;
+        // s4: cell c+3
+        double lX3 = 0.0, LD3 = 0.0, LT3 = 0.0, ID3 = 0.0;
+        const int e3 = c + 3;
+        if (e3 >= 1 && e3 <= n) {
+            const float out = fct::stage4(S, T3, A3, C3, A4, C4, dv3, rdv3);
+            const double g4 = (out >= 0.0f && out <= 1.0f) ? lf3 : 0.0;
+            ID3 = rcp64((double)dv3);
+            const double X = ((double)A4 * C4 - (double)A3 * C3) * iK4;
+            lX3 = -g4 * vold * ID3;
+            LD3 = g4 * X * vold * ID3 * ID3;
+            LT3 = g4;
+        }
+        // s5: face c+3 (lX of cells outside 1 .. n is 0)
+        double LRP3 = 0.0, LRM3 = 0.0, LA3 = 0.0;
+        if (c + 3 >= 1 && c + 3 <= n + 1) {
+            LA3 = (lX2 - lX3) * (double)C3 * iK4;
+            if (c + 3 >= 2) {
+                const double lC = (lX2 - lX3) * (double)A3 * iK4;
+                if (A3 >= 0.0f) {
+                    if (rp3 <= rm2) LRP3 += lC;
+                    else LRM2 += lC;
+                } else {
+                    if (rp2 <= rm3) LRP2 += lC;
+                    else LRM3 += lC;
+                }
+            }
+        }
+        // s6: cell c+2 (its lrp, lrm are complete)
+        if (c + 2 >= 1 && c + 2 <= n) {
+            const float a0 = A2, a1 = A3;
+            const float pp = fmaxf(0.0f, a0) - fminf(0.0f, a1);
+            const float pm = fmaxf(0.0f, a1) - fminf(0.0f, a0);
+            const float fc = T2, fl = T1, fh = T3;
+            // rp = fminf(1, RN(qp/pp)) follows qp/pp exactly when RN(qp/pp) < 1,
+            // i.e. qp < pp (1 - 2^-25) (exact in FP64): no division needed
+            double lqp = 0.0, lqm = 0.0, dpp = 0.0, dpm = 0.0;
+            if (LRP2 != 0.0) {
+                const float qp = (fmaxf(fc, fmaxf(fl, fh)) - fc) * S.hq;
+                if (pp > 0.0f && (double)qp < (double)pp * (1.0 - 0x1p-25)) {
+                    const double ip = rcp64((double)pp);
+                    lqp = LRP2 * ip;
+                    dpp = -lqp * (double)qp * ip;
+                }
+            }
+            if (LRM2 != 0.0) {
+                const float qm = (fc - fminf(fc, fminf(fl, fh))) * S.hq;
+                if (pm > 0.0f && (double)qm < (double)pm * (1.0 - 0x1p-25)) {
+                    const double ip = rcp64((double)pm);
+                    lqm = LRM2 * ip;
+                    dpm = -lqm * (double)qm * ip;
+                }
+            }
+            // the extrema: the cell each one returned (the first argument on a tie)
+            const int in_mx = (fl >= fh) ? 0 : 2;
+            const int smx = (fc >= (in_mx == 0 ? fl : fh)) ? 1 : in_mx;
+            const int in_mn = (fl <= fh) ? 0 : 2;
+            const int smn = (fc <= (in_mn == 0 ? fl : fh)) ? 1 : in_mn;
+            const double lmx = lqp * hq, lmn = -lqm * hq;
+            LT2 += -lqp * hq + lqm * hq;
+            // ghosts (cells 0, n+1) take no extremum adjoint
+            if (smx == 0) { if (c + 1 >= 1) LT1 += lmx; }
+            else if (smx == 1) LT2 += lmx;
+            else if (c + 3 <= n) LT3 += lmx;
+            if (smn == 0) { if (c + 1 >= 1) LT1 += lmn; }
+            else if (smn == 1) LT2 += lmn;
+            else if (c + 3 <= n) LT3 += lmn;
+            // pp, pm of this cell depend on A of its lower (a0) and upper (a1) face
+            LA2 += (a0 > 0.0f ? dpp : 0.0) - (a0 < 0.0f ? dpm : 0.0);
+            LA3 += -(a1 < 0.0f ? dpp : 0.0) + (a1 > 0.0f ? dpm : 0.0);
+        }
+        // s7: cell c+1 (the adjoint of its Ftd is complete)
+        double lterm1 = 0.0, ldv1 = 0.0, LF1 = 0.0;
+        if (c + 1 >= 1 && c + 1 <= n) {
+            const double h = (in1 & 1u) ? LT1 : 0.0;
+            lterm1 = h * vold * ID1;
+            ldv1 = LD1 - h * ((double)Fc1 + (double)TM1) * vold * ID1 * ID1;
+            LF1 = lterm1;
+        } else if (owned(c + 1)) {  // ghost cell: the sweep leaves it, its adjoint passes through
+            LF1 = lFl[(c + 1) * gs];
+        }
+        // s8: face c+1
+        if (c + 1 >= 1 && c + 1 <= n + 1) {
+            const double l_LF = K1 * (lterm1 - lterm0);
+            const double l_A = LA1;
+            const float uf = Vc1, Fc0 = F0;
+            const float Fh = (uf <= 0.0f) ? Fc0 : Fc1;
+            const float Flo = (uf >= 0.0f) ? Fc0 : Fc1;
+            if (owned(c + 1))
+                lvell[(c + 1) * gs] = lv1 + (l_LF * dt * (double)Flo + l_A * dt * ((double)Fh - (double)Flo) +
+                                             dvfac * (ldv1 - ldv0));
+            const double w = (double)uf * dt;
+            if (uf < 0.0f) LF1 += l_LF * w;  // upper cell of the face
+            LF1 += l_A * w * ((uf > 0.0f ? 1.0 : 0.0) - (uf < 0.0f ? 1.0 : 0.0));
+            if (uf >= 0.0f) LF0 += l_LF * w;  // lower cell
+            LF0 += l_A * w * ((uf <= 0.0f ? 1.0 : 0.0) - (uf >= 0.0f ? 1.0 : 0.0));
+        }
+        // s9: cell c
+        if (owned(c)) lFl[c * gs] = LF0;
+        // shift the windows by one position
+        F0 = Fc1;
+        F5 = F6;
+        V5 = V6;
+        lo5 = lo6;
+        A2 = A3; A3 = A4; A4 = A5; A5 = A6;
+        T1 = T2; T2 = T3; T3 = T4; T4 = T5;
+        TM1 = TM2; TM2 = TM3; TM3 = TM4; TM4 = TM5;
+        in1 = (in1 >> 1) | (I5 ? 8u : 0u);
+        dv3 = dv4; dv4 = dv5; rdv3 = rdv4; rdv4 = rdv5;
+        rp2 = rp3; rm2 = rm3; rp3 = rp4; rm3 = rm4;
+        C3 = C4;
+        lX2 = lX3;
+        LRP2 = LRP3; LRM2 = LRM3;
+        LT1 = LT2; LT2 = LT3;
+        LA1 = LA2; LA2 = LA3;
+        LD1 = LD2; LD2 = LD3;
+        ID1 = ID2; ID2 = ID3;
+        ldv0 = ldv1;
+        lterm0 = lterm1;
+        LF0 = LF1;
+    }
+};
+
+#ifndef VOF_FM_MINB
+#define VOF_FM_MINB 4
+#endif
+template <int DIR, int WARPS>
+__global__ void __launch_bounds__(FM_LANES * WARPS, VOF_FM_MINB) k_fct_adjoint_march(Geom g, const float* __restrict__ Fg,
+                                                                        const float* __restrict__ velg,
+                                                                        double* lFg, double* __restrict__ lvelg) {
+    FmLine<DIR> L(g);
+    const int n = L.S.n;
+    const int na = DIR == 0 ? g.ny : g.nx;  // lines along a (one per lane)
+    const int lane = threadIdx.x, warp = threadIdx.y;
+    int a = 1 + blockIdx.x * FM_LANES + lane;
+    const int b = 1 + blockIdx.y;
+    L.live = a <= na;
+    if (!L.live) a = na;  // a valid line to read; nothing is written
+    const int base = DIR == 0 ? gidx(g, 0, a, b) : (DIR == 1 ? gidx(g, a, 0, b) : gidx(g, a, b, 0));
+    L.gs = DIR == 0 ? 1 : (DIR == 1 ? g.px : g.plane);
+    L.n = n;
+    L.Fl = Fg + base;
+    L.Vl = velg + base;
+    L.lFl = lFg + base;
+    L.lvell = lvelg + base;
+    const int seg = (n + 2 + WARPS - 1) / WARPS;
+    L.c0 = warp * seg;
+    L.c1 = min(n + 1, L.c0 + seg - 1);
+    const float vol = g.dx * g.dy * g.dz;
+    L.vold = (double)vol;
+    L.dt = (double)g.dt;
+    L.iK4 = 1.0 / (double)L.S.h4;
+    L.hq = (double)L.S.hq;
+    L.K1 = DIR == 0 ? (double)g.dy * g.dz / L.vold
+                    : (DIR == 1 ? (double)g.dy / ((double)g.dx * g.dy) : (double)g.dy * g.dx / L.vold);
+    L.dvfac = (double)L.S.dvfac;
+    const int cs = L.c0 - FM_WARM;
+    L.init(cs);
+    L.load_tail();
+    L.prefetch(cs);
+    for (int t = 0; t < FM_WARM; ++t) L.step(cs + t);
+    __syncthreads();  // every warp has read the lF it needs from its neighbours
+    for (int c = L.c0; c <= L.c1; ++c) L.step(c);
+}
+
 // ---- boundary copies, reversed ---------------------------------------------------
 __global__ void k_adj_bcF_z(Geom g, double* __restrict__ l) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -699,7 +993,7 @@ __global__ void __launch_bounds__(256) k_adj_update(Geom g, Range R, const float
             const double gv = lvel[a][c];
             lvs_[a][c] = gv;
             if (gv != 0.0) {
-                const double ir = 1.0 / (double)(0.5f * (rho_c + rho_of(g, F[m])));
+                const double ir = rcp64((double)(0.5f * (rho_c + rho_of(g, F[m]))));
                 lpc -= gv * dt * ir * hinv[a];
                 lrc += 0.5 * gv * dt * (pc - (double)p[m]) * hinv[a] * ir * ir;
             }
@@ -708,7 +1002,7 @@ __global__ void __launch_bounds__(256) k_adj_update(Geom g, Range R, const float
             const int q = c + st[a];
             const double gv = lvel[a][q];
             if (gv != 0.0) {
-                const double ir = 1.0 / (double)(0.5f * (rho_of(g, F[q]) + rho_c));
+                const double ir = rcp64((double)(0.5f * (rho_of(g, F[q]) + rho_c)));
                 lpc += gv * dt * ir * hinv[a];
                 lrc += 0.5 * gv * dt * ((double)p[q] - pc) * hinv[a] * ir * ir;
             }
@@ -753,6 +1047,129 @@ __global__ void __launch_bounds__(256) k_adj_jacobi(Geom g, Range R, InvAp ia, c
     lrhs[c] = mode == 0 ? mu : lrhs[c] + mu;
 }
 
+// Two consecutive transposed sweeps in one pass (modes as k_adj_jacobi: A is 0
+// or 1, B is 1 or 2): stage A on lin gives mu_a, stage B on mu_a gives the
+// output; lrhs takes mu_a (A == 0: lrhs = mu_a, else lrhs += mu_a) and then
+// mu_b (B == 1).  A block owns a 32 x 8 column tile and a chunk of planes and
+// marches up in k with plane rings in shared memory: lin with a two-cell
+// in-plane halo, mu_a with a one-cell halo (computed redundantly at the tile
+// edge), so HBM sees lin, lrhs and the output once per two sweeps.
+constexpr int AJ_TX = 32, AJ_TY = 8, AJ_T = AJ_TX * AJ_TY;
+constexpr int AJ_NIN = (AJ_TY + 4) * (AJ_TX + 4), AJ_NA = (AJ_TY + 2) * (AJ_TX + 2);
+// A point of a plane tile with its in-plane geometry: shared index, global
+// in-plane offset, wall flags (bits 0..3 of wall_flags) and whether it is a cell.
+struct AjPoint {
+    int sidx, off, flags;
+    bool cell;
+};
+__device__ __forceinline__ AjPoint aj_point(const Geom& g, int q, int w, int h, int i0, int j0) {
+    const int y = q / w, x = q % w;
+    const int i = i0 - h + x, j = j0 - h + y;
+    AjPoint p;
+    p.sidx = q;
+    p.cell = i >= 1 && i <= g.nx && j >= 1 && j <= g.ny;
+    p.off = p.cell ? gidx(g, i, j, 0) : 0;
+    p.flags = (i == 1) | ((i == g.nx) << 1) | ((j == 1) << 2) | ((j == g.ny) << 3);
+    return p;
+}
+// -N at a point of a ring of planes (row width w) from its in-plane flags and k
+__device__ __forceinline__ double aj_negN(const double* pc, const double* pm, const double* pp, int q, int w,
+                                          int flags, int k, int nz, double cxx, double cyy, double czz) {
+    double s = 0.0;
+    if (!(flags & 2)) s += cxx * pc[q + 1];
+    if (!(flags & 1)) s += cxx * pc[q - 1];
+    if (!(flags & 8)) s += cyy * pc[q + w];
+    if (!(flags & 4)) s += cyy * pc[q - w];
+    if (k != nz) s += czz * pp[q];
+    if (k != 1) s += czz * pm[q];
+    return -s;
+}
+template <int A, int B>
+__global__ void __launch_bounds__(AJ_T) k_adj_jacobi2(Geom g, InvAp ia, const double* __restrict__ lin,
+                                                     double* __restrict__ lout, double* __restrict__ lrhs,
+                                                     int kchunk) {
+    constexpr int WI = AJ_TX + 4, WA = AJ_TX + 2;
+    __shared__ double sIn[3][AJ_NIN];
+    __shared__ double sA[3][AJ_NA];
+    const int tid = threadIdx.y * AJ_TX + threadIdx.x;
+    const int i0 = 1 + blockIdx.x * AJ_TX, j0 = 1 + blockIdx.y * AJ_TY;
+    const int k0 = 1 + blockIdx.z * kchunk, k1 = min(g.nz, k0 + kchunk - 1);
+    const double cxx = (double)(g.dxi * g.dxi), cyy = (double)(g.dyi * g.dyi), czz = (double)(g.dzi * g.dzi);
+    const int plane = g.plane;
+    // this thread's points: two of the lin tile (halo 2), two of the stage-A tile (halo 1), one output
+    const AjPoint L0 = aj_point(g, tid, WI, 2, i0, j0);
+    const bool has_l1 = tid + AJ_T < AJ_NIN;
+    const AjPoint L1 = aj_point(g, has_l1 ? tid + AJ_T : tid, WI, 2, i0, j0);
+    const AjPoint S0 = aj_point(g, tid, WA, 1, i0, j0);
+    const bool has_s1 = tid + AJ_T < AJ_NA;
+    const AjPoint S1 = aj_point(g, has_s1 ? tid + AJ_T : tid, WA, 1, i0, j0);
+    // the stage-A point's index in the lin tile: (y + 1) * WI + x + 1
+    const int S0in = (S0.sidx / WA + 1) * WI + S0.sidx % WA + 1, S1in = (S1.sidx / WA + 1) * WI + S1.sidx % WA + 1;
+    const int io = i0 + (int)threadIdx.x, jo = j0 + (int)threadIdx.y;
+    const bool out_ok = io <= g.nx && jo <= g.ny;
+    const int oflags = (io == 1) | ((io == g.nx) << 1) | ((jo == 1) << 2) | ((jo == g.ny) << 3);
+    const int ooff = out_ok ? gidx(g, io, jo, 0) : 0;
+    const int oA = (threadIdx.y + 1) * WA + threadIdx.x + 1;
+    auto slot = [](int k) { return (k + 3) % 3; };  // k >= -2
+    auto kflags = [&](int k) { return ((k == 1) << 4) | ((k == g.nz) << 5); };
+    auto ld = [&](const AjPoint& p, int k) { return (p.cell && k >= 1 && k <= g.nz) ? lin[p.off + k * plane] : 0.0; };
+    // lin of the first plane in registers
+    double n0 = ld(L0, k0 - 2), n1 = has_l1 ? ld(L1, k0 - 2) : 0.0;
+    for (int t = k0 - 3; t <= k1 + 1; ++t) {
+        // lin at plane t+1 into the ring; the next plane's loads go out now
+        {
+            const int sl = slot(t + 1);
+            sIn[sl][L0.sidx] = n0;
+            if (has_l1) sIn[sl][L1.sidx] = n1;
+            n0 = ld(L0, t + 2);
+            if (has_l1) n1 = ld(L1, t + 2);
+        }
+        const int kb = t - 1;
+        const bool do_b = kb >= k0 && out_ok;
+        const double rhs_old = (A == 1 && do_b) ? lrhs[ooff + kb * plane] : 0.0;
+        __syncthreads();
+        // stage A at plane t on the tile and its one-cell halo
+        if (t >= k0 - 1) {
+            const int sc = slot(t);
+            const double *pc = sIn[sc], *pm = sIn[slot(t - 1)], *pp = sIn[slot(t + 1)];
+            const bool kin = t >= 1 && t <= g.nz;
+            const int kf = kflags(t);
+            {
+                double v = 0.0;
+                if (S0.cell && kin)
+                    v = (A == 0 ? pc[S0in] : aj_negN(pc, pm, pp, S0in, WI, S0.flags, t, g.nz, cxx, cyy, czz)) *
+                        ia.v[S0.flags | kf];
+                sA[sc][S0.sidx] = v;
+            }
+            if (has_s1) {
+                double v = 0.0;
+                if (S1.cell && kin)
+                    v = (A == 0 ? pc[S1in] : aj_negN(pc, pm, pp, S1in, WI, S1.flags, t, g.nz, cxx, cyy, czz)) *
+                        ia.v[S1.flags | kf];
+                sA[sc][S1.sidx] = v;
+            }
+        }
+        __syncthreads();
+        // stage B at plane t-1 on the tile
+        if (do_b) {
+            const int sb = slot(kb);
+            const double mua = sA[sb][oA];
+            const double nb = aj_negN(sA[sb], sA[slot(kb - 1)], sA[slot(kb + 1)], oA, WA, oflags, kb, g.nz, cxx, cyy,
+                                      czz);
+            const int c = ooff + kb * plane;
+            const double r = A == 0 ? mua : rhs_old + mua;
+            if (B == 1) {
+                const double mub = nb * ia.v[oflags | kflags(kb)];
+                lout[c] = mub;
+                lrhs[c] = r + mub;
+            } else {
+                lout[c] = nb;
+                lrhs[c] = r;
+            }
+        }
+    }
+}
+
 // ---- rhs = rho/dt div(u*), reversed (gather over the cells sharing a face) -------
 // Also zeroes lu / lv / lw at the faces the correction overwrote (their
 // adjoints moved to lus / lvs / lws in k_adj_update).  has_rhs = 0: no
@@ -770,7 +1187,7 @@ __global__ void __launch_bounds__(256) k_adj_rhs(Geom g, Range R, const float* _
     if (j >= 2) lv[c] = 0.0;
     if (k >= 2) lw[c] = 0.0;
     if (!has_rhs) return;
-    const double idt = 1.0 / (double)g.dt, dxi = (double)g.dxi, dyi = (double)g.dyi, dzi = (double)g.dzi;
+    const double idt = rcp64((double)g.dt), dxi = (double)g.dxi, dyi = (double)g.dyi, dzi = (double)g.dzi;
     const double gr = lrhs[c];
     const double div = ((double)us[c + 1] - us[c]) * dxi + ((double)vs[c + sy] - vs[c]) * dyi +
                        ((double)ws[c + sz] - ws[c]) * dzi;
@@ -834,19 +1251,16 @@ __device__ __forceinline__ double adj_momentum(const Geom& g, int c, int i, int 
     const double Gd = G * (double)g.dt;
     lnu += Gd * ((qxm - 2.0 * qc + qxp) * hx2 + (qym - 2.0 * qc + qyp) * hy2 + (qzm - 2.0 * qc + qzp) * hz2);
     double own = G - Gd * nuc * 2.0 * (hx2 + hy2 + hz2);
-    atomicAdd(lq + c - sx, Gd * nuc * hx2);
-    atomicAdd(lq + c + sx, Gd * nuc * hx2);
-    atomicAdd(lq + c - sy, Gd * nuc * hy2);
-    atomicAdd(lq + c + sy, Gd * nuc * hy2);
-    atomicAdd(lq + c - sz, Gd * nuc * hz2);
-    atomicAdd(lq + c + sz, Gd * nuc * hz2);
+    // neighbours along each axis: viscous term, plus the upwind difference
+    // on the side the forward took (one atomic per neighbour)
     const double ga = -Gd * (double)a, gb = -Gd * (double)b, gc = -Gd * (double)cc;
-    if (ux) { own += ga * hx; atomicAdd(lq + c - sx, -ga * hx); }
-    else { atomicAdd(lq + c + sx, ga * hx); own -= ga * hx; }
-    if (uy) { own += gb * hy; atomicAdd(lq + c - sy, -gb * hy); }
-    else { atomicAdd(lq + c + sy, gb * hy); own -= gb * hy; }
-    if (uz) { own += gc * hz; atomicAdd(lq + c - sz, -gc * hz); }
-    else { atomicAdd(lq + c + sz, gc * hz); own -= gc * hz; }
+    const double vx = Gd * nuc * hx2, vy = Gd * nuc * hy2, vz = Gd * nuc * hz2;
+    if (ux) { own += ga * hx; atomicAdd(lq + c - sx, vx + -ga * hx); atomicAdd(lq + c + sx, vx); }
+    else { own -= ga * hx; atomicAdd(lq + c - sx, vx); atomicAdd(lq + c + sx, vx + ga * hx); }
+    if (uy) { own += gb * hy; atomicAdd(lq + c - sy, vy + -gb * hy); atomicAdd(lq + c + sy, vy); }
+    else { own -= gb * hy; atomicAdd(lq + c - sy, vy); atomicAdd(lq + c + sy, vy + gb * hy); }
+    if (uz) { own += gc * hz; atomicAdd(lq + c - sz, vz + -gc * hz); atomicAdd(lq + c + sz, vz); }
+    else { own -= gc * hz; atomicAdd(lq + c - sz, vz); atomicAdd(lq + c + sz, vz + gc * hz); }
     const double l_a = -Gd * dqdx, l_b = -Gd * dqdy, l_c = -Gd * dqdz;
     if (COMP == 0) {
         own += l_a;
@@ -995,9 +1409,24 @@ size_t fa_smem_limit() {
     return lim;
 }
 
+#ifndef VOF_FM_WARPS
+#define VOF_FM_WARPS 4
+#endif
+constexpr int FM_WARPS = VOF_FM_WARPS;
+template <int DIR>
+cudaError_t launch_fct_adjoint_march(const Geom& g, const float* Fs, const float* vel, double* lF, double* lvel,
+                                     cudaStream_t s) {
+    const int na = DIR == 0 ? g.ny : g.nx;
+    const int nb = DIR == 2 ? g.ny : g.nz;
+    k_fct_adjoint_march<DIR, FM_WARPS><<<dim3((na + FM_LANES - 1) / FM_LANES, nb), dim3(FM_LANES, FM_WARPS), 0, s>>>(
+        g, Fs, vel, lF, lvel);
+    return cudaGetLastError();
+}
+
 template <int DIR>
 cudaError_t sweep_adjoint(AdjEngine& e, const float* Fs, const float* vel, double* lvel, cudaStream_t s) {
     const Geom& g = e.g;
+    if (e.fct_march) return launch_fct_adjoint_march<DIR>(g, Fs, vel, e.lF, lvel, s);
     {  // one fused kernel when a block of lines fits in shared memory
         const int n = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
         // the most lines per block with at least two blocks per SM, else the most that fit
@@ -1162,14 +1591,26 @@ cudaError_t reverse_step(AdjEngine& e, const StepData& d, int istep, cudaStream_
         if (r != cudaSuccess) return r;
         if ((r = cudaMemsetAsync(e.lp[e.lp_cur], 0, e.elems * sizeof(double), s)) != cudaSuccess) return r;
     } else if (e.jacobi_iters > 0) {
-        k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.inv_ap, e.lp[e.lp_cur], e.lp[e.lp_cur ^ 1], e.lrhs, 0);
-        e.lp_cur ^= 1;
-        for (int it = 1; it < e.jacobi_iters; ++it) {
-            k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.inv_ap, e.lp[e.lp_cur], e.lp[e.lp_cur ^ 1], e.lrhs, 1);
+        // stages 0, 1 x (iters - 1), 2, two per launch
+        const int nst = e.jacobi_iters + 1;
+        const int nch = (g.nz + 23) / 24, kchunk = (g.nz + nch - 1) / nch;
+        const dim3 gj((g.nx + AJ_TX - 1) / AJ_TX, (g.ny + AJ_TY - 1) / AJ_TY, (g.nz + kchunk - 1) / kchunk);
+        const dim3 bj(AJ_TX, AJ_TY);
+        auto mode_of = [&](int q) { return q == 0 ? 0 : (q == nst - 1 ? 2 : 1); };
+        for (int q = 0; q < nst; q += 2) {
+            const double* in = e.lp[e.lp_cur];
+            double* out = e.lp[e.lp_cur ^ 1];
+            if (q + 1 < nst) {
+                const int a = mode_of(q), b = mode_of(q + 1);
+                if (a == 0 && b == 1) k_adj_jacobi2<0, 1><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
+                else if (a == 0) k_adj_jacobi2<0, 2><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
+                else if (b == 1) k_adj_jacobi2<1, 1><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
+                else k_adj_jacobi2<1, 2><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
+            } else {
+                k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.inv_ap, in, out, e.lrhs, mode_of(q));
+            }
             e.lp_cur ^= 1;
         }
-        k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.inv_ap, e.lp[e.lp_cur], e.lp[e.lp_cur ^ 1], e.lrhs, 2);
-        e.lp_cur ^= 1;
     }
     k_adj_rhs<<<gi, kBlk, 0, s>>>(g, I, d.F, d.us, d.vs, d.ws, e.lrhs, e.lus, e.lvs, e.lws, e.lrho, e.lu, e.lv, e.lw,
                                   e.conv || e.jacobi_iters > 0);
@@ -1187,16 +1628,16 @@ int adj_kernels_per_step(const AdjEngine& e) {
     // are not kept (front 2, pressure, correction 1, two sweeps), and the
     // adjoint kernels: F copies 3, the three sweep adjoints (1 launch each when
     // fused, else 8), velocity copies 3, correction 1, the transposed Jacobi
-    // sweeps (iters + 1), rhs 1, advection 1.  The convergent modes' pressure
+    // sweeps (iters + 1 stages, two per launch), rhs 1, advection 1.  The convergent modes' pressure
     // solves (multigrid graphs) are not counted.
     const Geom& g = e.g;
     const int P = e.conv ? 0 : plain_phase_launches(PHASE_JACOBI, e.jacobi_iters);
     int sweeps = 0;
     const int len[3] = {g.nx, g.ny, g.nz};
-    for (int a = 0; a < 3; ++a) sweeps += fa_smem_bytes(2, len[a]) <= fa_smem_limit() ? 1 : 8;
+    for (int a = 0; a < 3; ++a) sweeps += (e.fct_march || fa_smem_bytes(2, len[a]) <= fa_smem_limit()) ? 1 : 8;
     const int replay = 2 + P + 1 + 3;
     const int recompute = e.keep ? 0 : 2 + P + 1 + 2;
-    const int jac = (!e.conv && e.jacobi_iters > 0) ? e.jacobi_iters + 1 : 0;
+    const int jac = (!e.conv && e.jacobi_iters > 0) ? (e.jacobi_iters + 2) / 2 : 0;
     return replay + recompute + 3 + sweeps + 3 + 1 + jac + 1 + 1;
 }
 
@@ -1208,6 +1649,7 @@ cudaError_t adj_create(const Geom& g, int jacobi_iters, int mg_mode, double tol,
     e->conv = mg_mode != 0;
     e->tol = tol;
     e->max_outer = max_outer;
+    e->fct_march = 1;
     e->elems = (size_t)g.plane * (g.nz + 2);
     cudaError_t r;
     auto alloc = [&](void** p, size_t nb) -> cudaError_t {

@@ -15,11 +15,8 @@
 //   the limiter c of the first face (c[1]) is 0; the wall-face velocities
 //   are 0 after apply_bc_velocity, so the ghost F values enter only as 0*F.
 //
-// Q2 length factors of the reference, per sweep (x | y | z):
-//   stage 1 flux term  (f_l - f_r)*dy*dz/vol | (f_l - f_r)*dy/(dx*dy) | (f_l - f_r)*dy*dx/vol
-//   dv factor          dt*dy*dz              | dt*dx*dz               | dt*dx*dy
-//   limiter q          *dx                   | *dx                    | *dz
-//   stage 4 divisor    /dy                   | /dy                    | /dz
+// The per-cell expressions (and the reference's length factors per sweep)
+// are in fct_line.cuh, shared with the sweep adjoint.
 //
 // Kernel shape.  A block owns a tile of 32 lines (one per lane) over their
 // full length.  The tile's F and face velocity are staged once in shared
@@ -33,6 +30,7 @@
 // global memory; x results are staged and written back row-wise.
 #include <cuda_runtime.h>
 
+#include "fct_line.cuh"
 #include "fct_sweep.h"
 
 namespace vof {
@@ -49,36 +47,10 @@ constexpr int THREADS = LANES * WARPS;
 
 __host__ __device__ inline int odd_pitch(int npos) { return npos | 1; }
 
-template <int AXIS>
-struct Sweep {
-    // Per-sweep constants (see the table above) and the IEEE reciprocals of
-    // the constant divisors, for div_rn_pre.
-    float dt, vol, dvfac, hq, h4, t1a, t1b, dxdy;
-    float rvol, rh4, rdxdy;
-    int n;
-
-    __device__ Sweep(const Geom& g) {
-        dt = g.dt;
-        vol = g.dx * g.dy * g.dz;
-        n = AXIS == 0 ? g.nx : (AXIS == 1 ? g.ny : g.nz);
-        dvfac = AXIS == 0 ? g.dt * g.dy * g.dz : (AXIS == 1 ? g.dt * g.dx * g.dz : g.dt * g.dx * g.dy);
-        hq = AXIS == 2 ? g.dz : g.dx;
-        h4 = AXIS == 2 ? g.dz : g.dy;
-        t1a = g.dy;                                    // first factor of the stage-1 flux term
-        t1b = AXIS == 0 ? g.dz : (AXIS == 1 ? 0.0f : g.dx);
-        dxdy = g.dx * g.dy;
-        rvol = __frcp_rn(vol);
-        rh4 = __frcp_rn(h4);
-        rdxdy = __frcp_rn(dxdy);
-    }
-
-    // Stage-1 flux term from the low-order fluxes through the lower (fi) and
-    // upper (fo) faces of a cell.
-    __device__ __forceinline__ float term(float fi, float fo) const {
-        if (AXIS == 1) return div_rn_pre((fi - fo) * t1a, dxdy, rdxdy);
-        return div_rn_pre((fi - fo) * t1a * t1b, vol, rvol);
-    }
-};
+using fct::Sweep;
+using fct::face_limit;
+using fct::ftd_from;
+using fct::limiter;
 
 // Line accessor: smem values of one lane's line at position q.
 struct LineView {
@@ -92,49 +64,12 @@ struct LineView {
 // Low-order flux and antidiffusive flux through face fidx (between cells
 // fidx-1 and fidx), as fl_L / fl_H of the reference's stages 1-2.
 __device__ __forceinline__ void face_flux(const LineView& L, int fidx, float dt, float& lo, float& a) {
-    const float uf = L.V(fidx);
-    const float FL = L.F(fidx - 1), FR = L.F(fidx);
-    const float lo_ = (uf >= 0.0f) ? uf * dt * FL : uf * dt * FR;
-    const float hi_ = (uf <= 0.0f) ? uf * dt * FL : uf * dt * FR;
-    lo = lo_;
-    a = hi_ - lo_;
+    fct::flux(L.V(fidx), L.F(fidx - 1), L.F(fidx), dt, lo, a);
 }
 
 template <int AXIS>
 __device__ __forceinline__ float cell_dv(const Sweep<AXIS>& S, const LineView& L, int c) {
-    return S.vol - S.dvfac * (L.V(c + 1) - L.V(c));
-}
-
-// Stage 1: low-order update of cell c from its face fluxes; rdv = RN(1/dv).
-template <int AXIS>
-__device__ __forceinline__ float ftd_from(const Sweep<AXIS>& S, float Fc, float lo_in, float lo_out, float dv,
-                                         float rdv) {
-    float out = div_rn_pre((Fc + S.term(lo_in, lo_out)) * S.vol, dv, rdv);
-    if (out > 1.0f || out < 0.0f) out = clamp01f(out);
-    return out;
-}
-
-// Stage 2: Zalesak ratios of a cell.
-template <int AXIS>
-__device__ __forceinline__ void limiter(const Sweep<AXIS>& S, float tm, float tc, float tp, float al,
-                                        float ar, float& rp, float& rm) {
-    const float fmx = fmaxf(tc, fmaxf(tm, tp));
-    const float fmn = fminf(tc, fminf(tm, tp));
-    // rp = pp > 0 ? fminf(1, qp/pp) : 0, skipping the division when
-    // qp >= pp (then qp/pp >= 1 and its rounding is >= 1 too).
-    const float pp = fmaxf(0.0f, al) - fminf(0.0f, ar);
-    const float qp = (fmx - tc) * S.hq;
-    rp = 0.0f;
-    if (pp > 0.0f) rp = (qp >= pp) ? 1.0f : fminf(1.0f, qp / pp);
-    const float pm = fmaxf(0.0f, ar) - fminf(0.0f, al);
-    const float qm = (tc - fmn) * S.hq;
-    rm = 0.0f;
-    if (pm > 0.0f) rm = (qm >= pm) ? 1.0f : fminf(1.0f, qm / pm);
-}
-
-// Stage 3: limiter of face f from the ratios of its two cells.
-__device__ __forceinline__ float face_limit(float af, float rp_lo, float rm_lo, float rp_hi, float rm_hi) {
-    return (af >= 0.0f) ? fminf(rp_hi, rm_lo) : fminf(rp_lo, rm_hi);
+    return S.dv(L.V(c), L.V(c + 1));
 }
 
 // ---- from-scratch evaluation (segment warm-up only) -------------------------
@@ -273,7 +208,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, float* F, const floa
             float rp1 = 0.0f, rm1 = 0.0f;
             if (c + 1 <= n) limiter(S, T0, T1, T2, a1f, a2f, rp1, rm1);
             const float cf1 = face_limit(a1f, rp0, rm0, rp1, rm1);
-            float fnew = clamp01f(T0 - div_rn_pre(div_rn_pre(a1f * cf1 - a0f * cf0, S.h4, S.rh4) * S.vol, dv0, rdv0));
+            float fnew = clamp01f(fct::stage4(S, T0, a0f, cf0, a1f, cf1, dv0, rdv0));
             if (FINAL) fnew = clamp01f(fnew);  // post_process_f_kernel, voftrial1.cu:502-507
 
             if (AXIS == 0) {

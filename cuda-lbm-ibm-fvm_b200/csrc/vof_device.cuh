@@ -67,6 +67,21 @@ __device__ __forceinline__ float div_rn_pre(float x, float d, float rd) {
     return __fdiv_rn(x, d);
 }
 
+// 1/x for a positive normal FP64 x, to within about one ulp (not always
+// correctly rounded), for the FP64 partial derivatives of the adjoint; the
+// FP32 forward never uses it.  Method: Newton-Raphson iteration for the
+// reciprocal, r <- r + r (1 - x r), each step squaring the relative error,
+// started from the PTX approximation rcp.approx.ftz.f64; two steps take the
+// error of that approximation below the FP64 rounding error.
+__device__ __forceinline__ double rcp64(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = __fma_rn(-x, r, 1.0);
+    r = __fma_rn(r, e, r);
+    e = __fma_rn(-x, r, 1.0);
+    return __fma_rn(r, e, r);
+}
+
 // rho and nu from the volume fraction (voftrial1.cu:95-104), same operand order.
 __device__ __forceinline__ float rho_of(const Geom& g, float F) {
     const float f = clamp01f(F);

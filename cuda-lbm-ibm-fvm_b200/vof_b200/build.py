@@ -40,7 +40,8 @@ SOURCES = {
     "capi.cu": [],
     "noalloc.cu": [],
 }
-HEADERS = ["vof_device.cuh", "tma.cuh", "plain_step.h", "fct_sweep.h", "jacobi_tb.h", "mg_solve.h", "reduce.h", "adjoint.h"]
+HEADERS = ["vof_device.cuh", "tma.cuh", "plain_step.h", "fct_sweep.h", "fct_line.cuh", "jacobi_tb.h", "mg_solve.h",
+           "reduce.h", "adjoint.h"]
 
 
 def nvcc() -> str:

@@ -55,3 +55,28 @@ def test_constant_divisors_of_the_step(cuda, d):
     dd = np.full(n, d, dtype=np.float32)
     fast, ieee = run(x, dd)
     assert np.array_equal(fast.view(np.uint32), ieee.view(np.uint32))
+
+
+def test_fp64_reciprocal_within_one_ulp(cuda):
+    """vof::rcp64 (Newton-Raphson from rcp.approx.ftz.f64, used for the FP64
+    partial derivatives of the adjoint) against CUDA's correctly rounded
+    reciprocal, over the operands it sees (FP32 values widened to FP64: cell
+    volume changes, limiter sums) and random FP64 values."""
+    if not LIB.exists():
+        pytest.fail(f"{LIB} not built (__graft_entry__.build())")
+    lib = C.CDLL(str(LIB))
+    rng = np.random.default_rng(1)
+    n = 1 << 20
+    x = np.concatenate([
+        (rng.uniform(0.5, 2.0, n // 2) * np.exp2(rng.integers(-120, 120, n // 2))).astype(np.float32).astype(np.float64),
+        rng.uniform(1.0, 2.0, n // 2) * np.exp2(rng.integers(-1000, 1000, n // 2)),
+    ])
+    x[::2] *= -1.0
+    fast = np.empty_like(x)
+    ieee = np.empty_like(x)
+    P = C.POINTER(C.c_double)
+    rc = lib.rcp64test_run(x.ctypes.data_as(P), fast.ctypes.data_as(P), ieee.ctypes.data_as(P), C.c_int(x.size))
+    assert rc == 0
+    ulp = np.spacing(np.abs(ieee))
+    err = np.abs(fast - ieee) / ulp
+    assert err.max() <= 1.0, err.max()
