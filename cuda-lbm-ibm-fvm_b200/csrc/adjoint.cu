@@ -28,7 +28,9 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <initializer_list>
 #include <new>
+#include <utility>
 
 #include "adjoint.h"
 #include "fct_line.cuh"
@@ -909,9 +911,17 @@ __global__ void k_adj_bcF_x(Geom g, double* __restrict__ l) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
     if (j > g.ny + 1 || k > g.nz + 1) return;
     const int a = gidx(g, 0, j, k), b = gidx(g, 1, j, k), c = gidx(g, g.nx, j, k), d = gidx(g, g.nx + 1, j, k);
-    l[b] += l[a];
+    if (g.nx < 2) {  // b == c
+        l[b] += l[a];
+        l[a] = 0.0;
+        l[c] += l[d];
+        l[d] = 0.0;
+        return;
+    }
+    const double la = l[a], lb = l[b], lc = l[c], ld = l[d];
+    l[b] = lb + la;
     l[a] = 0.0;
-    l[c] += l[d];
+    l[c] = lc + ld;
     l[d] = 0.0;
 }
 __global__ void k_adj_bcF_y(Geom g, double* __restrict__ l) {
@@ -941,16 +951,32 @@ __global__ void k_adj_bcv_z(Geom g, double* __restrict__ lu, double* __restrict_
     lw[kf] = 0.0;
 }
 // set_bc_vel_i: u zero at i = 1 and nx + 1, v, w copied into the i ghosts.
+// (Its rows are strided in memory: all loads are issued before the stores.)
 __global__ void k_adj_bcv_x(Geom g, double* __restrict__ lu, double* __restrict__ lv, double* __restrict__ lw) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y * blockDim.y + threadIdx.y;
     if (j > g.ny + 1 || k > g.nz + 1) return;
     const int i0 = gidx(g, 0, j, k), i1 = gidx(g, 1, j, k), in = gidx(g, g.nx, j, k), ir = gidx(g, g.nx + 1, j, k);
+    if (g.nx < 2) {  // i = 1 is also i = nx
+        lu[i1] = 0.0;
+        mv(lv, i0, i1);
+        mv(lw, i0, i1);
+        lu[ir] = 0.0;
+        mv(lv, ir, in);
+        mv(lw, ir, in);
+        return;
+    }
+    const double v0 = lv[i0], v1 = lv[i1], vn = lv[in], vr = lv[ir];
+    const double w0 = lw[i0], w1 = lw[i1], wn = lw[in], wr = lw[ir];
     lu[i1] = 0.0;
-    mv(lv, i0, i1);
-    mv(lw, i0, i1);
     lu[ir] = 0.0;
-    mv(lv, ir, in);
-    mv(lw, ir, in);
+    lv[i1] = v1 + v0;
+    lv[i0] = 0.0;
+    lw[i1] = w1 + w0;
+    lw[i0] = 0.0;
+    lv[in] = vn + vr;
+    lv[ir] = 0.0;
+    lw[in] = wn + wr;
+    lw[ir] = 0.0;
 }
 // set_bc_vel_j: v zero at j = 1 and ny + 1, u, w copied into the j ghosts.
 __global__ void k_adj_bcv_y(Geom g, double* __restrict__ lu, double* __restrict__ lv, double* __restrict__ lw) {
@@ -968,21 +994,21 @@ __global__ void k_adj_bcv_y(Geom g, double* __restrict__ lu, double* __restrict_
 // ---- velocity correction, reversed (gather over the six faces of a cell) -----------
 // Face q along axis a (its cells q - st and q): u_q = u*_q - dt/r (p_q - p_{q-st}) h^-1,
 // r = (rho_q + rho_{q-st}) / 2.  Cell c collects, from its lower faces (q = c)
-// and upper faces (q = c + st), the adjoints of p_c and rho_c; the face
-// adjoint itself moves to lus / lvs / lws (the zeroing of lu / lv / lw at the
-// updated faces happens in k_adj_rhs, after every cell has read them).
+// and upper faces (q = c + st), the adjoints of p_c and rho_c.  The face
+// adjoint itself becomes the adjoint of u*, v*, w* at that face: the advection
+// kernel reads it from lu, lv, lw and accumulates the adjoint of the step's
+// start velocity into a cleared second set of fields (the correction wrote
+// every face, so nothing else of lu, lv, lw carries over), and the two sets
+// swap.
 __global__ void __launch_bounds__(256) k_adj_update(Geom g, Range R, const float* __restrict__ F,
                                                     const float* __restrict__ p, const double* __restrict__ lu,
                                                     const double* __restrict__ lv, const double* __restrict__ lw,
-                                                    double* __restrict__ lus, double* __restrict__ lvs,
-                                                    double* __restrict__ lws, double* __restrict__ lp,
-                                                    double* __restrict__ lrho) {
+                                                    double* __restrict__ lp, double* __restrict__ lrho) {
     RANGE_CELL(R);
     const int c = gidx(g, i, j, k);
     const int pos[3] = {i, j, k}, len[3] = {g.nx, g.ny, g.nz}, st[3] = {1, g.px, g.plane};
     const double hinv[3] = {(double)g.dxi, (double)g.dyi, (double)g.dzi};
     const double* lvel[3] = {lu, lv, lw};
-    double* lvs_[3] = {lus, lvs, lws};
     const float rho_c = rho_of(g, F[c]);
     const double dt = (double)g.dt, pc = (double)p[c];
     double lpc = 0.0, lrc = 0.0;
@@ -991,7 +1017,6 @@ __global__ void __launch_bounds__(256) k_adj_update(Geom g, Range R, const float
         if (pos[a] >= 2) {  // lower face: c is its upper cell
             const int m = c - st[a];
             const double gv = lvel[a][c];
-            lvs_[a][c] = gv;
             if (gv != 0.0) {
                 const double ir = rcp64((double)(0.5f * (rho_c + rho_of(g, F[m]))));
                 lpc -= gv * dt * ir * hinv[a];
@@ -1170,37 +1195,6 @@ __global__ void __launch_bounds__(AJ_T) k_adj_jacobi2(Geom g, InvAp ia, const do
     }
 }
 
-// ---- rhs = rho/dt div(u*), reversed (gather over the cells sharing a face) -------
-// Also zeroes lu / lv / lw at the faces the correction overwrote (their
-// adjoints moved to lus / lvs / lws in k_adj_update).  has_rhs = 0: no
-// Jacobi sweeps, so no rhs adjoint.
-__global__ void __launch_bounds__(256) k_adj_rhs(Geom g, Range R, const float* __restrict__ F,
-                                                 const float* __restrict__ us, const float* __restrict__ vs,
-                                                 const float* __restrict__ ws, const double* __restrict__ lrhs,
-                                                 double* __restrict__ lus, double* __restrict__ lvs,
-                                                 double* __restrict__ lws, double* __restrict__ lrho,
-                                                 double* __restrict__ lu, double* __restrict__ lv,
-                                                 double* __restrict__ lw, int has_rhs) {
-    RANGE_CELL(R);
-    const int c = gidx(g, i, j, k), sy = g.px, sz = g.plane;
-    if (i >= 2) lu[c] = 0.0;
-    if (j >= 2) lv[c] = 0.0;
-    if (k >= 2) lw[c] = 0.0;
-    if (!has_rhs) return;
-    const double idt = rcp64((double)g.dt), dxi = (double)g.dxi, dyi = (double)g.dyi, dzi = (double)g.dzi;
-    const double gr = lrhs[c];
-    const double div = ((double)us[c + 1] - us[c]) * dxi + ((double)vs[c + sy] - vs[c]) * dyi +
-                       ((double)ws[c + sz] - ws[c]) * dzi;
-    lrho[c] += gr * div * idt;
-    const double kk = gr * (double)rho_of(g, F[c]) * idt;
-    const double kx = i >= 2 ? lrhs[c - 1] * (double)rho_of(g, F[c - 1]) * idt : 0.0;
-    const double ky = j >= 2 ? lrhs[c - sy] * (double)rho_of(g, F[c - sy]) * idt : 0.0;
-    const double kz = k >= 2 ? lrhs[c - sz] * (double)rho_of(g, F[c - sz]) * idt : 0.0;
-    lus[c] += (kx - kk) * dxi;
-    lvs[c] += (ky - kk) * dyi;
-    lws[c] += (kz - kk) * dzi;
-}
-
 // ---- advection, reversed (scatter with FP64 atomics) --------------------------------
 // One momentum component q at face c: q* = q + dt (visc + adv + g_q),
 // adv = -a dq/dx - b dq/dy - cc dq/dz, upwinded by the signs of a, b, cc;
@@ -1276,15 +1270,26 @@ __device__ __forceinline__ double adj_momentum(const Geom& g, int c, int i, int 
     return Gd;
 }
 
-// Also the adjoint of rho and nu (cal_nu_rho_kernel, voftrial1.cu:95-104): with
-// lrho complete (correction and rhs) and lnu from the three momentum
-// equations of this cell, lF[c] += (lrho drho/dF + lnu dnu/dF).  dL/dg: each
-// block adds its sums to its own slot of `partial` (summed once at the end).
+// The rhs (voftrial1.cu:418-422: rhs = rho/dt div(u*)) reversed first, as a
+// gather over the cells sharing this cell's faces (has_rhs = 0: no Jacobi
+// sweeps, no rhs adjoint): u*, v*, w* at the cell's lower faces and rho take
+// lrhs of the cell and of its lower neighbours.  Then the advection of the
+// three momentum components at those faces, and the adjoint of rho and nu
+// (cal_nu_rho_kernel, voftrial1.cu:95-104): with lrho complete (correction
+// and rhs) and lnu from the three momentum equations of this cell,
+// lF[c] += (lrho drho/dF + lnu dnu/dF).  lu, lv, lw are zero on entry (the
+// correction overwrote every face).  lus, lvs, lws: the adjoints of u*, v*,
+// w* from the correction (the face adjoints of the corrected velocity).
+// dL/dg: each block adds its sums to its own slot of `partial` (summed once
+// at the end).
 __global__ void __launch_bounds__(256) k_adj_advect(Geom g, Range R, const float* __restrict__ F,
                                                     const float* __restrict__ u, const float* __restrict__ v,
-                                                    const float* __restrict__ w, const double* __restrict__ lus,
-                                                    const double* __restrict__ lvs, const double* __restrict__ lws,
-                                                    double* lu, double* lv, double* lw,
+                                                    const float* __restrict__ w, const float* __restrict__ us,
+                                                    const float* __restrict__ vs, const float* __restrict__ ws,
+                                                    const double* __restrict__ lrhs, int has_rhs,
+                                                    const double* __restrict__ lus, const double* __restrict__ lvs,
+                                                    const double* __restrict__ lws, double* __restrict__ lu,
+                                                    double* __restrict__ lv, double* __restrict__ lw,
                                                     const double* __restrict__ lrho, double* __restrict__ lF,
                                                     double* __restrict__ partial) {
     const int i = R.i0 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -1294,12 +1299,27 @@ __global__ void __launch_bounds__(256) k_adj_advect(Geom g, Range R, const float
     if (i <= R.i1 && j <= R.j1 && k <= R.k1) {
         const int c = gidx(g, i, j, k);
         const float Fc = F[c];
+        double Gu = lus[c], Gv = lvs[c], Gw = lws[c], lr = lrho[c];
+        if (has_rhs) {
+            const int sy = g.px, sz = g.plane;
+            const double idt = rcp64((double)g.dt), dxi = (double)g.dxi, dyi = (double)g.dyi, dzi = (double)g.dzi;
+            const double gr = lrhs[c];
+            const double div = ((double)us[c + 1] - us[c]) * dxi + ((double)vs[c + sy] - vs[c]) * dyi +
+                               ((double)ws[c + sz] - ws[c]) * dzi;
+            lr += gr * div * idt;
+            const double kk = gr * (double)rho_of(g, Fc) * idt;
+            const double kx = i >= 2 ? lrhs[c - 1] * (double)rho_of(g, F[c - 1]) * idt : 0.0;
+            const double ky = j >= 2 ? lrhs[c - sy] * (double)rho_of(g, F[c - sy]) * idt : 0.0;
+            const double kz = k >= 2 ? lrhs[c - sz] * (double)rho_of(g, F[c - sz]) * idt : 0.0;
+            Gu += (kx - kk) * dxi;
+            Gv += (ky - kk) * dyi;
+            Gw += (kz - kk) * dzi;
+        }
         const double nuc = (double)nu_of(g, Fc);
         double lnc = 0.0;
-        if (i >= 2 && lus[c] != 0.0) gsum[0] = adj_momentum<0>(g, c, i, j, k, u, v, w, lus[c], nuc, lu, lv, lw, lnc);
-        if (j >= 2 && lvs[c] != 0.0) gsum[1] = adj_momentum<1>(g, c, i, j, k, u, v, w, lvs[c], nuc, lu, lv, lw, lnc);
-        if (k >= 2 && lws[c] != 0.0) gsum[2] = adj_momentum<2>(g, c, i, j, k, u, v, w, lws[c], nuc, lu, lv, lw, lnc);
-        const double lr = lrho[c];
+        if (i >= 2 && Gu != 0.0) gsum[0] = adj_momentum<0>(g, c, i, j, k, u, v, w, Gu, nuc, lu, lv, lw, lnc);
+        if (j >= 2 && Gv != 0.0) gsum[1] = adj_momentum<1>(g, c, i, j, k, u, v, w, Gv, nuc, lu, lv, lw, lnc);
+        if (k >= 2 && Gw != 0.0) gsum[2] = adj_momentum<2>(g, c, i, j, k, u, v, w, Gw, nuc, lu, lv, lw, lnc);
         if ((lr != 0.0 || lnc != 0.0) && Fc >= 0.0f && Fc <= 1.0f)
             lF[c] += lr * ((double)g.rho_l - (double)g.rho_g) + lnc * ((double)g.nu_l - (double)g.nu_g);
     }
@@ -1521,15 +1541,20 @@ cudaError_t recompute_step(AdjEngine& e, const AdjState& x, int istep, StepData*
 
 // One step of the segment replay on the engine's buffers, keeping its
 // intermediates in mid: the predictor writes mid's u*, v*, w*; F is copied
-// out after the first and the second sweep.  *par: the Jacobi ping-pong
-// parity of the plain step; *pafter: the pressure after the solve.
-cudaError_t replay_step_keep(AdjEngine& e, int istep, const AdjMid& mid, int* par, const float** pafter,
-                             cudaStream_t s) {
+// out after the first and the second sweep.  The start velocity is read from
+// vin, the corrected velocity written to vout (which may be vin).  *par: the
+// Jacobi ping-pong parity of the plain step; *pafter: the pressure after the
+// solve.
+cudaError_t replay_step_keep(AdjEngine& e, int istep, const AdjMid& mid, float* const vin[3], float* const vout[3],
+                             int* par, const float** pafter, cudaStream_t s) {
     const Geom& g = e.g;
     PlainBuffers b = e.wb;
     b.us = mid.f[0];
     b.vs = mid.f[1];
     b.ws = mid.f[2];
+    b.u = vin[0];
+    b.v = vin[1];
+    b.w = vin[2];
     cudaError_t r;
     if ((r = plain_front(g, b, s)) != cudaSuccess) return r;
     if (e.conv) {
@@ -1538,6 +1563,9 @@ cudaError_t replay_step_keep(AdjEngine& e, int istep, const AdjMid& mid, int* pa
         if ((r = plain_pressure(g, b, e.jacobi_iters, par, s)) != cudaSuccess) return r;
         *pafter = *par ? b.p1 : b.p0;
     }
+    b.u = vout[0];
+    b.v = vout[1];
+    b.w = vout[2];
     if ((r = plain_correct(g, b, *pafter, s)) != cudaSuccess) return r;
     const int* dirs = sweep_order(istep);
     const float* velof[3] = {b.u, b.v, b.w};
@@ -1580,8 +1608,11 @@ cudaError_t reverse_step(AdjEngine& e, const StepData& d, int istep, cudaStream_
     }
     const Range I = interior(g);
     const dim3 gi = grid_of(I);
-    k_adj_update<<<gi, kBlk, 0, s>>>(g, I, d.F, d.p, e.lu, e.lv, e.lw, e.lus, e.lvs, e.lws, e.lp[e.lp_cur],
-                                     e.lrho);
+    k_adj_update<<<gi, kBlk, 0, s>>>(g, I, d.F, d.p, e.lu, e.lv, e.lw, e.lp[e.lp_cur], e.lrho);
+    // lu, lv, lw now hold the adjoints of u*, v*, w*; the start velocity's
+    // adjoint accumulates in the cleared second set
+    for (double* l : {e.lus, e.lvs, e.lws})
+        if ((r = cudaMemsetAsync(l, 0, e.elems * sizeof(double), s)) != cudaSuccess) return r;
     // the pressure solve reversed: convergent modes -- lrhs = the mean-free
     // solution of A mu = lp - mean(lp) (warm start: the previous step's), and
     // the state pressure (only a warm start) gets no adjoint; plain -- the
@@ -1612,11 +1643,12 @@ cudaError_t reverse_step(AdjEngine& e, const StepData& d, int istep, cudaStream_
             e.lp_cur ^= 1;
         }
     }
-    k_adj_rhs<<<gi, kBlk, 0, s>>>(g, I, d.F, d.us, d.vs, d.ws, e.lrhs, e.lus, e.lvs, e.lws, e.lrho, e.lu, e.lv, e.lw,
-                                  e.conv || e.jacobi_iters > 0);
-    // advection with rho and nu
-    k_adj_advect<<<gi, kBlk, 0, s>>>(g, I, d.F, d.u, d.v, d.w, e.lus, e.lvs, e.lws, e.lu, e.lv, e.lw, e.lrho, e.lF,
-                                     e.d_partial);
+    // rhs, advection, rho and nu
+    k_adj_advect<<<gi, kBlk, 0, s>>>(g, I, d.F, d.u, d.v, d.w, d.us, d.vs, d.ws, e.lrhs, e.conv || e.jacobi_iters > 0,
+                                     e.lu, e.lv, e.lw, e.lus, e.lvs, e.lws, e.lrho, e.lF, e.d_partial);
+    std::swap(e.lu, e.lus);
+    std::swap(e.lv, e.lvs);
+    std::swap(e.lw, e.lws);
     return cudaGetLastError();
 }
 
@@ -1628,7 +1660,7 @@ int adj_kernels_per_step(const AdjEngine& e) {
     // are not kept (front 2, pressure, correction 1, two sweeps), and the
     // adjoint kernels: F copies 3, the three sweep adjoints (1 launch each when
     // fused, else 8), velocity copies 3, correction 1, the transposed Jacobi
-    // sweeps (iters + 1 stages, two per launch), rhs 1, advection 1.  The convergent modes' pressure
+    // sweeps (iters + 1 stages, two per launch), rhs with advection 1.  The convergent modes' pressure
     // solves (multigrid graphs) are not counted.
     const Geom& g = e.g;
     const int P = e.conv ? 0 : plain_phase_launches(PHASE_JACOBI, e.jacobi_iters);
@@ -1638,7 +1670,7 @@ int adj_kernels_per_step(const AdjEngine& e) {
     const int replay = 2 + P + 1 + 3;
     const int recompute = e.keep ? 0 : 2 + P + 1 + 2;
     const int jac = (!e.conv && e.jacobi_iters > 0) ? (e.jacobi_iters + 2) / 2 : 0;
-    return replay + recompute + 3 + sweeps + 3 + 1 + jac + 1 + 1;
+    return replay + recompute + 3 + sweeps + 3 + 1 + jac + 1;
 }
 
 cudaError_t adj_create(const Geom& g, int jacobi_iters, int mg_mode, double tol, int max_outer, AdjEngine* e,
@@ -1896,11 +1928,16 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
             const float** pa = count <= 64 ? pafter : new (std::nothrow) const float*[count];
             if (!pa) return cudaErrorMemoryAllocation;
             for (int q = 0; q < count && r == cudaSuccess; ++q) {
-                r = replay_step_keep(*e, e->istep0 + first + q, e->mid[q], &par, &pa[q], s);
+                // velocity: from the loaded buffers or segment state q, into
+                // segment state q + 1 (or the engine's buffers after the last step)
+                float* const* vs = q == 0 ? nullptr : e->seg[q].f + 1;
+                float* const vin[3] = {q == 0 ? e->wb.u : vs[0], q == 0 ? e->wb.v : vs[1], q == 0 ? e->wb.w : vs[2]};
+                float* const* vn = q + 1 < count ? e->seg[q + 1].f + 1 : nullptr;
+                float* const vout[3] = {vn ? vn[0] : e->wb.u, vn ? vn[1] : e->wb.v, vn ? vn[2] : e->wb.w};
+                r = replay_step_keep(*e, e->istep0 + first + q, e->mid[q], vin, vout, &par, &pa[q], s);
                 if (r == cudaSuccess && q + 1 < count) {
-                    const float* src[5] = {e->wb.F, e->wb.u, e->wb.v, e->wb.w, pa[q]};
-                    for (int t = 0; t < 5 && r == cudaSuccess; ++t)
-                        r = copy_field(e->seg[q + 1].f[t], src[t], e->elems, s);
+                    if ((r = copy_field(e->seg[q + 1].f[0], e->wb.F, e->elems, s)) == cudaSuccess)
+                        r = copy_field(e->seg[q + 1].f[4], pa[q], e->elems, s);
                     pa[q] = e->seg[q + 1].f[4];
                 }
             }
