@@ -28,6 +28,9 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <stdlib.h>
+#include <string.h>
+
 #include <initializer_list>
 #include <new>
 #include <utility>
@@ -858,8 +861,11 @@ struct FmLine {
 #ifndef VOF_FM_MINB
 #define VOF_FM_MINB 4
 #endif
+#ifndef VOF_FM_MINB_X
+#define VOF_FM_MINB_X 1
+#endif
 template <int DIR, int WARPS>
-__global__ void __launch_bounds__(FM_LANES * WARPS, VOF_FM_MINB) k_fct_adjoint_march(Geom g, const float* __restrict__ Fg,
+__global__ void __launch_bounds__(FM_LANES * WARPS, DIR == 0 ? VOF_FM_MINB_X : VOF_FM_MINB) k_fct_adjoint_march(Geom g, const float* __restrict__ Fg,
                                                                         const float* __restrict__ velg,
                                                                         double* lFg, double* __restrict__ lvelg) {
     FmLine<DIR> L(g);
@@ -888,11 +894,12 @@ __global__ void __launch_bounds__(FM_LANES * WARPS, VOF_FM_MINB) k_fct_adjoint_m
     L.K1 = DIR == 0 ? (double)g.dy * g.dz / L.vold
                     : (DIR == 1 ? (double)g.dy / ((double)g.dx * g.dy) : (double)g.dy * g.dx / L.vold);
     L.dvfac = (double)L.S.dvfac;
-    const int cs = L.c0 - FM_WARM;
+    // (iterations before -6 see no position of the line)
+    const int cs = max(L.c0 - FM_WARM, -6);
     L.init(cs);
     L.load_tail();
     L.prefetch(cs);
-    for (int t = 0; t < FM_WARM; ++t) L.step(cs + t);
+    for (int c = cs; c < L.c0; ++c) L.step(c);
     __syncthreads();  // every warp has read the lF it needs from its neighbours
     for (int c = L.c0; c <= L.c1; ++c) L.step(c);
 }
@@ -1443,10 +1450,15 @@ cudaError_t launch_fct_adjoint_march(const Geom& g, const float* Fs, const float
     return cudaGetLastError();
 }
 
+// The line march runs one lane per grid line: it needs enough lines to fill
+// the GPU; smaller grids take the shared-memory kernel (threads along lines).
+constexpr long FM_MIN_LINES = 16384;
 template <int DIR>
 cudaError_t sweep_adjoint(AdjEngine& e, const float* Fs, const float* vel, double* lvel, cudaStream_t s) {
     const Geom& g = e.g;
-    if (e.fct_march) return launch_fct_adjoint_march<DIR>(g, Fs, vel, e.lF, lvel, s);
+    const long lines = DIR == 0 ? (long)g.ny * g.nz : (DIR == 1 ? (long)g.nx * g.nz : (long)g.nx * g.ny);
+    if (e.fct_march == 2 || (e.fct_march && lines >= FM_MIN_LINES))
+        return launch_fct_adjoint_march<DIR>(g, Fs, vel, e.lF, lvel, s);
     {  // one fused kernel when a block of lines fits in shared memory
         const int n = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
         // the most lines per block with at least two blocks per SM, else the most that fit
@@ -1666,7 +1678,12 @@ int adj_kernels_per_step(const AdjEngine& e) {
     const int P = e.conv ? 0 : plain_phase_launches(PHASE_JACOBI, e.jacobi_iters);
     int sweeps = 0;
     const int len[3] = {g.nx, g.ny, g.nz};
-    for (int a = 0; a < 3; ++a) sweeps += (e.fct_march || fa_smem_bytes(2, len[a]) <= fa_smem_limit()) ? 1 : 8;
+    const long lines[3] = {(long)g.ny * g.nz, (long)g.nx * g.nz, (long)g.nx * g.ny};
+    for (int a = 0; a < 3; ++a)
+        sweeps += (e.fct_march == 2 || (e.fct_march && lines[a] >= FM_MIN_LINES) ||
+                   fa_smem_bytes(2, len[a]) <= fa_smem_limit())
+                      ? 1
+                      : 8;
     const int replay = 2 + P + 1 + 3;
     const int recompute = e.keep ? 0 : 2 + P + 1 + 2;
     const int jac = (!e.conv && e.jacobi_iters > 0) ? (e.jacobi_iters + 2) / 2 : 0;
@@ -1681,7 +1698,12 @@ cudaError_t adj_create(const Geom& g, int jacobi_iters, int mg_mode, double tol,
     e->conv = mg_mode != 0;
     e->tol = tol;
     e->max_outer = max_outer;
+    // sweep adjoint kernel: by grid size, or forced by VOF_ADJ_SWEEP=march|shared
     e->fct_march = 1;
+    if (const char* v = getenv("VOF_ADJ_SWEEP")) {
+        if (!strcmp(v, "march")) e->fct_march = 2;
+        else if (!strcmp(v, "shared")) e->fct_march = 0;
+    }
     e->elems = (size_t)g.plane * (g.nz + 2);
     cudaError_t r;
     auto alloc = [&](void** p, size_t nb) -> cudaError_t {

@@ -78,7 +78,7 @@ struct AdjEngine {
     double *lX, *lown, *lmx, *lmn, *lpp, *lpm, *ldv, *lterm, *lLF, *lA;
     unsigned char* sel;
     int lp_cur;             // which lp buffer holds the pressure adjoint
-    int fct_march;          // sweep adjoints: the line-march kernel (else the shared-memory ones)
+    int fct_march;          // sweep adjoints: 0 shared-memory kernels, 1 line march on large grids, 2 always march
     InvAp inv_ap;
     double* d_partial;      // block partials (body force, loss)
     int npartial;

@@ -267,6 +267,12 @@ int vof_adjoint_kernels_per_step(const vof_ctx* ctx);
  * vof_forward_record when they do not fit).  The gradients do not depend on
  * the choice.  vof_adjoint_keeps: 1 when the recorded tape keeps them, 0 when
  * it recomputes them, VOF_E_STATE before the first vof_forward_record. */
+/* The FCT sweep adjoint has two kernels with the same results: a march along
+ * each grid line (one thread per line; grids with at least 16384 lines per
+ * sweep direction) and a shared-memory kernel (threads along lines; smaller
+ * grids).  The environment variable VOF_ADJ_SWEEP=march or =shared, read when
+ * a context's adjoint engine is created, forces one of them (a diagnostic
+ * override). */
 #define VOF_ADJ_AUTO      0
 #define VOF_ADJ_RECOMPUTE 1
 #define VOF_ADJ_KEEP      2

@@ -57,8 +57,12 @@ def check_against_host(orc, prm, st, istep0, nsteps, box, got, tol=1e-9):
     assert np.allclose(got["grad_g"], ref["grad_g"], rtol=tol, atol=1e-30), (got["grad_g"], ref["grad_g"])
 
 
-@pytest.mark.parametrize("shape,nsteps,istep0", [((16, 14, 12), 6, 1), ((13, 17, 11), 5, 0), ((12, 12, 20), 4, 2)])
-def test_device_adjoint_matches_host(cuda, V, orc, shape, nsteps, istep0):
+@pytest.mark.parametrize("sweep", ["march", "shared"])
+@pytest.mark.parametrize("shape,nsteps,istep0", [((16, 14, 12), 6, 1), ((13, 17, 11), 5, 0), ((12, 12, 20), 4, 2),
+                                                  ((70, 9, 8), 3, 1), ((7, 66, 9), 3, 2), ((9, 8, 75), 3, 0)])
+def test_device_adjoint_matches_host(cuda, V, orc, shape, nsteps, istep0, sweep, monkeypatch):
+    """Long lines along each axis split into several segments of the line march."""
+    monkeypatch.setenv("VOF_ADJ_SWEEP", sweep)
     prm, st = dam_state(V, *shape)
     box = box_of(prm)
     got = gpu_adjoint(V, prm, st, istep0, nsteps, box)
@@ -68,11 +72,14 @@ def test_device_adjoint_matches_host(cuda, V, orc, shape, nsteps, istep0):
     check_against_host(orc, prm, st, istep0, nsteps, box, got)
 
 
+@pytest.mark.parametrize("sweep", ["march", "shared"])
 @pytest.mark.parametrize("policy", ["ADJ_KEEP", "ADJ_RECOMPUTE"])
 @pytest.mark.parametrize("every", [1, 3, 4, 0])
-def test_checkpoint_spacing_does_not_change_the_gradient(cuda, V, orc, every, policy):
+def test_checkpoint_spacing_does_not_change_the_gradient(cuda, V, orc, every, policy, sweep, monkeypatch):
     """Kept intermediates (from the segment replay) and recomputed ones (from
-    each step's start state) are the forward's bits either way."""
+    each step's start state) are the forward's bits either way; both FCT sweep
+    adjoint kernels (line march, shared memory) give the host's gradient."""
+    monkeypatch.setenv("VOF_ADJ_SWEEP", sweep)
     prm, st = dam_state(V, 14, 12, 10, seed=5)
     box = box_of(prm)
     got = gpu_adjoint(V, prm, st, 1, 9, box, every=every, policy=getattr(V, policy))
