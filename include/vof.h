@@ -92,7 +92,9 @@ typedef struct vof_params {
     /* ---- additions (no counterpart in Params) ---- */
     int jacobi_iters;       /* plain mode: sweeps per step; voftrial1.cu:1371 hardcodes 10 */
     int mode;               /* VOF_MODE_*                                                   */
-    int inner_sweeps;       /* mixed/fp64 modes: smoothing sweeps per inner solve (default 32) */
+    int inner_sweeps;       /* reserved (kept for the ABI layout): the multigrid inner solve of the
+                               mixed/fp64 modes uses fixed Chebyshev smoothing degrees (3 on levels
+                               wider than 25 cells, 8 below); vof_params_init sets 32, unused */
     int max_outer;          /* mixed/fp64 modes: cap on defect-correction iterations        */
     double tol;             /* mixed/fp64 modes: target ||b-Ap||/||b|| (default 1e-8)       */
 } vof_params;
