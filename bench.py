@@ -32,6 +32,7 @@ import argparse
 import ctypes as C
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -84,6 +85,9 @@ def parse_args(argv=None):
                     help="steps of the 320^3 mixed-solve + adjoint rollout (0: skip; opt-in)")
     ap.add_argument("--adj-steps", type=int, default=400,
                     help="steps of the adjoint measurement at 64^3 (the bench size runs 1/8 of them; 0 disables)")
+    ap.add_argument("--drive-steps", type=int, default=300,
+                    help="steps of the drop-in program run (voftrial1.cu's main at 200^3 with a dump every "
+                         "100 steps), timed end to end (0 disables)")
     return ap.parse_args(argv)
 
 
@@ -597,6 +601,8 @@ def run_ours(args):
             ext["convergent_pressure"]["mixed"]["value"] / value, 3)
     if args.large_steps > 0 and world == 1:
         ext["large_mixed_adjoint"] = measure_large(V, args.large_steps, stream, dev)
+    if args.drive_steps > 0 and world == 1:
+        ext["drive"] = measure_drive(args.drive_steps)
     if args.adj_steps > 0 and world == 1:
         ext["adjoint"] = [measure_adjoint(V, 64, args.adj_steps, 20, stream, dev),
                           measure_adjoint(V, 64, args.adj_steps, 20, stream, dev, dense=True),
@@ -623,6 +629,56 @@ def run_ours(args):
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# the drop-in program: voftrial1.cu's main() end to end, dumps included
+# ---------------------------------------------------------------------------
+DRIVE_NSTEP = 100
+
+
+def finished_seconds(out: str):
+    """The "Finished at step N in T s" line of the reference's main()."""
+    m = re.search(r">>> Finished at step (\d+) in ([0-9.eE+-]+) s", out)
+    return (int(m.group(1)), float(m.group(2))) if m else (None, None)
+
+
+def time_program(cmd, steps):
+    """Run one drop-in program in a scratch directory (its dumps go to
+    output/ there, removed afterwards); wall time from its own timing line."""
+    import shutil
+    import subprocess
+    import tempfile
+
+    d = tempfile.mkdtemp(prefix="vofdrive_")
+    try:
+        r = subprocess.run(cmd, cwd=d, capture_output=True, text=True, timeout=1800)
+        n, sec = finished_seconds(r.stdout)
+        dumps = sorted(os.listdir(os.path.join(d, "output"))) if os.path.isdir(os.path.join(d, "output")) else []
+        size = sum(os.path.getsize(os.path.join(d, "output", f)) for f in dumps)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    if r.returncode != 0 or n != steps:
+        return {"error": (r.stderr or r.stdout)[-300:], "returncode": r.returncode}
+    return {"seconds": sec, "mcell_s": round(200 ** 3 * steps / sec / 1e6, 1), "dumps": len(dumps),
+            "dump_bytes": size}
+
+
+def measure_drive(steps):
+    """vof_drive (driver/vof_drive.cpp) with the reference program's own
+    set-up (200^3, ic 1, g = (0, -5, 0), 10 Jacobi sweeps): `steps` steps with
+    a dump of F every 100 steps as ASCII VTK (the reference's format), as
+    binary VTK and with no dumps.  Seconds from the program's own
+    "Finished at step N in T s" line (host wall clock around the loop,
+    including the dumps still being written at the end)."""
+    from vof_b200 import build as vb
+
+    exe = str(vb.DRIVER_PATH)
+    out = {"workload": f"voftrial1.cu main(): 200^3, ic 1, g=(0,-5,0), {steps} steps, F dumped every "
+                       f"{DRIVE_NSTEP} steps", "nstep": DRIVE_NSTEP, "steps": steps}
+    for kind in ("ascii", "binary", "none"):
+        out[kind] = time_program([exe, "--max_steps", str(steps), "--nstep", str(DRIVE_NSTEP), "--vtk", kind], steps)
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -678,6 +734,14 @@ def run_reference(args):
         "clocks": clk, "gpu_launches": orc.ref_lib(best).ref_kernels_per_step(prm.jacobi_iters) * K,
         "device": props.name,
     }
+    # the reference program itself, end to end with its dumps (voftrial1.cu main())
+    exe = orc.ORACLE_DIR / "_ref" / "vof3d_ref"
+    if args.drive_steps > 0 and exe.exists():
+        line["drive"] = {"workload": f"voftrial1.cu main() unmodified (sm_100a build): 200^3, ic 1, g=(0,-5,0), "
+                                     f"{args.drive_steps} steps, F dumped every {DRIVE_NSTEP} steps (ASCII VTK)",
+                         "nstep": DRIVE_NSTEP, "steps": args.drive_steps,
+                         "ascii": time_program([str(exe), "--max_steps", str(args.drive_steps), "--nstep",
+                                                str(DRIVE_NSTEP)], args.drive_steps)}
     print(json.dumps(line), flush=True)
 
 

@@ -86,5 +86,30 @@ def build(force: bool = False, verbose: bool = False, extra=(), lib_path: Path |
     return lib_out
 
 
+DRIVER_SRC = PKG_DIR.parent / "driver" / "vof_drive.cpp"
+DRIVER_PATH = PKG_DIR / "vof_drive"
+
+
+def cuda_home() -> Path:
+    return Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+
+
+def build_driver(force: bool = False, verbose: bool = False) -> Path:
+    """The C++ drop-in driver (driver/vof_drive.cpp) linked against
+    libvof_b200.so (found next to it at run time) and the CUDA runtime."""
+    lib = build(verbose=verbose)
+    if force or _stale(DRIVER_PATH, [DRIVER_SRC, INCLUDE_DIR / "vof.h", lib]):
+        cuda = cuda_home()
+        tmp = DRIVER_PATH.with_name(DRIVER_PATH.name + ".tmp")
+        cmd = [shutil.which("g++") or "g++", "-O2", "-std=c++17", "-pthread", "-Wall", "-I", str(INCLUDE_DIR),
+               "-I", str(cuda / "include"), str(DRIVER_SRC), "-o", str(tmp), "-L", str(lib.parent), "-lvof_b200",
+               "-L", str(cuda / "lib64"), "-lcudart", "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + str(cuda / "lib64")]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, DRIVER_PATH)
+    return DRIVER_PATH
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))

@@ -257,8 +257,30 @@ def ref_lib(variant: str = "sm100a"):
                                                                  C.POINTER(C.c_double), F]
         lib.ref_kernels_per_step.restype = C.c_int
         lib.ref_kernels_per_step.argtypes = [C.c_int]
+        lib.ref_initial_F.restype = C.c_int
+        lib.ref_initial_F.argtypes = [C.POINTER(Params), C.c_int, F]
+        lib.ref_write_vtk.restype = C.c_int
+        lib.ref_write_vtk.argtypes = [C.c_char_p, F, C.c_int, C.c_int, C.c_int]
         _refs[variant] = lib
     return _refs[variant]
+
+
+def ref_initial_F(prm, ic: int = 1, variant: str = "sm100a") -> np.ndarray:
+    """set_init_F_kernel + apply_bc_F of the reference (GPU), reference layout."""
+    F = np.zeros(prm.shape, dtype=np.float32)
+    rc = ref_lib(variant).ref_initial_F(C.byref(prm), int(ic), _ptr(F, C.c_float))
+    if rc != 0:
+        raise RuntimeError(f"ref_initial_F failed: {rc}")
+    return F
+
+
+def ref_write_vtk(path, F: np.ndarray, variant: str = "sm100a") -> None:
+    """The reference's write_legacy_vtk on a host field (host code; no GPU)."""
+    F = np.ascontiguousarray(F, dtype=np.float32)
+    nz, ny, nx = F.shape
+    rc = ref_lib(variant).ref_write_vtk(str(path).encode(), _ptr(F, C.c_float), nx, ny, nz)
+    if rc != 0:
+        raise RuntimeError(f"ref_write_vtk failed: {rc}")
 
 
 def ref_run(prm, state, istep0: int, nsteps: int, variant: str = "sm100a", extras: bool = False) -> dict:

@@ -202,4 +202,33 @@ int ref_time(const vof_params* prm, const float* F, const float* u, const float*
 // Kernel launches the reference enqueues per step.
 int ref_kernels_per_step(int jacobi_iters) { return 1 + 3 + jacobi_iters + 3 + 3 + 3 * 4 + 1 + 3; }
 
+// The reference's initial condition: set_init_F_kernel with its launch shape
+// and one apply_bc_F (voftrial1.cu:1328-1337); F_out gets nTot floats.
+int ref_initial_F(const vof_params* prm, int ic, float* F_out) {
+    if (!prm || !F_out) return VOF_E_INVALID;
+    load_params(prm);
+    const size_t bytes = (size_t)prm->nTot * sizeof(float);
+    float* F = nullptr;
+    alloc_field(&F, bytes);
+    const dim3 blockInit(8, 8, 4);
+    const dim3 gridInit((prm->nx + 2 + blockInit.x - 1) / blockInit.x, (prm->ny + 2 + blockInit.y - 1) / blockInit.y,
+                        (prm->nz + 2 + blockInit.z - 1) / blockInit.z);
+    set_init_F_kernel<<<gridInit, blockInit>>>(F, ic);
+    CHECK_CUDA(cudaPeekAtLastError());
+    apply_bc_F(F);
+    CHECK_CUDA(cudaDeviceSynchronize());
+    CHECK_CUDA(cudaMemcpy(F_out, F, bytes, cudaMemcpyDeviceToHost));
+    cudaFree(F);
+    return VOF_OK;
+}
+
+// The reference's dump writer (write_legacy_vtk, voftrial1.cu:907-941) on a
+// host field of nxTot * nyTot * nzTot floats; host code only, no GPU needed.
+int ref_write_vtk(const char* path, const float* field, int nxTot, int nyTot, int nzTot) {
+    if (!path || !field || nxTot < 2 || nyTot < 2 || nzTot < 2) return VOF_E_INVALID;
+    const std::vector<float> f(field, field + (size_t)nxTot * nyTot * nzTot);
+    write_legacy_vtk(path, f, nxTot, nyTot, nzTot);
+    return VOF_OK;
+}
+
 }  // extern "C"
