@@ -27,7 +27,7 @@
 // out so a warp's 32 lanes (32 lines, same position) hit 32 banks:
 //   x lines: [line][pos] with an odd row pitch;  y/z lines: [pos][line].
 // y/z lines are contiguous across lanes in HBM, so results go straight to
-// global memory; x results are staged and written back row-wise.
+// global memory; x results are staged in the F tile and written back row-wise.
 #include <cuda_runtime.h>
 
 #include "fct_line.cuh"
@@ -136,9 +136,8 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, float* F, const floa
     const int qs = AXIS == 0 ? 1 : LANES;
     auto si = [&](int l, int q) { return AXIS == 0 ? l * P + q : q * LANES + l; };
     const int tile = AXIS == 0 ? LANES * P : npos * LANES;
-    float* sF = smem;
+    float* sF = smem;  // x lines: also the staged results, written in place (below)
     float* sV = smem + tile;
-    float* sO = smem + 2 * tile;  // x only: staged results
 
     // ---- stage the tile (coalesced) ----
     if (AXIS == 0) {
@@ -168,10 +167,18 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, float* F, const floa
     const int a = a0 + lane;
     const bool live = lane < nl && c0 <= n;
 
+    // x lines: each result goes into sF in place.  The march at cell c reads
+    // F only at c+2 and c+3, so a warp never reads a cell it has written; the
+    // warm-up below reads the three cells before the segment (the previous
+    // warp's last cells), and the march reads the three after it (the next
+    // warp's first cells): hence a barrier after the warm-ups, and each warp
+    // holds its first three results in registers until every march is done.
+    const float dt = S.dt;
+    float lo2 = 0.0f, a0f = 0.0f, a1f = 0.0f, a2f = 0.0f, T0 = 0.0f, T1 = 0.0f, rp0 = 0.0f, rm0 = 0.0f;
+    float cf0 = 0.0f, dv0 = 1.0f, dv1 = 1.0f, rdv0 = 1.0f, rdv1 = 1.0f;
+    float held0 = 0.0f, held1 = 0.0f, held2 = 0.0f;
     if (live) {
-        const float dt = S.dt;
         // state before cell c0
-        float lo2, a0f, a1f, a2f, T0, T1, rp0, rm0, cf0, dv0, dv1, rdv0, rdv1;
         {
             float lo_tmp;
             face_flux(L, c0, dt, lo_tmp, a0f);
@@ -194,7 +201,9 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, float* F, const floa
             rdv0 = __frcp_rn(dv0);
             rdv1 = __frcp_rn(dv1);
         }
-
+    }
+    if (AXIS == 0) __syncthreads();
+    if (live) {
         for (int c = c0; c <= c1; ++c) {
             // face c+3, Ftd(c+2), ratios(c+1), limiter of face c+1, result of cell c
             float lo3 = 0.0f, a3f = 0.0f;
@@ -212,7 +221,10 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, float* F, const floa
             if (FINAL) fnew = clamp01f(fnew);  // post_process_f_kernel, voftrial1.cu:502-507
 
             if (AXIS == 0) {
-                sO[lane * P + c] = fnew;
+                if (c == c0) held0 = fnew;
+                else if (c == c0 + 1) held1 = fnew;
+                else if (c == c0 + 2) held2 = fnew;
+                else sF[lane * P + c] = fnew;
             } else if (!FINAL) {
                 F[gi(a, b, c)] = fnew;
             } else {
@@ -243,13 +255,19 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, float* F, const floa
     }
 
     if (AXIS == 0) {
-        // ---- write the staged x rows back (coalesced) ----
+        __syncthreads();  // every march is done: the held results go in
+        if (live) {
+            sF[lane * P + c0] = held0;
+            if (c0 + 1 <= c1) sF[lane * P + c0 + 1] = held1;
+            if (c0 + 2 <= c1) sF[lane * P + c0 + 2] = held2;
+        }
+        // ---- write the x rows back (coalesced) ----
         __syncthreads();
         for (int l = warp; l < nl; l += WARPS) {
             const int aa = a0 + l;
             if (!FINAL) {
                 const int base = gi(aa, b, 0);
-                for (int q = 1 + lane; q <= n; q += LANES) F[base + q] = sO[l * P + q];
+                for (int q = 1 + lane; q <= n; q += LANES) F[base + q] = sF[l * P + q];
             } else {
                 int av[3], bv[3];
                 const int nav = mirrors(aa, na, av), nbv = mirrors(b, nb, bv);
@@ -257,7 +275,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, float* F, const floa
                     for (int ia = 0; ia < nav; ++ia) {
                         const int base = gi(av[ia], bv[ib], 0);
                         for (int q = lane; q <= n + 1; q += LANES)
-                            F[base + q] = sO[l * P + (q < 1 ? 1 : (q > n ? n : q))];
+                            F[base + q] = sF[l * P + (q < 1 ? 1 : (q > n ? n : q))];
                     }
             }
         }
@@ -266,7 +284,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, float* F, const floa
 
 size_t fct_smem_bytes(int axis, int n) {
     const int npos = n + 2;
-    if (axis == 0) return sizeof(float) * 3u * (size_t)LANES * (size_t)odd_pitch(npos);
+    if (axis == 0) return sizeof(float) * 2u * (size_t)LANES * (size_t)odd_pitch(npos);
     return sizeof(float) * 2u * (size_t)npos * LANES;
 }
 
