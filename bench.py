@@ -85,6 +85,8 @@ def parse_args(argv=None):
                     help="steps of the 320^3 mixed-solve + adjoint rollout (0: skip; opt-in)")
     ap.add_argument("--adj-steps", type=int, default=400,
                     help="steps of the adjoint measurement at 64^3 (the bench size runs 1/8 of them; 0 disables)")
+    ap.add_argument("--no-small", dest="small", action="store_false",
+                    help="skip the 32^3 / 64^3 plain-step measurement")
     ap.add_argument("--drive-steps", type=int, default=300,
                     help="steps of the drop-in program run (voftrial1.cu's main at 200^3 with a dump every "
                          "100 steps), timed end to end (0 disables)")
@@ -601,6 +603,8 @@ def run_ours(args):
             ext["convergent_pressure"]["mixed"]["value"] / value, 3)
     if args.large_steps > 0 and world == 1:
         ext["large_mixed_adjoint"] = measure_large(V, args.large_steps, stream, dev)
+    if args.small and world == 1:
+        ext["small_grids"] = measure_small(V, stream, dev)
     if args.drive_steps > 0 and world == 1:
         ext["drive"] = measure_drive(args.drive_steps)
     if args.adj_steps > 0 and world == 1:
@@ -629,6 +633,45 @@ def run_ours(args):
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# small grids: configs[0] (32^3 x 200 steps) and the 64^3 adjoint grid
+# ---------------------------------------------------------------------------
+SMALL_GRIDS = ((32, 200), (64, 200))
+
+
+def small_state(V, n):
+    """The dam break with a flat interface (h0 = 0.06, no noise) at n^3."""
+    from vof_b200 import ic
+
+    prm = workload_params(V, n)
+    return prm, ic.rest_state(prm, ic.dam_break(prm))
+
+
+def measure_small(V, stream, dev):
+    """Plain steps at 32^3 and 64^3 (the bench's physics, flat interface):
+    3 warm-up steps, then the grid's step count through vof_run (captured
+    graphs), CUDA events on the library's stream."""
+    import torch
+
+    out = {}
+    for n, steps in SMALL_GRIDS:
+        prm, st = small_state(V, n)
+        with V.Solver(prm, stream=stream.cuda_stream) as s:
+            s.upload_state(**st)
+            s.run(1, 3)
+            s.upload_state(**st)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            e0.record(stream)
+            s.run(1, steps)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+        out[f"{n}^3"] = {"steps": steps, "ms_per_step": round(ms / steps, 5),
+                         "value": round(n ** 3 * steps / ms / 1e3, 1), "unit": UNIT}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -734,6 +777,15 @@ def run_reference(args):
         "clocks": clk, "gpu_launches": orc.ref_lib(best).ref_kernels_per_step(prm.jacobi_iters) * K,
         "device": props.name,
     }
+    # small grids through the reference's own kernels (the faster build)
+    if args.small:
+        line["small_grids"] = {}
+        for n, steps in SMALL_GRIDS:
+            prm_s, st_s = small_state(V, n)
+            ms_s, _ = orc.ref_time(prm_s, st_s, 1, 3, steps, variant=best)
+            line["small_grids"][f"{n}^3"] = {"steps": steps, "ms_per_step": round(ms_s / steps, 5),
+                                             "value": round(n ** 3 * steps / ms_s / 1e3, 1), "unit": UNIT,
+                                             "build": best}
     # the reference program itself, end to end with its dumps (voftrial1.cu main())
     exe = orc.ORACLE_DIR / "_ref" / "vof3d_ref"
     if args.drive_steps > 0 and exe.exists():

@@ -242,8 +242,13 @@ static dim3 tb_grid(const Geom& g, int kchunk) {
 cudaError_t jacobi_tb_launch(const Geom& g, int T, const CUtensorMap& map_in, const CUtensorMap& map_rhs,
                              float* pout, int* status, cudaStream_t s) {
     // z chunks long enough that the T-plane warm-up at each end is small,
-    // and enough blocks to fill the GPU for a few waves.
-    const int kchunk = g.nz < 16 ? g.nz : 16;
+    // and enough blocks to fill the GPU for a few waves.  On small grids the
+    // chunks shrink (down to one plane) until the launch has about 600
+    // blocks: a few blocks marching 16 planes each are bound by the latency
+    // of their plane pipeline.
+    const long long tiles = (long long)((g.nx + JB_TX - 1) / JB_TX + 1) * ((g.ny + JB_TX - 1) / JB_TX + 1);
+    const int target = (int)((long long)g.nz * tiles / 600);
+    const int kchunk = target < 1 ? 1 : (target > 16 ? 16 : target);
     const dim3 blk(JB_TX, JB_TY);
     switch (T) {
         case 1: k_jacobi_tb<1><<<tb_grid<1>(g, kchunk), blk, JTile<1>::SMEM, s>>>(g, map_in, map_rhs, pout, kchunk, status); break;

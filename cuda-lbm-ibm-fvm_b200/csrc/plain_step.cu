@@ -153,6 +153,8 @@ __global__ void __launch_bounds__(256) k_rhs(Geom g,
     int id = gidx(g, col.i, col.j, col.k0);
     float wsc = __ldg(ws + id);
     const float rdt = __frcp_rn(g.dt);
+    // (unrolled so that the loads of several planes are in flight together)
+#pragma unroll 4
     for (int k = col.k0; k <= col.k1; ++k, id += g.plane) {
         const float wsp = __ldg(ws + id + g.plane);
         const float rho = rho_of(g, __ldg(F + id));
@@ -362,10 +364,14 @@ int plain_kernels_per_step(int jacobi_iters) { return 1 + 1 + jacobi_launches(ja
 
 // Column-marching launch shape: 32 x 8 columns per block, z split into
 // chunks of about 16 planes (long enough to reuse the k-window, short enough
-// for a few waves of blocks per SM).
+// for a few waves of blocks per SM).  On small grids the chunks shrink (down
+// to one plane) until the launch has about 600 blocks: a launch of a few
+// blocks marching 16 planes each is bound by the latency of its march.
 static void column_launch(const Geom& g, dim3& grid, int& kchunk) {
     const int bx = (g.nx + TX - 1) / TX, by = (g.ny + TY - 1) / TY;
-    const int nch = (g.nz + 15) / 16;
+    const int target = (int)(((long long)g.nz * bx * by) / 600);
+    const int len = target < 1 ? 1 : (target > 16 ? 16 : target);
+    const int nch = (g.nz + len - 1) / len;
     kchunk = (g.nz + nch - 1) / nch;
     grid = dim3(bx, by, (g.nz + kchunk - 1) / kchunk);
 }
