@@ -1636,7 +1636,10 @@ cudaError_t reverse_step(AdjEngine& e, const StepData& d, int istep, cudaStream_
     } else if (e.jacobi_iters > 0) {
         // stages 0, 1 x (iters - 1), 2, two per launch
         const int nst = e.jacobi_iters + 1;
-        const int nch = (g.nz + 23) / 24, kchunk = (g.nz + nch - 1) / nch;
+        // chunks of up to 24 planes, shorter on small grids (about 600 blocks)
+        const long long cols = (long long)((g.nx + AJ_TX - 1) / AJ_TX) * ((g.ny + AJ_TY - 1) / AJ_TY);
+        const int target = (int)(g.nz * cols / 600), len = target < 1 ? 1 : (target > 24 ? 24 : target);
+        const int nch = (g.nz + len - 1) / len, kchunk = (g.nz + nch - 1) / nch;
         const dim3 gj((g.nx + AJ_TX - 1) / AJ_TX, (g.ny + AJ_TY - 1) / AJ_TY, (g.nz + kchunk - 1) / kchunk);
         const dim3 bj(AJ_TX, AJ_TY);
         auto mode_of = [&](int q) { return q == 0 ? 0 : (q == nst - 1 ? 2 : 1); };
