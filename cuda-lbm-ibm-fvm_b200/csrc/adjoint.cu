@@ -1082,7 +1082,9 @@ __global__ void __launch_bounds__(256) k_adj_jacobi(Geom g, Range R, InvAp ia, c
 // Two consecutive transposed sweeps in one pass (modes as k_adj_jacobi: A is 0
 // or 1, B is 1 or 2): stage A on lin gives mu_a, stage B on mu_a gives the
 // output; lrhs takes mu_a (A == 0: lrhs = mu_a, else lrhs += mu_a) and then
-// mu_b (B == 1).  A block owns a 32 x 8 column tile and a chunk of planes and
+// mu_b (B == 1).  A == 2: three stages, the pointwise mode 0 folded into the
+// loads (mu_0 = lin / ap as each plane arrives), then stages A (mode 1) and B:
+// lrhs = mu_0 + mu_a (+ mu_b).  A block owns a 32 x 8 column tile and a chunk of planes and
 // marches up in k with plane rings in shared memory: lin with a two-cell
 // in-plane halo, mu_a with a one-cell halo (computed redundantly at the tile
 // edge), so HBM sees lin, lrhs and the output once per two sweeps.
@@ -1144,7 +1146,12 @@ __global__ void __launch_bounds__(AJ_T) k_adj_jacobi2(Geom g, InvAp ia, const do
     const int oA = (threadIdx.y + 1) * WA + threadIdx.x + 1;
     auto slot = [](int k) { return (k + 3) % 3; };  // k >= -2
     auto kflags = [&](int k) { return ((k == 1) << 4) | ((k == g.nz) << 5); };
-    auto ld = [&](const AjPoint& p, int k) { return (p.cell && k >= 1 && k <= g.nz) ? lin[p.off + k * plane] : 0.0; };
+    auto ld = [&](const AjPoint& p, int k) {
+        if (!(p.cell && k >= 1 && k <= g.nz)) return 0.0;
+        const double x = lin[p.off + k * plane];
+        return A == 2 ? x * ia.v[p.flags | kflags(k)] : x;
+    };
+    const int oIn = (threadIdx.y + 2) * WI + threadIdx.x + 2;  // the output point in the lin tile
     // lin of the first plane in registers
     double n0 = ld(L0, k0 - 2), n1 = has_l1 ? ld(L1, k0 - 2) : 0.0;
     for (int t = k0 - 3; t <= k1 + 1; ++t) {
@@ -1189,7 +1196,7 @@ __global__ void __launch_bounds__(AJ_T) k_adj_jacobi2(Geom g, InvAp ia, const do
             const double nb = aj_negN(sA[sb], sA[slot(kb - 1)], sA[slot(kb + 1)], oA, WA, oflags, kb, g.nz, cxx, cyy,
                                       czz);
             const int c = ooff + kb * plane;
-            const double r = A == 0 ? mua : rhs_old + mua;
+            const double r = A == 0 ? mua : (A == 2 ? sIn[sb][oIn] + mua : rhs_old + mua);
             if (B == 1) {
                 const double mub = nb * ia.v[oflags | kflags(kb)];
                 lout[c] = mub;
@@ -1552,15 +1559,19 @@ cudaError_t recompute_step(AdjEngine& e, const AdjState& x, int istep, StepData*
 }
 
 // One step of the segment replay on the engine's buffers, keeping its
-// intermediates in mid: the predictor writes mid's u*, v*, w*; F is copied
-// out after the first and the second sweep.  The start velocity is read from
-// vin, the corrected velocity written to vout (which may be vin).  *par: the
-// Jacobi ping-pong parity of the plain step; *pafter: the pressure after the
-// solve.
-cudaError_t replay_step_keep(AdjEngine& e, int istep, const AdjMid& mid, float* const vin[3], float* const vout[3],
-                             int* par, const float** pafter, cudaStream_t s) {
+// intermediates in mid: the predictor writes mid's u*, v*, w*; the sweeps run
+// out of place, Fin -> mid's F after the first sweep -> mid's F after the
+// second -> Fout.  The start velocity is read from vin, the corrected velocity
+// written to vout (which may be vin).  *par: the Jacobi ping-pong parity of
+// the plain step; *pafter: the pressure after the solve.  (mid's F buffers
+// were cleared at allocation: their ghost cells, which the sweeps do not
+// write, enter the next sweep only through zero wall velocities.)
+cudaError_t replay_step_keep(AdjEngine& e, int istep, const AdjMid& mid, const float* Fin, float* Fout,
+                             float* const vin[3], float* const vout[3], int* par, const float** pafter,
+                             cudaStream_t s) {
     const Geom& g = e.g;
     PlainBuffers b = e.wb;
+    b.F = const_cast<float*>(Fin);  // read only by the predictor, rhs and correction
     b.us = mid.f[0];
     b.vs = mid.f[1];
     b.ws = mid.f[2];
@@ -1581,11 +1592,9 @@ cudaError_t replay_step_keep(AdjEngine& e, int istep, const AdjMid& mid, float* 
     if ((r = plain_correct(g, b, *pafter, s)) != cudaSuccess) return r;
     const int* dirs = sweep_order(istep);
     const float* velof[3] = {b.u, b.v, b.w};
-    if ((r = fct_launch(g, dirs[0], false, b.F, velof[dirs[0]], s)) != cudaSuccess ||
-        (r = copy_field(mid.f[3], b.F, e.elems, s)) != cudaSuccess ||
-        (r = fct_launch(g, dirs[1], false, b.F, velof[dirs[1]], s)) != cudaSuccess ||
-        (r = copy_field(mid.f[4], b.F, e.elems, s)) != cudaSuccess ||
-        (r = fct_launch(g, dirs[2], true, b.F, velof[dirs[2]], s)) != cudaSuccess)
+    if ((r = fct_launch_to(g, dirs[0], false, Fin, mid.f[3], velof[dirs[0]], s)) != cudaSuccess ||
+        (r = fct_launch_to(g, dirs[1], false, mid.f[3], mid.f[4], velof[dirs[1]], s)) != cudaSuccess ||
+        (r = fct_launch_to(g, dirs[2], true, mid.f[4], Fout, velof[dirs[2]], s)) != cudaSuccess)
         return r;
     return cudaSuccess;
 }
@@ -1634,7 +1643,7 @@ cudaError_t reverse_step(AdjEngine& e, const StepData& d, int istep, cudaStream_
         if (r != cudaSuccess) return r;
         if ((r = cudaMemsetAsync(e.lp[e.lp_cur], 0, e.elems * sizeof(double), s)) != cudaSuccess) return r;
     } else if (e.jacobi_iters > 0) {
-        // stages 0, 1 x (iters - 1), 2, two per launch
+        // stages 0, 1 x (iters - 1), 2: the first three in one launch, then two per launch
         const int nst = e.jacobi_iters + 1;
         // chunks of up to 24 planes, shorter on small grids (about 600 blocks)
         const long long cols = (long long)((g.nx + AJ_TX - 1) / AJ_TX) * ((g.ny + AJ_TY - 1) / AJ_TY);
@@ -1643,7 +1652,16 @@ cudaError_t reverse_step(AdjEngine& e, const StepData& d, int istep, cudaStream_
         const dim3 gj((g.nx + AJ_TX - 1) / AJ_TX, (g.ny + AJ_TY - 1) / AJ_TY, (g.nz + kchunk - 1) / kchunk);
         const dim3 bj(AJ_TX, AJ_TY);
         auto mode_of = [&](int q) { return q == 0 ? 0 : (q == nst - 1 ? 2 : 1); };
-        for (int q = 0; q < nst; q += 2) {
+        int q0 = 0;
+        if (nst >= 3) {  // stages 0, 1 and the next in one launch
+            const double* in = e.lp[e.lp_cur];
+            double* out = e.lp[e.lp_cur ^ 1];
+            if (mode_of(2) == 1) k_adj_jacobi2<2, 1><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
+            else k_adj_jacobi2<2, 2><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
+            e.lp_cur ^= 1;
+            q0 = 3;
+        }
+        for (int q = q0; q < nst; q += 2) {
             const double* in = e.lp[e.lp_cur];
             double* out = e.lp[e.lp_cur ^ 1];
             if (q + 1 < nst) {
@@ -1675,8 +1693,9 @@ int adj_kernels_per_step(const AdjEngine& e) {
     // are not kept (front 2, pressure, correction 1, two sweeps), and the
     // adjoint kernels: F copies 3, the three sweep adjoints (1 launch each when
     // fused, else 8), velocity copies 3, correction 1, the transposed Jacobi
-    // sweeps (iters + 1 stages, two per launch), rhs with advection 1.  The convergent modes' pressure
-    // solves (multigrid graphs) are not counted.
+    // sweeps (iters + 1 stages: three in the first launch, then two per
+    // launch), rhs with advection 1.  The convergent modes' pressure solves
+    // (multigrid graphs) are not counted.
     const Geom& g = e.g;
     const int P = e.conv ? 0 : plain_phase_launches(PHASE_JACOBI, e.jacobi_iters);
     int sweeps = 0;
@@ -1689,7 +1708,8 @@ int adj_kernels_per_step(const AdjEngine& e) {
                       : 8;
     const int replay = 2 + P + 1 + 3;
     const int recompute = e.keep ? 0 : 2 + P + 1 + 2;
-    const int jac = (!e.conv && e.jacobi_iters > 0) ? (e.jacobi_iters + 2) / 2 : 0;
+    const int nst = e.jacobi_iters + 1;
+    const int jac = (e.conv || e.jacobi_iters <= 0) ? 0 : (nst >= 3 ? 1 + (nst - 3 + 1) / 2 : 1);
     return replay + recompute + 3 + sweeps + 3 + 1 + jac + 1;
 }
 
@@ -1850,7 +1870,7 @@ static cudaError_t alloc_states(AdjState*& st, int n, int first, size_t elems, b
     return cudaSuccess;
 }
 
-static cudaError_t alloc_mid(AdjMid*& m, int n, size_t elems, size_t* bytes) {
+static cudaError_t alloc_mid(AdjMid*& m, int n, size_t elems, size_t* bytes, cudaStream_t s) {
     m = new (std::nothrow) AdjMid[n];
     if (!m) return cudaErrorMemoryAllocation;
     for (int q = 0; q < n; ++q)
@@ -1863,6 +1883,7 @@ static cudaError_t alloc_mid(AdjMid*& m, int n, size_t elems, size_t* bytes) {
                 return r;
             }
             *bytes += elems * sizeof(float);
+            if ((r = cudaMemsetAsync(m[q].f[t], 0, elems * sizeof(float), s)) != cudaSuccess) return r;
         }
     return cudaSuccess;
 }
@@ -1900,13 +1921,12 @@ cudaError_t adj_tape(AdjEngine* e, int istep0, int nsteps, int every, cudaStream
         if ((r = alloc_states(e->seg, every, keep ? 1 : 0, e->elems, e->conv && !keep, &e->tape_bytes)) !=
             cudaSuccess)
             return r;
-        if (keep && (r = alloc_mid(e->mid, every, e->elems, &e->tape_bytes)) != cudaSuccess) return r;
+        if (keep && (r = alloc_mid(e->mid, every, e->elems, &e->tape_bytes, s)) != cudaSuccess) return r;
     }
     e->istep0 = istep0;
     e->nsteps = nsteps;
     e->every = every;
     e->recorded = false;
-    (void)s;
     return cudaSuccess;
 }
 
@@ -1959,10 +1979,13 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
                 float* const vin[3] = {q == 0 ? e->wb.u : vs[0], q == 0 ? e->wb.v : vs[1], q == 0 ? e->wb.w : vs[2]};
                 float* const* vn = q + 1 < count ? e->seg[q + 1].f + 1 : nullptr;
                 float* const vout[3] = {vn ? vn[0] : e->wb.u, vn ? vn[1] : e->wb.v, vn ? vn[2] : e->wb.w};
-                r = replay_step_keep(*e, e->istep0 + first + q, e->mid[q], vin, vout, &par, &pa[q], s);
+                // F likewise: from the loaded buffer or segment state q, into
+                // segment state q + 1 (or the engine's buffer)
+                const float* Fin = q == 0 ? e->wb.F : e->seg[q].f[0];
+                float* Fout = q + 1 < count ? e->seg[q + 1].f[0] : e->wb.F;
+                r = replay_step_keep(*e, e->istep0 + first + q, e->mid[q], Fin, Fout, vin, vout, &par, &pa[q], s);
                 if (r == cudaSuccess && q + 1 < count) {
-                    if ((r = copy_field(e->seg[q + 1].f[0], e->wb.F, e->elems, s)) == cudaSuccess)
-                        r = copy_field(e->seg[q + 1].f[4], pa[q], e->elems, s);
+                    r = copy_field(e->seg[q + 1].f[4], pa[q], e->elems, s);
                     pa[q] = e->seg[q + 1].f[4];
                 }
             }

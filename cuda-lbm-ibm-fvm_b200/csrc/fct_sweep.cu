@@ -115,7 +115,13 @@ __device__ __forceinline__ int mirrors(int x, int n, int* out) {
 
 // ---- one tile ---------------------------------------------------------------
 template <int AXIS, bool FINAL>
-__global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, float* F, const float* __restrict__ vel) {
+// Fsrc: the sweep's input F (staged into shared memory first); F: its output
+// (interior cells, and on the final sweep every ghost cell).  They may be the
+// same buffer (in place); otherwise F's ghost cells must hold finite values
+// on a non-final sweep (the next sweep reads them only through wall-face
+// fluxes of zero velocity).
+__global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, const float* Fsrc, float* F,
+                                                    const float* __restrict__ vel) {
     extern __shared__ float smem[];
     const Sweep<AXIS> S(g);
     const int n = S.n;
@@ -144,7 +150,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, float* F, const floa
         for (int l = warp; l < nl; l += WARPS) {
             const int base = gi(a0 + l, b, 0);
             for (int q = lane; q < npos; q += LANES) {
-                sF[l * P + q] = F[base + q];
+                sF[l * P + q] = Fsrc[base + q];
                 sV[l * P + q] = __ldg(vel + base + q);
             }
         }
@@ -152,7 +158,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, float* F, const floa
         if (lane < nl) {
             for (int q = warp; q < npos; q += WARPS) {
                 const int gq = gi(a0 + lane, b, q);
-                sF[q * LANES + lane] = F[gq];
+                sF[q * LANES + lane] = Fsrc[gq];
                 sV[q * LANES + lane] = __ldg(vel + gq);
             }
         }
@@ -289,19 +295,26 @@ size_t fct_smem_bytes(int axis, int n) {
 }
 
 template <int AXIS, bool FINAL>
-static cudaError_t launch_axis(const Geom& g, float* F, const float* vel, cudaStream_t s) {
+static cudaError_t launch_axis(const Geom& g, const float* Fsrc, float* F, const float* vel, cudaStream_t s) {
     const int n = AXIS == 0 ? g.nx : (AXIS == 1 ? g.ny : g.nz);
     const int na = AXIS == 0 ? g.ny : g.nx;
     const int nb = AXIS == 2 ? g.ny : g.nz;
     dim3 grid((na + LANES - 1) / LANES, nb, 1);
-    k_fct<AXIS, FINAL><<<grid, dim3(LANES, WARPS), fct_smem_bytes(AXIS, n), s>>>(g, F, vel);
+    k_fct<AXIS, FINAL><<<grid, dim3(LANES, WARPS), fct_smem_bytes(AXIS, n), s>>>(g, Fsrc, F, vel);
     return cudaGetLastError();
 }
 
+cudaError_t fct_launch_to(const Geom& g, int axis, bool final_sweep, const float* Fin, float* Fout, const float* vel,
+                          cudaStream_t s) {
+    if (axis == 0)
+        return final_sweep ? launch_axis<0, true>(g, Fin, Fout, vel, s) : launch_axis<0, false>(g, Fin, Fout, vel, s);
+    if (axis == 1)
+        return final_sweep ? launch_axis<1, true>(g, Fin, Fout, vel, s) : launch_axis<1, false>(g, Fin, Fout, vel, s);
+    return final_sweep ? launch_axis<2, true>(g, Fin, Fout, vel, s) : launch_axis<2, false>(g, Fin, Fout, vel, s);
+}
+
 cudaError_t fct_launch(const Geom& g, int axis, bool final_sweep, float* F, const float* vel, cudaStream_t s) {
-    if (axis == 0) return final_sweep ? launch_axis<0, true>(g, F, vel, s) : launch_axis<0, false>(g, F, vel, s);
-    if (axis == 1) return final_sweep ? launch_axis<1, true>(g, F, vel, s) : launch_axis<1, false>(g, F, vel, s);
-    return final_sweep ? launch_axis<2, true>(g, F, vel, s) : launch_axis<2, false>(g, F, vel, s);
+    return fct_launch_to(g, axis, final_sweep, F, F, vel, s);
 }
 
 cudaError_t fct_configure() {

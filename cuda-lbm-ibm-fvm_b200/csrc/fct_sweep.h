@@ -12,6 +12,13 @@ namespace vof {
 // conditions.
 cudaError_t fct_launch(const Geom& g, int axis, bool final_sweep, float* F, const float* vel, cudaStream_t s);
 
+// The same sweep out of place: reads Fin, writes Fout (its interior cells;
+// on the final sweep also every ghost cell).  On a non-final sweep Fout's
+// ghost cells must already hold finite values (the next sweep reads them only
+// through wall-face fluxes of zero velocity).
+cudaError_t fct_launch_to(const Geom& g, int axis, bool final_sweep, const float* Fin, float* Fout, const float* vel,
+                          cudaStream_t s);
+
 // Dynamic shared memory of one sweep tile for lines of n cells.
 size_t fct_smem_bytes(int axis, int n);
 
