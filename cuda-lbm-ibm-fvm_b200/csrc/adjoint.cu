@@ -608,8 +608,8 @@ __global__ void __launch_bounds__(FA_THREADS) k_fct_adjoint(Geom g, const float*
 }
 
 // ---- the sweep adjoint as one march along each line, one lane per line ------------
-// A block owns FM_LANES lines (one per lane) and splits each line's positions
-// 0 .. n+1 into WARPS segments, one per warp.  A warp walks its segment once,
+// A block owns FM_LANES lines (one per lane, numbered over both cross axes)
+// and splits each line's positions 0 .. n+1 into WARPS segments, one per warp.  A warp walks its segment once,
 // starting FM_WARM positions early; iteration c evaluates, in registers, the
 // forward and reverse stages at staggered positions, each from values that
 // earlier stages or iterations produced:
@@ -870,12 +870,14 @@ __global__ void __launch_bounds__(FM_LANES * WARPS, DIR == 0 ? VOF_FM_MINB_X : V
                                                                         double* lFg, double* __restrict__ lvelg) {
     FmLine<DIR> L(g);
     const int n = L.S.n;
-    const int na = DIR == 0 ? g.ny : g.nx;  // lines along a (one per lane)
+    // lines (a, b) numbered a fastest over both cross axes, one per lane, so
+    // that no lane idles at the end of a row of lines
+    const int na = DIR == 0 ? g.ny : g.nx, nb = DIR == 2 ? g.ny : g.nz;
     const int lane = threadIdx.x, warp = threadIdx.y;
-    int a = 1 + blockIdx.x * FM_LANES + lane;
-    const int b = 1 + blockIdx.y;
-    L.live = a <= na;
-    if (!L.live) a = na;  // a valid line to read; nothing is written
+    int line = blockIdx.x * FM_LANES + lane;
+    L.live = line < na * nb;
+    if (!L.live) line = na * nb - 1;  // a valid line to read; nothing is written
+    const int a = 1 + line % na, b = 1 + line / na;
     const int base = DIR == 0 ? gidx(g, 0, a, b) : (DIR == 1 ? gidx(g, a, 0, b) : gidx(g, a, b, 0));
     L.gs = DIR == 0 ? 1 : (DIR == 1 ? g.px : g.plane);
     L.n = n;
@@ -1452,7 +1454,7 @@ cudaError_t launch_fct_adjoint_march(const Geom& g, const float* Fs, const float
                                      cudaStream_t s) {
     const int na = DIR == 0 ? g.ny : g.nx;
     const int nb = DIR == 2 ? g.ny : g.nz;
-    k_fct_adjoint_march<DIR, FM_WARPS><<<dim3((na + FM_LANES - 1) / FM_LANES, nb), dim3(FM_LANES, FM_WARPS), 0, s>>>(
+    k_fct_adjoint_march<DIR, FM_WARPS><<<dim3((na * nb + FM_LANES - 1) / FM_LANES), dim3(FM_LANES, FM_WARPS), 0, s>>>(
         g, Fs, vel, lF, lvel);
     return cudaGetLastError();
 }

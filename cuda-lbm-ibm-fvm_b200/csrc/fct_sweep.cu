@@ -18,9 +18,10 @@
 // The per-cell expressions (and the reference's length factors per sweep)
 // are in fct_line.cuh, shared with the sweep adjoint.
 //
-// Kernel shape.  A block owns a tile of 32 lines (one per lane) over their
-// full length.  The tile's F and face velocity are staged once in shared
-// memory with coalesced loads; then each warp marches one segment of the
+// Kernel shape.  A block owns a tile of 32 lines (one per lane; lines are
+// numbered over both cross axes) over their full length.  The tile's F and
+// face velocity are staged once in shared memory with coalesced loads; then
+// each warp marches one segment of the
 // lines, carrying the stage values of the last few cells in registers, so each
 // cell's fluxes, Ftd, Zalesak ratios and face limiters are computed exactly
 // once (plus a three-cell warm-up at segment starts).  Shared memory is laid
@@ -129,9 +130,12 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, const float* Fsrc, f
     const int na = AXIS == 0 ? g.ny : g.nx;           // lines along a
     const int nb = AXIS == 2 ? g.ny : g.nz;           // lines along b
     const int lane = threadIdx.x, warp = threadIdx.y;
-    const int a0 = 1 + blockIdx.x * LANES;            // first line of the tile
-    const int b = 1 + blockIdx.y;
-    const int nl = min(LANES, na - a0 + 1);
+    // the tile's lines (a, b), numbered a fastest over both cross axes so
+    // that no lane idles at the end of a row of lines
+    const int line0 = blockIdx.x * LANES;             // first line of the tile
+    const int nl = min(LANES, na * nb - line0);
+    auto line_a = [&](int l) { return 1 + (line0 + l) % na; };
+    auto line_b = [&](int l) { return 1 + (line0 + l) / na; };
     const int P = odd_pitch(npos);
 
     // global index of (line a, b; position q)
@@ -148,7 +152,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, const float* Fsrc, f
     // ---- stage the tile (coalesced) ----
     if (AXIS == 0) {
         for (int l = warp; l < nl; l += WARPS) {
-            const int base = gi(a0 + l, b, 0);
+            const int base = gi(line_a(l), line_b(l), 0);
             for (int q = lane; q < npos; q += LANES) {
                 sF[l * P + q] = Fsrc[base + q];
                 sV[l * P + q] = __ldg(vel + base + q);
@@ -157,7 +161,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, const float* Fsrc, f
     } else {
         if (lane < nl) {
             for (int q = warp; q < npos; q += WARPS) {
-                const int gq = gi(a0 + lane, b, q);
+                const int gq = gi(line_a(lane), line_b(lane), q);
                 sF[q * LANES + lane] = Fsrc[gq];
                 sV[q * LANES + lane] = __ldg(vel + gq);
             }
@@ -170,7 +174,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, const float* Fsrc, f
     const int c0 = 1 + warp * seg;
     const int c1 = min(n, c0 + seg - 1);
     const LineView L{sF + si(lane, 0), sV + si(lane, 0), qs};
-    const int a = a0 + lane;
+    const int a = line_a(lane), b = line_b(lane);
     const bool live = lane < nl && c0 <= n;
 
     // x lines: each result goes into sF in place.  The march at cell c reads
@@ -270,13 +274,13 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, const float* Fsrc, f
         // ---- write the x rows back (coalesced) ----
         __syncthreads();
         for (int l = warp; l < nl; l += WARPS) {
-            const int aa = a0 + l;
+            const int aa = line_a(l), bb = line_b(l);
             if (!FINAL) {
-                const int base = gi(aa, b, 0);
+                const int base = gi(aa, bb, 0);
                 for (int q = 1 + lane; q <= n; q += LANES) F[base + q] = sF[l * P + q];
             } else {
                 int av[3], bv[3];
-                const int nav = mirrors(aa, na, av), nbv = mirrors(b, nb, bv);
+                const int nav = mirrors(aa, na, av), nbv = mirrors(bb, nb, bv);
                 for (int ib = 0; ib < nbv; ++ib)
                     for (int ia = 0; ia < nav; ++ia) {
                         const int base = gi(av[ia], bv[ib], 0);
@@ -299,7 +303,7 @@ static cudaError_t launch_axis(const Geom& g, const float* Fsrc, float* F, const
     const int n = AXIS == 0 ? g.nx : (AXIS == 1 ? g.ny : g.nz);
     const int na = AXIS == 0 ? g.ny : g.nx;
     const int nb = AXIS == 2 ? g.ny : g.nz;
-    dim3 grid((na + LANES - 1) / LANES, nb, 1);
+    dim3 grid((na * nb + LANES - 1) / LANES, 1, 1);
     k_fct<AXIS, FINAL><<<grid, dim3(LANES, WARPS), fct_smem_bytes(AXIS, n), s>>>(g, Fsrc, F, vel);
     return cudaGetLastError();
 }
