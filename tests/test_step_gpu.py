@@ -300,3 +300,28 @@ def test_dam_break_vs_reference_kernels(cuda, V, orc):
     if orc.ref_available("nofma"):
         ref_nf = orc.ref_run(prm, state, 1, 200, variant="nofma")
         assert_bitwise(got, ref_nf, STATE, "32^3 x 200 vs reference -fmad=false")
+
+
+def test_full_size_dam_break_vs_reference_kernels(cuda, V, orc):
+    """The benchmark workload at its full size: 200^3 dam break with the
+    noisy interface (splitmix64 seed 1), 30 steps (every sweep order ten
+    times), graph-captured.  Bit-identical to the reference's kernels built
+    with -fmad=false; against its default (FMA) build rel-L2 <= 1e-5 for F,
+    u, v, w and p modulo its mean, max-abs |dF| <= 1e-4, and the total liquid
+    volume (FP64 sum of F) within 1e-7 relative."""
+    _need_ref(orc, "nofma")
+    prm = V.default_params(200, gy=0.0, gz=-9.81)
+    state = ic.rest_state(prm, ic.dam_break(prm, height=ic.noisy_height(prm, seed=1)))
+    got = run_gpu(V, prm, state, 1, 30, use_graph=True)
+    ref_nf = orc.ref_run(prm, state, 1, 30, variant="nofma")
+    assert_bitwise(got, ref_nf, STATE, "200^3 x 30 vs reference -fmad=false")
+    if orc.ref_available("sm100a"):
+        ref = orc.ref_run(prm, state, 1, 30, variant="sm100a")
+        for k in ("F", "u", "v", "w"):
+            assert rel_l2(got[k], ref[k]) <= 1e-5, (k, rel_l2(got[k], ref[k]))
+        assert np.abs(got["F"].astype(np.float64) - ref["F"]).max() <= 1e-4
+        pm = got["p"][1:-1, 1:-1, 1:-1].astype(np.float64)
+        qm = ref["p"][1:-1, 1:-1, 1:-1].astype(np.float64)
+        assert rel_l2(pm - pm.mean(), qm - qm.mean()) <= 1e-5
+        vol = lambda F: float(F[1:-1, 1:-1, 1:-1].astype(np.float64).sum())  # noqa: E731
+        assert abs(vol(got["F"]) - vol(ref["F"])) <= 1e-7 * vol(ref["F"])
