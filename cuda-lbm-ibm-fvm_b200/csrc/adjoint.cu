@@ -1699,7 +1699,7 @@ int adj_kernels_per_step(const AdjEngine& e) {
     // launch), rhs with advection 1.  The convergent modes' pressure solves
     // (multigrid graphs) are not counted.
     const Geom& g = e.g;
-    const int P = e.conv ? 0 : plain_phase_launches(PHASE_JACOBI, e.jacobi_iters);
+    const int P = e.conv ? 0 : plain_phase_launches(e.g, PHASE_JACOBI, e.jacobi_iters);
     int sweeps = 0;
     const int len[3] = {g.nx, g.ny, g.nz};
     const long lines[3] = {(long)g.ny * g.nz, (long)g.nx * g.nz, (long)g.nx * g.ny};

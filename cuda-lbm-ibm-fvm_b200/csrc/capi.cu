@@ -440,8 +440,9 @@ int vof_step_timed(vof_ctx* ctx, int istep, float* phase_ms, int* launches, int 
         e = cudaEventElapsedTime(&ms, ev[q], ev[q + 1]);
         if (phase_ms) phase_ms[q] = ms;
         if (launches)
-            launches[q] = (ctx->conv && q == vof::PHASE_JACOBI) ? ctx->stats.launches
-                                                                : vof::plain_phase_launches(q, ctx->prm.jacobi_iters);
+            launches[q] = (ctx->conv && q == vof::PHASE_JACOBI)
+                              ? ctx->stats.launches
+                              : vof::plain_phase_launches(ctx->g, q, ctx->prm.jacobi_iters);
     }
     for (int q = 0; q <= vof::PLAIN_PHASES; ++q)
         if (ev[q]) cudaEventDestroy(ev[q]);
@@ -600,7 +601,7 @@ int vof_last_cuda_error(const vof_ctx* ctx) { return ctx ? ctx->last_cuda_error 
 int vof_kernels_per_step(const vof_ctx* ctx) {
     if (!ctx) return VOF_E_INVALID;
     if (ctx->conv) return 2 + ctx->stats.launches + 4;  // the last step's count
-    return vof::plain_kernels_per_step(ctx->prm.jacobi_iters);
+    return vof::plain_kernels_per_step(ctx->g, ctx->prm.jacobi_iters);
 }
 
 size_t vof_device_bytes(const vof_ctx* ctx) {

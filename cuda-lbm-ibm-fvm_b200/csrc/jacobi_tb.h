@@ -20,6 +20,10 @@ cudaError_t jacobi_tb_maps(const Geom& g, const float* field, CUtensorMap* map);
 cudaError_t jacobi_tb_launch(const Geom& g, int T, const CUtensorMap& map_in, const CUtensorMap& map_rhs,
                              float* pout, int* status, cudaStream_t s);
 
+// One Jacobi sweep from pin (and rhs) into the interior of pout (a different
+// buffer; its ghost cells are left as they are), streaming along z.
+cudaError_t jacobi_col_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);
+
 // Dynamic shared memory of one block for T fused sweeps.
 size_t jacobi_tb_smem_bytes(int T);
 

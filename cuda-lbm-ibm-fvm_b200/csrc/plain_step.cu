@@ -13,6 +13,7 @@
 //   k_predict      advect_{u,v,w}_kernel + cal_nu_rho_kernel   voftrial1.cu:95-104, 230-399
 //   k_rhs          the rhs expression of solve_p_jacobi_kernel voftrial1.cu:418-422
 //   k_jacobi_tb<T> (jacobi_tb.cu) T solve_p_jacobi_kernel sweeps per launch  voftrial1.cu:401-439
+//                  (small grids: k_jacobi_col, one sweep per launch)
 //   k_correct      update_{u,v,w}_kernel + apply_bc_velocity   voftrial1.cu:441-493, 959-1051, 1107-1120
 //   k_fct<AXIS,FINAL>  (fct_sweep.cu) fct_{x,y,z}_sweep_stage1..4, and on
 //                  the last sweep post_process_f_kernel + apply_bc_F   voftrial1.cu:502-905, 1053-1135
@@ -334,7 +335,14 @@ static_assert(JACOBI_T >= 1 && JACOBI_T <= JACOBI_TB_MAX, "VOF_JACOBI_T out of r
 // Launches for `iters` sweeps: ceil(iters / JACOBI_T), except that a single
 // blocked launch cannot end in the buffer it reads, so iters == JACOBI_T
 // (even) runs as single sweeps.
-static int jacobi_launches(int iters) {
+// Grids of at most this many interior cells take one streaming sweep per
+// launch (k_jacobi_col), larger ones the blocked sweeps (k_jacobi_tb): the
+// measured crossover lies between 96^3 and 128^3.
+constexpr long long JACOBI_COL_MAX_CELLS = 1500000;
+static bool jacobi_streaming(const Geom& g) { return (long long)g.nx * g.ny * g.nz <= JACOBI_COL_MAX_CELLS; }
+
+static int jacobi_launches(const Geom& g, int iters) {
+    if (jacobi_streaming(g)) return iters;
     const int L = (iters + JACOBI_T - 1) / JACOBI_T;
     return (L == 1 && iters % 2 == 0) ? iters : L;
 }
@@ -360,7 +368,9 @@ static bool plan_buffers(int src, int dst, int L, int* seq) {
     return true;
 }
 
-int plain_kernels_per_step(int jacobi_iters) { return 1 + 1 + jacobi_launches(jacobi_iters) + 1 + 3; }
+int plain_kernels_per_step(const Geom& g, int jacobi_iters) {
+    return 1 + 1 + jacobi_launches(g, jacobi_iters) + 1 + 3;
+}
 
 // Column-marching launch shape: 32 x 8 columns per block, z split into
 // chunks of about 16 planes (long enough to reuse the k-window, short enough
@@ -424,7 +434,8 @@ cudaError_t plain_back(const Geom& g, const PlainBuffers& b, int istep, const fl
 cudaError_t plain_pressure(const Geom& g, const PlainBuffers& b, int jacobi_iters, int* p_parity, cudaStream_t s) {
     cudaError_t e;
 
-    // Jacobi (voftrial1.cu:1371-1375): JACOBI_T sweeps per launch.  The
+    // Jacobi (voftrial1.cu:1371-1375): one streaming sweep per launch on
+    // small grids, else JACOBI_T blocked sweeps per launch.  The
     // reference ping-pongs p <-> pt once per sweep, so after N sweeps its
     // pressure sits in the buffer it started in when N is even and in the
     // other one when N is odd; the launches route through the scratch
@@ -434,7 +445,13 @@ cudaError_t plain_pressure(const Geom& g, const PlainBuffers& b, int jacobi_iter
     const int src = *p_parity, dst = src ^ (jacobi_iters & 1);
     const int L = (jacobi_iters + JACOBI_T - 1) / JACOBI_T;
     int seq[64];
-    if (L > 62 || !plan_buffers(src, dst, L, seq)) {
+    if (jacobi_streaming(g)) {
+        int cur = src;
+        for (int it = 0; it < jacobi_iters; ++it) {
+            if ((e = jacobi_col_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s)) != cudaSuccess) return e;
+            cur ^= 1;
+        }
+    } else if (L > 62 || !plan_buffers(src, dst, L, seq)) {
         // fall back to one sweep per launch: a plain ping-pong always works
         int cur = src;
         for (int it = 0; it < jacobi_iters; ++it) {
@@ -463,8 +480,8 @@ cudaError_t plain_step(const Geom& g, const PlainBuffers& b, int istep, int jaco
     return plain_back(g, b, istep, pbuf[*p_parity], s, ev);
 }
 
-int plain_phase_launches(int phase, int jacobi_iters) {
-    return phase == PHASE_JACOBI ? jacobi_launches(jacobi_iters) : 1;
+int plain_phase_launches(const Geom& g, int phase, int jacobi_iters) {
+    return phase == PHASE_JACOBI ? jacobi_launches(g, jacobi_iters) : 1;
 }
 
 }  // namespace vof

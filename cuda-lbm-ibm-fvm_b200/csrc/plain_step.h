@@ -40,7 +40,7 @@ cudaError_t plain_density_pairs_on(Geom* g, float* dev6, cudaStream_t s);
 bool plain_supported(const Geom& g);
 
 // Kernel launches per plain step.
-int plain_kernels_per_step(int jacobi_iters);
+int plain_kernels_per_step(const Geom& g, int jacobi_iters);
 
 // Phases of one plain step, in launch order.
 enum {
@@ -74,6 +74,6 @@ cudaError_t plain_pressure(const Geom& g, const PlainBuffers& b, int jacobi_iter
 cudaError_t plain_correct(const Geom& g, const PlainBuffers& b, const float* p, cudaStream_t s);
 
 // Kernel launches of one phase.
-int plain_phase_launches(int phase, int jacobi_iters);
+int plain_phase_launches(const Geom& g, int phase, int jacobi_iters);
 
 }  // namespace vof
