@@ -206,35 +206,12 @@ __global__ void k_density_pairs(Geom g, float* out) {
     out[5] = g.dt / r2;
 }
 
-__global__ void __launch_bounds__(256) k_correct(Geom g,
-                                                 const float* __restrict__ F,
-                                                 const float* __restrict__ us,
-                                                 const float* __restrict__ vs,
-                                                 const float* __restrict__ ws,
-                                                 const float* __restrict__ p,
-                                                 float* __restrict__ u, float* __restrict__ v,
-                                                 float* __restrict__ w) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-    if (i > g.nx || j > g.ny || k > g.nz) return;
-    const int sy = g.px, sz = g.plane;
-    const int id = gidx(g, i, j, k);
-    const float rho_c = rho_of(g, __ldg(F + id));
-    const float p_c = __ldg(p + id);
-    float un = 0.0f, vn = 0.0f, wn = 0.0f;  // wall faces (i, j or k == 1) are 0
-    if (i >= 2) {
-        const float r = 0.5f * (rho_c + rho_of(g, __ldg(F + id - 1)));
-        un = __ldg(us + id) - dt_over(g, r) * (p_c - __ldg(p + id - 1)) * g.dxi;
-    }
-    if (j >= 2) {
-        const float r = 0.5f * (rho_c + rho_of(g, __ldg(F + id - sy)));
-        vn = __ldg(vs + id) - dt_over(g, r) * (p_c - __ldg(p + id - sy)) * g.dyi;
-    }
-    if (k >= 2) {
-        const float r = 0.5f * (rho_c + rho_of(g, __ldg(F + id - sz)));
-        wn = __ldg(ws + id) - dt_over(g, r) * (p_c - __ldg(p + id - sz)) * g.dzi;
-    }
+// Writes the corrected face velocities of cell (i, j, k) and, on the domain
+// edges, the boundary copies of apply_bc_velocity (voftrial1.cu:959-1051,
+// 1107-1120) in closed form.
+__device__ __forceinline__ void store_corrected(const Geom& g, float* __restrict__ u, float* __restrict__ v,
+                                                float* __restrict__ w, int i, int j, int k, int id, float un,
+                                                float vn, float wn) {
     const bool edge_i = (i == 1 || i == g.nx), edge_j = (j == 1 || j == g.ny), edge_k = (k == 1 || k == g.nz);
     if (!(edge_i || edge_j || edge_k)) {  // bulk: one write per component
         u[id] = un;
@@ -278,6 +255,38 @@ __global__ void __launch_bounds__(256) k_correct(Geom g,
             for (int a = 0; a < nmi; ++a)
                 if (a || b) w[gidx(g, mi[a], mj[b], 0)] = s0;
     }
+}
+
+__global__ void __launch_bounds__(256) k_correct(Geom g,
+                                                 const float* __restrict__ F,
+                                                 const float* __restrict__ us,
+                                                 const float* __restrict__ vs,
+                                                 const float* __restrict__ ws,
+                                                 const float* __restrict__ p,
+                                                 float* __restrict__ u, float* __restrict__ v,
+                                                 float* __restrict__ w) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.nx || j > g.ny || k > g.nz) return;
+    const int sy = g.px, sz = g.plane;
+    const int id = gidx(g, i, j, k);
+    const float rho_c = rho_of(g, __ldg(F + id));
+    const float p_c = __ldg(p + id);
+    float un = 0.0f, vn = 0.0f, wn = 0.0f;  // wall faces (i, j or k == 1) are 0
+    if (i >= 2) {
+        const float r = 0.5f * (rho_c + rho_of(g, __ldg(F + id - 1)));
+        un = __ldg(us + id) - dt_over(g, r) * (p_c - __ldg(p + id - 1)) * g.dxi;
+    }
+    if (j >= 2) {
+        const float r = 0.5f * (rho_c + rho_of(g, __ldg(F + id - sy)));
+        vn = __ldg(vs + id) - dt_over(g, r) * (p_c - __ldg(p + id - sy)) * g.dyi;
+    }
+    if (k >= 2) {
+        const float r = 0.5f * (rho_c + rho_of(g, __ldg(F + id - sz)));
+        wn = __ldg(ws + id) - dt_over(g, r) * (p_c - __ldg(p + id - sz)) * g.dzi;
+    }
+    store_corrected(g, u, v, w, i, j, k, id, un, vn, wn);
 }
 
 // ---------------------------------------------------------------------------
