@@ -640,6 +640,7 @@ struct FmLine {
     double* lvell;
     int gs, n, c0, c1;  // stride along the line; the warp's segment [c0, c1]
     bool live;          // the lane has a line
+    bool staged;        // Fl, Vl point to the line's copy in shared memory
     double vold, dt, iK4, hq, K1, dvfac;
     // forward windows (FP32), positions relative to the iteration's c
     float F5, V5, lo5;              // F, V and the low-order flux at position c+5
@@ -667,8 +668,16 @@ struct FmLine {
 
     __device__ FmLine(const Geom& g) : S(g) {}
 
-    __device__ __forceinline__ float ldF(int q) const { return (q >= 0 && q <= n + 1) ? __ldg(Fl + q * gs) : 0.0f; }
-    __device__ __forceinline__ float ldV(int f) const { return (f >= 1 && f <= n + 1) ? __ldg(Vl + f * gs) : 0.0f; }
+    // F and V of the line: from shared memory when staged (Fl, Vl point
+    // there, stride 1), else from global memory (read-only path)
+    __device__ __forceinline__ float ldF(int q) const {
+        if (!(q >= 0 && q <= n + 1)) return 0.0f;
+        return staged ? Fl[q] : __ldg(Fl + q * gs);
+    }
+    __device__ __forceinline__ float ldV(int f) const {
+        if (!(f >= 1 && f <= n + 1)) return 0.0f;
+        return staged ? Vl[f] : __ldg(Vl + f * gs);
+    }
     __device__ __forceinline__ bool owned(int q) const { return live && q >= c0 && q <= c1; }
     // lF of cell e as stage 4 reads it: own and earlier cells from memory, the
     // three after the segment from the registers loaded before the block barrier
@@ -864,10 +873,14 @@ struct FmLine {
 #ifndef VOF_FM_MINB_X
 #define VOF_FM_MINB_X 1
 #endif
-template <int DIR, int WARPS>
-__global__ void __launch_bounds__(FM_LANES * WARPS, DIR == 0 ? VOF_FM_MINB_X : VOF_FM_MINB) k_fct_adjoint_march(Geom g, const float* __restrict__ Fg,
-                                                                        const float* __restrict__ velg,
-                                                                        double* lFg, double* __restrict__ lvelg) {
+// STAGE (x lines): the block's F and V lines are first copied into shared
+// memory with coalesced row loads, [line][position] with an odd pitch; the
+// march then reads them there instead of 32 strided rows per warp load.
+template <int DIR, int WARPS, bool STAGE>
+__global__ void __launch_bounds__(FM_LANES * WARPS, DIR == 0 ? VOF_FM_MINB_X : VOF_FM_MINB)
+    k_fct_adjoint_march(Geom g, const float* __restrict__ Fg, const float* __restrict__ velg, double* lFg,
+                        double* __restrict__ lvelg) {
+    extern __shared__ __align__(16) float fm_line_smem[];
     FmLine<DIR> L(g);
     const int n = L.S.n;
     // lines (a, b) numbered a fastest over both cross axes, one per lane, so
@@ -883,6 +896,25 @@ __global__ void __launch_bounds__(FM_LANES * WARPS, DIR == 0 ? VOF_FM_MINB_X : V
     L.n = n;
     L.Fl = Fg + base;
     L.Vl = velg + base;
+    L.staged = false;
+    if (STAGE) {
+        const int P = (n + 2) | 1;
+        float* sF = fm_line_smem;
+        float* sV = fm_line_smem + FM_LANES * P;
+        for (int l = warp; l < FM_LANES; l += WARPS) {
+            int ln = blockIdx.x * FM_LANES + l;
+            if (ln >= na * nb) ln = na * nb - 1;
+            const int rb = gidx(g, 0, 1 + ln % na, 1 + ln / na);  // x lines: the row (j, k)
+            for (int q = lane; q < n + 2; q += FM_LANES) {
+                sF[l * P + q] = __ldg(Fg + rb + q);
+                sV[l * P + q] = __ldg(velg + rb + q);
+            }
+        }
+        __syncthreads();
+        L.Fl = sF + lane * P;
+        L.Vl = sV + lane * P;
+        L.staged = true;
+    }
     L.lFl = lFg + base;
     L.lvell = lvelg + base;
     const int seg = (n + 2 + WARPS - 1) / WARPS;
@@ -1454,8 +1486,17 @@ cudaError_t launch_fct_adjoint_march(const Geom& g, const float* Fs, const float
                                      cudaStream_t s) {
     const int na = DIR == 0 ? g.ny : g.nx;
     const int nb = DIR == 2 ? g.ny : g.nz;
-    k_fct_adjoint_march<DIR, FM_WARPS><<<dim3((na * nb + FM_LANES - 1) / FM_LANES), dim3(FM_LANES, FM_WARPS), 0, s>>>(
-        g, Fs, vel, lF, lvel);
+    const dim3 grid((na * nb + FM_LANES - 1) / FM_LANES), blk(FM_LANES, FM_WARPS);
+    const int n = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
+    const size_t smem = sizeof(float) * 2 * FM_LANES * (size_t)((n + 2) | 1);
+    if (DIR == 0 && smem <= fa_smem_limit()) {
+        cudaError_t r = cudaFuncSetAttribute(k_fct_adjoint_march<DIR, FM_WARPS, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (r != cudaSuccess) return r;
+        k_fct_adjoint_march<DIR, FM_WARPS, true><<<grid, blk, smem, s>>>(g, Fs, vel, lF, lvel);
+    } else {
+        k_fct_adjoint_march<DIR, FM_WARPS, false><<<grid, blk, 0, s>>>(g, Fs, vel, lF, lvel);
+    }
     return cudaGetLastError();
 }
 
