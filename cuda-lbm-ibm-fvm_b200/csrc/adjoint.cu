@@ -1116,9 +1116,7 @@ __global__ void __launch_bounds__(256) k_adj_jacobi(Geom g, Range R, InvAp ia, c
 // Two consecutive transposed sweeps in one pass (modes as k_adj_jacobi: A is 0
 // or 1, B is 1 or 2): stage A on lin gives mu_a, stage B on mu_a gives the
 // output; lrhs takes mu_a (A == 0: lrhs = mu_a, else lrhs += mu_a) and then
-// mu_b (B == 1).  A == 2: three stages, the pointwise mode 0 folded into the
-// loads (mu_0 = lin / ap as each plane arrives), then stages A (mode 1) and B:
-// lrhs = mu_0 + mu_a (+ mu_b).  A block owns a 32 x 8 column tile and a chunk of planes and
+// mu_b (B == 1).  A block owns a 32 x 8 column tile and a chunk of planes and
 // marches up in k with plane rings in shared memory: lin with a two-cell
 // in-plane halo, mu_a with a one-cell halo (computed redundantly at the tile
 // edge), so HBM sees lin, lrhs and the output once per two sweeps.
@@ -1180,12 +1178,7 @@ __global__ void __launch_bounds__(AJ_T) k_adj_jacobi2(Geom g, InvAp ia, const do
     const int oA = (threadIdx.y + 1) * WA + threadIdx.x + 1;
     auto slot = [](int k) { return (k + 3) % 3; };  // k >= -2
     auto kflags = [&](int k) { return ((k == 1) << 4) | ((k == g.nz) << 5); };
-    auto ld = [&](const AjPoint& p, int k) {
-        if (!(p.cell && k >= 1 && k <= g.nz)) return 0.0;
-        const double x = lin[p.off + k * plane];
-        return A == 2 ? x * ia.v[p.flags | kflags(k)] : x;
-    };
-    const int oIn = (threadIdx.y + 2) * WI + threadIdx.x + 2;  // the output point in the lin tile
+    auto ld = [&](const AjPoint& p, int k) { return (p.cell && k >= 1 && k <= g.nz) ? lin[p.off + k * plane] : 0.0; };
     // lin of the first plane in registers
     double n0 = ld(L0, k0 - 2), n1 = has_l1 ? ld(L1, k0 - 2) : 0.0;
     for (int t = k0 - 3; t <= k1 + 1; ++t) {
@@ -1230,7 +1223,7 @@ __global__ void __launch_bounds__(AJ_T) k_adj_jacobi2(Geom g, InvAp ia, const do
             const double nb = aj_negN(sA[sb], sA[slot(kb - 1)], sA[slot(kb + 1)], oA, WA, oflags, kb, g.nz, cxx, cyy,
                                       czz);
             const int c = ooff + kb * plane;
-            const double r = A == 0 ? mua : (A == 2 ? sIn[sb][oIn] + mua : rhs_old + mua);
+            const double r = A == 0 ? mua : rhs_old + mua;
             if (B == 1) {
                 const double mub = nb * ia.v[oflags | kflags(kb)];
                 lout[c] = mub;
@@ -1686,7 +1679,7 @@ cudaError_t reverse_step(AdjEngine& e, const StepData& d, int istep, cudaStream_
         if (r != cudaSuccess) return r;
         if ((r = cudaMemsetAsync(e.lp[e.lp_cur], 0, e.elems * sizeof(double), s)) != cudaSuccess) return r;
     } else if (e.jacobi_iters > 0) {
-        // stages 0, 1 x (iters - 1), 2: the first three in one launch, then two per launch
+        // stages 0, 1 x (iters - 1), 2, two per launch
         const int nst = e.jacobi_iters + 1;
         // chunks of up to 24 planes, shorter on small grids (about 600 blocks)
         const long long cols = (long long)((g.nx + AJ_TX - 1) / AJ_TX) * ((g.ny + AJ_TY - 1) / AJ_TY);
@@ -1695,16 +1688,7 @@ cudaError_t reverse_step(AdjEngine& e, const StepData& d, int istep, cudaStream_
         const dim3 gj((g.nx + AJ_TX - 1) / AJ_TX, (g.ny + AJ_TY - 1) / AJ_TY, (g.nz + kchunk - 1) / kchunk);
         const dim3 bj(AJ_TX, AJ_TY);
         auto mode_of = [&](int q) { return q == 0 ? 0 : (q == nst - 1 ? 2 : 1); };
-        int q0 = 0;
-        if (nst >= 3) {  // stages 0, 1 and the next in one launch
-            const double* in = e.lp[e.lp_cur];
-            double* out = e.lp[e.lp_cur ^ 1];
-            if (mode_of(2) == 1) k_adj_jacobi2<2, 1><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
-            else k_adj_jacobi2<2, 2><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
-            e.lp_cur ^= 1;
-            q0 = 3;
-        }
-        for (int q = q0; q < nst; q += 2) {
+        for (int q = 0; q < nst; q += 2) {
             const double* in = e.lp[e.lp_cur];
             double* out = e.lp[e.lp_cur ^ 1];
             if (q + 1 < nst) {
@@ -1736,8 +1720,7 @@ int adj_kernels_per_step(const AdjEngine& e) {
     // are not kept (front 2, pressure, correction 1, two sweeps), and the
     // adjoint kernels: F copies 3, the three sweep adjoints (1 launch each when
     // fused, else 8), velocity copies 3, correction 1, the transposed Jacobi
-    // sweeps (iters + 1 stages: three in the first launch, then two per
-    // launch), rhs with advection 1.  The convergent modes' pressure solves
+    // sweeps (iters + 1 stages, two per launch), rhs with advection 1.  The convergent modes' pressure solves
     // (multigrid graphs) are not counted.
     const Geom& g = e.g;
     const int P = e.conv ? 0 : plain_phase_launches(e.g, PHASE_JACOBI, e.jacobi_iters);
@@ -1751,8 +1734,7 @@ int adj_kernels_per_step(const AdjEngine& e) {
                       : 8;
     const int replay = 2 + P + 1 + 3;
     const int recompute = e.keep ? 0 : 2 + P + 1 + 2;
-    const int nst = e.jacobi_iters + 1;
-    const int jac = (e.conv || e.jacobi_iters <= 0) ? 0 : (nst >= 3 ? 1 + (nst - 3 + 1) / 2 : 1);
+    const int jac = (!e.conv && e.jacobi_iters > 0) ? (e.jacobi_iters + 2) / 2 : 0;
     return replay + recompute + 3 + sweeps + 3 + 1 + jac + 1;
 }
 
