@@ -35,6 +35,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdlib.h>
 
 #include <utility>
 #include <vector>
@@ -314,6 +315,276 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth2(MgLevel L, const __nv
         if (act) *reinterpret_cast<__nv_bfloat162*>(eout + c) = __floats2bfloat162_rn(o0, o1);
         em = ec;
         ec = ep;
+    }
+}
+
+// ---- flat BF16 kernels: two cells per thread, packed FP32 arithmetic ----------
+// The cell pairs (i, i + 1), i even, of a level of even width are numbered
+// over a plane, p = (j nx + i) / 2, so that a pair is the 32-bit word
+// k (nx ny / 2) + p of a BF16 vector.  The flat kernels give 32 consecutive
+// pairs (or coarse cells) to a warp across row ends, so every lane has work
+// at every width; a thread marches kc planes.  The x neighbours of a pair
+// come from the neighbouring lanes (from memory at the ends of a warp), the
+// z neighbours stay in registers.  A wall neighbour is replaced by the cell
+// itself, which gives at every cell
+//   A e = ax (e_w + e_e) + ay (e_s + e_n) + az (e_d + e_u) - 2 (ax + ay + az) e_c,
+// evaluated for both cells of a pair at once by the f32x2 instructions of
+// sm_100 (add/sub/mul/fma .rn.f32x2: one instruction for the pair).
+namespace pk {
+
+__device__ __forceinline__ float2 padd(float2 a, float2 b) {
+    float2 r;
+    asm("{.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+    float2 r;
+    asm("{.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) {
+    float2 r;
+    asm("{.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+// a b + c, one rounding per element
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) {
+    float2 r;
+    asm("{.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return r;
+}
+__device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
+// A BF16 pair word to FP32 (first cell in the low half) and back (RN).
+__device__ __forceinline__ float2 unpack(unsigned v) {
+    return make_float2(__uint_as_float(v << 16), __uint_as_float(v & 0xffff0000u));
+}
+__device__ __forceinline__ unsigned pack(float2 v) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+    return *reinterpret_cast<const unsigned*>(&h);
+}
+
+struct Op {
+    float2 ax, ay, az, nd;  // ax, ay, az; nd = -2 (ax + ay + az)
+};
+__device__ __forceinline__ Op op_of(const MgLevel& L) {
+    const float ax = (float)L.ax, ay = (float)L.ay, az = (float)L.az;
+    return {splat(ax), splat(ay), splat(az), splat(-2.0f * (ax + ay + az))};
+}
+
+// b - A e of a pair with value c, x neighbours xw (of its first cell) and xe
+// (of its second), neighbour pairs s, n along y and d, u along z.
+__device__ __forceinline__ float2 residual(const Op& o, float2 c, float xw, float xe, float2 s, float2 n, float2 d,
+                                           float2 u, float2 b) {
+    float2 t = pmul(o.ax, padd(make_float2(xw, c.x), make_float2(c.y, xe)));
+    t = pfma(o.ay, padd(s, n), t);
+    t = pfma(o.az, padd(d, u), t);
+    return psub(b, pfma(o.nd, c, t));
+}
+
+// Where a lane's x neighbours come from: hw / he, the pair has a west / east
+// neighbour cell; ldw / lde, that neighbour is read from memory (lane 0 / 31).
+struct XNb {
+    bool hw, he, ldw, lde;
+};
+__device__ __forceinline__ XNb xnb_of(int ip, int npr) {
+    const int lane = threadIdx.x & 31;
+    XNb f;
+    f.hw = ip > 0;
+    f.he = ip < npr - 1;
+    f.ldw = f.hw && lane == 0;
+    f.lde = f.he && lane == 31;
+    return f;
+}
+// The x neighbours of pair value c whose first cell is the 16-bit element h0
+// of h (every lane of the warp calls this).
+__device__ __forceinline__ void xnb(float2 c, const unsigned short* __restrict__ h, int h0, const XNb& f, float& xw,
+                                   float& xe) {
+    xw = __shfl_up_sync(0xffffffffu, c.y, 1);
+    xe = __shfl_down_sync(0xffffffffu, c.x, 1);
+    if (f.ldw) xw = __uint_as_float((unsigned)__ldg(h + h0 - 1) << 16);
+    if (f.lde) xe = __uint_as_float((unsigned)__ldg(h + h0 + 2) << 16);
+    if (!f.hw) xw = c.x;
+    if (!f.he) xe = c.y;
+}
+
+}  // namespace pk
+
+// One Chebyshev smoothing step (as column_sweep with mb = 0) on the pairs of
+// an even-width BF16 level; grid (pgx, pgz), pkc planes per block.
+template <bool READ_PREV>
+__global__ void __launch_bounds__(MG_FLAT_THREADS) k_mg_smooth_pairs(MgLevel L, const unsigned* __restrict__ ein,
+                                                                     unsigned* __restrict__ eout,
+                                                                     const unsigned* __restrict__ b, float alpha,
+                                                                     float beta) {
+    using namespace pk;
+    const int npr = L.nx >> 1, npl = npr * L.ny;
+    const int q0 = blockIdx.x * MG_FLAT_THREADS + threadIdx.x;
+    const bool act = q0 < npl;
+    const int p = act ? q0 : npl - 1;  // lanes past the end shadow the last pair
+    const int j = p / npr, ip = p - j * npr;
+    const XNb f = xnb_of(ip, npr);
+    const bool hs = j > 0, hn = j < L.ny - 1;
+    const int k0 = blockIdx.y * L.pkc, k1 = min(L.nz, k0 + L.pkc);
+    const Op op = op_of(L);
+    // beta / diag(A) of the two cells on inner planes and on the end planes
+    const int nby = ((int)hs + (int)hn) * 3;
+    const int n0 = ((int)f.hw + 1) * 9 + nby, n1 = (1 + (int)f.he) * 9 + nby;
+    const int ze = L.nz > 1 ? 1 : 0;
+    const float2 bmid = make_float2(beta * (float)L.idg[n0 + 2], beta * (float)L.idg[n1 + 2]);
+    const float2 bend = make_float2(beta * (float)L.idg[n0 + ze], beta * (float)L.idg[n1 + ze]);
+    const float2 al = splat(alpha);
+    const unsigned short* h = reinterpret_cast<const unsigned short*>(ein);
+    int w = k0 * npl + p;
+    float2 ec = unpack(__ldg(ein + w));
+    float2 ed = k0 > 0 ? unpack(__ldg(ein + w - npl)) : ec;
+    for (int k = k0; k < k1; ++k, w += npl) {
+        const float2 eu = k + 1 < L.nz ? unpack(__ldg(ein + w + npl)) : ec;
+        const float2 es = hs ? unpack(__ldg(ein + w - npr)) : ec;
+        const float2 en = hn ? unpack(__ldg(ein + w + npr)) : ec;
+        float xw, xe;
+        xnb(ec, h, 2 * w, f, xw, xe);
+        const float2 r = residual(op, ec, xw, xe, es, en, ed, eu, unpack(__ldg(b + w)));
+        const float2 xp = READ_PREV ? unpack(eout[w]) : make_float2(0.0f, 0.0f);
+        const float2 o = pfma((k == 0 || k == L.nz - 1) ? bend : bmid, r, pfma(al, psub(ec, xp), ec));
+        if (act) eout[w] = pack(o);
+        ed = ec;
+        ec = eu;
+    }
+}
+
+// Coarse right-hand side of a 2 x 2 x 2 coarsening of an even-width BF16
+// level F: one thread per coarse column (I, J), flat over the coarse plane
+// (grid (cgx, cgz) of the coarse level, ckc planes per block).  Per coarse
+// plane K the thread sums the fine residuals of the pairs (2I, 2I + 1) in rows
+// 2J, 2J + 1 of planes 2K, 2K + 1 (rows 2J - 1 .. 2J + 2 read, the planes
+// below and above kept in registers); ec (optional) = the first smoothing
+// step from zero at the coarse level.
+__global__ void __launch_bounds__(MG_FLAT_THREADS) k_mg_restrict_pairs(MgLevel F, const unsigned* __restrict__ e,
+                                                                       const unsigned* __restrict__ b, MgLevel Cl,
+                                                                       __nv_bfloat16* __restrict__ bc,
+                                                                       __nv_bfloat16* __restrict__ ec) {
+    using namespace pk;
+    const int cn = Cl.nx * Cl.ny;
+    const int q0 = blockIdx.x * MG_FLAT_THREADS + threadIdx.x;
+    const bool act = q0 < cn;
+    const int q = act ? q0 : cn - 1;
+    const int J = q / Cl.nx, I = q - J * Cl.nx;
+    const XNb f = xnb_of(I, Cl.nx);  // the fine pairs of a row number I = 0 .. Cl.nx - 1
+    const bool hs = J > 0, hn = J < Cl.ny - 1;
+    const int K0 = blockIdx.y * Cl.ckc, K1 = min(Cl.nz, K0 + Cl.ckc);
+    const Op op = op_of(F);
+    const int npr = F.nx >> 1, npl = npr * F.ny;  // fine pairs per row, per plane
+    const unsigned short* h = reinterpret_cast<const unsigned short*>(e);
+    const int nbxy = nb_count(I, Cl.nx) * 9 + nb_count(J, Cl.ny) * 3;
+    const float cb0 = (float)Cl.cb[0];
+    int w = 2 * K0 * npl + 2 * J * npr + I;  // pair of fine row 2J, plane 2K
+    // rows 2J, 2J + 1 of fine plane 2K - 1 (plane 2K itself at the bottom wall)
+    const int wd = K0 > 0 ? w - npl : w;
+    float2 da = unpack(__ldg(e + wd)), db = unpack(__ldg(e + wd + npr));
+    for (int K = K0; K < K1; ++K, w += 2 * npl) {
+        const int w1 = w + npl;  // plane 2K + 1
+        const float2 a0 = unpack(__ldg(e + w)), b0 = unpack(__ldg(e + w + npr));
+        const float2 s0 = hs ? unpack(__ldg(e + w - npr)) : a0;
+        const float2 n0 = hn ? unpack(__ldg(e + w + 2 * npr)) : b0;
+        const float2 a1 = unpack(__ldg(e + w1)), b1 = unpack(__ldg(e + w1 + npr));
+        const float2 s1 = hs ? unpack(__ldg(e + w1 - npr)) : a1;
+        const float2 n1 = hn ? unpack(__ldg(e + w1 + 2 * npr)) : b1;
+        // rows 2J, 2J + 1 of plane 2K + 2 (plane 2K + 1 itself at the top wall)
+        const bool up = K + 1 < Cl.nz;
+        const float2 ua = up ? unpack(__ldg(e + w1 + npl)) : a1;
+        const float2 ub = up ? unpack(__ldg(e + w1 + npl + npr)) : b1;
+        float xw, xe;
+        xnb(a0, h, 2 * w, f, xw, xe);
+        float2 acc = residual(op, a0, xw, xe, s0, b0, da, a1, unpack(__ldg(b + w)));
+        xnb(b0, h, 2 * (w + npr), f, xw, xe);
+        acc = padd(acc, residual(op, b0, xw, xe, a0, n0, db, b1, unpack(__ldg(b + w + npr))));
+        xnb(a1, h, 2 * w1, f, xw, xe);
+        acc = padd(acc, residual(op, a1, xw, xe, s1, b1, a0, ua, unpack(__ldg(b + w1))));
+        xnb(b1, h, 2 * (w1 + npr), f, xw, xe);
+        acc = padd(acc, residual(op, b1, xw, xe, a1, n1, b0, ub, unpack(__ldg(b + w1 + npr))));
+        if (act) {
+            const int c = K * cn + q;
+            const __nv_bfloat16 v = __float2bfloat16_rn((acc.x + acc.y) * 0.125f);
+            bc[c] = v;
+            if (ec)
+                ec[c] = __float2bfloat16_rn(cb0 * (float)Cl.idg[nbxy + nb_count(K, Cl.nz)] * __bfloat162float(v));
+        }
+        da = a1;
+        db = b1;
+    }
+}
+
+// e += P ec for a 2 x 2 x 2 coarsening of an even-width BF16 level F: one
+// thread per coarse column (I, J) (grid (cgx, cgz) of the coarse level),
+// marching the coarse planes; per coarse plane K it adds the trilinear
+// interpolant (weights 3/4 and 1/4 along each axis, the coarse index clamped
+// at the ends: zero gradient) to the fine pairs (2I, 2I + 1) of rows 2J,
+// 2J + 1 in planes 2K, 2K + 1.
+__global__ void __launch_bounds__(MG_FLAT_THREADS) k_mg_prolong_pairs(MgLevel F, unsigned* __restrict__ e,
+                                                                      MgLevel Cl,
+                                                                      const __nv_bfloat16* __restrict__ ecrs) {
+    using namespace pk;
+    const int cn = Cl.nx * Cl.ny;
+    const int q0 = blockIdx.x * MG_FLAT_THREADS + threadIdx.x;
+    const bool act = q0 < cn;
+    const int q = act ? q0 : cn - 1;
+    const int J = q / Cl.nx, I = q - J * Cl.nx;
+    const XNb f = xnb_of(I, Cl.nx);
+    const int dS = J > 0 ? -Cl.nx : 0, dN = J < Cl.ny - 1 ? Cl.nx : 0;  // coarse rows J -/+ 1, clamped
+    const int K0 = blockIdx.y * Cl.ckc, K1 = min(Cl.nz, K0 + Cl.ckc);
+    const int npr = F.nx >> 1, npl = npr * F.ny;
+    const float2 w1 = splat(0.25f), w3 = splat(0.75f);
+    // x interpolation of the coarse row holding element c: values at fine 2I, 2I + 1
+    auto xrow = [&](int c) -> float2 {
+        const float v = __bfloat162float(__ldg(ecrs + c));
+        float vw = __shfl_up_sync(0xffffffffu, v, 1), ve = __shfl_down_sync(0xffffffffu, v, 1);
+        if (f.ldw) vw = __bfloat162float(__ldg(ecrs + c - 1));
+        if (f.lde) ve = __bfloat162float(__ldg(ecrs + c + 1));
+        if (!f.hw) vw = v;
+        if (!f.he) ve = v;
+        return pfma(w3, splat(v), pmul(w1, make_float2(vw, ve)));
+    };
+    // fine rows 2J (from J - 1, J) and 2J + 1 (from J, J + 1) of coarse plane K
+    auto yplane = [&](int K, float2& r0, float2& r1) {
+        const int c = K * cn + q;
+        const float2 xs = xrow(c + dS), xc = xrow(c), xn = xrow(c + dN);
+        r0 = pfma(w3, xc, pmul(w1, xs));
+        r1 = pfma(w3, xc, pmul(w1, xn));
+    };
+    float2 d0, d1, c0, c1;  // coarse planes K - 1 (clamped) and K
+    yplane(K0 > 0 ? K0 - 1 : 0, d0, d1);
+    yplane(K0, c0, c1);
+    int w = 2 * K0 * npl + 2 * J * npr + I;
+    for (int K = K0; K < K1; ++K, w += 2 * npl) {
+        float2 u0, u1;
+        yplane(K + 1 < Cl.nz ? K + 1 : K, u0, u1);
+        if (act) {
+            const int ws[4] = {w, w + npr, w + npl, w + npl + npr};
+            const float2 v[4] = {pfma(w3, c0, pmul(w1, d0)), pfma(w3, c1, pmul(w1, d1)), pfma(w3, c0, pmul(w1, u0)),
+                                 pfma(w3, c1, pmul(w1, u1))};
+#pragma unroll
+            for (int t = 0; t < 4; ++t) e[ws[t]] = pack(padd(unpack(e[ws[t]]), v[t]));
+        }
+        d0 = c0;
+        d1 = c1;
+        c0 = u0;
+        c1 = u1;
     }
 }
 
@@ -679,6 +950,17 @@ static int smallest_factor(int n) {
     return 1;
 }
 
+// Flat tiling: gx blocks of MG_FLAT_THREADS over `cols` columns of a plane,
+// gz blocks of kc planes, about two waves of blocks in all.
+static void flat_tiling(int cols, int nz, int& gx, int& gz, int& kc) {
+    gx = (cols + MG_FLAT_THREADS - 1) / MG_FLAT_THREADS;
+    const int want = 2 * 148 * 8;
+    int zc = (want + gx - 1) / gx;
+    zc = zc < 1 ? 1 : (zc > nz ? nz : zc);
+    kc = (nz + zc - 1) / zc;
+    gz = (nz + kc - 1) / kc;
+}
+
 static void tiling(MgLevel& m) {
     m.gx = (m.nx + MG_BX - 1) / MG_BX;
     m.gy = (m.ny + MG_BY - 1) / MG_BY;
@@ -687,6 +969,11 @@ static void tiling(MgLevel& m) {
     zc = zc < 1 ? 1 : (zc > m.nz ? m.nz : zc);
     m.kc = (m.nz + zc - 1) / zc;
     m.gz = (m.nz + m.kc - 1) / m.kc;
+    if ((m.nx & 1) == 0)
+        flat_tiling(m.nx / 2 * m.ny, m.nz, m.pgx, m.pgz, m.pkc);
+    else
+        m.pgx = m.pgz = m.pkc = 0;
+    flat_tiling(m.nx * m.ny, m.nz, m.cgx, m.cgz, m.ckc);
 }
 
 // Coefficients of the Chebyshev smoother of degree nu on [lo, hi] in the
@@ -797,6 +1084,8 @@ static bool dense_inverse(const MgLevel& L, std::vector<double>& inv) {
 cudaError_t mg_create(const Geom& g, int mode, MgSolver* m, cudaStream_t s, size_t* bytes) {
     *m = MgSolver{};
     m->mode = mode;
+    m->pairs = 1;
+    if (const char* v = getenv("VOF_MG_PAIRS")) m->pairs = atoi(v) != 0;
     m->nlev = mg_plan(g, m->lv, MG_MAX_LEVELS);
     cudaError_t e;
     const size_t vb = mode == MG_MIXED ? sizeof(__nv_bfloat16) : sizeof(double);
@@ -899,12 +1188,24 @@ static void* final_buffer(const MgSolver& m, int l) {
     return L.e1;
 }
 
-// One smoothing step of a multi-block level: the paired BF16 kernel on levels
-// of even width, the generic one otherwise.
+// One smoothing step of a multi-block level: on BF16 levels of even width
+// the flat paired kernel (or, with m.pairs = 0, the row-paired one), the
+// generic one otherwise.
 template <typename S>
-static void smooth(const MgLevel& L, const S* ein, S* eout, const S* b, double ca, double cb, bool read_prev,
-                   cudaStream_t s) {
+static void smooth(const MgSolver& m, const MgLevel& L, const S* ein, S* eout, const S* b, double ca, double cb,
+                   bool read_prev, cudaStream_t s) {
     if constexpr (sizeof(S) == 2) {
+        if ((L.nx & 1) == 0 && m.pairs) {
+            const dim3 gp(L.pgx, L.pgz);
+            const unsigned* wi = reinterpret_cast<const unsigned*>(ein);
+            unsigned* wo = reinterpret_cast<unsigned*>(eout);
+            const unsigned* wb = reinterpret_cast<const unsigned*>(b);
+            if (read_prev)
+                k_mg_smooth_pairs<true><<<gp, MG_FLAT_THREADS, 0, s>>>(L, wi, wo, wb, (float)ca, (float)cb);
+            else
+                k_mg_smooth_pairs<false><<<gp, MG_FLAT_THREADS, 0, s>>>(L, wi, wo, wb, (float)ca, (float)cb);
+            return;
+        }
         if ((L.nx & 1) == 0) {
             const dim3 g2((L.nx / 2 + MG_BX - 1) / MG_BX, L.gy, L.gz);
             k_mg_smooth2<<<g2, kBlock, 0, s>>>(L, ein, eout, b, ca, cb, read_prev ? 1 : 0);
@@ -917,6 +1218,12 @@ static void smooth(const MgLevel& L, const S* ein, S* eout, const S* b, double c
 // A level above the one-block tail that is smoothed by multi-block kernels.
 static bool multi(const MgSolver& m, int l) { return l < m.tail && l < m.nlev - 1; }
 
+// Restriction from / prolongation to level L by the flat paired kernels
+// (BF16 vectors, 2 x 2 x 2 coarsening).
+static bool pairs2(const MgSolver& m, const MgLevel& L) {
+    return m.pairs && m.mode == MG_MIXED && L.rx == 2 && L.ry == 2 && L.rz == 2;
+}
+
 template <typename S>
 static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t s, int& launches) {
     using C = typename St<S>::C;
@@ -928,10 +1235,14 @@ static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t 
         const S* b = static_cast<const S*>(L.b);
         int cur = 0;  // the first step (from zero) was written together with b
         for (int q = 1; q < L.nu; ++q, cur ^= 1, ++launches)
-            smooth<S>(L, e[cur], e[cur ^ 1], b, L.ca[q], L.cb[q], q >= 2, s);
+            smooth<S>(m, L, e[cur], e[cur ^ 1], b, L.ca[q], L.cb[q], q >= 2, s);
         const MgLevel& Cl = m.lv[l + 1];
         S* ec = multi(m, l + 1) ? static_cast<S*>(Cl.e0) : nullptr;
-        if (L.rx * L.ry * L.rz > 8)
+        if (sizeof(S) == 2 && pairs2(m, L))
+            k_mg_restrict_pairs<<<dim3(Cl.cgx, Cl.cgz), MG_FLAT_THREADS, 0, s>>>(
+                L, reinterpret_cast<const unsigned*>(e[cur]), reinterpret_cast<const unsigned*>(b), Cl,
+                reinterpret_cast<__nv_bfloat16*>(Cl.b), reinterpret_cast<__nv_bfloat16*>(ec));
+        else if (L.rx * L.ry * L.rz > 8)
             k_mg_restrict_wide<S><<<Cl.ncell, RW_THREADS, 0, s>>>(L, e[cur], b, Cl, static_cast<S*>(Cl.b), ec);
         else
             k_mg_restrict<S><<<grid_of(Cl), kBlock, 0, s>>>(L, e[cur], b, Cl, static_cast<S*>(Cl.b), ec);
@@ -961,14 +1272,20 @@ static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t 
         S* e[2] = {static_cast<S*>(L.e0), static_cast<S*>(L.e1)};
         const S* b = static_cast<const S*>(L.b);
         int cur = pre_cur[lc];
-        k_mg_prolong<S><<<grid_of(L), kBlock, 0, s>>>(L, e[cur], Cl, static_cast<const S*>(final_buffer(m, lc + 1)));
+        if (sizeof(S) == 2 && pairs2(m, L))
+            k_mg_prolong_pairs<<<dim3(Cl.cgx, Cl.cgz), MG_FLAT_THREADS, 0, s>>>(
+                L, reinterpret_cast<unsigned*>(e[cur]), Cl,
+                static_cast<const __nv_bfloat16*>(final_buffer(m, lc + 1)));
+        else
+            k_mg_prolong<S><<<grid_of(L), kBlock, 0, s>>>(L, e[cur], Cl,
+                                                          static_cast<const S*>(final_buffer(m, lc + 1)));
         ++launches;
         for (int q = 0; q < L.nu; ++q, cur ^= 1, ++launches) {
             if (lc == 0 && q == L.nu - 1)
                 k_smooth_update<S><<<grid_of(L), kBlock, 0, s>>>(g, L, e[cur], e[cur ^ 1], b, p64, L.ca[q], L.cb[q],
                                                                  q >= 1);
             else
-                smooth<S>(L, e[cur], e[cur ^ 1], b, L.ca[q], L.cb[q], q >= 1, s);
+                smooth<S>(m, L, e[cur], e[cur ^ 1], b, L.ca[q], L.cb[q], q >= 1, s);
         }
     }
     if (l == 0) {  // the fine level was solved by the tail or as the coarsest level

@@ -23,6 +23,7 @@ constexpr int MG_TAIL_CELLS = 4096;     // largest level that may run inside the
 constexpr int MG_TAIL_SMEM = 200 * 1024;  // shared-memory budget of the one-block kernel
 constexpr int MG_DENSE_MAX = 128;       // coarsest levels this small are solved exactly
 constexpr int MG_BX = 32, MG_BY = 8;    // block of the multi-block level kernels
+constexpr int MG_FLAT_THREADS = 256;    // block of the flat BF16 kernels (consecutive pairs or cells of a plane)
 
 // One multigrid level: compact layout (i fastest, no ghosts); A e = sum over
 // the non-wall neighbours of a (e_nb - e_c) with a = ax, ay, az; ratio
@@ -38,6 +39,12 @@ struct MgLevel {
     int rx, ry, rz;
     int nu;                  // pre/post smoothing degree
     int gx, gy, gz, kc;      // launch tiling: grid (gx, gy, gz) of MG_BX x MG_BY blocks, kc planes per block
+    // tilings of the flat kernels (1-D blocks of MG_FLAT_THREADS, grid (x, z),
+    // kc planes per block): over the cell pairs of a plane (even nx; the
+    // paired smoother) and over the cells of a plane (the coarse side of the
+    // paired restriction and prolongation)
+    int pgx, pgz, pkc;
+    int cgx, cgz, ckc;
     void* e0;                // correction, ping-pong pair
     void* e1;
     void* b;                 // right-hand side of this level
@@ -45,6 +52,10 @@ struct MgLevel {
 
 struct MgSolver {
     int mode;        // MG_MIXED or MG_FP64
+    // MIXED: the flat paired kernels (two cells per thread, packed FP32) on
+    // levels of even width and for 2x2x2 coarsening; 0: the row kernels
+    // (VOF_MG_PAIRS=0)
+    int pairs;
     int nlev;
     int tail;        // first level handled by the one-block kernel (nlev: none)
     int dense;       // the coarsest level is solved with the stored inverse
