@@ -64,6 +64,34 @@ struct St<double> {
 constexpr int MG_THREADS = MG_BX * MG_BY;
 constexpr int TAIL_THREADS = 1024;
 
+// Programmatic dependent launch.  Every kernel of the solve is launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization (pdl_launch) and begins
+// with pdl_enter(): it waits for the grid before it to complete (and its
+// writes to be visible) before its first global memory access, then lets the
+// next grid launch.  The launch and prologue of a kernel so overlap the end of
+// the one before, which removes most of the gap between the short kernels of
+// the coarse levels.  Launched without the attribute, the wait returns at once.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+static cudaError_t pdl_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 __host__ __device__ __forceinline__ int nb_count(int x, int n) { return (x > 0) + (x < n - 1); }
 
 // Sigma over the x/y non-wall neighbours of a (e_nb - ec) at compact index c.
@@ -219,6 +247,7 @@ __device__ __forceinline__ int block_linear() { return blockIdx.x + gridDim.x * 
 
 __global__ void __launch_bounds__(MG_THREADS) k_fold2(const double* __restrict__ partial, int nblk,
                                                       double* __restrict__ out, double* host_out) {
+    pdl_enter();
     double a = 0, b = 0;
     for (int q = threadIdx.x; q < nblk; q += blockDim.x) {
         a += partial[2 * q];
@@ -249,6 +278,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth(MgLevel L, const S* __
                                                           S* __restrict__ eout, const S* __restrict__ b,
                                                           const double* __restrict__ bsum, double alpha, double beta,
                                                           int read_prev) {
+    pdl_enter();
     using C = typename St<S>::C;
     LEVEL_TILE(L);
     if (!active) return;
@@ -266,6 +296,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_smooth2(MgLevel L, const __nv
                                                            __nv_bfloat16* __restrict__ eout,
                                                            const __nv_bfloat16* __restrict__ b, double alpha_d,
                                                            double beta_d, int read_prev) {
+    pdl_enter();
     const int pi = blockIdx.x * MG_BX + threadIdx.x;  // pair index along x
     const int i0 = 2 * pi;
     const int j = blockIdx.y * MG_BY + threadIdx.y;
@@ -432,6 +463,7 @@ __global__ void __launch_bounds__(MG_FLAT_THREADS) k_mg_smooth_pairs(MgLevel L, 
                                                                      unsigned* __restrict__ eout,
                                                                      const unsigned* __restrict__ b, float alpha,
                                                                      float beta) {
+    pdl_enter();
     using namespace pk;
     const int npr = L.nx >> 1, npl = npr * L.ny;
     const int q0 = blockIdx.x * MG_FLAT_THREADS + threadIdx.x;
@@ -479,6 +511,7 @@ __global__ void __launch_bounds__(MG_FLAT_THREADS) k_mg_restrict_pairs(MgLevel F
                                                                        const unsigned* __restrict__ b, MgLevel Cl,
                                                                        __nv_bfloat16* __restrict__ bc,
                                                                        __nv_bfloat16* __restrict__ ec) {
+    pdl_enter();
     using namespace pk;
     const int cn = Cl.nx * Cl.ny;
     const int q0 = blockIdx.x * MG_FLAT_THREADS + threadIdx.x;
@@ -539,6 +572,7 @@ __global__ void __launch_bounds__(MG_FLAT_THREADS) k_mg_restrict_pairs(MgLevel F
 __global__ void __launch_bounds__(MG_FLAT_THREADS) k_mg_prolong_pairs(MgLevel F, unsigned* __restrict__ e,
                                                                       MgLevel Cl,
                                                                       const __nv_bfloat16* __restrict__ ecrs) {
+    pdl_enter();
     using namespace pk;
     const int cn = Cl.nx * Cl.ny;
     const int q0 = blockIdx.x * MG_FLAT_THREADS + threadIdx.x;
@@ -594,6 +628,7 @@ template <typename S>
 __global__ void __launch_bounds__(MG_THREADS) k_mg_restrict(MgLevel F, const S* __restrict__ e,
                                                             const S* __restrict__ b, MgLevel Cl,
                                                             S* __restrict__ bc, S* __restrict__ ec) {
+    pdl_enter();
     using T = St<S>;
     using C = typename T::C;
     LEVEL_TILE(Cl);
@@ -620,6 +655,7 @@ template <typename S>
 __global__ void __launch_bounds__(RW_THREADS) k_mg_restrict_wide(MgLevel F, const S* __restrict__ e,
                                                                  const S* __restrict__ b, MgLevel Cl,
                                                                  S* __restrict__ bc, S* __restrict__ ec) {
+    pdl_enter();
     using T = St<S>;
     using C = typename T::C;
     __shared__ C part[RW_THREADS / 32];
@@ -648,6 +684,7 @@ __global__ void __launch_bounds__(RW_THREADS) k_mg_restrict_wide(MgLevel F, cons
 template <typename S>
 __global__ void __launch_bounds__(MG_THREADS) k_mg_prolong(MgLevel F, S* __restrict__ e, MgLevel Cl,
                                                            const S* __restrict__ ec) {
+    pdl_enter();
     LEVEL_TILE(F);
     if (!active) return;
     for (int k = k0; k < k1; ++k) prolong_cell<S>(F, e, Cl, ec, i, j, k);
@@ -656,6 +693,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_mg_prolong(MgLevel F, S* __restr
 template <typename S>
 __global__ void __launch_bounds__(MG_THREADS) k_level_sum(MgLevel L, const S* __restrict__ b,
                                                           double* __restrict__ partial) {
+    pdl_enter();
     LEVEL_TILE(L);
     double a = 0, z = 0;
     if (active)
@@ -671,6 +709,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_level_sum(MgLevel L, const S* __
 template <typename R>
 __global__ void __launch_bounds__(MG_THREADS) k_sum_rhs(Geom g, MgLevel L0, const R* __restrict__ rhs,
                                                         double* __restrict__ partial) {
+    pdl_enter();
     LEVEL_TILE(L0);
     double a = 0, z = 0;
     if (active)
@@ -689,6 +728,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_resid0(Geom g, MgLevel L0, const
                                                        const double* __restrict__ sums, const double* __restrict__ p,
                                                        S* __restrict__ b0, S* __restrict__ e0,
                                                        double* __restrict__ partial) {
+    pdl_enter();
     using T = St<S>;
     using C = typename T::C;
     LEVEL_TILE(L0);
@@ -734,6 +774,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_smooth_update(Geom g, MgLevel L0
                                                               const S* __restrict__ prev, const S* __restrict__ b,
                                                               double* __restrict__ p, double alpha, double beta,
                                                               int read_prev) {
+    pdl_enter();
     using T = St<S>;
     using C = typename T::C;
     LEVEL_TILE(L0);
@@ -758,6 +799,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_smooth_update(Geom g, MgLevel L0
 template <typename S>
 __global__ void __launch_bounds__(MG_THREADS) k_update64(Geom g, MgLevel L0, double* __restrict__ p,
                                                          const S* __restrict__ e) {
+    pdl_enter();
     LEVEL_TILE(L0);
     if (!active) return;
     for (int k = k0; k < k1; ++k) p[gidx(g, i + 1, j + 1, k + 1)] += (double)St<S>::ld(e, (k * L0.ny + j) * L0.nx + i);
@@ -765,6 +807,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_update64(Geom g, MgLevel L0, dou
 
 __global__ void __launch_bounds__(MG_THREADS) k_sum_p(Geom g, MgLevel L0, const double* __restrict__ p,
                                                       double* __restrict__ partial) {
+    pdl_enter();
     LEVEL_TILE(L0);
     double a = 0, z = 0;
     if (active)
@@ -779,6 +822,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_sum_p(Geom g, MgLevel L0, const 
 // p -= mean(p) (gauge), p32 = float(p) on the interior.
 __global__ void __launch_bounds__(MG_THREADS) k_gauge_cast(Geom g, MgLevel L0, double* __restrict__ p,
                                                            const double* __restrict__ sump, float* __restrict__ p32) {
+    pdl_enter();
     LEVEL_TILE(L0);
     if (!active) return;
     const double mean = sump[0] / (double)L0.ncell;
@@ -792,6 +836,7 @@ __global__ void __launch_bounds__(MG_THREADS) k_gauge_cast(Geom g, MgLevel L0, d
 
 __global__ void __launch_bounds__(MG_THREADS) k_widen(Geom g, MgLevel L0, const float* __restrict__ p32,
                                                       double* __restrict__ p) {
+    pdl_enter();
     LEVEL_TILE(L0);
     if (!active) return;
     for (int k = k0; k < k1; ++k) {
@@ -862,6 +907,7 @@ __host__ __device__ __forceinline__ int tail_vec_bytes(int ncell, int elem) { re
 template <typename S>
 __global__ void __launch_bounds__(TAIL_THREADS) k_mg_tail(const MgLevel* lv, int nl,
                                                           const typename St<S>::C* cinv_g, S* out) {
+    pdl_enter();
     using T = St<S>;
     using C = typename T::C;
     extern __shared__ __align__(16) unsigned char tail_smem[];
@@ -1201,18 +1247,18 @@ static void smooth(const MgSolver& m, const MgLevel& L, const S* ein, S* eout, c
             unsigned* wo = reinterpret_cast<unsigned*>(eout);
             const unsigned* wb = reinterpret_cast<const unsigned*>(b);
             if (read_prev)
-                k_mg_smooth_pairs<true><<<gp, MG_FLAT_THREADS, 0, s>>>(L, wi, wo, wb, (float)ca, (float)cb);
+                pdl_launch(k_mg_smooth_pairs<true>, gp, MG_FLAT_THREADS, 0, s, L, wi, wo, wb, (float)ca, (float)cb);
             else
-                k_mg_smooth_pairs<false><<<gp, MG_FLAT_THREADS, 0, s>>>(L, wi, wo, wb, (float)ca, (float)cb);
+                pdl_launch(k_mg_smooth_pairs<false>, gp, MG_FLAT_THREADS, 0, s, L, wi, wo, wb, (float)ca, (float)cb);
             return;
         }
         if ((L.nx & 1) == 0) {
             const dim3 g2((L.nx / 2 + MG_BX - 1) / MG_BX, L.gy, L.gz);
-            k_mg_smooth2<<<g2, kBlock, 0, s>>>(L, ein, eout, b, ca, cb, read_prev ? 1 : 0);
+            pdl_launch(k_mg_smooth2, g2, kBlock, 0, s, L, ein, eout, b, ca, cb, read_prev ? 1 : 0);
             return;
         }
     }
-    k_mg_smooth<S><<<grid_of(L), kBlock, 0, s>>>(L, ein, eout, b, nullptr, ca, cb, read_prev);
+    pdl_launch(k_mg_smooth<S>, grid_of(L), kBlock, 0, s, L, ein, eout, b, nullptr, ca, cb, read_prev);
 }
 
 // A level above the one-block tail that is smoothed by multi-block kernels.
@@ -1239,32 +1285,33 @@ static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t 
         const MgLevel& Cl = m.lv[l + 1];
         S* ec = multi(m, l + 1) ? static_cast<S*>(Cl.e0) : nullptr;
         if (sizeof(S) == 2 && pairs2(m, L))
-            k_mg_restrict_pairs<<<dim3(Cl.cgx, Cl.cgz), MG_FLAT_THREADS, 0, s>>>(
-                L, reinterpret_cast<const unsigned*>(e[cur]), reinterpret_cast<const unsigned*>(b), Cl,
-                reinterpret_cast<__nv_bfloat16*>(Cl.b), reinterpret_cast<__nv_bfloat16*>(ec));
+            pdl_launch(k_mg_restrict_pairs, dim3(Cl.cgx, Cl.cgz), MG_FLAT_THREADS, 0, s, L,
+                       reinterpret_cast<const unsigned*>(e[cur]), reinterpret_cast<const unsigned*>(b), Cl,
+                       reinterpret_cast<__nv_bfloat16*>(Cl.b), reinterpret_cast<__nv_bfloat16*>(ec));
         else if (L.rx * L.ry * L.rz > 8)
-            k_mg_restrict_wide<S><<<Cl.ncell, RW_THREADS, 0, s>>>(L, e[cur], b, Cl, static_cast<S*>(Cl.b), ec);
+            pdl_launch(k_mg_restrict_wide<S>, Cl.ncell, RW_THREADS, 0, s, L, e[cur], b, Cl, static_cast<S*>(Cl.b),
+                       ec);
         else
-            k_mg_restrict<S><<<grid_of(Cl), kBlock, 0, s>>>(L, e[cur], b, Cl, static_cast<S*>(Cl.b), ec);
+            pdl_launch(k_mg_restrict<S>, grid_of(Cl), kBlock, 0, s, L, e[cur], b, Cl, static_cast<S*>(Cl.b), ec);
         ++launches;
         pre_cur[l] = cur;
     }
     if (m.tail < m.nlev) {
-        k_mg_tail<S><<<1, TAIL_THREADS, m.tail_smem, s>>>(m.d_lv + m.tail, m.nlev - m.tail,
-                                                           static_cast<const C*>(m.d_cinv),
-                                                           static_cast<S*>(final_buffer(m, m.tail)));
+        pdl_launch(k_mg_tail<S>, 1, TAIL_THREADS, m.tail_smem, s, m.d_lv + m.tail, m.nlev - m.tail,
+                   static_cast<const C*>(m.d_cinv), static_cast<S*>(final_buffer(m, m.tail)));
         ++launches;
     } else {  // large coarsest level below no tail: mean-free sweeps from zero
         const MgLevel& L = m.lv[l];
         S* e[2] = {static_cast<S*>(L.e0), static_cast<S*>(L.e1)};
         const S* b = static_cast<const S*>(L.b);
-        k_level_sum<S><<<grid_of(L), kBlock, 0, s>>>(L, b, m.d_partial);
-        k_fold2<<<1, MG_THREADS, 0, s>>>(m.d_partial, L.gx * L.gy * L.gz, m.d_result + 6, nullptr);
-        k_mg_smooth<S><<<grid_of(L), kBlock, 0, s>>>(L, nullptr, e[0], b, m.d_result + 6, 0.0, MG_OMEGA, 0);
+        pdl_launch(k_level_sum<S>, grid_of(L), kBlock, 0, s, L, b, m.d_partial);
+        pdl_launch(k_fold2, 1, MG_THREADS, 0, s, m.d_partial, L.gx * L.gy * L.gz, m.d_result + 6, nullptr);
+        pdl_launch(k_mg_smooth<S>, grid_of(L), kBlock, 0, s, L, nullptr, e[0], b, m.d_result + 6, 0.0, MG_OMEGA,
+                   0);
         launches += 3;
         for (int q = 1; q < MG_COARSE_SWEEPS; ++q, ++launches)
-            k_mg_smooth<S><<<grid_of(L), kBlock, 0, s>>>(L, e[(q - 1) & 1], e[q & 1], b, m.d_result + 6, 0.0,
-                                                         MG_OMEGA, 0);
+            pdl_launch(k_mg_smooth<S>, grid_of(L), kBlock, 0, s, L, e[(q - 1) & 1], e[q & 1], b, m.d_result + 6,
+                       0.0, MG_OMEGA, 0);
     }
     for (int lc = l - 1; lc >= 0; --lc) {
         const MgLevel& L = m.lv[lc];
@@ -1273,30 +1320,31 @@ static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t 
         const S* b = static_cast<const S*>(L.b);
         int cur = pre_cur[lc];
         if (sizeof(S) == 2 && pairs2(m, L))
-            k_mg_prolong_pairs<<<dim3(Cl.cgx, Cl.cgz), MG_FLAT_THREADS, 0, s>>>(
-                L, reinterpret_cast<unsigned*>(e[cur]), Cl,
-                static_cast<const __nv_bfloat16*>(final_buffer(m, lc + 1)));
+            pdl_launch(k_mg_prolong_pairs, dim3(Cl.cgx, Cl.cgz), MG_FLAT_THREADS, 0, s, L,
+                       reinterpret_cast<unsigned*>(e[cur]), Cl,
+                       static_cast<const __nv_bfloat16*>(final_buffer(m, lc + 1)));
         else
-            k_mg_prolong<S><<<grid_of(L), kBlock, 0, s>>>(L, e[cur], Cl,
-                                                          static_cast<const S*>(final_buffer(m, lc + 1)));
+            pdl_launch(k_mg_prolong<S>, grid_of(L), kBlock, 0, s, L, e[cur], Cl,
+                       static_cast<const S*>(final_buffer(m, lc + 1)));
         ++launches;
         for (int q = 0; q < L.nu; ++q, cur ^= 1, ++launches) {
             if (lc == 0 && q == L.nu - 1)
-                k_smooth_update<S><<<grid_of(L), kBlock, 0, s>>>(g, L, e[cur], e[cur ^ 1], b, p64, L.ca[q], L.cb[q],
-                                                                 q >= 1);
+                pdl_launch(k_smooth_update<S>, grid_of(L), kBlock, 0, s, g, L, e[cur], e[cur ^ 1], b, p64, L.ca[q],
+                           L.cb[q], q >= 1);
             else
                 smooth<S>(m, L, e[cur], e[cur ^ 1], b, L.ca[q], L.cb[q], q >= 1, s);
         }
     }
     if (l == 0) {  // the fine level was solved by the tail or as the coarsest level
-        k_update64<S><<<grid_of(m.lv[0]), kBlock, 0, s>>>(g, m.lv[0], p64, static_cast<const S*>(final_buffer(m, 0)));
+        pdl_launch(k_update64<S>, grid_of(m.lv[0]), kBlock, 0, s, g, m.lv[0], p64,
+                   static_cast<const S*>(final_buffer(m, 0)));
         ++launches;
     }
     return cudaGetLastError();
 }
 
 cudaError_t mg_widen(const Geom& g, const MgSolver& m, const float* p32, double* p64, cudaStream_t s) {
-    k_widen<<<grid_of(m.lv[0]), kBlock, 0, s>>>(g, m.lv[0], p32, p64);
+    pdl_launch(k_widen, grid_of(m.lv[0]), kBlock, 0, s, g, m.lv[0], p32, p64);
     return cudaGetLastError();
 }
 
@@ -1308,9 +1356,9 @@ static cudaError_t outer_iteration(const Geom& g, MgSolver& m, const R* rhs, dou
     cudaError_t e = vcycle<S>(g, m, p64, s, launches);
     if (e != cudaSuccess) return e;
     const MgLevel& L0 = m.lv[0];
-    k_resid0<S, R><<<grid_of(L0), kBlock, 0, s>>>(g, L0, rhs, m.d_result + 2, p64, static_cast<S*>(L0.b),
-                                               multi(m, 0) ? static_cast<S*>(L0.e0) : nullptr, m.d_partial);
-    k_fold2<<<1, MG_THREADS, 0, s>>>(m.d_partial, m.nblk, m.d_result, m.h_result_dev);
+    pdl_launch(k_resid0<S, R>, grid_of(L0), kBlock, 0, s, g, L0, rhs, m.d_result + 2, p64, static_cast<S*>(L0.b),
+               multi(m, 0) ? static_cast<S*>(L0.e0) : nullptr, m.d_partial);
+    pdl_launch(k_fold2, 1, MG_THREADS, 0, s, m.d_partial, m.nblk, m.d_result, m.h_result_dev);
     launches += 2;
     return cudaGetLastError();
 }
@@ -1356,11 +1404,11 @@ static cudaError_t solve_impl(const Geom& g, MgSolver& m, const R* rhs, double* 
     if (!m.iter_graph || m.graph_key[0] != rhs || m.graph_key[1] != p64 || m.graph_key[2] != p32)
         if ((e = capture_iteration<S, R>(g, m, rhs, p64, p32, cap)) != cudaSuccess) return e;
     int launches = 0;
-    k_sum_rhs<R><<<grid, kBlock, 0, s>>>(g, L0, rhs, part);
-    k_fold2<<<1, MG_THREADS, 0, s>>>(part, m.nblk, res + 2, nullptr);
-    k_resid0<S, R><<<grid, kBlock, 0, s>>>(g, L0, rhs, res + 2, p64, static_cast<S*>(L0.b),
-                                        multi(m, 0) ? static_cast<S*>(L0.e0) : nullptr, part);
-    k_fold2<<<1, MG_THREADS, 0, s>>>(part, m.nblk, res, m.h_result_dev);
+    pdl_launch(k_sum_rhs<R>, grid, kBlock, 0, s, g, L0, rhs, part);
+    pdl_launch(k_fold2, 1, MG_THREADS, 0, s, part, m.nblk, res + 2, nullptr);
+    pdl_launch(k_resid0<S, R>, grid, kBlock, 0, s, g, L0, rhs, res + 2, p64, static_cast<S*>(L0.b),
+               multi(m, 0) ? static_cast<S*>(L0.e0) : nullptr, part);
+    pdl_launch(k_fold2, 1, MG_THREADS, 0, s, part, m.nblk, res, m.h_result_dev);
     launches += 4;
     int it = 0;
     double rel = 0, r0 = -1;
@@ -1373,9 +1421,9 @@ static cudaError_t solve_impl(const Geom& g, MgSolver& m, const R* rhs, double* 
         if ((e = cudaGraphLaunch(m.iter_graph, s)) != cudaSuccess) return e;
         launches += m.graph_launches;
     }
-    k_sum_p<<<grid, kBlock, 0, s>>>(g, L0, p64, part);
-    k_fold2<<<1, MG_THREADS, 0, s>>>(part, m.nblk, res + 4, nullptr);
-    k_gauge_cast<<<grid, kBlock, 0, s>>>(g, L0, p64, res + 4, p32);
+    pdl_launch(k_sum_p, grid, kBlock, 0, s, g, L0, p64, part);
+    pdl_launch(k_fold2, 1, MG_THREADS, 0, s, part, m.nblk, res + 4, nullptr);
+    pdl_launch(k_gauge_cast, grid, kBlock, 0, s, g, L0, p64, res + 4, p32);
     launches += 3;
     if (st) {
         st->outer = it;
