@@ -63,8 +63,6 @@ struct St<double> {
 
 constexpr int MG_THREADS = MG_BX * MG_BY;
 constexpr int TAIL_THREADS = 1024;
-constexpr int MG_CLUSTER_CTAS = 8;  // portable cluster size
-constexpr int MG_CLUSTER_CELLS = 2 * MG_CLUSTER_CTAS * TAIL_THREADS;  // two cells per thread at most
 
 // Programmatic dependent launch.  Every kernel of the solve is launched with
 // cudaLaunchAttributeProgrammaticStreamSerialization (pdl_launch) and begins
@@ -624,56 +622,6 @@ __global__ void __launch_bounds__(MG_FLAT_THREADS) k_mg_prolong_pairs(MgLevel F,
     }
 }
 
-// ---- small multi-block levels: the smoothing steps of one visit in one launch -----
-// Chebyshev steps q0 .. q1 - 1 of a level of at most MG_CLUSTER_CELLS cells
-// run in one launch of one thread-block cluster (MG_CLUSTER_CTAS blocks of
-// TAIL_THREADS threads) instead of one launch per step: every thread updates
-// its cells, then the cluster barrier (arrive with release, wait with acquire
-// semantics at cluster scope) orders the step before the next.  The vectors
-// stay in global memory (they are L2-resident at these sizes) and are read past
-// L1 (ld.global.cg), so no block reads a stale copy of another block's writes.
-// The arithmetic is column_sweep's, in the same order.
-__device__ __forceinline__ float ld_l2(const __nv_bfloat16* p, int i) {
-    return __uint_as_float((unsigned)__ldcg(reinterpret_cast<const unsigned short*>(p) + i) << 16);
-}
-__device__ __forceinline__ double ld_l2(const double* p, int i) { return __ldcg(p + i); }
-
-__device__ __forceinline__ void cluster_barrier() {
-    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
-}
-
-// The step q reads the previous iterate (the value eout holds) when q >= prev_from.
-template <typename S>
-__global__ void __launch_bounds__(TAIL_THREADS) k_mg_smooth_cluster(MgLevel L, S* e0, S* e1,
-                                                                    const S* __restrict__ b, int q0, int q1,
-                                                                    int cur, int prev_from) {
-    pdl_enter();
-    using T = St<S>;
-    using C = typename T::C;
-    const int plane = L.nx * L.ny;
-    const C ax = (C)L.ax, ay = (C)L.ay, az = (C)L.az;
-    for (int q = q0; q < q1; ++q, cur ^= 1) {
-        const S* ein = cur ? e1 : e0;
-        S* eout = cur ? e0 : e1;
-        const C alpha = (C)L.ca[q], beta = (C)L.cb[q];
-        for (int c = blockIdx.x * TAIL_THREADS + threadIdx.x; c < L.ncell; c += MG_CLUSTER_CTAS * TAIL_THREADS) {
-            const int i = c % L.nx, j = (c / L.nx) % L.ny, k = c / plane;
-            const C ec = ld_l2(ein, c);
-            C sxy = 0, sz = 0;
-            if (i > 0) sxy += ax * (ld_l2(ein, c - 1) - ec);
-            if (i < L.nx - 1) sxy += ax * (ld_l2(ein, c + 1) - ec);
-            if (j > 0) sxy += ay * (ld_l2(ein, c - L.nx) - ec);
-            if (j < L.ny - 1) sxy += ay * (ld_l2(ein, c + L.nx) - ec);
-            if (k > 0) sz += az * (ld_l2(ein, c - plane) - ec);
-            if (k < L.nz - 1) sz += az * (ld_l2(ein, c + plane) - ec);
-            const C xp = q >= prev_from ? ld_l2(eout, c) : (C)0;
-            const int nb = nb_count(i, L.nx) * 9 + nb_count(j, L.ny) * 3 + nb_count(k, L.nz);
-            T::st(eout, c, ec + alpha * (ec - xp) + beta * (C)L.idg[nb] * ((C)T::ld(b, c) - (C)0 - (sxy + sz)));
-        }
-        cluster_barrier();
-    }
-}
-
 // Coarse right-hand side = average of the fine residual over each coarse
 // cell; ec (optional) = the first smoothing step from zero at the coarse level.
 template <typename S>
@@ -793,7 +741,6 @@ __global__ void __launch_bounds__(MG_THREADS) k_resid0(Geom g, MgLevel L0, const
         int id = gidx(g, i + 1, j + 1, k0 + 1);
         int c = (k0 * L0.ny + j) * L0.nx + i;
         double pm = k0 > 0 ? p[id - g.plane] : 0.0, pc = p[id];
-#pragma unroll 4  // loads of several planes in flight per thread
         for (int k = k0; k < k1; ++k, id += g.plane, c += cplane) {
             const double pp = k + 1 < L0.nz ? p[id + g.plane] : 0.0;
             double s = 0;
@@ -837,7 +784,6 @@ __global__ void __launch_bounds__(MG_THREADS) k_smooth_update(Geom g, MgLevel L0
     int c = (k0 * L0.ny + j) * L0.nx + i;
     int id = gidx(g, i + 1, j + 1, k0 + 1);
     C em = k0 > 0 ? (C)T::ld(ein, c - plane) : (C)0, ec = (C)T::ld(ein, c);
-#pragma unroll 4  // loads of several planes in flight per thread
     for (int k = k0; k < k1; ++k, c += plane, id += g.plane) {
         const C ep = k + 1 < L0.nz ? (C)T::ld(ein, c + plane) : (C)0;
         const C Ae = lap_xy<S, C>(L0, ein, c, i, j, ec) + lap_z<C>(L0, k, ec, em, ep);
@@ -1186,8 +1132,6 @@ cudaError_t mg_create(const Geom& g, int mode, MgSolver* m, cudaStream_t s, size
     m->mode = mode;
     m->pairs = 1;
     if (const char* v = getenv("VOF_MG_PAIRS")) m->pairs = atoi(v) != 0;
-    m->cluster = 1;
-    if (const char* v = getenv("VOF_MG_CLUSTER")) m->cluster = atoi(v) != 0;
     m->nlev = mg_plan(g, m->lv, MG_MAX_LEVELS);
     cudaError_t e;
     const size_t vb = mode == MG_MIXED ? sizeof(__nv_bfloat16) : sizeof(double);
@@ -1320,30 +1264,6 @@ static void smooth(const MgSolver& m, const MgLevel& L, const S* ein, S* eout, c
 // A level above the one-block tail that is smoothed by multi-block kernels.
 static bool multi(const MgSolver& m, int l) { return l < m.tail && l < m.nlev - 1; }
 
-// A multi-block level small enough for the one-cluster smoothing kernel.
-static bool clustered(const MgSolver& m, const MgLevel& L) { return m.cluster && L.ncell <= MG_CLUSTER_CELLS; }
-
-// Chebyshev steps q0 .. q1 - 1 of level L from buffer e[cur] in one cluster
-// launch; returns the buffer holding the result.
-template <typename S>
-static int smooth_cluster(const MgLevel& L, S* const e[2], const S* b, int q0, int q1, int cur, int prev_from,
-                          cudaStream_t s) {
-    if (q1 <= q0) return cur;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(MG_CLUSTER_CTAS);
-    cfg.blockDim = dim3(TAIL_THREADS);
-    cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = MG_CLUSTER_CTAS;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_mg_smooth_cluster<S>, L, e[0], e[1], b, q0, q1, cur, prev_from);
-    return cur ^ ((q1 - q0) & 1);
-}
-
 // Restriction from / prolongation to level L by the flat paired kernels
 // (BF16 vectors, 2 x 2 x 2 coarsening).
 static bool pairs2(const MgSolver& m, const MgLevel& L) {
@@ -1360,13 +1280,8 @@ static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t 
         S* e[2] = {static_cast<S*>(L.e0), static_cast<S*>(L.e1)};
         const S* b = static_cast<const S*>(L.b);
         int cur = 0;  // the first step (from zero) was written together with b
-        if (clustered(m, L)) {
-            cur = smooth_cluster<S>(L, e, b, 1, L.nu, cur, 2, s);
-            launches += L.nu > 1;
-        } else {
-            for (int q = 1; q < L.nu; ++q, cur ^= 1, ++launches)
-                smooth<S>(m, L, e[cur], e[cur ^ 1], b, L.ca[q], L.cb[q], q >= 2, s);
-        }
+        for (int q = 1; q < L.nu; ++q, cur ^= 1, ++launches)
+            smooth<S>(m, L, e[cur], e[cur ^ 1], b, L.ca[q], L.cb[q], q >= 2, s);
         const MgLevel& Cl = m.lv[l + 1];
         S* ec = multi(m, l + 1) ? static_cast<S*>(Cl.e0) : nullptr;
         if (sizeof(S) == 2 && pairs2(m, L))
@@ -1412,14 +1327,7 @@ static cudaError_t vcycle(const Geom& g, MgSolver& m, double* p64, cudaStream_t 
             pdl_launch(k_mg_prolong<S>, grid_of(L), kBlock, 0, s, L, e[cur], Cl,
                        static_cast<const S*>(final_buffer(m, lc + 1)));
         ++launches;
-        int q = 0;
-        if (clustered(m, L)) {  // all steps but a last one fused with p += e
-            const int q1 = lc == 0 ? L.nu - 1 : L.nu;
-            cur = smooth_cluster<S>(L, e, b, 0, q1, cur, 1, s);
-            launches += q1 > 0;
-            q = q1;
-        }
-        for (; q < L.nu; ++q, cur ^= 1, ++launches) {
+        for (int q = 0; q < L.nu; ++q, cur ^= 1, ++launches) {
             if (lc == 0 && q == L.nu - 1)
                 pdl_launch(k_smooth_update<S>, grid_of(L), kBlock, 0, s, g, L, e[cur], e[cur ^ 1], b, p64, L.ca[q],
                            L.cb[q], q >= 1);

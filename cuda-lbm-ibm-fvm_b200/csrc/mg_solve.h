@@ -56,10 +56,6 @@ struct MgSolver {
     // levels of even width and for 2x2x2 coarsening; 0: the row kernels
     // (VOF_MG_PAIRS=0)
     int pairs;
-    // multi-block levels of at most 16384 cells: the smoothing steps of a
-    // visit in one thread-block cluster launch; 0: one launch per step
-    // (VOF_MG_CLUSTER=0)
-    int cluster;
     int nlev;
     int tail;        // first level handled by the one-block kernel (nlev: none)
     int dense;       // the coarsest level is solved with the stored inverse

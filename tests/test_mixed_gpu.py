@@ -146,26 +146,20 @@ def test_upload_of_pressure_seeds_the_solver(cuda, V):
     assert st2["rel_initial"] < 1e-5 and st2["outer"] < st1["outer"]
 
 
-@pytest.mark.parametrize("switch,mode", [("VOF_MG_PAIRS", "MODE_MIXED"), ("VOF_MG_CLUSTER", "MODE_MIXED"),
-                                         ("VOF_MG_CLUSTER", "MODE_FP64")])
 @pytest.mark.parametrize("shape", [(64, 64, 64), (60, 48, 40), (30, 20, 18)])
-def test_fast_level_kernels_agree_with_step_kernels(cuda, V, monkeypatch, switch, mode, shape):
+def test_flat_paired_kernels_agree_with_row_kernels(cuda, V, monkeypatch, shape):
     """MIXED levels of even width are smoothed, restricted and prolongated by
-    the flat paired kernels (packed FP32 on cell pairs; VOF_MG_PAIRS=0 selects
-    the row kernels), and multi-block levels of at most 16384 cells run the
-    smoothing steps of a visit in one thread-block cluster launch
-    (VOF_MG_CLUSTER=0: one launch per step; 30x24x20 and 30x20x18 here, the
-    latter with its last step fused with p += e).  Both ways solve the same
-    system to the same tolerance: the fields agree to the tolerance's level and
-    the cycle counts match within 1."""
-    prm = V.default_params(*shape, dt=2e-4, mode=getattr(V, mode), tol=1e-10, max_outer=100)
+    the flat paired kernels (packed FP32 on cell pairs); VOF_MG_PAIRS=0 selects
+    the row kernels.  Both solve the same system to the same tolerance: the
+    fields agree to the tolerance's level and the cycle counts match within 1."""
+    prm = V.default_params(*shape, dt=2e-4, mode=V.MODE_MIXED, tol=1e-10, max_outer=100)
     state = ic.random_state(prm, seed=11, vel_scale=0.5)
-    monkeypatch.setenv(switch, "0")
-    ref, st_ref = run_mode(V, prm, state, 1, 3)
-    monkeypatch.setenv(switch, "1")
-    got, st_got = run_mode(V, prm, state, 1, 3)
-    assert all(s["rel_final"] <= 1e-10 for s in st_ref + st_got)
-    for a, b in zip(st_ref, st_got):
-        assert abs(a["outer"] - b["outer"]) <= 1, (st_ref, st_got)
+    monkeypatch.setenv("VOF_MG_PAIRS", "0")
+    rows, st_rows = run_mode(V, prm, state, 1, 3)
+    monkeypatch.setenv("VOF_MG_PAIRS", "1")
+    flat, st_flat = run_mode(V, prm, state, 1, 3)
+    assert all(s["rel_final"] <= 1e-10 for s in st_rows + st_flat)
+    for a, b in zip(st_rows, st_flat):
+        assert abs(a["outer"] - b["outer"]) <= 1, (st_rows, st_flat)
     for k in STATE:
-        assert rel_l2(got[k], ref[k], interior=(k == "p")) <= 1e-6, (k, rel_l2(got[k], ref[k], interior=(k == "p")))
+        assert rel_l2(flat[k], rows[k], interior=(k == "p")) <= 1e-6, (k, rel_l2(flat[k], rows[k], interior=(k == "p")))
