@@ -22,6 +22,7 @@
 // never writes pressure ghosts, and they enter interior updates only through
 // zero coefficients.
 #include <cuda_runtime.h>
+#include <stdlib.h>
 
 #include "jacobi_tb.h"
 #include "tma.cuh"
@@ -285,7 +286,169 @@ cudaError_t jacobi_col_launch(const Geom& g, const float* pin, const float* rhs,
     const int target = (int)((long long)g.nz * bx * by / 600);
     const int len = target < 1 ? 1 : (target > 16 ? 16 : target);
     const int nch = (g.nz + len - 1) / len, kchunk = (g.nz + nch - 1) / nch;
-    k_jacobi_col<<<dim3(bx, by, (g.nz + kchunk - 1) / kchunk), dim3(JC_TX, JC_TY), 0, s>>>(g, pin, rhs, pout, kchunk);
+    k_jacobi_col<<<dim3(bx, by, (g.nz + kchunk - 1) / kchunk), dim3(JC_TX, JC_TY), 0, s>>>(g, pin, rhs, pout,
+                                                                                         kchunk);
+    return cudaGetLastError();
+}
+
+// ---- one sweep, two cells per thread, streaming along z ---------------------
+// Cells are paired by padded column (2m, 2m + 1): pair m of a row is one
+// aligned 8-byte word (px is a multiple of 32).  The pairs of rows 1..ny are
+// numbered flat, q = (j - 1) npair + m, and 32 consecutive pairs make a warp
+// across row ends, so every lane has work at every width.  A thread marches
+// kchunk planes with its pair's p(k - 1), p(k), p(k + 1) in registers; the y
+// neighbours are loads (served by L1), the x neighbours come from the
+// neighbouring lanes, or from memory at the ends of a warp and of a row; the
+// next plane's operands are loaded a plane ahead.  The update is the
+// reference's expression evaluated for both cells at once with the IEEE
+// f32x2 instructions of sm_100 (mul.rn / sub.rn / fma.rn .f32x2 round each
+// element exactly as the scalar instructions do), so the result is the scalar
+// kernels' bit for bit; the ghost cell of a pair (column 0 or nx + 1) is
+// never stored.
+constexpr int JP_THREADS = 256;
+
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) {
+    float2 r;
+    asm("{.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) {
+    float2 r;
+    asm("{.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) {
+    float2 r;
+    asm("{.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return r;
+}
+
+// div_rn_pre(x, d, 1/d) given its first product q0 = x (1/d) and corrected
+// quotient q1 = q0 + (x - q0 d) (1/d), computed for a pair: the same range
+// cases, so the same result.
+__device__ __forceinline__ float div_finish(float x, float d, float q0, float q1) {
+    const float ax = fabsf(x), aq = fabsf(q0);
+    if (ax >= 0x1p-96f && aq >= 0x1p-96f && aq <= 0x1p+96f) return q1;
+    if (x == 0.0f) return q0;
+    return __fdiv_rn(x, d);
+}
+
+__global__ void __launch_bounds__(JP_THREADS) k_jacobi_pairs(Geom g, const float* __restrict__ pin,
+                                                             const float* __restrict__ rhs,
+                                                             float* __restrict__ pout, int kchunk) {
+    const int npair = g.nx / 2 + 1;  // pairs covering columns 0 .. nx
+    const int nq = npair * g.ny;
+    const int qt = blockIdx.x * JP_THREADS + threadIdx.x;
+    const bool qa = qt < nq;
+    const int q = qa ? qt : nq - 1;  // lanes past the end shadow the last pair
+    const int jr = q / npair, m = q - jr * npair;
+    const int j = jr + 1, i0 = 2 * m, i1 = i0 + 1;
+    const bool a0 = qa && i0 >= 1, a1 = qa && i1 <= g.nx;
+    const int lane = threadIdx.x & 31;
+    const bool ldw = lane == 0 && m > 0;             // x- neighbour of cell i0 from memory
+    const bool lde = lane == 31 || m == npair - 1;   // x+ neighbour of cell i1 from memory
+    const int k0 = 1 + blockIdx.y * kchunk, k1 = min(g.nz, k0 + kchunk - 1);
+    const int plane = g.plane;
+    const int c = gidx(g, i0, j, 0);  // even
+    const int cw = c - 1, ce = c + min(2, g.px - 1 - i0);
+    const float cx = g.dxi * g.dxi, cy = g.dyi * g.dyi, cz = g.dzi * g.dzi;
+    const float ae0 = (i0 != g.nx) ? cx : 0.0f, aw0 = (i0 != 1) ? cx : 0.0f;
+    const float ae1 = (i1 != g.nx) ? cx : 0.0f, aw1 = (i1 != 1) ? cx : 0.0f;
+    const float an = (j != g.ny) ? cy : 0.0f, as = (j != 1) ? cy : 0.0f;
+    const float2 AE = make_float2(ae0, ae1), AW = make_float2(aw0, aw1);
+    const float2 AN = make_float2(an, an), AS = make_float2(as, as);
+    // diagonal by plane class (interior, first, last, first and last) in the
+    // reference's operand order, its IEEE reciprocal and its negation
+    const float2 d0 = make_float2(-(ae0 + aw0 + an + as + cz + cz), -(ae1 + aw1 + an + as + cz + cz));
+    const float2 d1 = make_float2(-(ae0 + aw0 + an + as + cz + 0.0f), -(ae1 + aw1 + an + as + cz + 0.0f));
+    const float2 d2 = make_float2(-(ae0 + aw0 + an + as + 0.0f + cz), -(ae1 + aw1 + an + as + 0.0f + cz));
+    const float2 d3 = make_float2(-(ae0 + aw0 + an + as + 0.0f + 0.0f), -(ae1 + aw1 + an + as + 0.0f + 0.0f));
+    const float2 r0 = make_float2(__frcp_rn(d0.x), __frcp_rn(d0.y)), r1 = make_float2(__frcp_rn(d1.x), __frcp_rn(d1.y));
+    const float2 r2 = make_float2(__frcp_rn(d2.x), __frcp_rn(d2.y)), r3 = make_float2(__frcp_rn(d3.x), __frcp_rn(d3.y));
+    const float2* P = reinterpret_cast<const float2*>(pin);
+    const float2* R = reinterpret_cast<const float2*>(rhs);
+    float2* O = reinterpret_cast<float2*>(pout);
+    const int w = c >> 1, wp = plane >> 1, wr = g.px >> 1;
+    const float2 zero = make_float2(0.0f, 0.0f);
+    float2 pm = P[w + (k0 - 1) * wp], pc = P[w + k0 * wp], pp = P[w + (k0 + 1) * wp];
+    float2 pS = P[w + k0 * wp - wr], pN = P[w + k0 * wp + wr], rc = R[w + k0 * wp];
+    float xw = ldw ? pin[cw + k0 * plane] : 0.0f, xe = lde ? pin[ce + k0 * plane] : 0.0f;
+    for (int k = k0; k <= k1; ++k) {
+        // operands of the next plane
+        const bool more = k < k1;
+        const float2 pq = (more && k + 2 <= g.nz + 1) ? P[w + (k + 2) * wp] : zero;
+        const float2 sn = more ? P[w + (k + 1) * wp - wr] : zero;
+        const float2 nn = more ? P[w + (k + 1) * wp + wr] : zero;
+        const float2 rn = more ? R[w + (k + 1) * wp] : zero;
+        const float xwn = (more && ldw) ? pin[cw + (k + 1) * plane] : 0.0f;
+        const float xen = (more && lde) ? pin[ce + (k + 1) * plane] : 0.0f;
+        float pw = __shfl_up_sync(0xffffffffu, pc.y, 1), pe = __shfl_down_sync(0xffffffffu, pc.x, 1);
+        if (ldw) pw = xw;
+        if (lde) pe = xe;
+        const bool kb = k == 1, kt = k == g.nz;
+        const float af = kt ? 0.0f : cz, ab = kb ? 0.0f : cz;
+        float2 x = f2sub(rc, f2mul(AE, make_float2(pc.y, pe)));
+        x = f2sub(x, f2mul(AW, make_float2(pw, pc.x)));
+        x = f2sub(x, f2mul(AN, pN));
+        x = f2sub(x, f2mul(AS, pS));
+        x = f2sub(x, f2mul(make_float2(af, af), pp));
+        x = f2sub(x, f2mul(make_float2(ab, ab), pm));
+        const float2 d = kb ? (kt ? d3 : d1) : (kt ? d2 : d0);
+        const float2 rd = kb ? (kt ? r3 : r1) : (kt ? r2 : r0);
+        const float2 q0 = f2mul(x, rd);
+        const float2 q1 = f2fma(f2fma(q0, make_float2(-d.x, -d.y), x), rd, q0);
+        const float v0 = div_finish(x.x, d.x, q0.x, q1.x), v1 = div_finish(x.y, d.y, q0.y, q1.y);
+        const int o = w + k * wp;
+        if (a0 && a1)
+            O[o] = make_float2(v0, v1);
+        else if (a0)
+            pout[2 * o] = v0;
+        else if (a1)
+            pout[2 * o + 1] = v1;
+        pm = pc;
+        pc = pp;
+        pp = pq;
+        pS = sn;
+        pN = nn;
+        rc = rn;
+        xw = xwn;
+        xe = xen;
+    }
+}
+
+// z chunk of the paired sweep: about `want` blocks in all, 1 .. 16 planes
+// (VOF_JACOBI_KCHUNK overrides).
+static int jacobi_pairs_kchunk(const Geom& g, int bx) {
+    static int forced = -1;
+    if (forced < 0) {
+        const char* v = getenv("VOF_JACOBI_KCHUNK");
+        forced = v ? atoi(v) : 0;
+    }
+    if (forced > 0) return forced < g.nz ? forced : g.nz;
+    const long long want = 3 * 148 * 8;
+    const int target = (int)(((long long)g.nz * bx) / want);
+    const int len = target < 1 ? 1 : (target > 16 ? 16 : target);
+    const int nch = (g.nz + len - 1) / len;
+    return (g.nz + nch - 1) / nch;
+}
+
+cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s) {
+    const int nq = (g.nx / 2 + 1) * g.ny;
+    const int bx = (nq + JP_THREADS - 1) / JP_THREADS;
+    const int kchunk = jacobi_pairs_kchunk(g, bx);
+    k_jacobi_pairs<<<dim3(bx, (g.nz + kchunk - 1) / kchunk), JP_THREADS, 0, s>>>(g, pin, rhs, pout, kchunk);
     return cudaGetLastError();
 }
 

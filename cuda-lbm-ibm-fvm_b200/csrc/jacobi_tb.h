@@ -24,6 +24,9 @@ cudaError_t jacobi_tb_launch(const Geom& g, int T, const CUtensorMap& map_in, co
 // buffer; its ghost cells are left as they are), streaming along z.
 cudaError_t jacobi_col_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);
 
+// The same sweep with two cells per thread (packed FP32, same bits).
+cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);
+
 // Dynamic shared memory of one block for T fused sweeps.
 size_t jacobi_tb_smem_bytes(int T);
 

@@ -23,6 +23,8 @@
 #include "jacobi_tb.h"
 
 #include <cuda_runtime.h>
+#include <stdlib.h>
+#include <string.h>
 
 namespace vof {
 
@@ -344,11 +346,22 @@ static_assert(JACOBI_T >= 1 && JACOBI_T <= JACOBI_TB_MAX, "VOF_JACOBI_T out of r
 // Launches for `iters` sweeps: ceil(iters / JACOBI_T), except that a single
 // blocked launch cannot end in the buffer it reads, so iters == JACOBI_T
 // (even) runs as single sweeps.
-// Grids of at most this many interior cells take one streaming sweep per
-// launch (k_jacobi_col), larger ones the blocked sweeps (k_jacobi_tb): the
-// measured crossover lies between 96^3 and 128^3.
-constexpr long long JACOBI_COL_MAX_CELLS = 1500000;
-static bool jacobi_streaming(const Geom& g) { return (long long)g.nx * g.ny * g.nz <= JACOBI_COL_MAX_CELLS; }
+// Jacobi kernels: one streaming sweep per launch with two cells per thread
+// (k_jacobi_pairs, the default), the same with one cell per thread
+// (k_jacobi_col), or JACOBI_T blocked sweeps per launch (k_jacobi_tb).
+// VOF_JACOBI=pairs|col|tb forces one.
+enum { JACOBI_PAIRS = 0, JACOBI_COL = 1, JACOBI_TB = 2 };
+static int jacobi_kind(const Geom&) {
+    static int forced = -2;
+    if (forced == -2) {
+        const char* v = getenv("VOF_JACOBI");
+        forced = !v ? -1
+                    : (!strcmp(v, "pairs") ? JACOBI_PAIRS
+                                           : (!strcmp(v, "col") ? JACOBI_COL : (!strcmp(v, "tb") ? JACOBI_TB : -1)));
+    }
+    return forced >= 0 ? forced : JACOBI_PAIRS;
+}
+static bool jacobi_streaming(const Geom& g) { return jacobi_kind(g) != JACOBI_TB; }
 
 static int jacobi_launches(const Geom& g, int iters) {
     if (jacobi_streaming(g)) return iters;
@@ -456,8 +469,11 @@ cudaError_t plain_pressure(const Geom& g, const PlainBuffers& b, int jacobi_iter
     int seq[64];
     if (jacobi_streaming(g)) {
         int cur = src;
+        const bool pairs = jacobi_kind(g) == JACOBI_PAIRS;
         for (int it = 0; it < jacobi_iters; ++it) {
-            if ((e = jacobi_col_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s)) != cudaSuccess) return e;
+            e = pairs ? jacobi_pairs_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s)
+                      : jacobi_col_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s);
+            if (e != cudaSuccess) return e;
             cur ^= 1;
         }
     } else if (L > 62 || !plan_buffers(src, dst, L, seq)) {
