@@ -299,51 +299,14 @@ cudaError_t jacobi_col_launch(const Geom& g, const float* pin, const float* rhs,
 // kchunk planes with its pair's p(k - 1), p(k), p(k + 1) in registers; the y
 // neighbours are loads (served by L1), the x neighbours come from the
 // neighbouring lanes, or from memory at the ends of a warp and of a row; the
-// next plane's operands are loaded a plane ahead.  The update is the
-// reference's expression evaluated for both cells at once with the IEEE
-// f32x2 instructions of sm_100 (mul.rn / sub.rn / fma.rn .f32x2 round each
-// element exactly as the scalar instructions do), so the result is the scalar
-// kernels' bit for bit; the ghost cell of a pair (column 0 or nx + 1) is
-// never stored.
+// next plane's operands are loaded a plane ahead; no shared memory, no
+// barrier.  Each cell's update is the scalar expression of k_jacobi_tb, in the
+// same operand order.  (The packed f32x2 instructions are not used here: in a
+// chain of them the code generator fuses a product into the following
+// subtraction, which changes the rounding; a probe on a B200 found a quarter
+// of such two-term chains off by an ulp even with .rn on every instruction.)
+// The ghost cell of a pair (column 0 or nx + 1) is never stored.
 constexpr int JP_THREADS = 256;
-
-__device__ __forceinline__ float2 f2mul(float2 a, float2 b) {
-    float2 r;
-    asm("{.reg .b64 ra, rb, rd;\n\t"
-        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-}
-__device__ __forceinline__ float2 f2sub(float2 a, float2 b) {
-    float2 r;
-    asm("{.reg .b64 ra, rb, rd;\n\t"
-        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-}
-__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) {
-    float2 r;
-    asm("{.reg .b64 ra, rb, rc, rd;\n\t"
-        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
-        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-    return r;
-}
-
-// div_rn_pre(x, d, 1/d) given its first product q0 = x (1/d) and corrected
-// quotient q1 = q0 + (x - q0 d) (1/d), computed for a pair: the same range
-// cases, so the same result.
-__device__ __forceinline__ float div_finish(float x, float d, float q0, float q1) {
-    const float ax = fabsf(x), aq = fabsf(q0);
-    if (ax >= 0x1p-96f && aq >= 0x1p-96f && aq <= 0x1p+96f) return q1;
-    if (x == 0.0f) return q0;
-    return __fdiv_rn(x, d);
-}
 
 __global__ void __launch_bounds__(JP_THREADS) k_jacobi_pairs(Geom g, const float* __restrict__ pin,
                                                              const float* __restrict__ rhs,
@@ -367,16 +330,16 @@ __global__ void __launch_bounds__(JP_THREADS) k_jacobi_pairs(Geom g, const float
     const float ae0 = (i0 != g.nx) ? cx : 0.0f, aw0 = (i0 != 1) ? cx : 0.0f;
     const float ae1 = (i1 != g.nx) ? cx : 0.0f, aw1 = (i1 != 1) ? cx : 0.0f;
     const float an = (j != g.ny) ? cy : 0.0f, as = (j != 1) ? cy : 0.0f;
-    const float2 AE = make_float2(ae0, ae1), AW = make_float2(aw0, aw1);
-    const float2 AN = make_float2(an, an), AS = make_float2(as, as);
     // diagonal by plane class (interior, first, last, first and last) in the
-    // reference's operand order, its IEEE reciprocal and its negation
+    // reference's operand order and its IEEE reciprocal
     const float2 d0 = make_float2(-(ae0 + aw0 + an + as + cz + cz), -(ae1 + aw1 + an + as + cz + cz));
     const float2 d1 = make_float2(-(ae0 + aw0 + an + as + cz + 0.0f), -(ae1 + aw1 + an + as + cz + 0.0f));
     const float2 d2 = make_float2(-(ae0 + aw0 + an + as + 0.0f + cz), -(ae1 + aw1 + an + as + 0.0f + cz));
     const float2 d3 = make_float2(-(ae0 + aw0 + an + as + 0.0f + 0.0f), -(ae1 + aw1 + an + as + 0.0f + 0.0f));
-    const float2 r0 = make_float2(__frcp_rn(d0.x), __frcp_rn(d0.y)), r1 = make_float2(__frcp_rn(d1.x), __frcp_rn(d1.y));
-    const float2 r2 = make_float2(__frcp_rn(d2.x), __frcp_rn(d2.y)), r3 = make_float2(__frcp_rn(d3.x), __frcp_rn(d3.y));
+    const float2 r0 = make_float2(__frcp_rn(d0.x), __frcp_rn(d0.y));
+    const float2 r1 = make_float2(__frcp_rn(d1.x), __frcp_rn(d1.y));
+    const float2 r2 = make_float2(__frcp_rn(d2.x), __frcp_rn(d2.y));
+    const float2 r3 = make_float2(__frcp_rn(d3.x), __frcp_rn(d3.y));
     const float2* P = reinterpret_cast<const float2*>(pin);
     const float2* R = reinterpret_cast<const float2*>(rhs);
     float2* O = reinterpret_cast<float2*>(pout);
@@ -399,17 +362,12 @@ __global__ void __launch_bounds__(JP_THREADS) k_jacobi_pairs(Geom g, const float
         if (lde) pe = xe;
         const bool kb = k == 1, kt = k == g.nz;
         const float af = kt ? 0.0f : cz, ab = kb ? 0.0f : cz;
-        float2 x = f2sub(rc, f2mul(AE, make_float2(pc.y, pe)));
-        x = f2sub(x, f2mul(AW, make_float2(pw, pc.x)));
-        x = f2sub(x, f2mul(AN, pN));
-        x = f2sub(x, f2mul(AS, pS));
-        x = f2sub(x, f2mul(make_float2(af, af), pp));
-        x = f2sub(x, f2mul(make_float2(ab, ab), pm));
         const float2 d = kb ? (kt ? d3 : d1) : (kt ? d2 : d0);
         const float2 rd = kb ? (kt ? r3 : r1) : (kt ? r2 : r0);
-        const float2 q0 = f2mul(x, rd);
-        const float2 q1 = f2fma(f2fma(q0, make_float2(-d.x, -d.y), x), rd, q0);
-        const float v0 = div_finish(x.x, d.x, q0.x, q1.x), v1 = div_finish(x.y, d.y, q0.y, q1.y);
+        const float v0 =
+            div_rn_pre(rc.x - ae0 * pc.y - aw0 * pw - an * pN.x - as * pS.x - af * pp.x - ab * pm.x, d.x, rd.x);
+        const float v1 =
+            div_rn_pre(rc.y - ae1 * pe - aw1 * pc.x - an * pN.y - as * pS.y - af * pp.y - ab * pm.y, d.y, rd.y);
         const int o = w + k * wp;
         if (a0 && a1)
             O[o] = make_float2(v0, v1);
