@@ -330,16 +330,10 @@ __global__ void __launch_bounds__(JP_THREADS) k_jacobi_pairs(Geom g, const float
     const float ae0 = (i0 != g.nx) ? cx : 0.0f, aw0 = (i0 != 1) ? cx : 0.0f;
     const float ae1 = (i1 != g.nx) ? cx : 0.0f, aw1 = (i1 != 1) ? cx : 0.0f;
     const float an = (j != g.ny) ? cy : 0.0f, as = (j != 1) ? cy : 0.0f;
-    // diagonal by plane class (interior, first, last, first and last) in the
-    // reference's operand order and its IEEE reciprocal
-    const float2 d0 = make_float2(-(ae0 + aw0 + an + as + cz + cz), -(ae1 + aw1 + an + as + cz + cz));
-    const float2 d1 = make_float2(-(ae0 + aw0 + an + as + cz + 0.0f), -(ae1 + aw1 + an + as + cz + 0.0f));
-    const float2 d2 = make_float2(-(ae0 + aw0 + an + as + 0.0f + cz), -(ae1 + aw1 + an + as + 0.0f + cz));
-    const float2 d3 = make_float2(-(ae0 + aw0 + an + as + 0.0f + 0.0f), -(ae1 + aw1 + an + as + 0.0f + 0.0f));
-    const float2 r0 = make_float2(__frcp_rn(d0.x), __frcp_rn(d0.y));
-    const float2 r1 = make_float2(__frcp_rn(d1.x), __frcp_rn(d1.y));
-    const float2 r2 = make_float2(__frcp_rn(d2.x), __frcp_rn(d2.y));
-    const float2 r3 = make_float2(__frcp_rn(d3.x), __frcp_rn(d3.y));
+    // diagonal of an inner plane in the reference's operand order and its IEEE
+    // reciprocal (the first and last planes compute theirs when they come)
+    const float2 dm = make_float2(-(ae0 + aw0 + an + as + cz + cz), -(ae1 + aw1 + an + as + cz + cz));
+    const float2 rm = make_float2(__frcp_rn(dm.x), __frcp_rn(dm.y));
     const float2* P = reinterpret_cast<const float2*>(pin);
     const float2* R = reinterpret_cast<const float2*>(rhs);
     float2* O = reinterpret_cast<float2*>(pout);
@@ -362,8 +356,11 @@ __global__ void __launch_bounds__(JP_THREADS) k_jacobi_pairs(Geom g, const float
         if (lde) pe = xe;
         const bool kb = k == 1, kt = k == g.nz;
         const float af = kt ? 0.0f : cz, ab = kb ? 0.0f : cz;
-        const float2 d = kb ? (kt ? d3 : d1) : (kt ? d2 : d0);
-        const float2 rd = kb ? (kt ? r3 : r1) : (kt ? r2 : r0);
+        float2 d = dm, rd = rm;
+        if (kb || kt) {
+            d = make_float2(-(ae0 + aw0 + an + as + af + ab), -(ae1 + aw1 + an + as + af + ab));
+            rd = make_float2(__frcp_rn(d.x), __frcp_rn(d.y));
+        }
         const float v0 =
             div_rn_pre(rc.x - ae0 * pc.y - aw0 * pw - an * pN.x - as * pS.x - af * pp.x - ab * pm.x, d.x, rd.x);
         const float v1 =
