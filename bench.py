@@ -62,9 +62,12 @@ ALG_BYTES = {
     "sweep3": 12,
 }
 KERNEL_NAMES = {
-    "predict": "k_predict", "rhs": "k_rhs", "jacobi": "k_jacobi_tb", "correct": "k_correct",
+    "predict": "k_predict", "rhs": "k_rhs", "jacobi": "k_jacobi_pairs", "correct": "k_correct",
     "sweep1": "k_fct", "sweep2": "k_fct", "sweep3": "k_fct",
 }
+# the Jacobi kernel the library runs (VOF_JACOBI=pairs|col|tb; pairs by default)
+KERNEL_NAMES["jacobi"] = {"col": "k_jacobi_col", "tb": "k_jacobi_tb"}.get(os.environ.get("VOF_JACOBI", ""),
+                                                                       "k_jacobi_pairs")
 STEP_MODEL_BYTES = 188  # B per cell-step of the fused plain path (10 sweeps, FP32)
 
 
