@@ -1,6 +1,8 @@
-// jacobi_tb.cu -- T Jacobi sweeps of the pressure system per launch
-// (solve_p_jacobi_kernel, voftrial1.cu:401-439, applied T times with the
-// ping-pong of voftrial1.cu:1371-1375), temporally blocked in shared memory.
+// jacobi_tb.cu -- Jacobi sweeps of the pressure system (solve_p_jacobi_kernel,
+// voftrial1.cu:401-439, with the ping-pong of voftrial1.cu:1371-1375): one
+// sweep per launch with two cells per thread (k_jacobi_pairs, the default),
+// one sweep per launch with one cell per thread (k_jacobi_col), or T sweeps
+// per launch temporally blocked in shared memory (k_jacobi_tb<T>, below).
 //
 // Compiled with -fmad=false: each cell update keeps the reference's
 //     pt = (rhs - ae*pE - aw*pW - an*pN - as*pS - af*pF - ab*pB) / ap
@@ -213,12 +215,10 @@ __global__ void __launch_bounds__(JB_THREADS) k_jacobi_tb(Geom g, const __grid_c
 // two planes up, its halo cells and rhs one plane up) are issued a plane
 // ahead.  Same per-cell expression and operand order as k_jacobi_tb.
 //
-// Used on small grids, where it is faster than the blocked kernel (measured
-// on a B200: 64^3 0.088 vs 0.103 ms per plain step, 32^3 0.055 vs 0.069): a
-// blocked launch there has few tiles, each bound by the latency of its plane
-// pipeline.  From about 128^3 up the blocked kernel is faster (200^3: 34.6 vs
-// 41 us per sweep); keeping more planes of loads in flight here made the
-// large grids slower still.
+// Selected with VOF_JACOBI=col.  Measured on a B200: faster than the blocked
+// kernel on small grids (64^3 0.088 vs 0.103 ms per plain step), slower from
+// about 128^3 up (200^3: 41 vs 34.6 us per sweep); the paired kernel below
+// (no shared memory, no barrier) beats both at every size.
 constexpr int JC_TX = 32, JC_TY = 8;
 __global__ void __launch_bounds__(JC_TX * JC_TY) k_jacobi_col(Geom g, const float* __restrict__ pin,
                                                              const float* __restrict__ rhs,

@@ -12,8 +12,9 @@
 // Kernel map (reference kernels each one replaces):
 //   k_predict      advect_{u,v,w}_kernel + cal_nu_rho_kernel   voftrial1.cu:95-104, 230-399
 //   k_rhs          the rhs expression of solve_p_jacobi_kernel voftrial1.cu:418-422
-//   k_jacobi_tb<T> (jacobi_tb.cu) T solve_p_jacobi_kernel sweeps per launch  voftrial1.cu:401-439
-//                  (small grids: k_jacobi_col, one sweep per launch)
+//   k_jacobi_pairs (jacobi_tb.cu) one solve_p_jacobi_kernel sweep per launch,  voftrial1.cu:401-439
+//                  two cells per thread (VOF_JACOBI=tb: k_jacobi_tb<T>, T sweeps
+//                  per launch; VOF_JACOBI=col: k_jacobi_col)
 //   k_correct      update_{u,v,w}_kernel + apply_bc_velocity   voftrial1.cu:441-493, 959-1051, 1107-1120
 //   k_fct<AXIS,FINAL>  (fct_sweep.cu) fct_{x,y,z}_sweep_stage1..4, and on
 //                  the last sweep post_process_f_kernel + apply_bc_F   voftrial1.cu:502-905, 1053-1135
