@@ -1032,6 +1032,23 @@ __global__ void k_adj_bcv_y(Geom g, double* __restrict__ lu, double* __restrict_
     mv(lw, jt, jn);
 }
 
+// Wall flags of a cell (i==1, i==nx, j==1, j==ny, k==1, k==nz; bits 0..5) and
+// -N mu of the transposed Jacobi sweep (below) at cell c.
+__device__ __forceinline__ int wall_flags(const Geom& g, int i, int j, int k) {
+    return (i == 1) | ((i == g.nx) << 1) | ((j == 1) << 2) | ((j == g.ny) << 3) | ((k == 1) << 4) |
+           ((k == g.nz) << 5);
+}
+__device__ __forceinline__ double neg_N(const Geom& g, const double* mu, int c, int i, int j, int k) {
+    const double cxx = (double)(g.dxi * g.dxi), cyy = (double)(g.dyi * g.dyi), czz = (double)(g.dzi * g.dzi);
+    double s = 0.0;
+    if (i != g.nx) s += cxx * mu[c + 1];
+    if (i != 1) s += cxx * mu[c - 1];
+    if (j != g.ny) s += cyy * mu[c + g.px];
+    if (j != 1) s += cyy * mu[c - g.px];
+    if (k != g.nz) s += czz * mu[c + g.plane];
+    if (k != 1) s += czz * mu[c - g.plane];
+    return -s;
+}
 // ---- velocity correction, reversed (gather over the six faces of a cell) -----------
 // Face q along axis a (its cells q - st and q): u_q = u*_q - dt/r (p_q - p_{q-st}) h^-1,
 // r = (rho_q + rho_{q-st}) / 2.  Cell c collects, from its lower faces (q = c)
@@ -1041,10 +1058,20 @@ __global__ void k_adj_bcv_y(Geom g, double* __restrict__ lu, double* __restrict_
 // start velocity into a cleared second set of fields (the correction wrote
 // every face, so nothing else of lu, lv, lw carries over), and the two sets
 // swap.
+//
+// FUSE (plain step with Jacobi sweeps): the cell's pressure adjoint is -N mu_prev
+// (the last transposed Jacobi stage of the later step, deferred to here while
+// `pending`; N and the stages are those of k_adj_jacobi) or lp[c], plus the
+// correction's contribution; the first transposed stage follows at once:
+// mu0 = that / ap into mu_out, lrhs = mu0 -- the same operations, in the same
+// order, as the separate stage kernels.  Otherwise lp[c] += the contribution.
+template <bool FUSE>
 __global__ void __launch_bounds__(256) k_adj_update(Geom g, Range R, const float* __restrict__ F,
                                                     const float* __restrict__ p, const double* __restrict__ lu,
                                                     const double* __restrict__ lv, const double* __restrict__ lw,
-                                                    double* __restrict__ lp, double* __restrict__ lrho) {
+                                                    double* __restrict__ lp, double* __restrict__ lrho,
+                                                    int pending, InvAp ia, double* __restrict__ mu_out,
+                                                    double* __restrict__ lrhs) {
     RANGE_CELL(R);
     const int c = gidx(g, i, j, k);
     const int pos[3] = {i, j, k}, len[3] = {g.nx, g.ny, g.nz}, st[3] = {1, g.px, g.plane};
@@ -1074,7 +1101,14 @@ __global__ void __launch_bounds__(256) k_adj_update(Geom g, Range R, const float
             }
         }
     }
-    lp[c] += lpc;
+    if (FUSE) {
+        const double lpf = (pending ? neg_N(g, lp, c, i, j, k) : lp[c]) + lpc;
+        const double mu = lpf * ia.v[wall_flags(g, i, j, k)];
+        mu_out[c] = mu;
+        lrhs[c] = mu;
+    } else {
+        lp[c] += lpc;
+    }
     lrho[c] = lrc;
 }
 
@@ -1083,21 +1117,6 @@ __global__ void __launch_bounds__(256) k_adj_update(Geom g, Range R, const float
 // lrhs += mu_k, lambda_{k-1} = -N mu_k; carried as mu: mu_{k-1} = -N mu_k / ap.
 // inv_ap[flags] = 1 / ap (FP32 ap of the forward, in its order) for the six
 // wall flags (i==1, i==nx, j==1, j==ny, k==1, k==nz) of a cell.
-__device__ __forceinline__ int wall_flags(const Geom& g, int i, int j, int k) {
-    return (i == 1) | ((i == g.nx) << 1) | ((j == 1) << 2) | ((j == g.ny) << 3) | ((k == 1) << 4) |
-           ((k == g.nz) << 5);
-}
-__device__ __forceinline__ double neg_N(const Geom& g, const double* mu, int c, int i, int j, int k) {
-    const double cxx = (double)(g.dxi * g.dxi), cyy = (double)(g.dyi * g.dyi), czz = (double)(g.dzi * g.dzi);
-    double s = 0.0;
-    if (i != g.nx) s += cxx * mu[c + 1];
-    if (i != 1) s += cxx * mu[c - 1];
-    if (j != g.ny) s += cyy * mu[c + g.px];
-    if (j != 1) s += cyy * mu[c - g.px];
-    if (k != g.nz) s += czz * mu[c + g.plane];
-    if (k != 1) s += czz * mu[c - g.plane];
-    return -s;
-}
 // mode 0: mu = lin / ap, lrhs = mu;  1: mu = -N lin / ap, lrhs += mu;  2: out = -N lin.
 __global__ void __launch_bounds__(256) k_adj_jacobi(Geom g, Range R, InvAp ia, const double* __restrict__ lin,
                                                     double* __restrict__ lout, double* __restrict__ lrhs, int mode) {
@@ -1328,8 +1347,8 @@ __global__ void __launch_bounds__(256) k_adj_advect(Geom g, Range R, const float
                                                     const float* __restrict__ w, const float* __restrict__ us,
                                                     const float* __restrict__ vs, const float* __restrict__ ws,
                                                     const double* __restrict__ lrhs, int has_rhs,
-                                                    const double* __restrict__ lus, const double* __restrict__ lvs,
-                                                    const double* __restrict__ lws, double* __restrict__ lu,
+                                                    double* __restrict__ lus, double* __restrict__ lvs,
+                                                    double* __restrict__ lws, double* __restrict__ lu,
                                                     double* __restrict__ lv, double* __restrict__ lw,
                                                     const double* __restrict__ lrho, double* __restrict__ lF,
                                                     double* __restrict__ partial) {
@@ -1341,6 +1360,11 @@ __global__ void __launch_bounds__(256) k_adj_advect(Geom g, Range R, const float
         const int c = gidx(g, i, j, k);
         const float Fc = F[c];
         double Gu = lus[c], Gv = lvs[c], Gw = lws[c], lr = lrho[c];
+        // this thread is the only reader of these entries: clear them, so that
+        // the set is zero when it next serves as the accumulator
+        lus[c] = 0.0;
+        lvs[c] = 0.0;
+        lws[c] = 0.0;
         if (has_rhs) {
             const int sy = g.px, sz = g.plane;
             const double idt = rcp64((double)g.dt), dxi = (double)g.dxi, dyi = (double)g.dyi, dzi = (double)g.dzi;
@@ -1665,11 +1689,21 @@ cudaError_t reverse_step(AdjEngine& e, const StepData& d, int istep, cudaStream_
     }
     const Range I = interior(g);
     const dim3 gi = grid_of(I);
-    k_adj_update<<<gi, kBlk, 0, s>>>(g, I, d.F, d.p, e.lu, e.lv, e.lw, e.lp[e.lp_cur], e.lrho);
-    // lu, lv, lw now hold the adjoints of u*, v*, w*; the start velocity's
-    // adjoint accumulates in the cleared second set
-    for (double* l : {e.lus, e.lvs, e.lws})
-        if ((r = cudaMemsetAsync(l, 0, e.elems * sizeof(double), s)) != cudaSuccess) return r;
+    // plain step with sweeps: the update also applies the later step's
+    // deferred last transposed stage and this step's first one (mu0 into the
+    // other lp buffer, lrhs = mu0)
+    const bool fuse = !e.conv && e.jacobi_iters > 0;
+    if (fuse) {
+        k_adj_update<true><<<gi, kBlk, 0, s>>>(g, I, d.F, d.p, e.lu, e.lv, e.lw, e.lp[e.lp_cur], e.lrho,
+                                               e.lp_pending ? 1 : 0, e.inv_ap, e.lp[e.lp_cur ^ 1], e.lrhs);
+        e.lp_cur ^= 1;
+    } else {
+        k_adj_update<false><<<gi, kBlk, 0, s>>>(g, I, d.F, d.p, e.lu, e.lv, e.lw, e.lp[e.lp_cur], e.lrho, 0,
+                                                e.inv_ap, nullptr, nullptr);
+    }
+    // lu, lv, lw then hold the adjoints of u*, v*, w*; the start velocity's
+    // adjoint accumulates in the second set, which is zero (cleared at the
+    // start of the reverse pass, then by the advection kernel that last read it)
     // the pressure solve reversed: convergent modes -- lrhs = the mean-free
     // solution of A mu = lp - mean(lp) (warm start: the previous step's), and
     // the state pressure (only a warm start) gets no adjoint; plain -- the
@@ -1679,29 +1713,26 @@ cudaError_t reverse_step(AdjEngine& e, const StepData& d, int istep, cudaStream_
         if (r != cudaSuccess) return r;
         if ((r = cudaMemsetAsync(e.lp[e.lp_cur], 0, e.elems * sizeof(double), s)) != cudaSuccess) return r;
     } else if (e.jacobi_iters > 0) {
-        // stages 0, 1 x (iters - 1), 2, two per launch
-        const int nst = e.jacobi_iters + 1;
+        // stages 1 .. iters - 1 (mode 1), two per launch; stage 0 ran in the
+        // update, the last one (mode 2) is deferred to the update of the
+        // earlier step, or to the end of the reverse pass
+        const int n1 = e.jacobi_iters - 1;
         // chunks of up to 24 planes, shorter on small grids (about 600 blocks)
         const long long cols = (long long)((g.nx + AJ_TX - 1) / AJ_TX) * ((g.ny + AJ_TY - 1) / AJ_TY);
         const int target = (int)(g.nz * cols / 600), len = target < 1 ? 1 : (target > 24 ? 24 : target);
         const int nch = (g.nz + len - 1) / len, kchunk = (g.nz + nch - 1) / nch;
         const dim3 gj((g.nx + AJ_TX - 1) / AJ_TX, (g.ny + AJ_TY - 1) / AJ_TY, (g.nz + kchunk - 1) / kchunk);
         const dim3 bj(AJ_TX, AJ_TY);
-        auto mode_of = [&](int q) { return q == 0 ? 0 : (q == nst - 1 ? 2 : 1); };
-        for (int q = 0; q < nst; q += 2) {
+        for (int q = 0; q < n1; q += 2) {
             const double* in = e.lp[e.lp_cur];
             double* out = e.lp[e.lp_cur ^ 1];
-            if (q + 1 < nst) {
-                const int a = mode_of(q), b = mode_of(q + 1);
-                if (a == 0 && b == 1) k_adj_jacobi2<0, 1><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
-                else if (a == 0) k_adj_jacobi2<0, 2><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
-                else if (b == 1) k_adj_jacobi2<1, 1><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
-                else k_adj_jacobi2<1, 2><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
-            } else {
-                k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.inv_ap, in, out, e.lrhs, mode_of(q));
-            }
+            if (q + 1 < n1)
+                k_adj_jacobi2<1, 1><<<gj, bj, 0, s>>>(g, e.inv_ap, in, out, e.lrhs, kchunk);
+            else
+                k_adj_jacobi<<<gi, kBlk, 0, s>>>(g, I, e.inv_ap, in, out, e.lrhs, 1);
             e.lp_cur ^= 1;
         }
+        e.lp_pending = true;
     }
     // rhs, advection, rho and nu
     k_adj_advect<<<gi, kBlk, 0, s>>>(g, I, d.F, d.u, d.v, d.w, d.us, d.vs, d.ws, e.lrhs, e.conv || e.jacobi_iters > 0,
@@ -1719,8 +1750,9 @@ int adj_kernels_per_step(const AdjEngine& e) {
     // correction 1, three sweeps), the recomputation when the intermediates
     // are not kept (front 2, pressure, correction 1, two sweeps), and the
     // adjoint kernels: F copies 3, the three sweep adjoints (1 launch each when
-    // fused, else 8), velocity copies 3, correction 1, the transposed Jacobi
-    // sweeps (iters + 1 stages, two per launch), rhs with advection 1.  The convergent modes' pressure solves
+    // fused, else 8), velocity copies 3, correction 1 (with the first and the
+    // deferred last transposed Jacobi stage), the other iters - 1 stages two
+    // per launch, rhs with advection 1.  The convergent modes' pressure solves
     // (multigrid graphs) are not counted.
     const Geom& g = e.g;
     const int P = e.conv ? 0 : plain_phase_launches(e.g, PHASE_JACOBI, e.jacobi_iters);
@@ -1734,7 +1766,7 @@ int adj_kernels_per_step(const AdjEngine& e) {
                       : 8;
     const int replay = 2 + P + 1 + 3;
     const int recompute = e.keep ? 0 : 2 + P + 1 + 2;
-    const int jac = (!e.conv && e.jacobi_iters > 0) ? (e.jacobi_iters + 2) / 2 : 0;
+    const int jac = (!e.conv && e.jacobi_iters > 0) ? e.jacobi_iters / 2 : 0;
     return replay + recompute + 3 + sweeps + 3 + 1 + jac + 1;
 }
 
@@ -1970,11 +2002,12 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
     const Geom& g = e->g;
     cudaError_t r;
     // seed and loss
-    double* zero[] = {e->lu, e->lv, e->lw, e->lp[0], e->lp[1], e->lrho, e->lrhs};
+    double* zero[] = {e->lu, e->lv, e->lw, e->lus, e->lvs, e->lws, e->lp[0], e->lp[1], e->lrho, e->lrhs};
     for (double* p : zero)
         if ((r = cudaMemsetAsync(p, 0, e->elems * sizeof(double), s)) != cudaSuccess) return r;
     if ((r = cudaMemsetAsync(e->d_sums, 0, 4 * sizeof(double), s)) != cudaSuccess) return r;
     e->lp_cur = 0;
+    e->lp_pending = false;
     {
         const Range full{0, g.nx + 1, 0, g.ny + 1, 0, g.nz + 1};
         const dim3 gf = grid_of(full);
@@ -2063,6 +2096,12 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
                 (r = reverse_step(*e, d, e->istep0 + first + q, s)) != cudaSuccess)
                 return r;
         }
+    }
+    if (e->lp_pending) {  // the first step's deferred last Jacobi stage: the initial pressure's adjoint
+        const Range I = interior(g);
+        k_adj_jacobi<<<grid_of(I), kBlk, 0, s>>>(g, I, e->inv_ap, e->lp[e->lp_cur], e->lp[e->lp_cur ^ 1], e->lrhs, 2);
+        e->lp_cur ^= 1;
+        e->lp_pending = false;
     }
     k_fold_add<<<1, 256, 0, s>>>(e->d_partial, e->npartial, 3, e->d_sums);
     if ((r = cudaGetLastError()) != cudaSuccess) return r;

@@ -78,6 +78,9 @@ struct AdjEngine {
     double *lX, *lown, *lmx, *lmn, *lpp, *lpm, *ldv, *lterm, *lLF, *lA;
     unsigned char* sel;
     int lp_cur;             // which lp buffer holds the pressure adjoint
+    // plain step: lp[lp_cur] holds mu of the last transposed Jacobi stage
+    // whose -N mu (the pressure adjoint) the next update applies
+    bool lp_pending;
     int fct_march;          // sweep adjoints: 0 shared-memory kernels, 1 line march on large grids, 2 always march
     InvAp inv_ap;
     double* d_partial;      // block partials (body force, loss)
