@@ -1347,8 +1347,8 @@ __global__ void __launch_bounds__(256) k_adj_advect(Geom g, Range R, const float
                                                     const float* __restrict__ w, const float* __restrict__ us,
                                                     const float* __restrict__ vs, const float* __restrict__ ws,
                                                     const double* __restrict__ lrhs, int has_rhs,
-                                                    double* __restrict__ lus, double* __restrict__ lvs,
-                                                    double* __restrict__ lws, double* __restrict__ lu,
+                                                    const double* __restrict__ lus, const double* __restrict__ lvs,
+                                                    const double* __restrict__ lws, double* __restrict__ lu,
                                                     double* __restrict__ lv, double* __restrict__ lw,
                                                     const double* __restrict__ lrho, double* __restrict__ lF,
                                                     double* __restrict__ partial) {
@@ -1360,11 +1360,6 @@ __global__ void __launch_bounds__(256) k_adj_advect(Geom g, Range R, const float
         const int c = gidx(g, i, j, k);
         const float Fc = F[c];
         double Gu = lus[c], Gv = lvs[c], Gw = lws[c], lr = lrho[c];
-        // this thread is the only reader of these entries: clear them, so that
-        // the set is zero when it next serves as the accumulator
-        lus[c] = 0.0;
-        lvs[c] = 0.0;
-        lws[c] = 0.0;
         if (has_rhs) {
             const int sy = g.px, sz = g.plane;
             const double idt = rcp64((double)g.dt), dxi = (double)g.dxi, dyi = (double)g.dyi, dzi = (double)g.dzi;
@@ -1701,9 +1696,10 @@ cudaError_t reverse_step(AdjEngine& e, const StepData& d, int istep, cudaStream_
         k_adj_update<false><<<gi, kBlk, 0, s>>>(g, I, d.F, d.p, e.lu, e.lv, e.lw, e.lp[e.lp_cur], e.lrho, 0,
                                                 e.inv_ap, nullptr, nullptr);
     }
-    // lu, lv, lw then hold the adjoints of u*, v*, w*; the start velocity's
-    // adjoint accumulates in the second set, which is zero (cleared at the
-    // start of the reverse pass, then by the advection kernel that last read it)
+    // lu, lv, lw now hold the adjoints of u*, v*, w*; the start velocity's
+    // adjoint accumulates in the cleared second set
+    for (double* l : {e.lus, e.lvs, e.lws})
+        if ((r = cudaMemsetAsync(l, 0, e.elems * sizeof(double), s)) != cudaSuccess) return r;
     // the pressure solve reversed: convergent modes -- lrhs = the mean-free
     // solution of A mu = lp - mean(lp) (warm start: the previous step's), and
     // the state pressure (only a warm start) gets no adjoint; plain -- the
@@ -2002,7 +1998,7 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
     const Geom& g = e->g;
     cudaError_t r;
     // seed and loss
-    double* zero[] = {e->lu, e->lv, e->lw, e->lus, e->lvs, e->lws, e->lp[0], e->lp[1], e->lrho, e->lrhs};
+    double* zero[] = {e->lu, e->lv, e->lw, e->lp[0], e->lp[1], e->lrho, e->lrhs};
     for (double* p : zero)
         if ((r = cudaMemsetAsync(p, 0, e->elems * sizeof(double), s)) != cudaSuccess) return r;
     if ((r = cudaMemsetAsync(e->d_sums, 0, 4 * sizeof(double), s)) != cudaSuccess) return r;
