@@ -1980,6 +1980,57 @@ cudaError_t adj_tape(AdjEngine* e, int istep0, int nsteps, int every, cudaStream
     e->nsteps = nsteps;
     e->every = every;
     e->recorded = false;
+    e->tail_kept = false;
+    e->tail_p = nullptr;
+    return cudaSuccess;
+}
+
+int adj_segment_first(const AdjEngine& e, int m) {
+    if (m >= e.ncp) return e.nsteps;
+    const long long f = (long long)e.nsteps - (long long)(e.ncp - m) * e.every;
+    return f > 0 ? (int)f : 0;
+}
+
+bool adj_can_record_tail(const AdjEngine& e) { return e.keep && !e.conv && e.jacobi_iters % 2 == 0 && e.ncp > 0; }
+
+// One step of a kept segment replay: step q of the segment that starts at
+// `first` (count steps), from the engine's buffers (q == 0: loaded from the
+// checkpoint) or segment state q, into segment state q + 1 or the engine's
+// buffers (last step); the pressure after the sweeps is copied into segment
+// state q + 1.  *pa: where that pressure is afterwards.
+static cudaError_t replay_kept(AdjEngine& e, int first, int count, int q, int* par, const float** pa,
+                               cudaStream_t s) {
+    float* const* vs = q == 0 ? nullptr : e.seg[q].f + 1;
+    float* const vin[3] = {q == 0 ? e.wb.u : vs[0], q == 0 ? e.wb.v : vs[1], q == 0 ? e.wb.w : vs[2]};
+    float* const* vn = q + 1 < count ? e.seg[q + 1].f + 1 : nullptr;
+    float* const vout[3] = {vn ? vn[0] : e.wb.u, vn ? vn[1] : e.wb.v, vn ? vn[2] : e.wb.w};
+    const float* Fin = q == 0 ? e.wb.F : e.seg[q].f[0];
+    float* Fout = q + 1 < count ? e.seg[q + 1].f[0] : e.wb.F;
+    cudaError_t r = replay_step_keep(e, e.istep0 + first + q, e.mid[q], Fin, Fout, vin, vout, par, pa, s);
+    if (r == cudaSuccess && q + 1 < count) {
+        r = copy_field(e.seg[q + 1].f[4], *pa, e.elems, s);
+        *pa = e.seg[q + 1].f[4];
+    }
+    return r;
+}
+
+cudaError_t adj_record_tail(AdjEngine* e, const AdjState& out, float* const extra[4], cudaStream_t s) {
+    if (!adj_can_record_tail(*e)) return cudaErrorNotSupported;
+    const int m = e->ncp - 1;
+    const int first = adj_segment_first(*e, m), count = e->nsteps - first;
+    cudaError_t r = load_state(*e, e->cp[m], s);
+    int par = 0;
+    const float* pa = nullptr;
+    for (int q = 0; q < count && r == cudaSuccess; ++q) r = replay_kept(*e, first, count, q, &par, &pa, s);
+    if (r != cudaSuccess) return r;
+    const float* src[5] = {e->wb.F, e->wb.u, e->wb.v, e->wb.w, pa};
+    for (int q = 0; q < 5; ++q)
+        if ((r = copy_field(out.f[q], src[q], e->elems, s)) != cudaSuccess) return r;
+    const float* xs[4] = {e->mid[count - 1].f[0], e->mid[count - 1].f[1], e->mid[count - 1].f[2], e->wb.rhs};
+    for (int q = 0; q < 4; ++q)
+        if (extra[q] && (r = copy_field(extra[q], xs[q], e->elems, s)) != cudaSuccess) return r;
+    e->tail_kept = true;
+    e->tail_p = pa;
     return cudaSuccess;
 }
 
@@ -2016,32 +2067,24 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
     }
     // segments, last first
     for (int m = e->ncp - 1; m >= 0; --m) {
-        const int first = m * e->every;
-        const int count = (e->nsteps - first) < e->every ? (e->nsteps - first) : e->every;
+        const int first = adj_segment_first(*e, m);
+        const int count = adj_segment_first(*e, m + 1) - first;
         if (e->keep) {
             // replay every step of the segment from checkpoint m, keeping its
-            // intermediates and the states after steps 0 .. count - 2
-            if ((r = load_state(*e, e->cp[m], s)) != cudaSuccess) return r;
+            // intermediates and the states after steps 0 .. count - 2; the
+            // record did so already for the last segment when tail_kept
+            const bool tail = m == e->ncp - 1 && e->tail_kept;
+            if (!tail && (r = load_state(*e, e->cp[m], s)) != cudaSuccess) return r;
             int par = 0;
             const float* pafter[64];
             const float** pa = count <= 64 ? pafter : new (std::nothrow) const float*[count];
             if (!pa) return cudaErrorMemoryAllocation;
-            for (int q = 0; q < count && r == cudaSuccess; ++q) {
-                // velocity: from the loaded buffers or segment state q, into
-                // segment state q + 1 (or the engine's buffers after the last step)
-                float* const* vs = q == 0 ? nullptr : e->seg[q].f + 1;
-                float* const vin[3] = {q == 0 ? e->wb.u : vs[0], q == 0 ? e->wb.v : vs[1], q == 0 ? e->wb.w : vs[2]};
-                float* const* vn = q + 1 < count ? e->seg[q + 1].f + 1 : nullptr;
-                float* const vout[3] = {vn ? vn[0] : e->wb.u, vn ? vn[1] : e->wb.v, vn ? vn[2] : e->wb.w};
-                // F likewise: from the loaded buffer or segment state q, into
-                // segment state q + 1 (or the engine's buffer)
-                const float* Fin = q == 0 ? e->wb.F : e->seg[q].f[0];
-                float* Fout = q + 1 < count ? e->seg[q + 1].f[0] : e->wb.F;
-                r = replay_step_keep(*e, e->istep0 + first + q, e->mid[q], Fin, Fout, vin, vout, &par, &pa[q], s);
-                if (r == cudaSuccess && q + 1 < count) {
-                    r = copy_field(e->seg[q + 1].f[4], pa[q], e->elems, s);
-                    pa[q] = e->seg[q + 1].f[4];
-                }
+            if (tail) {
+                for (int q = 0; q < count; ++q) pa[q] = q + 1 < count ? e->seg[q + 1].f[4] : e->tail_p;
+                e->tail_kept = false;  // the engine's buffers are reused from here on
+            } else {
+                for (int q = 0; q < count && r == cudaSuccess; ++q)
+                    r = replay_kept(*e, first, count, q, &par, &pa[q], s);
             }
             // reverse: step q's next state is seg[q + 1], or the replay's
             // buffers after the segment's last step

@@ -66,6 +66,11 @@ struct AdjEngine {
     AdjMid* mid;             // kept tapes: the intermediates of every steps; else null
     int policy;              // ADJ_STORE_* for the next tape
     int keep;                // the current tape keeps the intermediates
+    // the record replayed its last segment with the intermediates kept
+    // (adj_record_tail): the reverse pass starts without a replay; tail_p is
+    // that segment's last pressure (an engine buffer)
+    bool tail_kept;
+    const float* tail_p;
     size_t tape_bytes;       // device bytes of the tape
     bool recorded;
     // recompute buffers (FP32)
@@ -106,6 +111,23 @@ cudaError_t adj_tape(AdjEngine* e, int istep0, int nsteps, int every, cudaStream
 
 // Copy the state x into checkpoint m.
 cudaError_t adj_save(AdjEngine* e, int m, const AdjState& x, cudaStream_t s);
+
+// First step (counted from istep0) of tape segment m, m = 0 .. ncp (ncp: the
+// step count).  Segments are aligned to the end of the run: the last one holds
+// `every` steps, the first one the remainder.
+int adj_segment_first(const AdjEngine& e, int m);
+
+// Whether the record may run its last segment through adj_record_tail: a tape
+// that keeps intermediates, the plain pressure with an even number of sweeps
+// (the pressure then ends each step in the buffer it started in).
+bool adj_can_record_tail(const AdjEngine& e);
+
+// The record's last segment, from checkpoint ncp - 1 (saved before): its steps
+// run as the reverse pass replays them (intermediates and segment states
+// kept, the same kernels, so the same bits), and the final state is copied to
+// `out` (F, u, v, w, p) and the last step's u*, v*, w*, rhs to extra[0..3].
+// The reverse pass then starts on this segment without a replay.
+cudaError_t adj_record_tail(AdjEngine* e, const AdjState& out, float* const extra[4], cudaStream_t s);
 
 // Reverse the recorded run: L = sum over the box of F dV of the final state
 // `fin`; afterwards lF, lu, lv, lw, lp[lp_cur] hold dL/d(initial state) and

@@ -523,12 +523,21 @@ int vof_forward_record(vof_ctx* ctx, int istep0, int nsteps, int checkpoint_ever
     if ((e = vof::adj_tape(A, istep0, nsteps, checkpoint_every, ctx->stream)) != cudaSuccess)
         return e == cudaErrorMemoryAllocation ? VOF_E_NOMEM : fail_cuda(ctx, e);
     int not_conv = 0;
+    int m = 0;  // next checkpoint
     for (int n = 0; n < nsteps; ++n) {
-        if (n % A->every == 0) {
+        if (m < A->ncp && n == vof::adj_segment_first(*A, m)) {
             vof::AdjState x;
             for (int q = 0; q < 5; ++q) x.f[q] = field_ptr(ctx, q);
             x.p64 = ctx->conv ? ctx->p64 : nullptr;
-            if ((e = vof::adj_save(A, n / A->every, x, ctx->stream)) != cudaSuccess) return fail_cuda(ctx, e);
+            if ((e = vof::adj_save(A, m, x, ctx->stream)) != cudaSuccess) return fail_cuda(ctx, e);
+            if (m == A->ncp - 1 && vof::adj_can_record_tail(*A)) {
+                // the last segment runs as the reverse pass would replay it,
+                // so that pass starts on it without a replay
+                float* const extra[4] = {ctx->b.us, ctx->b.vs, ctx->b.ws, ctx->b.rhs};
+                if ((e = vof::adj_record_tail(A, x, extra, ctx->stream)) != cudaSuccess) return fail_cuda(ctx, e);
+                break;
+            }
+            ++m;
         }
         if (ctx->conv) {
             const int st = conv_step(ctx, istep0 + n, nullptr);

@@ -133,6 +133,36 @@ def test_velocity_perturbation_gradient_32(cuda, V, orc):
     assert np.linalg.norm(got["lu"]) > 0
 
 
+@pytest.mark.parametrize("every", [3, 7, 1])
+def test_second_reverse_pass_replays_the_recorded_tail(cuda, V, every):
+    """The record runs its last segment (segments align to the end of the run:
+    7 steps in 3 give 1 + 3 + 3) as the reverse pass replays it, and the first
+    reverse pass starts there without a replay; a second reverse pass of the
+    same record replays every segment.  Both give the same bits, and the
+    recorded state is the plain run's."""
+    prm, st = dam_state(V, 16, 14, 12)
+    box = box_of(prm)
+    with V.Solver(prm) as s:
+        s.upload_state(**st)
+        s.run(1, 7)
+        plain = s.state()
+    with V.Solver(prm) as s:
+        s.adjoint_storage(V.ADJ_KEEP)
+        s.upload_state(**st)
+        s.forward_record(1, 7, every)
+        rec = s.state()
+        r1 = s.backward(box)
+        a1 = {k: s.adjoint(f) for k, f in GRADS}
+        r2 = s.backward(box)
+        a2 = {k: s.adjoint(f) for k, f in GRADS}
+    for k in ("F", "u", "v", "w", "p"):
+        assert np.array_equal(rec[k], plain[k]), k
+    assert r1["loss"] == r2["loss"]
+    assert np.array_equal(np.asarray(r1["grad_g"]), np.asarray(r2["grad_g"]))
+    for k in a1:
+        assert np.array_equal(a1[k], a2[k]), k
+
+
 def test_state_errors(cuda, V):
     prm, st = dam_state(V, 10, 10, 10)
     with V.Solver(prm) as s:
