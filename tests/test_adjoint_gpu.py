@@ -138,8 +138,8 @@ def test_second_reverse_pass_replays_the_recorded_tail(cuda, V, every):
     """The record runs its last segment (segments align to the end of the run:
     7 steps in 3 give 1 + 3 + 3) as the reverse pass replays it, and the first
     reverse pass starts there without a replay; a second reverse pass of the
-    same record replays every segment.  Both give the same bits, and the
-    recorded state is the plain run's."""
+    same record replays every segment.  The recorded state is the plain run's
+    bit for bit; the two passes agree to the order of their FP64 atomic sums."""
     prm, st = dam_state(V, 16, 14, 12)
     box = box_of(prm)
     with V.Solver(prm) as s:
@@ -158,9 +158,9 @@ def test_second_reverse_pass_replays_the_recorded_tail(cuda, V, every):
     for k in ("F", "u", "v", "w", "p"):
         assert np.array_equal(rec[k], plain[k]), k
     assert r1["loss"] == r2["loss"]
-    assert np.array_equal(np.asarray(r1["grad_g"]), np.asarray(r2["grad_g"]))
+    assert np.allclose(r1["grad_g"], r2["grad_g"], rtol=1e-11, atol=1e-30)
     for k in a1:
-        assert np.array_equal(a1[k], a2[k]), k
+        assert rel(a1[k], a2[k]) <= 1e-11, (k, rel(a1[k], a2[k]))
 
 
 def test_state_errors(cuda, V):
