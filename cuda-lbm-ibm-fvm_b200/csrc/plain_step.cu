@@ -292,124 +292,13 @@ __global__ void __launch_bounds__(256) k_correct(Geom g,
     store_corrected(g, u, v, w, i, j, k, id, un, vn, wn);
 }
 
-// The same correction with two cells per thread: padded columns (2m, 2m + 1)
-// are one aligned 8-byte word of every field, the pairs of rows 1..ny are
-// numbered flat (32 consecutive pairs per warp, across row ends), and a thread
-// marches kchunk planes keeping p and rho of the plane below in registers;
-// the x neighbour of the pair's first cell comes from the neighbouring lane
-// (from memory at a warp's first lane), the row below is loaded.  Each cell's
-// values are k_correct's expressions in the same order; pairs with a cell on
-// a wall (or a ghost column) go through store_corrected cell by cell.
-constexpr int CP_THREADS = 256;
-__global__ void __launch_bounds__(CP_THREADS) k_correct_pairs(Geom g, const float* __restrict__ F,
-                                                              const float* __restrict__ us,
-                                                              const float* __restrict__ vs,
-                                                              const float* __restrict__ ws,
-                                                              const float* __restrict__ p, float* __restrict__ u,
-                                                              float* __restrict__ v, float* __restrict__ w,
-                                                              int kchunk) {
-    const int npair = g.nx / 2 + 1;  // pairs covering columns 0 .. nx
-    const int nq = npair * g.ny;
-    const int qt = blockIdx.x * CP_THREADS + threadIdx.x;
-    const bool qa = qt < nq;
-    const int q = qa ? qt : nq - 1;  // lanes past the end shadow the last pair
-    const int jr = q / npair, m = q - jr * npair;
-    const int j = jr + 1, i0 = 2 * m, i1 = i0 + 1;
-    const bool a0 = qa && i0 >= 1, a1 = qa && i1 <= g.nx;
-    const bool ldw = (threadIdx.x & 31) == 0 && m > 0;  // cell i0 - 1 from memory
-    const bool bulk_ij = a0 && a1 && i0 != 1 && i1 != g.nx && j != 1 && j != g.ny;
-    const int k0 = 1 + blockIdx.y * kchunk, k1 = min(g.nz, k0 + kchunk - 1);
-    const int sz = g.plane;
-    const int c = gidx(g, i0, j, 0);  // even
-    const float2* F2 = reinterpret_cast<const float2*>(F);
-    const float2* P2 = reinterpret_cast<const float2*>(p);
-    const float2* U2 = reinterpret_cast<const float2*>(us);
-    const float2* V2 = reinterpret_cast<const float2*>(vs);
-    const float2* W2 = reinterpret_cast<const float2*>(ws);
-    const int wd = c >> 1, wp = sz >> 1, wr = g.px >> 1;
-    // p and rho of the plane below
-    float2 pb = P2[wd + (k0 - 1) * wp];
-    const float2 Fb = F2[wd + (k0 - 1) * wp];
-    float rb0 = rho_of(g, Fb.x), rb1 = rho_of(g, Fb.y);
-    for (int k = k0; k <= k1; ++k) {
-        const int o = wd + k * wp;
-        const float2 Fc = F2[o], pc = P2[o], Fs = F2[o - wr], ps = P2[o - wr];
-        const float2 usv = U2[o], vsv = V2[o], wsv = W2[o];
-        float Fw = __shfl_up_sync(0xffffffffu, Fc.y, 1), pw = __shfl_up_sync(0xffffffffu, pc.y, 1);
-        if (ldw) {
-            Fw = __ldg(F + c - 1 + k * sz);
-            pw = __ldg(p + c - 1 + k * sz);
-        }
-        const float rc0 = rho_of(g, Fc.x), rc1 = rho_of(g, Fc.y);
-        float un0 = 0.0f, vn0 = 0.0f, wn0 = 0.0f, un1 = 0.0f, vn1 = 0.0f, wn1 = 0.0f;
-        if (i0 >= 2) {
-            const float r = 0.5f * (rc0 + rho_of(g, Fw));
-            un0 = usv.x - dt_over(g, r) * (pc.x - pw) * g.dxi;
-        }
-        if (i1 >= 2) {
-            const float r = 0.5f * (rc1 + rc0);
-            un1 = usv.y - dt_over(g, r) * (pc.y - pc.x) * g.dxi;
-        }
-        if (j >= 2) {
-            const float r0 = 0.5f * (rc0 + rho_of(g, Fs.x)), r1 = 0.5f * (rc1 + rho_of(g, Fs.y));
-            vn0 = vsv.x - dt_over(g, r0) * (pc.x - ps.x) * g.dyi;
-            vn1 = vsv.y - dt_over(g, r1) * (pc.y - ps.y) * g.dyi;
-        }
-        if (k >= 2) {
-            const float r0 = 0.5f * (rc0 + rb0), r1 = 0.5f * (rc1 + rb1);
-            wn0 = wsv.x - dt_over(g, r0) * (pc.x - pb.x) * g.dzi;
-            wn1 = wsv.y - dt_over(g, r1) * (pc.y - pb.y) * g.dzi;
-        }
-        if (bulk_ij && k != 1 && k != g.nz) {
-            reinterpret_cast<float2*>(u)[o] = make_float2(un0, un1);
-            reinterpret_cast<float2*>(v)[o] = make_float2(vn0, vn1);
-            reinterpret_cast<float2*>(w)[o] = make_float2(wn0, wn1);
-        } else {
-            if (a0) store_corrected(g, u, v, w, i0, j, k, 2 * o, un0, vn0, wn0);
-            if (a1) store_corrected(g, u, v, w, i1, j, k, 2 * o + 1, un1, vn1, wn1);
-        }
-        pb = pc;
-        rb0 = rc0;
-        rb1 = rc1;
-    }
-}
-
-// Blocks of k_correct_pairs resident at once (SMs x blocks per SM), set by
-// plain_configure.
-static int cp_wave = 4 * 148;
-
-// z chunk of the paired correction: the longest whose launch fills its last
-// wave of blocks to 85 % or more, else the one that fills it best.
-static int correct_pairs_kchunk(const Geom& g, int bx) {
-    int best = g.nz;
-    double best_fill = -1.0;
-    for (int n = 1; n <= g.nz; ++n) {
-        const int kc = (g.nz + n - 1) / n;
-        const long long blocks = (long long)bx * ((g.nz + kc - 1) / kc);
-        const long long waves = (blocks + cp_wave - 1) / cp_wave;
-        const double fill = (double)blocks / (double)(waves * cp_wave);
-        if (fill >= 0.85) return kc;
-        if (fill > best_fill) {
-            best_fill = fill;
-            best = kc;
-        }
-    }
-    return best;
-}
-
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
 cudaError_t plain_configure(int max_line) {
     (void)max_line;
     cudaError_t e = fct_configure();
-    if (e == cudaSuccess) e = jacobi_tb_configure();
-    int dev = 0, sms = 0, occ = 0;
-    if (e == cudaSuccess && (e = cudaGetDevice(&dev)) == cudaSuccess &&
-        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) == cudaSuccess &&
-        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_correct_pairs, CP_THREADS, 0)) == cudaSuccess)
-        cp_wave = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
-    return e;
+    return e == cudaSuccess ? jacobi_tb_configure() : e;
 }
 
 cudaError_t plain_density_pairs(Geom* g) {
@@ -540,26 +429,7 @@ cudaError_t plain_front(const Geom& g, const PlainBuffers& b, cudaStream_t s, cu
     return cudaSuccess;
 }
 
-// The correction kernel: two cells per thread (k_correct_pairs, the default)
-// or one (k_correct, VOF_CORRECT=cells).
-static bool correct_pairs() {
-    static int forced = -1;
-    if (forced < 0) {
-        const char* v = getenv("VOF_CORRECT");
-        forced = (v && !strcmp(v, "cells")) ? 0 : 1;
-    }
-    return forced == 1;
-}
-
 cudaError_t plain_correct(const Geom& g, const PlainBuffers& b, const float* p, cudaStream_t s) {
-    if (correct_pairs()) {
-        const int nq = (g.nx / 2 + 1) * g.ny;
-        const int bx = (nq + CP_THREADS - 1) / CP_THREADS;
-        const int kc = correct_pairs_kchunk(g, bx);
-        k_correct_pairs<<<dim3(bx, (g.nz + kc - 1) / kc), CP_THREADS, 0, s>>>(g, b.F, b.us, b.vs, b.ws, p, b.u, b.v,
-                                                                              b.w, kc);
-        return cudaGetLastError();
-    }
     const dim3 cb(32, 4, 2);
     const dim3 cg((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + 1) / 2);
     k_correct<<<cg, cb, 0, s>>>(g, b.F, b.us, b.vs, b.ws, p, b.u, b.v, b.w);
