@@ -47,14 +47,16 @@ __device__ void block_reduce_store(double (&val)[NV], const int (&op)[NV], doubl
     }
 }
 
-// Interior-cell iterator: linear index over nx*ny*nz, grid-stride.
-#define FOR_INTERIOR(g, i, j, k)                                                        \
-    for (long long t_ = (long long)blockIdx.x * blockDim.x + threadIdx.x,               \
-                   n_ = (long long)(g).nx * (g).ny * (g).nz;                            \
-         t_ < n_; t_ += (long long)gridDim.x * blockDim.x)                              \
-        for (int i = 1 + (int)(t_ % (g).nx), j = 1 + (int)((t_ / (g).nx) % (g).ny),      \
-                 k = 1 + (int)(t_ / ((long long)(g).nx * (g).ny)), once_ = 1;           \
-             once_; once_ = 0)
+// Interior-cell iterator: the rows (j, k) are dealt to the warps of the grid
+// in a fixed order (row r = (k-1) ny + j-1 to warp r mod the warp count), the
+// lanes of a warp striding along x: coalesced loads and one integer division
+// per row.  A fixed mapping for the fixed grid, so the sums are reproducible.
+#define FOR_INTERIOR(g, i, j, k)                                                                        \
+    for (int r_ = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nr_ = (g).ny * (g).nz,          \
+             sr_ = (int)((gridDim.x * blockDim.x) >> 5);                                                \
+         r_ < nr_; r_ += sr_)                                                                           \
+        for (int j = 1 + r_ % (g).ny, k = 1 + r_ / (g).ny, i = 1 + (int)(threadIdx.x & 31); i <= (g).nx; \
+             i += 32)
 
 __global__ void __launch_bounds__(RED_THREADS) k_red_field(Geom g, const float* __restrict__ a,
                                                            double* partial) {
@@ -125,16 +127,16 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_nonfinite(Geom g, const flo
                                                                double* partial) {
     double val[1] = {0.0};
     const int op[1] = {OP_SUM};
-    const long long n = (long long)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(t % (g.nx + 2));
-        const int j = (int)((t / (g.nx + 2)) % (g.ny + 2));
-        const int k = (int)(t / ((long long)(g.nx + 2) * (g.ny + 2)));
-        const int id = gidx(g, i, j, k);
-        val[0] += (double)(!isfinite(f0[id])) + (double)(!isfinite(f1[id])) +
-                  (double)(!isfinite(f2[id])) + (double)(!isfinite(f3[id])) +
-                  (double)(!isfinite(f4[id]));
+    // every cell with its ghosts: rows (j, k) of ny+2 x nz+2 to the warps, lanes along x
+    const int nrow = (g.ny + 2) * (g.nz + 2), srow = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int r = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); r < nrow; r += srow) {
+        const int row = gidx(g, 0, r % (g.ny + 2), r / (g.ny + 2));
+        for (int i = (int)(threadIdx.x & 31); i <= g.nx + 1; i += 32) {
+            const int id = row + i;
+            val[0] += (double)(!isfinite(f0[id])) + (double)(!isfinite(f1[id])) +
+                      (double)(!isfinite(f2[id])) + (double)(!isfinite(f3[id])) +
+                      (double)(!isfinite(f4[id]));
+        }
     }
     block_reduce_store<1>(val, op, partial);
 }
