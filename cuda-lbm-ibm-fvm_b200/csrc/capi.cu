@@ -475,9 +475,20 @@ int vof_reduce_async(vof_ctx* ctx, int what, double* host_out) {
     in.w = ctx->b.w;
     in.p = ctx->p_parity ? ctx->b.p1 : ctx->b.p0;
     in.rhs = ctx->b.rhs;
+    // page-locked host memory mapped into the device: the reduction kernel
+    // writes the value there itself (no copy in the stream)
+    double* alias = nullptr;
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, host_out) == cudaSuccess) {
+        if (pa.type == cudaMemoryTypeHost && pa.devicePointer) alias = static_cast<double*>(pa.devicePointer);
+    } else {
+        cudaGetLastError();  // not a pointer CUDA knows: an ordinary host address
+    }
+    bool wrote = false;
     cudaError_t e = vof::reduce_launch(ctx->g, in, what, ctx->d_red_scratch, ctx->d_red_result,
-                                       ctx->stream);
+                                       ctx->stream, alias, &wrote);
     if (e != cudaSuccess) return fail_cuda(ctx, e);
+    if (wrote) return VOF_OK;
     e = cudaMemcpyAsync(host_out, ctx->d_red_result + vof::reduce_result_slot(what), sizeof(double),
                         cudaMemcpyDeviceToHost, ctx->stream);
     return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);

@@ -147,16 +147,16 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_nonfinite(Geom g, const flo
 // MODE_VOLUME multiplies result[0] by the cell volume.
 enum Post { POST_NONE = 0, POST_MEAN = 1, POST_SQRT = 2, POST_RATIO = 3, POST_SCALE = 4 };
 
-__global__ void __launch_bounds__(RED_THREADS) k_red_finish(const double* __restrict__ partial,
-                                                            int nblk, int nv, int op0, int op1,
-                                                            int op2, int post, double scale,
-                                                            double* result) {
+// The fold of pass 2 by one block of RED_THREADS threads (partials read past
+// L1: they may have been written by other blocks of the same launch).
+__device__ void fold_partials(const double* __restrict__ partial, int nblk, int nv, int op0, int op1, int op2,
+                              int post, double scale, double* result) {
     __shared__ double sh[3][RED_THREADS];
     const int ops[3] = {op0, op1, op2};
     for (int v = 0; v < nv; ++v) {
         double x = identity(ops[v]);
         for (int b = threadIdx.x; b < nblk; b += RED_THREADS)
-            x = combine(x, partial[(size_t)nv * b + v], ops[v]);
+            x = combine(x, __ldcg(partial + (size_t)nv * b + v), ops[v]);
         sh[v][threadIdx.x] = x;
     }
     __syncthreads();
@@ -177,20 +177,64 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_finish(const double* __rest
     }
 }
 
+__global__ void __launch_bounds__(RED_THREADS) k_red_finish(const double* __restrict__ partial,
+                                                            int nblk, int nv, int op0, int op1,
+                                                            int op2, int post, double scale,
+                                                            double* result) {
+    fold_partials(partial, nblk, nv, op0, op1, op2, post, scale, result);
+}
+
+// k_red_field and k_red_finish in one launch: every block stores its partial
+// and counts itself done; the last one folds all partials in the same fixed
+// order as k_red_finish (the same bits), copies result[slot] to the mapped
+// host double when given, and clears the counter for the next launch.
+__global__ void __launch_bounds__(RED_THREADS) k_red_field_fold(Geom g, const float* __restrict__ a,
+                                                                double* partial, unsigned* counter,
+                                                                double scale, double* result,
+                                                                double* host_alias, int slot) {
+    double val[3] = {0.0, -INFINITY, INFINITY};
+    const int op[3] = {OP_SUM, OP_MAX, OP_MIN};
+    FOR_INTERIOR(g, i, j, k) {
+        const double x = (double)a[gidx(g, i, j, k)];
+        val[0] += x;
+        val[1] = fmax(val[1], x);
+        val[2] = fmin(val[2], x);
+    }
+    block_reduce_store<3>(val, op, partial);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        __threadfence();  // the partial before the count
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    fold_partials(partial, gridDim.x, 3, OP_SUM, OP_MAX, OP_MIN, POST_SCALE, scale, result);
+    if (threadIdx.x == 0) {
+        if (host_alias) {
+            *host_alias = result[slot];
+            __threadfence_system();
+        }
+        *counter = 0u;
+    }
+}
+
 cudaError_t reduce_launch(const Geom& g, const ReduceInputs& in, int what, double* d_scratch,
-                          double* d_result, cudaStream_t s) {
+                          double* d_result, cudaStream_t s, double* host_alias, bool* wrote_host) {
     const int nblk = RED_BLOCKS;
     double* part = d_scratch;
     const double ncell = (double)g.nx * g.ny * g.nz;
+    if (wrote_host) *wrote_host = false;
     switch (what) {
         case RED_VOLUME:
         case RED_F_MIN:
         case RED_F_MAX: {
-            k_red_field<<<nblk, RED_THREADS, 0, s>>>(g, in.F, part);
             const double vol = (double)g.dx * (double)g.dy * (double)g.dz;
             // result[0] = volume, [1] = max, [2] = min
-            k_red_finish<<<1, RED_THREADS, 0, s>>>(part, nblk, 3, OP_SUM, OP_MAX, OP_MIN,
-                                                   POST_SCALE, vol, d_result);
+            unsigned* counter = reinterpret_cast<unsigned*>(d_scratch + 3 * RED_BLOCKS);
+            k_red_field_fold<<<nblk, RED_THREADS, 0, s>>>(g, in.F, part, counter, vol, d_result, host_alias,
+                                                          reduce_result_slot(what));
+            if (wrote_host) *wrote_host = host_alias != nullptr;
             break;
         }
         case RED_DIV_L2:

@@ -19,8 +19,10 @@ enum {
 
 constexpr int RED_BLOCKS = 592;  // 4 x 148 SMs; fixed so results are bitwise reproducible
 
-// Scratch doubles reduce_launch needs (partials of up to 3 values per block).
-constexpr int RED_SCRATCH_DOUBLES = 3 * RED_BLOCKS;
+// Scratch doubles reduce_launch needs: partials of up to 3 values per block,
+// then one slot whose first 4 bytes count the finished blocks of the
+// single-launch field reduction (zero between launches).
+constexpr int RED_SCRATCH_DOUBLES = 3 * RED_BLOCKS + 1;
 // Device doubles of the result area (result slots plus the rhs mean).
 constexpr int RED_RESULT_DOUBLES = 8;
 
@@ -34,8 +36,12 @@ struct ReduceInputs {
 };
 
 // Enqueue reduction `what`; the value lands in d_result[reduce_result_slot(what)].
+// host_alias (optional): the device address of a mapped host double that
+// receives the value too.  Returns in *wrote_host whether it did (the volume
+// and F min / max reductions, one launch whose last block folds the partials).
 cudaError_t reduce_launch(const Geom& g, const ReduceInputs& in, int what, double* d_scratch,
-                          double* d_result, cudaStream_t s);
+                          double* d_result, cudaStream_t s, double* host_alias = nullptr,
+                          bool* wrote_host = nullptr);
 
 int reduce_result_slot(int what);
 

@@ -189,7 +189,10 @@ int vof_reduce(vof_ctx* ctx, int what, double* out);
 /*
  * Stream-ordered reduction: the result is written to *host_out (which should
  * be pinned host memory) when the stream reaches this point; the host must
- * vof_sync before reading it.  No host synchronisation inside.
+ * vof_sync before reading it.  No host synchronisation inside.  For pinned
+ * memory mapped into the device (cudaHostAlloc / cudaHostRegister on a 64-bit
+ * system) the volume and F min / max reductions are one kernel that writes
+ * *host_out itself; otherwise a copy follows the kernels.
  */
 int vof_reduce_async(vof_ctx* ctx, int what, double* host_out);
 

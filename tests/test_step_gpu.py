@@ -183,6 +183,32 @@ def test_reductions_deterministic(cuda, V):
     assert a == b
 
 
+def test_async_reductions_into_mapped_and_pageable_memory(cuda, V):
+    """vof_reduce_async into pinned (mapped) memory -- one kernel writes the
+    value itself -- and into pageable memory -- a copy follows: the same bits
+    as the blocking call, call after call (the completion counter resets)."""
+    import torch
+
+    prm = V.default_params(30, 26, 22, dt=5e-4)
+    state = ic.random_state(prm, seed=32, vel_scale=1.0)
+    names = ("volume", "f_min", "f_max", "div_l2")
+    pinned = torch.zeros(4 * len(names), dtype=torch.float64).pin_memory()
+    pageable = np.zeros(4 * len(names), dtype=np.float64)
+    with V.Solver(prm) as s:
+        s.upload_state(**state)
+        s.step(1)
+        want = [s.reduce(k) for k in names]
+        for rep in range(4):
+            for q, k in enumerate(names):
+                s.reduce_async(k, pinned.data_ptr() + 8 * (rep * len(names) + q))
+                s.reduce_async(k, pageable.ctypes.data + 8 * (rep * len(names) + q))
+        s.sync()
+    got_p = pinned.numpy().reshape(4, len(names))
+    got_h = pageable.reshape(4, len(names))
+    for rep in range(4):
+        assert list(got_p[rep]) == want and list(got_h[rep]) == want, (rep, got_p[rep], got_h[rep], want)
+
+
 def test_nonfinite_watchdog(cuda, V):
     prm = V.default_params(10, 10, 10)
     state = ic.random_state(prm, seed=3)
