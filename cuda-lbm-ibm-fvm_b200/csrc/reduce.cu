@@ -49,14 +49,15 @@ __device__ void block_reduce_store(double (&val)[NV], const int (&op)[NV], doubl
 
 // Interior-cell iterator: the rows (j, k) are dealt to the warps of the grid
 // in a fixed order (row r = (k-1) ny + j-1 to warp r mod the warp count), the
-// lanes of a warp striding along x: coalesced loads and one integer division
-// per row.  A fixed mapping for the fixed grid, so the sums are reproducible.
+// lanes of a warp striding along x (unrolled by 4, so that several loads of a
+// lane are in flight): coalesced loads and one integer division per row.  A
+// fixed mapping for the fixed grid, so the sums are reproducible.
 #define FOR_INTERIOR(g, i, j, k)                                                                        \
     for (int r_ = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nr_ = (g).ny * (g).nz,          \
              sr_ = (int)((gridDim.x * blockDim.x) >> 5);                                                \
          r_ < nr_; r_ += sr_)                                                                           \
-        for (int j = 1 + r_ % (g).ny, k = 1 + r_ / (g).ny, i = 1 + (int)(threadIdx.x & 31); i <= (g).nx; \
-             i += 32)
+        _Pragma("unroll 4") for (int j = 1 + r_ % (g).ny, k = 1 + r_ / (g).ny, i = 1 + (int)(threadIdx.x & 31); \
+                                 i <= (g).nx; i += 32)
 
 __global__ void __launch_bounds__(RED_THREADS) k_red_field(Geom g, const float* __restrict__ a,
                                                            double* partial) {
