@@ -33,7 +33,6 @@
 
 #include "fct_line.cuh"
 #include "fct_sweep.h"
-#include "pdl.cuh"
 
 namespace vof {
 
@@ -124,7 +123,6 @@ template <int AXIS, bool FINAL>
 // fluxes of zero velocity).
 __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, const float* Fsrc, float* F,
                                                     const float* __restrict__ vel) {
-    pdl_enter();
     extern __shared__ float smem[];
     const Sweep<AXIS> S(g);
     const int n = S.n;
@@ -306,7 +304,7 @@ static cudaError_t launch_axis(const Geom& g, const float* Fsrc, float* F, const
     const int na = AXIS == 0 ? g.ny : g.nx;
     const int nb = AXIS == 2 ? g.ny : g.nz;
     dim3 grid((na * nb + LANES - 1) / LANES, 1, 1);
-    pdl_launch(k_fct<AXIS, FINAL>, grid, dim3(LANES, WARPS), fct_smem_bytes(AXIS, n), s, g, Fsrc, F, vel);
+    k_fct<AXIS, FINAL><<<grid, dim3(LANES, WARPS), fct_smem_bytes(AXIS, n), s>>>(g, Fsrc, F, vel);
     return cudaGetLastError();
 }
 

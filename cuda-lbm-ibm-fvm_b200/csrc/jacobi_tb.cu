@@ -27,7 +27,6 @@
 #include <stdlib.h>
 
 #include "jacobi_tb.h"
-#include "pdl.cuh"
 #include "tma.cuh"
 
 namespace vof {
@@ -312,7 +311,6 @@ constexpr int JP_THREADS = 256;
 __global__ void __launch_bounds__(JP_THREADS) k_jacobi_pairs(Geom g, const float* __restrict__ pin,
                                                              const float* __restrict__ rhs,
                                                              float* __restrict__ pout, int kchunk) {
-    pdl_enter();
     const int npair = g.nx / 2 + 1;  // pairs covering columns 0 .. nx
     const int nq = npair * g.ny;
     const int qt = blockIdx.x * JP_THREADS + threadIdx.x;
@@ -422,8 +420,7 @@ cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rh
     const int nq = (g.nx / 2 + 1) * g.ny;
     const int bx = (nq + JP_THREADS - 1) / JP_THREADS;
     const int kchunk = jacobi_pairs_kchunk(g, bx);
-    pdl_launch(k_jacobi_pairs, dim3(bx, (g.nz + kchunk - 1) / kchunk), dim3(JP_THREADS), 0, s, g, pin, rhs, pout,
-               kchunk);
+    k_jacobi_pairs<<<dim3(bx, (g.nz + kchunk - 1) / kchunk), JP_THREADS, 0, s>>>(g, pin, rhs, pout, kchunk);
     return cudaGetLastError();
 }
 

@@ -41,7 +41,6 @@
 #include <vector>
 
 #include "mg_solve.h"
-#include "pdl.cuh"
 
 namespace vof {
 
@@ -65,10 +64,33 @@ struct St<double> {
 constexpr int MG_THREADS = MG_BX * MG_BY;
 constexpr int TAIL_THREADS = 1024;
 
-// Every kernel of the solve is launched with programmatic dependent launch
-// (pdl.cuh: pdl_launch, and pdl_enter() at the top of each kernel), so the
-// launch of the next kernel overlaps the end of the current one, which
-// removes most of the gap between the short kernels of the coarse levels.
+// Programmatic dependent launch.  Every kernel of the solve is launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization (pdl_launch) and begins
+// with pdl_enter(): it waits for the grid before it to complete (and its
+// writes to be visible) before its first global memory access, then lets the
+// next grid launch.  The launch and prologue of a kernel so overlap the end of
+// the one before, which removes most of the gap between the short kernels of
+// the coarse levels.  Launched without the attribute, the wait returns at once.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+static cudaError_t pdl_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 __host__ __device__ __forceinline__ int nb_count(int x, int n) { return (x > 0) + (x < n - 1); }
 

@@ -22,7 +22,6 @@
 
 #include "fct_sweep.h"
 #include "jacobi_tb.h"
-#include "pdl.cuh"
 
 #include <cuda_runtime.h>
 #include <stdlib.h>
@@ -76,7 +75,6 @@ __global__ void __launch_bounds__(256) k_predict(Geom g,
                                                  float* __restrict__ us,
                                                  float* __restrict__ vs,
                                                  float* __restrict__ ws, int kchunk) {
-    pdl_enter();
     const Column col(g, 1, 1, kchunk);
     const int i = col.i, j = col.j;
     if (i > g.nx || j > g.ny || col.k0 > g.nz) return;
@@ -154,7 +152,6 @@ __global__ void __launch_bounds__(256) k_rhs(Geom g,
                                              const float* __restrict__ vs,
                                              const float* __restrict__ ws,
                                              float* __restrict__ rhs, int kchunk) {
-    pdl_enter();
     const Column col(g, 1, 1, kchunk);
     if (col.i > g.nx || col.j > g.ny || col.k0 > g.nz) return;
     int id = gidx(g, col.i, col.j, col.k0);
@@ -271,7 +268,6 @@ __global__ void __launch_bounds__(256) k_correct(Geom g,
                                                  const float* __restrict__ p,
                                                  float* __restrict__ u, float* __restrict__ v,
                                                  float* __restrict__ w) {
-    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
@@ -426,9 +422,9 @@ cudaError_t plain_front(const Geom& g, const PlainBuffers& b, cudaStream_t s, cu
     column_launch(g, grid, kchunk);
     cudaError_t e;
     if ((e = mark(ev, 0, s)) != cudaSuccess) return e;
-    pdl_launch(k_predict, grid, blk, 0, s, g, b.F, b.u, b.v, b.w, b.us, b.vs, b.ws, kchunk);
+    k_predict<<<grid, blk, 0, s>>>(g, b.F, b.u, b.v, b.w, b.us, b.vs, b.ws, kchunk);
     if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(ev, 1, s)) != cudaSuccess) return e;
-    pdl_launch(k_rhs, grid, blk, 0, s, g, b.F, b.us, b.vs, b.ws, b.rhs, kchunk);
+    k_rhs<<<grid, blk, 0, s>>>(g, b.F, b.us, b.vs, b.ws, b.rhs, kchunk);
     if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(ev, 2, s)) != cudaSuccess) return e;
     return cudaSuccess;
 }
@@ -436,7 +432,7 @@ cudaError_t plain_front(const Geom& g, const PlainBuffers& b, cudaStream_t s, cu
 cudaError_t plain_correct(const Geom& g, const PlainBuffers& b, const float* p, cudaStream_t s) {
     const dim3 cb(32, 4, 2);
     const dim3 cg((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + 1) / 2);
-    pdl_launch(k_correct, cg, cb, 0, s, g, b.F, b.us, b.vs, b.ws, p, b.u, b.v, b.w);
+    k_correct<<<cg, cb, 0, s>>>(g, b.F, b.us, b.vs, b.ws, p, b.u, b.v, b.w);
     return cudaGetLastError();
 }
 

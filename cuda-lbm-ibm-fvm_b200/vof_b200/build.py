@@ -41,7 +41,7 @@ SOURCES = {
     "noalloc.cu": [],
 }
 HEADERS = ["vof_device.cuh", "tma.cuh", "plain_step.h", "fct_sweep.h", "fct_line.cuh", "jacobi_tb.h", "mg_solve.h",
-           "reduce.h", "adjoint.h", "pdl.cuh"]
+           "reduce.h", "adjoint.h"]
 
 
 def nvcc() -> str:
