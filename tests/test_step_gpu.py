@@ -72,6 +72,38 @@ def test_random_state_bitwise_vs_oracle(cuda, V, orc, nx, ny, nz, seed, dt, vs):
     assert_bitwise(got, want, STATE + ("ustar", "vstar", "wstar", "rhs"), f"{nx}x{ny}x{nz}")
 
 
+@pytest.mark.parametrize("env", [{"VOF_JACOBI": "tb"}, {"VOF_JACOBI": "col"}, {"VOF_JACOBI_KCHUNK": "1"},
+                                 {"VOF_JACOBI_KCHUNK": "5"}])
+def test_jacobi_kernel_choices_give_the_same_bits(cuda, V, orc, tmp_path, env):
+    """The Jacobi kernels a process may select (the blocked two-sweep kernel,
+    the one-cell streaming sweep, other z chunks of the paired sweep; read
+    once per process, so each runs in a child process) give the oracle's bits."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    prm = V.default_params(40, 33, 21, dt=2e-4, gy=0.0, gz=-9.81)
+    state = ic.random_state(prm, seed=5, vel_scale=3.0)
+    np.savez(tmp_path / "in.npz", **state)
+    root = Path(__file__).resolve().parent.parent
+    code = (
+        "import sys, numpy as np\n"
+        f"sys.path.insert(0, {str(root / 'cuda-lbm-ibm-fvm_b200')!r})\n"
+        "import vof_b200 as V\n"
+        "prm = V.default_params(40, 33, 21, dt=2e-4, gy=0.0, gz=-9.81)\n"
+        f"st = dict(np.load({str(tmp_path / 'in.npz')!r}))\n"
+        "with V.Solver(prm) as s:\n"
+        "    s.upload_state(**st)\n"
+        "    for t in range(3):\n"
+        "        s.step(1 + t)\n"
+        f"    np.savez({str(tmp_path / 'out.npz')!r}, **s.state())\n")
+    subprocess.run([sys.executable, "-c", code], env={**os.environ, **env}, check=True, timeout=600)
+    got = dict(np.load(tmp_path / "out.npz"))
+    want = orc.run_f32(prm, state, 1, 3)
+    assert_bitwise(got, want, STATE, str(env))
+
+
 @pytest.mark.parametrize("istep", [1, 2, 3])
 def test_each_sweep_order_bitwise(cuda, V, orc, istep):
     prm = V.default_params(20, 18, 16, dt=5e-4)
