@@ -639,7 +639,7 @@ def run_ours(args):
 
 
 # ---------------------------------------------------------------------------
-# small grids: configs[0] (32^3 x 200 steps) and the 64^3 adjoint grid
+# small grids: the 32^3 dam break with a flat interface (200 steps) and 64^3
 # ---------------------------------------------------------------------------
 SMALL_GRIDS = ((32, 200), (64, 200))
 

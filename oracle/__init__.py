@@ -1,1 +1,1 @@
-"""Checkers for the CUDA step -- test infrastructure only (see oracle.py)."""
+"""The oracle of the CUDA step -- test infrastructure only (see oracle.py)."""

@@ -1,4 +1,4 @@
-"""ctypes loaders of the checkers under oracle/ -- TEST INFRASTRUCTURE ONLY.
+"""ctypes loaders of the oracle libraries under oracle/ -- TEST INFRASTRUCTURE ONLY.
 
 Imported by tests/, __graft_entry__.smoke() and bench.py (CPU-baseline leg and
 ``--impl reference``); never by the library.

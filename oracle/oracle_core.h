@@ -1,7 +1,7 @@
 // oracle_core.h -- the CPU restatement of the voftrial1.cu time step, shared
 // by vof_oracle.cpp (the forward oracle) and vof_adjoint.cpp (its adjoint).
 //
-// TEST INFRASTRUCTURE ONLY: included by the checkers under oracle/, never by
+// TEST INFRASTRUCTURE ONLY: included by the oracle sources under oracle/, never by
 // the product.
 //
 // It follows the reference kernel by kernel, with all twenty DeviceFields

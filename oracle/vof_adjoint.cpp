@@ -2,7 +2,7 @@
 // dual-number tangent it is the transpose of, and the switch tape.
 //
 // TEST INFRASTRUCTURE ONLY: loaded by tests/ (and bench.py's CPU leg) as the
-// checker of the CUDA adjoint (vof_forward_record / vof_backward); the
+// oracle of the CUDA adjoint (vof_forward_record / vof_backward); the
 // product never links or calls it.  The reference has no adjoint: this is the
 // reverse mode of the step in oracle_core.h, kernel by kernel
 // (voftrial1.cu:1364-1401 backwards), with every non-smooth choice frozen at

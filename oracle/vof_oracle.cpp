@@ -1,7 +1,7 @@
 // vof_oracle.cpp -- CPU restatement of the voftrial1.cu time step (the
 // forward oracle; the step itself is in oracle_core.h).
 //
-// TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA step in
+// TEST INFRASTRUCTURE ONLY.  This file is the oracle of the CUDA step in
 // cuda-lbm-ibm-fvm_b200/csrc; it is loaded only by tests/, by
 // __graft_entry__.smoke() and by bench.py's CPU-baseline leg.  The product
 // never links or calls it.
