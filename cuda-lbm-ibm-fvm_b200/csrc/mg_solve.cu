@@ -1137,8 +1137,7 @@ cudaError_t mg_create(const Geom& g, int mode, MgSolver* m, cudaStream_t s, size
     const size_t vb = mode == MG_MIXED ? sizeof(__nv_bfloat16) : sizeof(double);
     const size_t cb = mode == MG_MIXED ? sizeof(float) : sizeof(double);
     const MgLevel& Lc = m->lv[m->nlev - 1];
-    // The tail: the deepest run of levels (at most MG_TAIL_CELLS cells each,
-    // MG_TAIL_CELLS_BF16 in MIXED)
+    // The tail: the deepest run of levels (at most MG_TAIL_CELLS cells each)
     // whose vectors and dense coarse inverse fit in MG_TAIL_SMEM bytes.
     const bool dense_ok = Lc.ncell <= MG_DENSE_MAX;
     const size_t inv_bytes = dense_ok ? (size_t)Lc.ncell * Lc.ncell * cb : 0;
@@ -1148,9 +1147,7 @@ cudaError_t mg_create(const Geom& g, int mode, MgSolver* m, cudaStream_t s, size
         size_t acc = inv_bytes;
         for (int l = m->nlev - 1; l >= 0; --l) {
             const size_t lb = 3 * (size_t)tail_vec_bytes(m->lv[l].ncell, (int)vb);
-            if (m->lv[l].ncell > (mode == MG_MIXED ? MG_TAIL_CELLS_BF16 : MG_TAIL_CELLS) ||
-                acc + lb > MG_TAIL_SMEM)
-                break;
+            if (m->lv[l].ncell > MG_TAIL_CELLS || acc + lb > MG_TAIL_SMEM) break;
             acc += lb;
             m->tail = l;
             m->tail_smem = (int)acc;
