@@ -1185,7 +1185,7 @@ cudaError_t mg_create(const Geom& g, int mode, MgSolver* m, cudaStream_t s, size
         (e = alloc((void**)&m->d_result, sizeof(double) * 8)) != cudaSuccess ||
         (e = alloc((void**)&m->d_lv, sizeof(MgLevel) * m->nlev)) != cudaSuccess)
         return e;
-    if ((e = cudaHostAlloc((void**)&m->h_result, sizeof(double) * 4, cudaHostAllocMapped)) != cudaSuccess) {
+    if ((e = cudaHostAlloc((void**)&m->h_result, sizeof(double) * 2, cudaHostAllocMapped)) != cudaSuccess) {
         m->h_result = nullptr;
         return e;
     }
@@ -1408,30 +1408,19 @@ static cudaError_t solve_impl(const Geom& g, MgSolver& m, const R* rhs, double* 
     pdl_launch(k_fold2, 1, MG_THREADS, 0, s, part, m.nblk, res + 2, nullptr);
     pdl_launch(k_resid0<S, R>, grid, kBlock, 0, s, g, L0, rhs, res + 2, p64, static_cast<S*>(L0.b),
                multi(m, 0) ? static_cast<S*>(L0.e0) : nullptr, part);
-    pdl_launch(k_fold2, 1, MG_THREADS, 0, s, part, m.nblk, res, m.h_result_dev + 2);
+    pdl_launch(k_fold2, 1, MG_THREADS, 0, s, part, m.nblk, res, m.h_result_dev);
     launches += 4;
-    // The outer iterations the previous solve needed, less one, run before the
-    // first look at the residual (with warm starts the count is steady, so
-    // the host waits once instead of once per iteration); then one at a time
-    // until the residual is small enough.  Each iteration writes its residual
-    // sums to h_result[0..1]; the entry sums went to h_result[2..3].
     int it = 0;
-    const int ahead = m.last_outer > 1 ? (m.last_outer - 1 < max_outer ? m.last_outer - 1 : max_outer) : 0;
-    for (; it < ahead; ++it) {
-        if ((e = cudaGraphLaunch(m.iter_graph, s)) != cudaSuccess) return e;
-        launches += m.graph_launches;
-    }
     double rel = 0, r0 = -1;
     for (;; ++it) {
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-        if (r0 < 0) r0 = m.h_result[3] > 0 ? sqrt(m.h_result[2] / m.h_result[3]) : 0.0;
-        const double rr = m.h_result[it == 0 ? 2 : 0], bb = m.h_result[it == 0 ? 3 : 1];
+        const double rr = m.h_result[0], bb = m.h_result[1];
         rel = bb > 0 ? sqrt(rr / bb) : 0.0;
+        if (r0 < 0) r0 = rel;
         if (rel <= tol || it >= max_outer) break;
         if ((e = cudaGraphLaunch(m.iter_graph, s)) != cudaSuccess) return e;
         launches += m.graph_launches;
     }
-    m.last_outer = it;
     pdl_launch(k_sum_p, grid, kBlock, 0, s, g, L0, p64, part);
     pdl_launch(k_fold2, 1, MG_THREADS, 0, s, part, m.nblk, res + 4, nullptr);
     pdl_launch(k_gauge_cast, grid, kBlock, 0, s, g, L0, p64, res + 4, p32);

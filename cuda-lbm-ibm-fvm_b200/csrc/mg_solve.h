@@ -66,9 +66,7 @@ struct MgSolver {
     double* d_partial;  // reduction partials, 2 per block of the largest tiling
     int nblk;           // blocks of the fine tiling
     double* d_result;   // [0..1] residual sums, [2..3] sum of rhs, [4..5] sum of p, [6..7] coarse mean
-    double* h_result;   // mapped pinned host copies of the residual sums: [0..1] after the
-                        // last outer iteration, [2..3] at entry
-    int last_outer;     // outer iterations of the previous solve
+    double* h_result;   // mapped pinned host copy of the residual sums (2 doubles)
     double* h_result_dev;  // its device alias
     // One outer iteration (V-cycle, p += e, new residual) captured once as a graph.
     cudaGraphExec_t iter_graph;
