@@ -20,7 +20,7 @@
 
 using vof::Geom;
 
-static_assert(sizeof(vof_params) == 136, "vof_params layout is part of the ABI");
+static_assert(sizeof(vof_params) == 144, "vof_params layout is part of the ABI");
 static_assert(VOF_PHASES == vof::PLAIN_PHASES, "phase count");
 static_assert(VOF_ADJ_AUTO == vof::ADJ_STORE_AUTO && VOF_ADJ_RECOMPUTE == vof::ADJ_STORE_RECOMPUTE &&
                   VOF_ADJ_KEEP == vof::ADJ_STORE_KEEP,
@@ -93,6 +93,7 @@ int validate(const vof_params* p) {
         return VOF_E_INVALID;
     if (p->mode != VOF_MODE_PLAIN && (!(p->tol > 0.0) || p->max_outer < 1 || p->max_outer > 100000))
         return VOF_E_INVALID;
+    if (p->surface_tension != 0 && p->surface_tension != 1) return VOF_E_INVALID;
     return VOF_OK;
 }
 
@@ -113,6 +114,8 @@ void free_ctx(vof_ctx* c) {
     if (c->b.p0) cudaFree(c->b.p0);
     if (c->b.p1) cudaFree(c->b.p1);
     if (c->b.p2) cudaFree(c->b.p2);
+    for (int q = 0; q < 4; ++q)
+        if (c->b.csf[q]) cudaFree(c->b.csf[q]);
     if (c->d_red_scratch) cudaFree(c->d_red_scratch);
     if (c->d_red_result) cudaFree(c->d_red_result);
     if (c->h_red_result) cudaFreeHost(c->h_red_result);
@@ -218,6 +221,7 @@ int vof_params_init(vof_params* p, int nx, int ny, int nz) {
     p->inner_sweeps = 32;
     p->max_outer = 200;
     p->tol = 1e-8;
+    p->surface_tension = 0;
     return vof_params_finalize(p);
 }
 
@@ -259,6 +263,8 @@ int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
     g.gx = p->gx;
     g.gy = p->gy;
     g.gz = p->gz;
+    g.csf = p->surface_tension;
+    g.sigma = p->sigma;
     if (!vof::plain_supported(g)) {
         free_ctx(c);
         return VOF_E_SIZE;
@@ -278,6 +284,7 @@ int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
     for (int f = 0; f < VOF_NUM_FIELDS - 1 && ok; ++f) ok = alloc((void**)&c->fields[f], fbytes);
     ok = ok && alloc((void**)&c->b.p0, fbytes) && alloc((void**)&c->b.p1, fbytes) &&
          alloc((void**)&c->b.p2, fbytes);
+    for (int q = 0; q < 4 && ok && g.csf; ++q) ok = alloc((void**)&c->b.csf[q], fbytes);
     ok = ok && alloc((void**)&c->d_red_scratch, sizeof(double) * vof::RED_SCRATCH_DOUBLES);
     ok = ok && alloc((void**)&c->d_red_result, sizeof(double) * vof::RED_RESULT_DOUBLES);
     ok = ok && alloc((void**)&c->d_status, sizeof(int));
@@ -515,6 +522,7 @@ int vof_solver_stats(const vof_ctx* ctx, int* outer, double* rel_initial, double
 
 int vof_forward_record(vof_ctx* ctx, int istep0, int nsteps, int checkpoint_every) {
     if (!ctx || nsteps < 1 || checkpoint_every < 0) return VOF_E_INVALID;
+    if (ctx->prm.surface_tension) return VOF_E_UNSUPPORTED;  // the adjoint has no surface-tension term
     DeviceGuard dg(ctx->device);
     cudaError_t e;
     if (!ctx->adj) {

@@ -66,6 +66,7 @@ int check_params(const vof_params* p) {
     if (!(p->dt > 0.0f) || !(p->dx > 0.0f) || !(p->dy > 0.0f) || !(p->dz > 0.0f)) return VOF_E_INVALID;
     if (p->jacobi_iters < 0 || p->jacobi_iters > 100000) return VOF_E_INVALID;
     if (p->mode != VOF_MODE_PLAIN) return VOF_E_UNSUPPORTED;
+    if (p->surface_tension != 0) return VOF_E_UNSUPPORTED;  // its fields would need allocation
     return VOF_OK;
 }
 
@@ -131,6 +132,7 @@ extern "C" int vof_step_noalloc(const vof_params* prm, float* F, float* u, float
         if (vof::jacobi_tb_maps(g, mapped[q], &maps[q]) != cudaSuccess) return VOF_E_UNSUPPORTED;
 
     vof::PlainBuffers b;
+    memset(&b, 0, sizeof(b));
     b.F = f[0];
     b.u = f[1];
     b.v = f[2];

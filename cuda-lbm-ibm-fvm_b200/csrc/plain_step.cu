@@ -142,6 +142,74 @@ __global__ void __launch_bounds__(256) k_predict(Geom g,
 }
 
 // ---------------------------------------------------------------------------
+// Continuum surface force (extension; no counterpart in the reference, whose
+// sigma no kernel reads).  J. U. Brackbill, D. B. Kothe, C. Zemach, "A
+// continuum method for modeling surface tension", J. Comput. Phys. 100 (1992):
+// the body force sigma kappa grad(F) with the interface normal n = grad F /
+// |grad F| and kappa = -div n, both by central differences at cell centres;
+// F's ghosts are the zero-gradient copies, and a normal beyond a wall is the
+// mirror image of the one inside (its wall-normal component negated: a 90
+// degree contact angle).  On a face, kappa is the mean of its two cells,
+// grad F their difference, and the acceleration is divided by the face
+// density of the correction, 0.5 (rho_a + rho_b); it is added to u*, v*, w*
+// on the faces the predictor updates.  FP32, operations in a fixed order.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_csf_normal(Geom g, const float* __restrict__ F, float* __restrict__ nx_,
+                                                    float* __restrict__ ny_, float* __restrict__ nz_) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.nx || j > g.ny || k > g.nz) return;
+    const int id = gidx(g, i, j, k);
+    const float hx = 0.5f * g.dxi, hy = 0.5f * g.dyi, hz = 0.5f * g.dzi;
+    const float gxv = (F[id + 1] - F[id - 1]) * hx;
+    const float gyv = (F[id + g.px] - F[id - g.px]) * hy;
+    const float gzv = (F[id + g.plane] - F[id - g.plane]) * hz;
+    const float mag = sqrtf(gxv * gxv + gyv * gyv + gzv * gzv);
+    const float eps = 1e-6f * g.dxi;
+    const bool has = mag > eps;
+    nx_[id] = has ? gxv / mag : 0.0f;
+    ny_[id] = has ? gyv / mag : 0.0f;
+    nz_[id] = has ? gzv / mag : 0.0f;
+}
+
+__global__ void __launch_bounds__(256) k_csf_curv(Geom g, const float* __restrict__ nx_,
+                                                  const float* __restrict__ ny_, const float* __restrict__ nz_,
+                                                  float* __restrict__ kap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.nx || j > g.ny || k > g.nz) return;
+    const int id = gidx(g, i, j, k);
+    const float hx = 0.5f * g.dxi, hy = 0.5f * g.dyi, hz = 0.5f * g.dzi;
+    // neighbours beyond a wall: the mirror image of the cell at the wall
+    const float xe = i < g.nx ? nx_[id + 1] : -nx_[id], xw = i > 1 ? nx_[id - 1] : -nx_[id];
+    const float yn = j < g.ny ? ny_[id + g.px] : -ny_[id], ys = j > 1 ? ny_[id - g.px] : -ny_[id];
+    const float zu = k < g.nz ? nz_[id + g.plane] : -nz_[id], zd = k > 1 ? nz_[id - g.plane] : -nz_[id];
+    kap[id] = -((xe - xw) * hx + (yn - ys) * hy + (zu - zd) * hz);
+}
+
+__device__ __forceinline__ float csf_accel(const Geom& g, float Fa, float Fb, float ka, float kb, float hinv) {
+    const float f = g.sigma * (0.5f * (ka + kb)) * ((Fb - Fa) * hinv);
+    const float r = 0.5f * (rho_of(g, Fa) + rho_of(g, Fb));
+    return f / r;
+}
+
+__global__ void __launch_bounds__(256) k_csf_force(Geom g, const float* __restrict__ F,
+                                                   const float* __restrict__ kap, float* __restrict__ us,
+                                                   float* __restrict__ vs, float* __restrict__ ws) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.nx || j > g.ny || k > g.nz) return;
+    const int id = gidx(g, i, j, k);
+    const float Fc = F[id], kc = kap[id];
+    if (i >= 2) us[id] = us[id] + g.dt * csf_accel(g, F[id - 1], Fc, kap[id - 1], kc, g.dxi);
+    if (j >= 2) vs[id] = vs[id] + g.dt * csf_accel(g, F[id - g.px], Fc, kap[id - g.px], kc, g.dyi);
+    if (k >= 2) ws[id] = ws[id] + g.dt * csf_accel(g, F[id - g.plane], Fc, kap[id - g.plane], kc, g.dzi);
+}
+
+// ---------------------------------------------------------------------------
 // Pressure right-hand side rho/dt * div(u*) (voftrial1.cu:418-422).  Without
 // FMA contraction the stored value is exactly the one the reference forms
 // inside every Jacobi sweep, so computing it once per step changes nothing.
@@ -392,7 +460,7 @@ static bool plan_buffers(int src, int dst, int L, int* seq) {
 }
 
 int plain_kernels_per_step(const Geom& g, int jacobi_iters) {
-    return 1 + 1 + jacobi_launches(g, jacobi_iters) + 1 + 3;
+    return 1 + (g.csf ? 3 : 0) + 1 + jacobi_launches(g, jacobi_iters) + 1 + 3;
 }
 
 // Column-marching launch shape: 32 x 8 columns per block, z split into
@@ -423,6 +491,13 @@ cudaError_t plain_front(const Geom& g, const PlainBuffers& b, cudaStream_t s, cu
     cudaError_t e;
     if ((e = mark(ev, 0, s)) != cudaSuccess) return e;
     k_predict<<<grid, blk, 0, s>>>(g, b.F, b.u, b.v, b.w, b.us, b.vs, b.ws, kchunk);
+    if (g.csf && b.csf[0]) {  // surface tension (extension): normals, curvature, face accelerations
+        const dim3 cb(32, 4, 2);
+        const dim3 cg((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + 1) / 2);
+        k_csf_normal<<<cg, cb, 0, s>>>(g, b.F, b.csf[0], b.csf[1], b.csf[2]);
+        k_csf_curv<<<cg, cb, 0, s>>>(g, b.csf[0], b.csf[1], b.csf[2], b.csf[3]);
+        k_csf_force<<<cg, cb, 0, s>>>(g, b.F, b.csf[3], b.us, b.vs, b.ws);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(ev, 1, s)) != cudaSuccess) return e;
     k_rhs<<<grid, blk, 0, s>>>(g, b.F, b.us, b.vs, b.ws, b.rhs, kchunk);
     if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(ev, 2, s)) != cudaSuccess) return e;
@@ -507,7 +582,8 @@ cudaError_t plain_step(const Geom& g, const PlainBuffers& b, int istep, int jaco
 }
 
 int plain_phase_launches(const Geom& g, int phase, int jacobi_iters) {
-    return phase == PHASE_JACOBI ? jacobi_launches(g, jacobi_iters) : 1;
+    if (phase == PHASE_JACOBI) return jacobi_launches(g, jacobi_iters);
+    return (phase == PHASE_PREDICT && g.csf) ? 4 : 1;
 }
 
 }  // namespace vof

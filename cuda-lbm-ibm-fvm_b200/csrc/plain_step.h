@@ -22,6 +22,7 @@ struct PlainBuffers {
     float* p2;   // scratch pressure buffer for the blocked sweeps
     const CUtensorMap* maps;  // TMA descriptors of p0, p1, p2, rhs (in that order)
     int* status;              // device status word (DEV_* codes, tma.cuh)
+    float* csf[4];            // g.csf: interface normal x, y, z and curvature per cell; else null
 };
 
 // Raise the dynamic shared-memory limit of the FCT kernels for lines of up to

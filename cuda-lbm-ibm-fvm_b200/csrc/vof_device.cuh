@@ -24,6 +24,9 @@ struct Geom {
     // 0.5*(rho_a + rho_b) for the pure-phase pairs (gas-gas, liquid-liquid,
     // gas-liquid) and dt divided by each, formed on the device at set-up.
     float rpair[3], qpair[3];
+    // continuum surface force (extension, off unless csf): sigma from Params
+    int csf;
+    float sigma;
 };
 
 __host__ __device__ __forceinline__ int gidx(const Geom& g, int i, int j, int k) {

@@ -54,6 +54,7 @@ class Params(C.Structure):
         ("nTot", C.c_int),
         ("jacobi_iters", C.c_int), ("mode", C.c_int), ("inner_sweeps", C.c_int),
         ("max_outer", C.c_int), ("tol", C.c_double),
+        ("surface_tension", C.c_int),
     ]
 
     @property

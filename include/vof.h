@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define VOF_ABI_VERSION 1
+#define VOF_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 #define VOF_OK               0
@@ -97,6 +97,10 @@ typedef struct vof_params {
                                wider than 25 cells, 8 below); vof_params_init sets 32, unused */
     int max_outer;          /* mixed/fp64 modes: cap on defect-correction iterations        */
     double tol;             /* mixed/fp64 modes: target ||b-Ap||/||b|| (default 1e-8)       */
+    int surface_tension;    /* 1: add the continuum-surface-force acceleration sigma kappa
+                               grad(F) / rho to u*, v*, w* after the predictor (an extension:
+                               the reference has no surface tension, so 1 departs from it);
+                               0 (default): the reference's step                             */
 } vof_params;
 
 typedef struct vof_ctx vof_ctx;

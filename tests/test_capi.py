@@ -26,14 +26,19 @@ def test_library_exports_every_declared_symbol(V):
 
 
 def test_abi_version(V):
-    assert V.lib().vof_abi_version() == 1
+    assert V.lib().vof_abi_version() == 2
 
 
 def test_params_struct_layout(V):
-    # vof_params: 9 int + 18 float + int nTot + 4 int + double, natural alignment
-    assert C.sizeof(V.Params) == 136
+    # vof_params: 9 int + 18 float + int nTot + 4 int + double + int, natural alignment
+    assert C.sizeof(V.Params) == 144
     assert V.Params.tol.offset == 128
     assert V.Params.nTot.offset == 108
+    assert V.Params.surface_tension.offset == 136
+
+
+def test_params_init_leaves_surface_tension_off(V):
+    assert V.default_params(8).surface_tension == 0
 
 
 def test_params_init_matches_reference_constants(V):
