@@ -296,6 +296,7 @@ struct Options {
     Vtk vtk = Vtk::Ascii;
     int threads = 0;
     bool ic_only = false;
+    float sigma = -1.0f;  // < 0: no surface-tension term (the reference's step)
 };
 
 void usage() {
@@ -309,6 +310,7 @@ void usage() {
               << "  --dt DT              time step (default 4e-6)\n"
               << "  --jacobi N           Jacobi sweeps per step in plain mode (default 10)\n"
               << "  --mode M             plain | mixed | fp64 (default plain)\n"
+              << "  --surface-tension S  add the continuum-surface-force term with sigma S (N/m)\n"
               << "  --out DIR            dump directory (default output)\n"
               << "  --vtk K              ascii (the reference's format) | binary | none\n"
               << "  --threads N          formatting threads for ASCII dumps (default: hardware)\n"
@@ -340,6 +342,9 @@ int parse(int argc, char** argv, Options& o) {
             else if (m == "mixed") o.mode = VOF_MODE_MIXED;
             else if (m == "fp64") o.mode = VOF_MODE_FP64;
             else return -1;
+        } else if (arg == "--surface-tension" && need(1)) {
+            o.sigma = std::strtof(argv[++a], nullptr);
+            if (!(o.sigma >= 0.0f)) return -1;
         } else if (arg == "--out" && need(1)) o.out = argv[++a];
         else if (arg == "--vtk" && need(1)) {
             const std::string k = argv[++a];
@@ -416,6 +421,10 @@ int main(int argc, char** argv) {
     p.dt = o.dt;
     p.jacobi_iters = o.jacobi;
     p.mode = o.mode;
+    if (o.sigma >= 0.0f) {
+        p.sigma = o.sigma;
+        p.surface_tension = 1;
+    }
     if ((st = vof_params_finalize(&p)) != VOF_OK) return fail("vof_params_finalize", st, nullptr);
 
     // the initial F in the reference layout, then apply_bc_F once (voftrial1.cu:1334-1337)

@@ -83,7 +83,8 @@ typedef struct vof_params {
     float Lx, Ly, Lz;
     float rho_l, rho_g;
     float nu_l, nu_g;
-    float sigma;            /* stored and reported; no kernel reads it (as in the reference) */
+    float sigma;            /* stored and reported; read only by the optional surface-tension
+                               term (surface_tension = 1; the reference's kernels never read it) */
     float gx, gy, gz;
     float dt;
     float dx, dy, dz;

@@ -118,7 +118,7 @@ def test_binary_dump_and_ic_file(V, tmp_path):
 
 def test_help_lists_the_reference_options():
     out = drive("--help").stdout
-    for opt in ("-ic", "--nstep", "--max_steps", "--grid", "--vtk", "--mode"):
+    for opt in ("-ic", "--nstep", "--max_steps", "--grid", "--vtk", "--mode", "--surface-tension"):
         assert opt in out
 
 
