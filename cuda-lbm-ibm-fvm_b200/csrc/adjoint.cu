@@ -1648,9 +1648,11 @@ cudaError_t replay_step_keep(AdjEngine& e, int istep, const AdjMid& mid, const f
     const int* dirs = sweep_order(istep);
     const float* velof[3] = {b.u, b.v, b.w};
     if ((r = fct_launch_to(g, dirs[0], false, Fin, mid.f[3], velof[dirs[0]], s)) != cudaSuccess ||
-        (r = fct_launch_to(g, dirs[1], false, mid.f[3], mid.f[4], velof[dirs[1]], s)) != cudaSuccess ||
-        (r = fct_launch_to(g, dirs[2], true, mid.f[4], Fout, velof[dirs[2]], s)) != cudaSuccess)
+        (r = fct_launch_to(g, dirs[1], false, mid.f[3], mid.f[4], velof[dirs[1]], s)) != cudaSuccess)
         return r;
+    // the step's final F: the next step's input (a reversed step reads only
+    // F before each sweep); Fout == nullptr when no step follows
+    if (Fout && (r = fct_launch_to(g, dirs[2], true, mid.f[4], Fout, velof[dirs[2]], s)) != cudaSuccess) return r;
     return cudaSuccess;
 }
 
@@ -1999,13 +2001,13 @@ bool adj_can_record_tail(const AdjEngine& e) { return e.keep && !e.conv && e.jac
 // buffers (last step); the pressure after the sweeps is copied into segment
 // state q + 1.  *pa: where that pressure is afterwards.
 static cudaError_t replay_kept(AdjEngine& e, int first, int count, int q, int* par, const float** pa,
-                               cudaStream_t s) {
+                               cudaStream_t s, bool final_F = true) {
     float* const* vs = q == 0 ? nullptr : e.seg[q].f + 1;
     float* const vin[3] = {q == 0 ? e.wb.u : vs[0], q == 0 ? e.wb.v : vs[1], q == 0 ? e.wb.w : vs[2]};
     float* const* vn = q + 1 < count ? e.seg[q + 1].f + 1 : nullptr;
     float* const vout[3] = {vn ? vn[0] : e.wb.u, vn ? vn[1] : e.wb.v, vn ? vn[2] : e.wb.w};
     const float* Fin = q == 0 ? e.wb.F : e.seg[q].f[0];
-    float* Fout = q + 1 < count ? e.seg[q + 1].f[0] : e.wb.F;
+    float* Fout = q + 1 < count ? e.seg[q + 1].f[0] : (final_F ? e.wb.F : nullptr);
     cudaError_t r = replay_step_keep(e, e.istep0 + first + q, e.mid[q], Fin, Fout, vin, vout, par, pa, s);
     if (r == cudaSuccess && q + 1 < count) {
         r = copy_field(e.seg[q + 1].f[4], *pa, e.elems, s);
@@ -2083,8 +2085,8 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
                 for (int q = 0; q < count; ++q) pa[q] = q + 1 < count ? e->seg[q + 1].f[4] : e->tail_p;
                 e->tail_kept = false;  // the engine's buffers are reused from here on
             } else {
-                for (int q = 0; q < count && r == cudaSuccess; ++q)
-                    r = replay_kept(*e, first, count, q, &par, &pa[q], s);
+                for (int q = 0; q < count && r == cudaSuccess; ++q)  // (the segment's final F is not needed)
+                    r = replay_kept(*e, first, count, q, &par, &pa[q], s, false);
             }
             // reverse: step q's next state is seg[q + 1], or the replay's
             // buffers after the segment's last step
