@@ -1866,8 +1866,10 @@ static void free_tape(AdjEngine* e) {
     free_states(e->cp, e->ncp);
     free_states(e->seg, e->every);
     free_mid(e->mid, e->every);
-    e->cp = e->seg = nullptr;
-    e->mid = nullptr;
+    free_states(e->seg2, e->every);
+    free_mid(e->mid2, e->every);
+    e->cp = e->seg = e->seg2 = nullptr;
+    e->mid = e->mid2 = nullptr;
     e->ncp = 0;
     e->keep = 0;
     e->tape_bytes = 0;
@@ -1978,12 +1980,40 @@ cudaError_t adj_tape(AdjEngine* e, int istep0, int nsteps, int every, cudaStream
             return r;
         if (keep && (r = alloc_mid(e->mid, every, e->elems, &e->tape_bytes, s)) != cudaSuccess) return r;
     }
+    // a second kept segment, where the record can keep one and memory allows
+    // (a tape that keeps intermediates, FP32 Jacobi with an even sweep count)
+    const bool want2 = keep && !e->conv && e->jacobi_iters % 2 == 0 && ncp >= 2;
+    if (!want2 && e->seg2) {
+        free_states(e->seg2, e->every);
+        free_mid(e->mid2, e->every);
+        e->seg2 = nullptr;
+        e->mid2 = nullptr;
+    }
+    if (want2 && !e->seg2) {
+        size_t fr = 0, tot = 0;
+        const size_t need2 = (size_t)(2 * every - 1) * 5 * fb;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && need2 + tot / 32 <= fr) {
+            size_t b2 = 0;
+            r = alloc_states(e->seg2, every, 1, e->elems, false, &b2);
+            if (r == cudaSuccess) r = alloc_mid(e->mid2, every, e->elems, &b2, s);
+            if (r != cudaSuccess) {  // (only an optimisation: go without it)
+                free_states(e->seg2, e->every);
+                free_mid(e->mid2, e->every);
+                e->seg2 = nullptr;
+                e->mid2 = nullptr;
+                cudaGetLastError();
+            } else {
+                e->tape_bytes += b2;
+            }
+        }
+    }
     e->istep0 = istep0;
     e->nsteps = nsteps;
     e->every = every;
     e->recorded = false;
     e->tail_kept = false;
     e->tail_p = nullptr;
+    e->kept2 = false;
     return cudaSuccess;
 }
 
@@ -1997,21 +2027,22 @@ bool adj_can_record_tail(const AdjEngine& e) { return e.keep && !e.conv && e.jac
 
 // One step of a kept segment replay: step q of the segment that starts at
 // `first` (count steps), from the engine's buffers (q == 0: loaded from the
-// checkpoint) or segment state q, into segment state q + 1 or the engine's
-// buffers (last step); the pressure after the sweeps is copied into segment
-// state q + 1.  *pa: where that pressure is afterwards.
-static cudaError_t replay_kept(AdjEngine& e, int first, int count, int q, int* par, const float** pa,
-                               cudaStream_t s, bool final_F = true) {
-    float* const* vs = q == 0 ? nullptr : e.seg[q].f + 1;
+// checkpoint) or segment state seg[q], into seg[q + 1] or the engine's
+// buffers (last step), keeping its intermediates in mid[q]; the pressure after
+// the sweeps is copied into seg[q + 1].  *pa: where that pressure is
+// afterwards.
+static cudaError_t replay_kept(AdjEngine& e, AdjState* seg, AdjMid* mid, int first, int count, int q, int* par,
+                               const float** pa, cudaStream_t s, bool final_F = true) {
+    float* const* vs = q == 0 ? nullptr : seg[q].f + 1;
     float* const vin[3] = {q == 0 ? e.wb.u : vs[0], q == 0 ? e.wb.v : vs[1], q == 0 ? e.wb.w : vs[2]};
-    float* const* vn = q + 1 < count ? e.seg[q + 1].f + 1 : nullptr;
+    float* const* vn = q + 1 < count ? seg[q + 1].f + 1 : nullptr;
     float* const vout[3] = {vn ? vn[0] : e.wb.u, vn ? vn[1] : e.wb.v, vn ? vn[2] : e.wb.w};
-    const float* Fin = q == 0 ? e.wb.F : e.seg[q].f[0];
-    float* Fout = q + 1 < count ? e.seg[q + 1].f[0] : (final_F ? e.wb.F : nullptr);
-    cudaError_t r = replay_step_keep(e, e.istep0 + first + q, e.mid[q], Fin, Fout, vin, vout, par, pa, s);
+    const float* Fin = q == 0 ? e.wb.F : seg[q].f[0];
+    float* Fout = q + 1 < count ? seg[q + 1].f[0] : (final_F ? e.wb.F : nullptr);
+    cudaError_t r = replay_step_keep(e, e.istep0 + first + q, mid[q], Fin, Fout, vin, vout, par, pa, s);
     if (r == cudaSuccess && q + 1 < count) {
-        r = copy_field(e.seg[q + 1].f[4], *pa, e.elems, s);
-        *pa = e.seg[q + 1].f[4];
+        r = copy_field(seg[q + 1].f[4], *pa, e.elems, s);
+        *pa = seg[q + 1].f[4];
     }
     return r;
 }
@@ -2023,7 +2054,8 @@ cudaError_t adj_record_tail(AdjEngine* e, const AdjState& out, float* const extr
     cudaError_t r = load_state(*e, e->cp[m], s);
     int par = 0;
     const float* pa = nullptr;
-    for (int q = 0; q < count && r == cudaSuccess; ++q) r = replay_kept(*e, first, count, q, &par, &pa, s);
+    for (int q = 0; q < count && r == cudaSuccess; ++q)
+        r = replay_kept(*e, e->seg, e->mid, first, count, q, &par, &pa, s);
     if (r != cudaSuccess) return r;
     const float* src[5] = {e->wb.F, e->wb.u, e->wb.v, e->wb.w, pa};
     for (int q = 0; q < 5; ++q)
@@ -2033,6 +2065,25 @@ cudaError_t adj_record_tail(AdjEngine* e, const AdjState& out, float* const extr
         if (extra[q] && (r = copy_field(extra[q], xs[q], e->elems, s)) != cudaSuccess) return r;
     e->tail_kept = true;
     e->tail_p = pa;
+    return cudaSuccess;
+}
+
+bool adj_can_keep2(const AdjEngine& e) { return adj_can_record_tail(e) && e.ncp >= 2 && e.seg2 && e.mid2; }
+
+cudaError_t adj_record_keep2(AdjEngine* e, const AdjState& out, cudaStream_t s) {
+    if (!adj_can_keep2(*e)) return cudaErrorNotSupported;
+    const int m = e->ncp - 2;
+    const int first = adj_segment_first(*e, m), count = adj_segment_first(*e, m + 1) - first;
+    cudaError_t r = load_state(*e, e->cp[m], s);
+    int par = 0;
+    const float* pa = nullptr;
+    for (int q = 0; q < count && r == cudaSuccess; ++q)
+        r = replay_kept(*e, e->seg2, e->mid2, first, count, q, &par, &pa, s);
+    if (r != cudaSuccess) return r;
+    const float* src[5] = {e->wb.F, e->wb.u, e->wb.v, e->wb.w, pa};
+    for (int q = 0; q < 5; ++q)
+        if ((r = copy_field(out.f[q], src[q], e->elems, s)) != cudaSuccess) return r;
+    e->kept2 = true;
     return cudaSuccess;
 }
 
@@ -2074,28 +2125,37 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
         if (e->keep) {
             // replay every step of the segment from checkpoint m, keeping its
             // intermediates and the states after steps 0 .. count - 2; the
-            // record did so already for the last segment when tail_kept
+            // record did so already for the last segment when tail_kept, and
+            // for the one before it in seg2 / mid2 when kept2
             const bool tail = m == e->ncp - 1 && e->tail_kept;
-            if (!tail && (r = load_state(*e, e->cp[m], s)) != cudaSuccess) return r;
+            const bool k2 = m == e->ncp - 2 && e->kept2;
+            AdjState* const seg = k2 ? e->seg2 : e->seg;
+            AdjMid* const mid = k2 ? e->mid2 : e->mid;
+            // the state after the segment's last step: the replay's buffers,
+            // or checkpoint m + 1 for seg2
+            const AdjState wbs{{e->wb.F, e->wb.u, e->wb.v, e->wb.w, nullptr}, nullptr};
+            const AdjState& after = k2 ? e->cp[m + 1] : wbs;
+            if (!tail && !k2 && (r = load_state(*e, e->cp[m], s)) != cudaSuccess) return r;
             int par = 0;
             const float* pafter[64];
             const float** pa = count <= 64 ? pafter : new (std::nothrow) const float*[count];
             if (!pa) return cudaErrorMemoryAllocation;
-            if (tail) {
-                for (int q = 0; q < count; ++q) pa[q] = q + 1 < count ? e->seg[q + 1].f[4] : e->tail_p;
-                e->tail_kept = false;  // the engine's buffers are reused from here on
+            if (tail || k2) {
+                for (int q = 0; q < count; ++q)
+                    pa[q] = q + 1 < count ? seg[q + 1].f[4] : (k2 ? after.f[4] : e->tail_p);
+                if (tail) e->tail_kept = false;  // the engine's buffers are reused from here on
             } else {
                 for (int q = 0; q < count && r == cudaSuccess; ++q)  // (the segment's final F is not needed)
-                    r = replay_kept(*e, first, count, q, &par, &pa[q], s, false);
+                    r = replay_kept(*e, seg, mid, first, count, q, &par, &pa[q], s, false);
             }
-            // reverse: step q's next state is seg[q + 1], or the replay's
-            // buffers after the segment's last step
+            // reverse: step q's next state is seg[q + 1], or `after` for the
+            // segment's last step
             for (int q = count - 1; q >= 0 && r == cudaSuccess; --q) {
-                const AdjState& x = q == 0 ? e->cp[m] : e->seg[q];
-                const AdjMid& md = e->mid[q];
-                const float* nu = q + 1 < count ? e->seg[q + 1].f[1] : e->wb.u;
-                const float* nv = q + 1 < count ? e->seg[q + 1].f[2] : e->wb.v;
-                const float* nw = q + 1 < count ? e->seg[q + 1].f[3] : e->wb.w;
+                const AdjState& x = q == 0 ? e->cp[m] : seg[q];
+                const AdjMid& md = mid[q];
+                const float* nu = q + 1 < count ? seg[q + 1].f[1] : after.f[1];
+                const float* nv = q + 1 < count ? seg[q + 1].f[2] : after.f[2];
+                const float* nw = q + 1 < count ? seg[q + 1].f[3] : after.f[3];
                 const StepData d{x.f[0], x.f[1], x.f[2], x.f[3], md.f[0], md.f[1], md.f[2], pa[q],
                                  {nu, nv, nw}, {x.f[0], md.f[3], md.f[4]}};
                 r = reverse_step(*e, d, e->istep0 + first + q, s);

@@ -71,6 +71,13 @@ struct AdjEngine {
     // that segment's last pressure (an engine buffer)
     bool tail_kept;
     const float* tail_p;
+    // a second set of segment states and intermediates (null unless the tape
+    // keeps intermediates and memory allows): the record keeps the segment
+    // before the last one there too (kept2), so the reverse pass replays
+    // neither of the last two segments
+    AdjState* seg2;
+    AdjMid* mid2;
+    bool kept2;
     size_t tape_bytes;       // device bytes of the tape
     bool recorded;
     // recompute buffers (FP32)
@@ -128,6 +135,15 @@ bool adj_can_record_tail(const AdjEngine& e);
 // `out` (F, u, v, w, p) and the last step's u*, v*, w*, rhs to extra[0..3].
 // The reverse pass then starts on this segment without a replay.
 cudaError_t adj_record_tail(AdjEngine* e, const AdjState& out, float* const extra[4], cudaStream_t s);
+
+// Whether the record may also keep the segment before the last one
+// (adj_record_keep2): adj_can_record_tail, at least two segments, seg2/mid2.
+bool adj_can_keep2(const AdjEngine& e);
+
+// The record's segment ncp - 2, from checkpoint ncp - 2 (saved before), run
+// like adj_record_tail into seg2 / mid2; the final state goes to `out`.  The
+// record then saves checkpoint ncp - 1 from `out` and runs adj_record_tail.
+cudaError_t adj_record_keep2(AdjEngine* e, const AdjState& out, cudaStream_t s);
 
 // Reverse the recorded run: L = sum over the box of F dV of the final state
 // `fin`; afterwards lF, lu, lv, lw, lp[lp_cur] hold dL/d(initial state) and
