@@ -247,7 +247,11 @@ int vof_solver_stats(const vof_ctx* ctx, int* outer, double* rel_initial, double
  * states of five fields (and the FP64 pressure in the convergent modes), plus
  * the engine's work fields (allocated once); with the intermediates kept
  * (vof_adjoint_storage), every - 1 segment states of five FP32 fields and
- * every x five FP32 intermediate fields instead of every segment states.  In VOF_MODE_MIXED / FP64 the
+ * every x five FP32 intermediate fields instead of every segment states; in
+ * the plain mode with an even jacobi_iters, when 1/32 of the device memory
+ * stays free, as much again for a second kept segment (the record then runs
+ * the last two segments as the reverse pass would replay them, and that pass
+ * replays neither).  In VOF_MODE_MIXED / FP64 the
  * pressure is taken as the exact solution of the mean-free system (its
  * adjoint is the same solve on the pressure's adjoint, to prm.tol; the state
  * pressure, only a warm start, gets a zero adjoint).
