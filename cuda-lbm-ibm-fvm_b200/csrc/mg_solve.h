@@ -20,7 +20,7 @@ constexpr int MG_MAX_NU = 8;
 constexpr int MG_COARSE_SWEEPS = 100;   // sweeps on a coarsest level too large for the dense solve
 constexpr int MG_MAX_LEVELS = 16;
 constexpr int MG_TAIL_CELLS = 4096;     // largest level that may run inside the one-block kernel
-constexpr int MG_TAIL_SMEM = 200 * 1024;  // shared-memory budget of the one-block kernel
+constexpr int MG_TAIL_SMEM = 200 * 1024;  // shared-memory limit of the one-block kernel
 constexpr int MG_DENSE_MAX = 128;       // coarsest levels this small are solved exactly
 constexpr int MG_BX = 32, MG_BY = 8;    // block of the multi-block level kernels
 constexpr int MG_FLAT_THREADS = 256;    // block of the flat BF16 kernels (consecutive pairs or cells of a plane)
