@@ -225,7 +225,18 @@ int vof_params_init(vof_params* p, int nx, int ny, int nz) {
     return vof_params_finalize(p);
 }
 
+// vof_debug_fail_alloc's setting: the number of the allocation of the next
+// vof_create that fails (-1: none).
+static int g_fail_alloc_at = -1;
+
+int vof_debug_fail_alloc(int n) {
+    g_fail_alloc_at = n < 0 ? -1 : n;
+    return VOF_OK;
+}
+
 int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
+    const int fail_at = g_fail_alloc_at;  // (consumed by this call)
+    g_fail_alloc_at = -1;
     if (!out) return VOF_E_INVALID;
     *out = nullptr;
     int st = validate(p);
@@ -272,7 +283,9 @@ int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
 
     c->elems = (size_t)g.plane * (size_t)(p->nz + 2);
     const size_t fbytes = c->elems * sizeof(float);
+    int alloc_no = 0;
     auto alloc = [&](void** ptr, size_t bytes) -> bool {
+        if (alloc_no++ == fail_at) return false;  // injected (vof_debug_fail_alloc)
         if (cudaMalloc(ptr, bytes) != cudaSuccess) {
             cudaGetLastError();
             return false;

@@ -296,6 +296,16 @@ int vof_adjoint_keeps(const vof_ctx* ctx);
 /* cudaError_t of the most recent failing CUDA call in this context (0 if none). */
 int vof_last_cuda_error(const vof_ctx* ctx);
 
+/* Fault injection for tests; no counterpart in the reference, whose set-up
+ * (alloc_field, voftrial1.cu:1176-1203) exits on the first failing
+ * cudaMalloc.  The context's own device allocations in the next vof_create
+ * are numbered from 0; the one numbered n fails as if the device were out of
+ * memory, and vof_create frees what it had allocated and returns
+ * VOF_E_NOMEM.  That vof_create consumes the setting whether it fires or
+ * not; n < 0 clears it.  Process-wide and not thread-safe: set it from the
+ * thread that calls vof_create. */
+int vof_debug_fail_alloc(int n);
+
 /* Number of kernel launches one vof_step enqueues for the current settings. */
 int vof_kernels_per_step(const vof_ctx* ctx);
 

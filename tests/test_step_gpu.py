@@ -383,3 +383,63 @@ def test_full_size_dam_break_vs_reference_kernels(cuda, V, orc):
         assert rel_l2(pm - pm.mean(), qm - qm.mean()) <= 1e-5
         vol = lambda F: float(F[1:-1, 1:-1, 1:-1].astype(np.float64).sum())  # noqa: E731
         assert abs(vol(got["F"]) - vol(ref["F"])) <= 1e-7 * vol(ref["F"])
+
+
+def test_allocation_failure_in_create(cuda, V, tmp_path):
+    """Each device allocation of vof_create made to fail in turn
+    (vof_debug_fail_alloc, a host-side fake of an out-of-memory cudaMalloc):
+    VOF_E_NOMEM and no context, nothing left allocated (device free memory
+    back to within 16 MiB of what it was: less than one 160^3 field, 19.2
+    MiB), and the next vof_create, which finds no setting left, works.  In a child process, so
+    that the free-memory count sees only these contexts."""
+    import json
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parent.parent
+    out = tmp_path / "alloc.json"
+    code = f"""
+import ctypes as C, json, sys
+sys.path.insert(0, {str(root / 'cuda-lbm-ibm-fvm_b200')!r})
+import torch
+import vof_b200 as V
+lib = V.lib()
+torch.cuda.mem_get_info(0)  # (torch's own CUDA set-up before any count)
+res = {{}}
+for name, kw in (("plain", {{}}), ("csf", {{"surface_tension": 1}}), ("mixed", {{"mode": V.MODE_MIXED}})):
+    prm = V.default_params(160, **kw)
+    ctx = C.c_void_p()
+    assert lib.vof_create(C.byref(prm), None, C.byref(ctx)) == 0
+    if name == "plain":
+        assert lib.vof_step(ctx, 1) == 0 and lib.vof_sync(ctx) == 0
+    lib.vof_destroy(ctx)
+    free0 = torch.cuda.mem_get_info(0)[0]
+    n = 0
+    while True:
+        lib.vof_debug_fail_alloc(n)
+        ctx = C.c_void_p()
+        rc = lib.vof_create(C.byref(prm), None, C.byref(ctx))
+        if rc == 0:
+            break
+        assert rc == V.E_NOMEM and not ctx.value, (name, n, rc)
+        n += 1
+        assert n < 64, name
+    if name == "plain":
+        assert lib.vof_step(ctx, 1) == 0 and lib.vof_sync(ctx) == 0
+    lib.vof_destroy(ctx)
+    ctx = C.c_void_p()
+    assert lib.vof_create(C.byref(prm), None, C.byref(ctx)) == 0
+    lib.vof_destroy(ctx)
+    res[name] = [n, free0 - torch.cuda.mem_get_info(0)[0]]
+json.dump(res, open({str(out)!r}, "w"))
+"""
+    subprocess.run([sys.executable, "-c", code], env=dict(os.environ), check=True, timeout=600)
+    res = json.loads(out.read_text())
+    n_plain = res["plain"][0]
+    assert n_plain >= 10
+    assert res["csf"][0] == n_plain + 4  # the four surface-tension fields
+    assert res["mixed"][0] == n_plain + 1  # the FP64 pressure
+    for name, (n, leaked) in res.items():
+        assert leaked < 16 * 2**20, (name, leaked)
