@@ -79,6 +79,8 @@ def parse_args(argv=None):
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--n", type=int, default=200, help="grid cells per side (default 200)")
     ap.add_argument("--profile-steps", type=int, default=6)
+    ap.add_argument("--repeats", type=int, default=3,
+                    help="extra K-step regions timed after the reported one (diagnostic spread)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0,
                     help="target CPU time of the CPU-baseline sample (0 disables)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -128,6 +130,13 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_first(self, timeout: float = 3.0):
+        """Block until the sampler has produced its first line (nvidia-smi
+        start-up is done), so that it does not start inside a timed region."""
+        t0 = time.perf_counter()
+        while self.proc is not None and not self.lines and time.perf_counter() - t0 < timeout:
+            time.sleep(0.01)
+
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
@@ -168,10 +177,15 @@ def summarize_clocks(lines) -> dict:
 # ---------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------
-def workload_params(V, n):
-    # 0.1 m box, rho 1000/50, nu 1e-6/1.5e-5, dt 4e-6, 10 Jacobi sweeps; gravity
-    # -9.81 along z (the reference's kernels add gx,gy,gz from the parameters).
-    return V.default_params(n, gx=0.0, gy=0.0, gz=-9.81)
+def workload_params(n, **over):
+    """0.1 m box, rho 1000/50, nu 1e-6/1.5e-5, dt 4e-6, 10 Jacobi sweeps;
+    gravity -9.81 along z (the reference's kernels add gx, gy, gz from the
+    parameters).  Filled on the host (vof_b200.params, checked against the
+    library's vof_params_init by a CPU test), so the reference arm never maps
+    the library."""
+    from vof_b200.params import host_params
+
+    return host_params(n, gx=0.0, gy=0.0, gz=-9.81, **over)
 
 
 def workload_state(prm):
@@ -502,7 +516,7 @@ def run_ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
 
-    prm = workload_params(V, args.n)
+    prm = workload_params(args.n)
     state = workload_state(prm)
     cells = prm.nx * prm.ny * prm.nz
     K, W = args.steps, max(3, args.warmup)
@@ -520,10 +534,11 @@ def run_ours(args):
     solver.run(istep, W)  # warm-up; also captures the three per-order graphs
     istep += W
 
-    barrier(world, dev)
-    torch.cuda.synchronize(dev)
     clocks = ClockSampler(gpu_id)
     clocks.start()
+    clocks.wait_first()
+    barrier(world, dev)
+    torch.cuda.synchronize(dev)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -531,11 +546,30 @@ def run_ours(args):
     e1.record(stream)
     e1.synchronize()
     torch.cuda.synchronize(dev)
-    clk = clocks.stop()
     barrier(world, dev)
     ms = e0.elapsed_time(e1)
     istep += K
     ms_max, value = replica_throughput(world, cells, K, ms, dev)
+    # the same K-step region again (diagnostic: spread between regions) and
+    # single steps one by one (launch-to-launch variation)
+    repeats = []
+    for _ in range(max(0, args.repeats)):
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        solver.run(istep, K)
+        e1.record(stream)
+        e1.synchronize()
+        repeats.append(round(e0.elapsed_time(e1) / K, 5))
+        istep += K
+    singles = []
+    for _ in range(25):
+        e0.record(stream)
+        solver.run(istep, 1)
+        e1.record(stream)
+        e1.synchronize()
+        singles.append(round(e0.elapsed_time(e1), 4))
+        istep += 1
+    clk = clocks.stop()
     vol = solver.reduce("volume")
     nonfinite = solver.reduce("nonfinite")
 
@@ -577,24 +611,31 @@ def run_ours(args):
         t0 = time.perf_counter()
         a0 = torch.cuda.Event(enable_timing=True)
         a1 = torch.cuda.Event(enable_timing=True)
+        au = torch.cuda.Event(enable_timing=True)
+        ad = torch.cuda.Event(enable_timing=True)
         a0.record(stream)
         for k in V.STATE_FIELDS:
             solver2._check(lib.vof_upload(solver2._ctx, V.FIELDS[k], C.c_void_p(host[k].data_ptr()), 0),
                            "vof_upload")
+        au.record(stream)
         vptr = vols.data_ptr()
         for s in range(K):
             solver2.run(1 + s, 1)
             solver2.reduce_async("volume", vptr + 8 * s)
+        ad.record(stream)
         solver2.download("F", Fout.numpy())  # synchronizes the stream
         a1.record(stream)
         a1.synchronize()
         wall = time.perf_counter() - t0
         e2e_ms, e2e_value = replica_throughput(world, cells, K, a0.elapsed_time(a1), dev)
+        up_ms, dn_ms = a0.elapsed_time(au), ad.elapsed_time(a1)
         solver2.close()
         nbytes = prm.nTot * 4
         e2e = {"value": round(e2e_value, 1), "unit": UNIT,
                "h2d_bytes_per_step": 5 * nbytes / K, "d2h_bytes_per_step": (nbytes + 8 * K) / K,
                "ms": round(e2e_ms, 3), "wall_ms": round(wall * 1e3, 3),
+               "upload_ms": round(up_ms, 3), "upload_gbs": round(5 * nbytes / up_ms / 1e6, 1),
+               "download_ms": round(dn_ms, 3), "download_gbs": round(nbytes / dn_ms / 1e6, 1),
                "api": "vof_upload x5 (pinned) + K x (vof_run 1 step + vof_reduce_async volume) + vof_download F",
                "final_volume": float(vols[-1])}
 
@@ -623,6 +664,8 @@ def run_ours(args):
         "roofline": roofline, "step_roofline": step_roofline,
         "cpu_baseline": cpu, "clocks": clk, "e2e": e2e,
         "gpu_launches": solver.kernels_per_step * K,
+        "repeat_ms_per_step": repeats, "single_step_ms": singles,
+        "native_so_loaded": mapped_libraries(),
         "phases_ms": {k: round(v, 5) for k, v in phase_ms.items()},
         "phase_launches": phase_launches,
         "check": {"volume_after": vol, "nonfinite": nonfinite},
@@ -644,11 +687,11 @@ def run_ours(args):
 SMALL_GRIDS = ((32, 200), (64, 200))
 
 
-def small_state(V, n):
+def small_state(n):
     """The dam break with a flat interface (h0 = 0.06, no noise) at n^3."""
     from vof_b200 import ic
 
-    prm = workload_params(V, n)
+    prm = workload_params(n)
     return prm, ic.rest_state(prm, ic.dam_break(prm))
 
 
@@ -660,7 +703,7 @@ def measure_small(V, stream, dev):
 
     out = {}
     for n, steps in SMALL_GRIDS:
-        prm, st = small_state(V, n)
+        prm, st = small_state(n)
         with V.Solver(prm, stream=stream.cuda_stream) as s:
             s.upload_state(**st)
             s.run(1, 3)
@@ -734,7 +777,6 @@ def run_reference(args):
     rank, world, local = dist_env()
     if rank != 0:
         return
-    import vof_b200 as V
     from oracle import oracle as orc
 
     variants = [v for v in ("sm100a", "readme") if orc.ref_available(v)]
@@ -751,7 +793,7 @@ def run_reference(args):
         gpu_id = "GPU-" + str(props.uuid)
     except Exception:
         pass
-    prm = workload_params(V, args.n)
+    prm = workload_params(args.n)
     state = workload_state(prm)
     cells = prm.nx * prm.ny * prm.nz
     K, W = args.steps, max(3, args.warmup)
@@ -784,7 +826,7 @@ def run_reference(args):
     if args.small:
         line["small_grids"] = {}
         for n, steps in SMALL_GRIDS:
-            prm_s, st_s = small_state(V, n)
+            prm_s, st_s = small_state(n)
             ms_s, _ = orc.ref_time(prm_s, st_s, 1, 3, steps, variant=best)
             line["small_grids"][f"{n}^3"] = {"steps": steps, "ms_per_step": round(ms_s / steps, 5),
                                              "value": round(n ** 3 * steps / ms_s / 1e3, 1), "unit": UNIT,
@@ -797,7 +839,28 @@ def run_reference(args):
                          "nstep": DRIVE_NSTEP, "steps": args.drive_steps,
                          "ascii": time_program([str(exe), "--max_steps", str(args.drive_steps), "--nstep",
                                                 str(DRIVE_NSTEP)], args.drive_steps)}
+    # the arm must run the reference's code only: no library of this repository mapped
+    line["native_so_loaded"] = mapped_libraries()
+    own = [x for x in line["native_so_loaded"] if "libvof_b200" in x]
+    if own:
+        raise RuntimeError(f"reference arm mapped this repository's library: {own}")
     print(json.dumps(line), flush=True)
+
+
+def mapped_libraries() -> list:
+    """Shared objects of this repository mapped into the process (from
+    /proc/self/maps): the oracle's and the reference harness's on the
+    reference arm, the library's on ours."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as fh:
+            for ln in fh:
+                parts = ln.split()
+                if len(parts) >= 6 and parts[-1].endswith(".so") and str(ROOT) in parts[-1]:
+                    out.add(os.path.relpath(parts[-1], ROOT))
+    except OSError:
+        pass
+    return sorted(out)
 
 
 def main(argv=None):

@@ -8,6 +8,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <atomic>
 #include <new>
 
 #include "../../include/vof.h"
@@ -35,6 +36,7 @@ struct vof_ctx {
     vof::PlainBuffers b;
     int p_parity;               // which of p0/p1 holds the current pressure
     float* fields[VOF_NUM_FIELDS - 1];  // all but P (P depends on parity)
+    float* stage;               // one field in the reference layout: host copies land here whole
     double* d_red_scratch;
     double* d_red_result;
     double* h_red_result;       // pinned, for vof_reduce
@@ -114,6 +116,7 @@ void free_ctx(vof_ctx* c) {
     if (c->b.p0) cudaFree(c->b.p0);
     if (c->b.p1) cudaFree(c->b.p1);
     if (c->b.p2) cudaFree(c->b.p2);
+    if (c->stage) cudaFree(c->stage);
     for (int q = 0; q < 4; ++q)
         if (c->b.csf[q]) cudaFree(c->b.csf[q]);
     if (c->d_red_scratch) cudaFree(c->d_red_scratch);
@@ -128,6 +131,43 @@ void free_ctx(vof_ctx* c) {
     }
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     delete c;
+}
+
+// Layout conversion of one field on the device: `rows` rows of `width`
+// floats from pitch spitch to pitch dpitch (reference layout <-> padded
+// layout).  Host copies move the reference-layout field whole, in one
+// contiguous cudaMemcpyAsync through the context's staging buffer, and this
+// kernel repacks it: a row of (nx+2) floats is 808 bytes at 200^3, and
+// row-by-row host copies of that size run far below the link's bandwidth.
+__global__ void __launch_bounds__(256) k_repack(const float* __restrict__ src, int spitch, float* __restrict__ dst,
+                                                int dpitch, int width, int rows) {
+    for (int r = blockIdx.x * 8 + threadIdx.y; r < rows; r += gridDim.x * 8) {
+        const float* a = src + (size_t)r * spitch;
+        float* b = dst + (size_t)r * dpitch;
+        for (int i = threadIdx.x; i < width; i += 32) b[i] = a[i];
+    }
+}
+
+cudaError_t repack(const float* src, int spitch, float* dst, int dpitch, int width, int rows, cudaStream_t s) {
+    int blocks = (rows + 7) / 8;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_repack<<<blocks, dim3(32, 8), 0, s>>>(src, spitch, dst, dpitch, width, rows);
+    return cudaGetLastError();
+}
+
+// vof_debug_wait_timeout's kernel: one wait that can only run out.  The
+// mbarrier expects 16 bytes of asynchronous copies that nothing issues, so
+// after `limit` tries the wait gives up and the kernel records
+// DEV_TMA_TIMEOUT in the context's status word, exactly as the blocked
+// Jacobi kernel does when a TMA load does not land in time (mbar_wait of
+// tma.cuh, the same bounded loop).  No copy is ever in flight.
+__global__ void k_wait_unfed(int* status, uint32_t limit) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        vof::mbar_init(&bar, 1);
+        vof::mbar_arrive_expect_tx(&bar, 16);
+        if (!vof::mbar_wait(&bar, 0, limit)) atomicOr(status, vof::DEV_TMA_TIMEOUT);
+    }
 }
 
 // Read (and clear) the device status word after the stream has drained.
@@ -227,16 +267,15 @@ int vof_params_init(vof_params* p, int nx, int ny, int nz) {
 
 // vof_debug_fail_alloc's setting: the number of the allocation of the next
 // vof_create that fails (-1: none).
-static int g_fail_alloc_at = -1;
+static std::atomic<int> g_fail_alloc_at{-1};
 
 int vof_debug_fail_alloc(int n) {
-    g_fail_alloc_at = n < 0 ? -1 : n;
+    g_fail_alloc_at.store(n < 0 ? -1 : n);
     return VOF_OK;
 }
 
 int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
-    const int fail_at = g_fail_alloc_at;  // (consumed by this call)
-    g_fail_alloc_at = -1;
+    const int fail_at = g_fail_alloc_at.exchange(-1);  // consumed by this call
     if (!out) return VOF_E_INVALID;
     *out = nullptr;
     int st = validate(p);
@@ -298,6 +337,7 @@ int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
     ok = ok && alloc((void**)&c->b.p0, fbytes) && alloc((void**)&c->b.p1, fbytes) &&
          alloc((void**)&c->b.p2, fbytes);
     for (int q = 0; q < 4 && ok && g.csf; ++q) ok = alloc((void**)&c->b.csf[q], fbytes);
+    ok = ok && alloc((void**)&c->stage, (size_t)p->nTot * sizeof(float));
     ok = ok && alloc((void**)&c->d_red_scratch, sizeof(double) * vof::RED_SCRATCH_DOUBLES);
     ok = ok && alloc((void**)&c->d_red_result, sizeof(double) * vof::RED_RESULT_DOUBLES);
     ok = ok && alloc((void**)&c->d_status, sizeof(int));
@@ -305,7 +345,7 @@ int vof_create(const vof_params* p, void* stream, vof_ctx** out) {
     if (ok && c->conv) {
         ok = alloc((void**)&c->p64, c->elems * sizeof(double));
         if (ok && vof::mg_create(g, p->mode == VOF_MODE_MIXED ? vof::MG_MIXED : vof::MG_FP64, &c->mg, c->stream,
-                                 &c->bytes) != cudaSuccess)
+                                 &c->bytes, &alloc_no, fail_at) != cudaSuccess)
             ok = false;
     }
     if (ok && cudaMallocHost((void**)&c->h_red_result, sizeof(double) * 4) != cudaSuccess) ok = false;
@@ -366,11 +406,15 @@ int vof_upload(vof_ctx* ctx, int field, const float* src, int src_is_device) {
     if (!dst) return VOF_E_INVALID;
     DeviceGuard dg(ctx->device);
     const Geom& g = ctx->g;
-    const size_t w = (size_t)(g.nx + 2) * sizeof(float);
-    cudaError_t e = cudaMemcpy2DAsync(dst, (size_t)g.px * sizeof(float), src, w, w,
-                                      (size_t)(g.ny + 2) * (g.nz + 2),
-                                      src_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                      ctx->stream);
+    const int rows = (g.ny + 2) * (g.nz + 2);
+    cudaError_t e = cudaSuccess;
+    const float* from = src;
+    if (!src_is_device) {  // one contiguous copy of the whole field, then the repack
+        e = cudaMemcpyAsync(ctx->stage, src, (size_t)ctx->prm.nTot * sizeof(float), cudaMemcpyHostToDevice,
+                            ctx->stream);
+        from = ctx->stage;
+    }
+    if (e == cudaSuccess) e = repack(from, g.nx + 2, dst, g.px, g.nx + 2, rows, ctx->stream);
     if (e == cudaSuccess && ctx->conv && field == VOF_FIELD_P) e = vof::mg_widen(g, ctx->mg, dst, ctx->p64, ctx->stream);
     return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
 }
@@ -381,12 +425,13 @@ int vof_download(vof_ctx* ctx, int field, float* dst, int dst_is_device) {
     if (!src) return VOF_E_INVALID;
     DeviceGuard dg(ctx->device);
     const Geom& g = ctx->g;
-    const size_t w = (size_t)(g.nx + 2) * sizeof(float);
-    cudaError_t e = cudaMemcpy2DAsync(dst, w, src, (size_t)g.px * sizeof(float), w,
-                                      (size_t)(g.ny + 2) * (g.nz + 2),
-                                      dst_is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                                      ctx->stream);
-    if (e == cudaSuccess && !dst_is_device) e = cudaStreamSynchronize(ctx->stream);
+    const int rows = (g.ny + 2) * (g.nz + 2);
+    cudaError_t e = repack(src, g.px, dst_is_device ? dst : ctx->stage, g.nx + 2, g.nx + 2, rows, ctx->stream);
+    if (e == cudaSuccess && !dst_is_device) {  // the repacked field in one contiguous copy
+        e = cudaMemcpyAsync(dst, ctx->stage, (size_t)ctx->prm.nTot * sizeof(float), cudaMemcpyDeviceToHost,
+                            ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    }
     return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
 }
 
@@ -644,6 +689,14 @@ int vof_adjoint_keeps(const vof_ctx* ctx) {
     if (!ctx) return VOF_E_INVALID;
     if (!ctx->adj || !ctx->adj->cp) return VOF_E_STATE;
     return ctx->adj->keep ? 1 : 0;
+}
+
+int vof_debug_wait_timeout(vof_ctx* ctx, unsigned limit) {
+    if (!ctx) return VOF_E_INVALID;
+    DeviceGuard dg(ctx->device);
+    k_wait_unfed<<<1, 32, 0, ctx->stream>>>(ctx->d_status, limit < vof::MBAR_SPIN_LIMIT ? limit : vof::MBAR_SPIN_LIMIT);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
 }
 
 int vof_last_cuda_error(const vof_ctx* ctx) { return ctx ? ctx->last_cuda_error : 0; }

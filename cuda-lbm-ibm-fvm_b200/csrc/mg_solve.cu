@@ -1127,7 +1127,8 @@ static bool dense_inverse(const MgLevel& L, std::vector<double>& inv) {
     return true;
 }
 
-cudaError_t mg_create(const Geom& g, int mode, MgSolver* m, cudaStream_t s, size_t* bytes) {
+cudaError_t mg_create(const Geom& g, int mode, MgSolver* m, cudaStream_t s, size_t* bytes, int* alloc_no,
+                      int fail_at) {
     *m = MgSolver{};
     m->mode = mode;
     m->pairs = 1;
@@ -1162,6 +1163,10 @@ cudaError_t mg_create(const Geom& g, int mode, MgSolver* m, cudaStream_t s, size
         if (e != cudaSuccess) return e;
     }
     auto alloc = [&](void** p, size_t nb) -> cudaError_t {
+        if (alloc_no && (*alloc_no)++ == fail_at) {  // injected (vof_debug_fail_alloc)
+            *p = nullptr;
+            return cudaErrorMemoryAllocation;
+        }
         cudaError_t r = cudaMalloc(p, nb);
         if (r != cudaSuccess) {
             *p = nullptr;

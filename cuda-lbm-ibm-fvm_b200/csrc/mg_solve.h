@@ -86,7 +86,12 @@ int mg_plan(const Geom& g, MgLevel* lv, int max_levels);
 
 // Plan and allocate the solver for grid g (zeroed buffers, the dense coarse
 // inverse, the device level table); bytes += device bytes allocated.
-cudaError_t mg_create(const Geom& g, int mode, MgSolver* m, cudaStream_t s, size_t* bytes);
+// alloc_no / fail_at (optional): the caller's running count of device
+// allocations and the number of the one that is to fail as if the device
+// were out of memory (vof_debug_fail_alloc); the count goes on across the
+// solver's own allocations.
+cudaError_t mg_create(const Geom& g, int mode, MgSolver* m, cudaStream_t s, size_t* bytes, int* alloc_no = nullptr,
+                      int fail_at = -1);
 void mg_destroy(MgSolver* m);
 
 // Solve A p = rhs - mean(rhs) to ||r|| <= tol ||b|| (FP64 defect correction,

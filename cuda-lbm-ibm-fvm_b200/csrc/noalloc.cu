@@ -148,13 +148,17 @@ extern "C" int vof_step_noalloc(const vof_params* prm, float* F, float* u, float
     b.status = status;
     int parity = 0;
     e = vof::plain_step(g, b, istep, prm->jacobi_iters, &parity, s, nullptr);
-    float* pres = parity ? b.p1 : b.p0;
-    float* out[5] = {b.F, b.u, b.v, b.w, pres};
-    for (int q = 0; q < 5 && e == cudaSuccess; ++q)
-        e = cudaMemcpy2DAsync(user[q], wref, out[q], wpad, wref, rows, cudaMemcpyDeviceToDevice, s);
+    // The status word first: on a timed-out wait the step's results are
+    // invalid, and the caller's buffers keep the state they passed in.
     int dev_status = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&dev_status, status, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return VOF_E_CUDA;
-    return dev_status ? VOF_E_TIMEOUT : VOF_OK;
+    if (dev_status) return VOF_E_TIMEOUT;
+    float* pres = parity ? b.p1 : b.p0;
+    float* out[5] = {b.F, b.u, b.v, b.w, pres};
+    for (int q = 0; q < 5 && e == cudaSuccess; ++q)
+        e = cudaMemcpy2DAsync(user[q], wref, out[q], wpad, wref, rows, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e == cudaSuccess ? VOF_OK : VOF_E_CUDA;
 }

@@ -43,10 +43,11 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
                  : "memory");
 }
 
-// Wait for phase `parity` of the barrier to complete; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Wait for phase `parity` of the barrier to complete, at most `limit` tries;
+// false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = MBAR_SPIN_LIMIT) {
     const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < MBAR_SPIN_LIMIT; ++it) {
+    for (uint32_t it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

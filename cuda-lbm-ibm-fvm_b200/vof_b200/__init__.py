@@ -119,6 +119,7 @@ def _declare(lib):
         "vof_adjoint_storage": (C.c_int, [vp, C.c_int]),
         "vof_adjoint_keeps": (C.c_int, [vp]),
         "vof_debug_fail_alloc": (C.c_int, [C.c_int]),
+        "vof_debug_wait_timeout": (C.c_int, [vp, C.c_uint]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -147,7 +148,7 @@ def exported_symbols():
             "vof_last_cuda_error", "vof_kernels_per_step", "vof_device_bytes",
             "vof_step_timed", "vof_phase_name", "vof_solver_stats", "vof_step_noalloc",
             "vof_forward_record", "vof_backward", "vof_adjoint_download", "vof_adjoint_kernels_per_step",
-            "vof_adjoint_storage", "vof_adjoint_keeps", "vof_debug_fail_alloc"]
+            "vof_adjoint_storage", "vof_adjoint_keeps", "vof_debug_fail_alloc", "vof_debug_wait_timeout"]
 
 
 def default_params(nx: int, ny: int | None = None, nz: int | None = None, **overrides) -> Params:

@@ -217,7 +217,8 @@ int vof_reduce_async(vof_ctx* ctx, int what, double* host_out);
  * device current); make that first call before any stream capture.  All calls
  * share the array (each clears what it uses first), so calls that overlap on
  * the GPU race.  The call waits for `stream` before returning.  Only
- * VOF_MODE_PLAIN.
+ * VOF_MODE_PLAIN.  On VOF_E_TIMEOUT (a bounded device-side wait ran out) the
+ * caller's buffers are left as they were passed in.
  */
 #define VOF_NOALLOC_ARENA_FLOATS (2u << 20)
 int vof_step_noalloc(const vof_params* p, float* F, float* u, float* v, float* w, float* pres, int istep,
@@ -301,10 +302,22 @@ int vof_last_cuda_error(const vof_ctx* ctx);
  * cudaMalloc.  The context's own device allocations in the next vof_create
  * are numbered from 0; the one numbered n fails as if the device were out of
  * memory, and vof_create frees what it had allocated and returns
- * VOF_E_NOMEM.  That vof_create consumes the setting whether it fires or
- * not; n < 0 clears it.  Process-wide and not thread-safe: set it from the
- * thread that calls vof_create. */
+ * VOF_E_NOMEM.  The count includes the multigrid solver's allocations of
+ * the convergent modes.  The next vof_create consumes the setting (one
+ * atomic exchange) whether it fires or not; n < 0 clears it.  The setting is
+ * process-wide: with several threads creating contexts, whichever create
+ * comes first takes it. */
 int vof_debug_fail_alloc(int n);
+
+/* Failure-path check for tests; no counterpart in the reference, which has
+ * no device-side waits.  Enqueues on the context's stream one kernel whose
+ * only wait can never be satisfied: an mbarrier that expects asynchronous
+ * copy bytes nothing will deliver, polled at most `limit` times (capped at
+ * the library's own limit) by the same bounded wait the TMA kernels use.
+ * When the wait runs out the kernel sets the context's device status word,
+ * so the next vof_sync (or vof_reduce) returns VOF_E_TIMEOUT and clears it;
+ * the context stays usable.  No copy is in flight at any time. */
+int vof_debug_wait_timeout(vof_ctx* ctx, unsigned limit);
 
 /* Number of kernel launches one vof_step enqueues for the current settings. */
 int vof_kernels_per_step(const vof_ctx* ctx);

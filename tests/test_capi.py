@@ -64,6 +64,19 @@ def test_params_nonuniform(V):
     assert p.nTot == 18 * 14 * 12
 
 
+@pytest.mark.parametrize("dims,over", [((200, 200, 200), {}), ((200, 200, 200), {"gy": 0.0, "gz": -9.81}),
+                                       ((32, 32, 32), {"gy": 0.0, "gz": -9.81}), ((17, 9, 13), {"Lx": 0.2}),
+                                       ((320, 320, 320), {"gy": 0.0, "gz": -9.81, "dt": 2e-6})])
+def test_host_params_match_the_library(V, dims, over):
+    """The numpy fill used where the library must not be loaded (the
+    benchmark's reference arm) gives vof_params_init's values bit for bit."""
+    from vof_b200.params import host_params
+
+    a = V.default_params(*dims, **over)
+    b = host_params(*dims, **over)
+    assert bytes(a) == bytes(b)
+
+
 def test_params_finalize_rejects_bad_sizes(V):
     p = V.Params()
     assert V.lib().vof_params_init(C.byref(p), 0, 4, 4) == V.E_SIZE

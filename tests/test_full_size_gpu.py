@@ -1,0 +1,136 @@
+"""Full-size parity: the 200^3 workloads at their stated lengths.
+
+* Dam break 200^3, 2000 steps (interface height 0.06 + 0.5 dx U(-1, 1),
+  splitmix64 seed 1; gravity -9.81 along z; dt 4e-6; 10 Jacobi sweeps), run
+  by this library and by the reference's own kernels (voftrial1.cu compiled
+  into oracle/_ref by oracle/Makefile, driven through its loop body
+  voftrial1.cu:1361-1401):
+    - against the -fmad=false build: bit-identical in F, u, v, w and p;
+    - against the build with nvcc's defaults (FMA contraction, the README's
+      kind of build): F max-abs <= 1e-3 and rel-L2 <= 1e-4; u, v, w rel-L2
+      <= 1e-3; p (mean removed, interior) rel-L2 <= 1e-3; the liquid volume
+      drift of the two runs differs by <= 1e-7 of the volume, and each stays
+      within 1e-5 of the initial volume.
+* MIXED convergent projection at 200^3 (the same inputs; BF16-stored /
+  FP32-arithmetic multigrid inside FP64 defect correction to a relative
+  residual <= 1e-8) against the FP64 oracle whose pressure is solved by
+  conjugate gradients to 1e-12, after 2 steps: F rel-L2 <= 1e-5, u, v, w
+  rel-L2 <= 1e-4, p (interior) rel-L2 <= 1e-5, every step's residual <= 1e-8.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from vof_b200 import ic
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("F", "u", "v", "w", "p")
+N, STEPS = 200, 2000
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def interior(a):
+    return np.asarray(a, dtype=np.float64)[1:-1, 1:-1, 1:-1]
+
+
+def volume(F):
+    return float(interior(F).sum())
+
+
+def report(name, values):
+    """Measured figures next to the bounds, for the run's log (and a JSON file
+    when VOF_TEST_REPORT names a directory)."""
+    print(f"{name}: {json.dumps(values)}")
+    d = os.environ.get("VOF_TEST_REPORT")
+    if d:
+        with open(os.path.join(d, f"{name}.json"), "w") as fh:
+            json.dump(values, fh, indent=1)
+
+
+@pytest.fixture(scope="module")
+def workload(V):
+    prm = V.default_params(N, gx=0.0, gy=0.0, gz=-9.81)
+    state = ic.rest_state(prm, ic.dam_break(prm, height=ic.noisy_height(prm, seed=1)))
+    return prm, state
+
+
+@pytest.fixture(scope="module")
+def ours_2000(V, workload):
+    prm, state = workload
+    with V.Solver(prm) as s:
+        s.upload_state(**state)
+        s.run(1, STEPS)
+        return s.state()
+
+
+def _need_ref(orc, variant):
+    if not orc.ref_available(variant):
+        pytest.skip(f"reference harness {variant} not built (needs the reference source at build time)")
+
+
+def test_dam_break_200_2000_steps_bitwise_vs_reference_nofma(cuda, orc, workload, ours_2000):
+    _need_ref(orc, "nofma")
+    prm, state = workload
+    ref = orc.ref_run(prm, state, 1, STEPS, variant="nofma")
+    bad = {k: int(np.count_nonzero(ours_2000[k] != ref[k])) for k in STATE}
+    report("dam_break_200_2000_vs_nofma", {"cells_differing": bad})
+    assert not any(bad.values()), bad
+
+
+def test_dam_break_200_2000_steps_vs_reference_default_build(cuda, orc, workload, ours_2000):
+    _need_ref(orc, "sm100a")
+    prm, state = workload
+    ref = orc.ref_run(prm, state, 1, STEPS, variant="sm100a")
+    got = ours_2000
+    v0, vg, vr = volume(state["F"]), volume(got["F"]), volume(ref["F"])
+    pg, pr = interior(got["p"]), interior(ref["p"])
+    m = {
+        "F_max_abs": float(np.abs(got["F"].astype(np.float64) - ref["F"]).max()),
+        "F_rel_l2": rel_l2(got["F"], ref["F"]),
+        "u_rel_l2": rel_l2(got["u"], ref["u"]),
+        "v_rel_l2": rel_l2(got["v"], ref["v"]),
+        "w_rel_l2": rel_l2(got["w"], ref["w"]),
+        "p_rel_l2_mean_removed": rel_l2(pg - pg.mean(), pr - pr.mean()),
+        "volume_drift_ours": (vg - v0) / v0,
+        "volume_drift_ref": (vr - v0) / v0,
+    }
+    report("dam_break_200_2000_vs_default_build", m)
+    assert m["F_max_abs"] <= 1e-3 and m["F_rel_l2"] <= 1e-4, m
+    for k in ("u", "v", "w"):
+        assert m[f"{k}_rel_l2"] <= 1e-3, m
+    assert m["p_rel_l2_mean_removed"] <= 1e-3, m
+    assert abs(m["volume_drift_ours"] - m["volume_drift_ref"]) <= 1e-7, m
+    assert abs(m["volume_drift_ours"]) <= 1e-5 and abs(m["volume_drift_ref"]) <= 1e-5, m
+
+
+def test_mixed_200_vs_fp64_oracle(cuda, V, orc):
+    steps = 2
+    prm = V.default_params(N, gx=0.0, gy=0.0, gz=-9.81, mode=V.MODE_MIXED, tol=1e-8, max_outer=200)
+    state = ic.rest_state(prm, ic.dam_break(prm, height=ic.noisy_height(prm, seed=1)))
+    stats = []
+    with V.Solver(prm) as s:
+        s.upload_state(**state)
+        for t in range(steps):
+            s.step(1 + t)
+            stats.append(s.solver_stats())
+        got = s.state()
+    ref = orc.run_conv_f64(prm, state, 1, steps, tol=1e-12)
+    pg, pr = interior(got["p"]), interior(ref["p"])
+    m = {"F_rel_l2": rel_l2(got["F"], ref["F"]), "u_rel_l2": rel_l2(got["u"], ref["u"]),
+         "v_rel_l2": rel_l2(got["v"], ref["v"]), "w_rel_l2": rel_l2(got["w"], ref["w"]),
+         "p_rel_l2": rel_l2(pg, pr), "stats": stats}
+    report("mixed_200_vs_fp64_oracle", m)
+    assert all(st["rel_final"] <= 1e-8 for st in stats), stats
+    assert m["F_rel_l2"] <= 1e-5, m
+    for k in ("u", "v", "w"):
+        assert m[f"{k}_rel_l2"] <= 1e-4, m
+    assert m["p_rel_l2"] <= 1e-5, m

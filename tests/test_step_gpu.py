@@ -269,6 +269,61 @@ def test_upload_download_roundtrip_and_device_pointers(cuda, V):
         assert torch.equal(o, t)
 
 
+def test_host_copies_pinned_pageable_and_full_size(cuda, V):
+    """Host uploads and downloads go whole through the staging buffer and are
+    repacked on the device: pageable and pinned memory, a grid whose row
+    pitch is not a multiple of 16 bytes, and 200^3, round trip exactly; the
+    context's other fields are untouched by a field's copy."""
+    import torch
+
+    for dims in ((13, 11, 9), (200, 200, 200)):
+        prm = V.default_params(*dims)
+        state = ic.random_state(prm, seed=7) if dims[0] < 100 else {
+            k: (np.arange(prm.nTot, dtype=np.float32).reshape(prm.shape) * (q + 1)) for q, k in enumerate(STATE)}
+        with V.Solver(prm) as s:
+            pinned = {k: torch.from_numpy(state[k]).pin_memory() for k in STATE}
+            for k in STATE:
+                s._check(s._lib.vof_upload(s._ctx, V.FIELDS[k], pinned[k].data_ptr(), 0), "vof_upload")
+            s.sync()
+            for k in STATE:
+                assert np.array_equal(s.download(k), state[k]), (dims, k)
+                out = torch.empty(prm.shape, dtype=torch.float32).pin_memory()
+                s._check(s._lib.vof_download(s._ctx, V.FIELDS[k], out.data_ptr(), 0), "vof_download")
+                assert np.array_equal(out.numpy(), state[k]), (dims, k, "pinned")
+            s.upload("u", state["v"])  # pageable
+            assert np.array_equal(s.download("u"), state["v"])
+            assert np.array_equal(s.download("w"), state["w"])
+
+
+def test_bounded_wait_timeout_is_reported_and_cleared(cuda, V, orc):
+    """A device-side wait that runs out (vof_debug_wait_timeout: an mbarrier
+    armed for copy bytes that never come, polled a few times by the TMA
+    kernels' bounded wait) sets the context's status word: vof_sync returns
+    VOF_E_TIMEOUT once and clears it, for every limit; vof_reduce reports it
+    too; the context keeps working (the next steps are still bit-identical
+    to the oracle)."""
+    prm = V.default_params(12, 10, 8, dt=5e-4)
+    state = ic.random_state(prm, seed=21)
+    lib = V.lib()
+    with V.Solver(prm) as s:
+        s.upload_state(**state)
+        assert lib.vof_sync(s._ctx) == V.OK
+        for limit in (0, 1, 1024):
+            assert lib.vof_debug_wait_timeout(s._ctx, limit) == V.OK
+            assert lib.vof_sync(s._ctx) == V.E_TIMEOUT, limit
+            assert lib.vof_sync(s._ctx) == V.OK, limit  # cleared
+        assert lib.vof_debug_wait_timeout(s._ctx, 4) == V.OK
+        with pytest.raises(V.VofError) as e:
+            s.reduce("volume")  # vof_reduce waits through vof_sync
+        assert e.value.status == V.E_TIMEOUT
+        s.run(1, 2)
+        assert lib.vof_sync(s._ctx) == V.OK
+        got = s.state()
+    assert lib.vof_debug_wait_timeout(None, 1) == V.E_INVALID
+    want = orc.run_f32(prm, state, 1, 2)
+    assert_bitwise(got, want, STATE, "after timeouts")
+
+
 def test_user_stream(cuda, V, orc):
     import torch
 
@@ -386,8 +441,9 @@ def test_full_size_dam_break_vs_reference_kernels(cuda, V, orc):
 
 
 def test_allocation_failure_in_create(cuda, V, tmp_path):
-    """Each device allocation of vof_create made to fail in turn
-    (vof_debug_fail_alloc, a host-side fake of an out-of-memory cudaMalloc):
+    """Each device allocation of vof_create (the multigrid solver's in the
+    MIXED mode included) made to fail in turn (vof_debug_fail_alloc, a
+    host-side fake of an out-of-memory cudaMalloc):
     VOF_E_NOMEM and no context, nothing left allocated (device free memory
     back to within 16 MiB of what it was: less than one 160^3 field, 19.2
     MiB), and the next vof_create, which finds no setting left, works.  In a child process, so
@@ -440,6 +496,8 @@ json.dump(res, open({str(out)!r}, "w"))
     n_plain = res["plain"][0]
     assert n_plain >= 10
     assert res["csf"][0] == n_plain + 4  # the four surface-tension fields
-    assert res["mixed"][0] == n_plain + 1  # the FP64 pressure
+    # the FP64 pressure and the multigrid solver's buffers (three per level
+    # over at least four levels at 160^3, its partials, result and level table)
+    assert res["mixed"][0] >= n_plain + 1 + 3 * 4 + 3
     for name, (n, leaked) in res.items():
         assert leaked < 16 * 2**20, (name, leaked)
