@@ -435,6 +435,42 @@ int vof_download(vof_ctx* ctx, int field, float* dst, int dst_is_device) {
     return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
 }
 
+int vof_get_planes(vof_ctx* ctx, int field, int k0, int nk, float* dst, int dst_is_device) {
+    if (!ctx || !dst || nk < 1 || k0 < 0 || k0 + nk > ctx->g.nz + 2) return VOF_E_INVALID;
+    const float* src = field_ptr(ctx, field);
+    if (!src) return VOF_E_INVALID;
+    DeviceGuard dg(ctx->device);
+    const Geom& g = ctx->g;
+    const int rows = (g.ny + 2) * nk;
+    cudaError_t e = repack(src + (size_t)k0 * g.plane, g.px, dst_is_device ? dst : ctx->stage, g.nx + 2, g.nx + 2,
+                           rows, ctx->stream);
+    if (e == cudaSuccess && !dst_is_device) {
+        e = cudaMemcpyAsync(dst, ctx->stage, (size_t)rows * (g.nx + 2) * sizeof(float), cudaMemcpyDeviceToHost,
+                            ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    }
+    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
+}
+
+int vof_put_planes(vof_ctx* ctx, int field, int k0, int nk, const float* src, int src_is_device) {
+    if (!ctx || !src || nk < 1 || k0 < 0 || k0 + nk > ctx->g.nz + 2) return VOF_E_INVALID;
+    float* dst = field_ptr(ctx, field);
+    if (!dst) return VOF_E_INVALID;
+    if (ctx->conv && field == VOF_FIELD_P) return VOF_E_UNSUPPORTED;  // its FP64 copy is the state there
+    DeviceGuard dg(ctx->device);
+    const Geom& g = ctx->g;
+    const int rows = (g.ny + 2) * nk;
+    cudaError_t e = cudaSuccess;
+    const float* from = src;
+    if (!src_is_device) {
+        e = cudaMemcpyAsync(ctx->stage, src, (size_t)rows * (g.nx + 2) * sizeof(float), cudaMemcpyHostToDevice,
+                            ctx->stream);
+        from = ctx->stage;
+    }
+    if (e == cudaSuccess) e = repack(from, g.nx + 2, dst + (size_t)k0 * g.plane, g.px, g.nx + 2, rows, ctx->stream);
+    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
+}
+
 int vof_step(vof_ctx* ctx, int istep) {
     if (!ctx) return VOF_E_INVALID;
     DeviceGuard dg(ctx->device);
@@ -564,6 +600,35 @@ int vof_reduce(vof_ctx* ctx, int what, double* out) {
     int st = vof_reduce_async(ctx, what, ctx->h_red_result);
     if (st != VOF_OK) return st;
     st = vof_sync(ctx);
+    if (st != VOF_OK) return st;
+    *out = ctx->h_red_result[0];
+    return VOF_OK;
+}
+
+int vof_reduce_range(vof_ctx* ctx, int what, int k0, int k1, double* out) {
+    if (!ctx || !out || k0 < 1 || k1 > ctx->g.nz || k0 > k1) return VOF_E_INVALID;
+    if (what != VOF_RED_VOLUME && what != VOF_RED_F_MIN && what != VOF_RED_F_MAX && what != VOF_RED_DIV_L2 &&
+        what != VOF_RED_DIV_MAX)
+        return what >= 0 && what < VOF_NUM_REDUCTIONS ? VOF_E_UNSUPPORTED : VOF_E_INVALID;
+    DeviceGuard dg(ctx->device);
+    // the planes k0..k1 as a grid of their own: the same rows, the base moved
+    // k0 - 1 planes up (every reduction here reads a cell and its upper faces)
+    Geom sub = ctx->g;
+    sub.nz = k1 - k0 + 1;
+    const size_t off = (size_t)(k0 - 1) * ctx->g.plane;
+    vof::ReduceInputs in;
+    in.F = ctx->b.F + off;
+    in.u = ctx->b.u + off;
+    in.v = ctx->b.v + off;
+    in.w = ctx->b.w + off;
+    in.p = (ctx->p_parity ? ctx->b.p1 : ctx->b.p0) + off;
+    in.rhs = ctx->b.rhs + off;
+    cudaError_t e = vof::reduce_launch(sub, in, what, ctx->d_red_scratch, ctx->d_red_result, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ctx->h_red_result, ctx->d_red_result + vof::reduce_result_slot(what), sizeof(double),
+                            cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) return fail_cuda(ctx, e);
+    const int st = vof_sync(ctx);
     if (st != VOF_OK) return st;
     *out = ctx->h_red_result[0];
     return VOF_OK;

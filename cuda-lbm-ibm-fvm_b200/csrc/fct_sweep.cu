@@ -292,6 +292,335 @@ __global__ void __launch_bounds__(THREADS, 2) k_fct(Geom g, const float* Fsrc, f
     }
 }
 
+// ---- y and z sweeps out of place: one thread per line segment ------------------
+// Lines along y or z are contiguous across the 32 lanes of a warp (lanes run
+// along x), so a lane reads its line's F and face velocity straight from
+// memory, one coalesced row per position, with the next position's operands
+// loaded an iteration ahead; no shared memory and no barrier.  The march and
+// its register window are those of k_fct; the state before the segment's
+// first cell comes from the Ftd of the four cells before it and the two
+// ratios it needs.  Fin and Fout must be different buffers: a segment's
+// warm-up reads the cells of the segment before it.
+struct GLine {
+    const float* f;
+    const float* v;
+    int qs;
+    __device__ __forceinline__ float F(int q) const { return __ldg(f + (ptrdiff_t)q * qs); }
+    __device__ __forceinline__ float V(int q) const { return __ldg(v + (ptrdiff_t)q * qs); }
+};
+
+template <int AXIS>
+__device__ __forceinline__ float gftd(const Sweep<AXIS>& S, const GLine& L, int c) {
+    if (c < 1 || c > S.n) return 0.0f;
+    float lo_in, lo_out, a;
+    fct::flux(L.V(c), L.F(c - 1), L.F(c), S.dt, lo_in, a);
+    fct::flux(L.V(c + 1), L.F(c), L.F(c + 1), S.dt, lo_out, a);
+    const float dv = S.dv(L.V(c), L.V(c + 1));
+    return ftd_from(S, L.F(c), lo_in, lo_out, dv, __frcp_rn(dv));
+}
+
+__device__ __forceinline__ float ga(const GLine& L, int f, int n, float dt) {
+    if (f < 1 || f > n + 1) return 0.0f;
+    float lo, a;
+    fct::flux(L.V(f), L.F(f - 1), L.F(f), dt, lo, a);
+    return a;
+}
+
+constexpr int MARCH_THREADS = 256;
+
+// Lines are numbered flat, i fastest (a warp may span two rows of lines:
+// two coalesced pieces per load), blockIdx.y is the segment.
+template <int AXIS, bool FINAL>
+__global__ void __launch_bounds__(MARCH_THREADS, 4) k_fct_march(Geom g, const float* __restrict__ Fin,
+                                                                float* __restrict__ F,
+                                                                const float* __restrict__ vel, int seg) {
+    static_assert(AXIS == 1 || AXIS == 2, "lines along y or z");
+    const Sweep<AXIS> S(g);
+    const int n = S.n;
+    const int nb = AXIS == 1 ? g.nz : g.ny;
+    const int line = blockIdx.x * MARCH_THREADS + threadIdx.x;
+    const int a = 1 + line % g.nx;  // i
+    const int b = 1 + line / g.nx;  // k (y lines) or j (z lines)
+    const int c0 = 1 + blockIdx.y * seg;
+    if (b > nb || c0 > n) return;
+    const int c1 = min(n, c0 + seg - 1);
+    auto gi = [&](int aa, int bb, int q) { return AXIS == 1 ? gidx(g, aa, q, bb) : gidx(g, aa, bb, q); };
+    const int qs = AXIS == 1 ? g.px : g.plane;
+    const int base = gi(a, b, 0);
+    const GLine L{Fin + base, vel + base, qs};
+    const float dt = S.dt;
+
+    // state before cell c0 (as k_fct's march carries it into c0)
+    float a0f, a1f, a2f, lo2 = 0.0f;
+    {
+        float lo_tmp;
+        fct::flux(L.V(c0), L.F(c0 - 1), L.F(c0), dt, lo_tmp, a0f);
+    }
+    a1f = ga(L, c0 + 1, n, dt);
+    a2f = 0.0f;
+    if (c0 + 2 <= n + 1) fct::flux(L.V(c0 + 2), L.F(c0 + 1), L.F(c0 + 2), dt, lo2, a2f);
+    const float Tm2 = gftd(S, L, c0 - 2), Tm1 = gftd(S, L, c0 - 1);
+    float T0 = gftd(S, L, c0), T1 = gftd(S, L, c0 + 1);
+    float rp0 = 0.0f, rm0 = 0.0f;
+    limiter(S, Tm1, T0, T1, a0f, a1f, rp0, rm0);  // c0 is interior
+    float cf0 = 0.0f;                             // c[1] is never written
+    if (c0 > 1) {
+        float rpm, rmm;
+        limiter(S, Tm2, Tm1, T0, ga(L, c0 - 1, n, dt), a0f, rpm, rmm);
+        cf0 = face_limit(a0f, rpm, rmm, rp0, rm0);
+    }
+    float dv0 = S.dv(L.V(c0), L.V(c0 + 1));
+    float dv1 = (c0 + 1 <= n) ? S.dv(L.V(c0 + 1), L.V(c0 + 2)) : 1.0f;
+    // operands of position c+3 for the first iteration, and a window of F/V
+    float F2 = L.F(c0 + 2 <= n + 1 ? c0 + 2 : n + 1);
+    float V3 = (c0 + 3 <= n + 1) ? L.V(c0 + 3) : 0.0f, F3 = (c0 + 3 <= n + 1) ? L.F(c0 + 3) : 0.0f;
+    float V2 = (c0 + 2 <= n + 1) ? L.V(c0 + 2) : 0.0f;
+    const int nm = AXIS == 1 ? g.ny : g.nz;
+    // Run of positions, up to c+2 here and c+3 in the loop, where F is 0 and
+    // |face velocity| < vq (positions off the line count as such).  vq keeps
+    // every cell's dv = vol - dvfac (v_hi - v_lo) above 0.01 vol: finite and
+    // positive, so a zero numerator gives a zero quotient.
+    const float vq = 0.49f * S.vol / S.dvfac;
+    int zrun = 0;
+    for (int q = c0 - 3; q <= c0 + 2; ++q) {
+        const bool in = q >= 0 && q <= n + 1;
+        zrun = (!in || (L.F(q) == 0.0f && fabsf(L.V(q)) < vq)) ? zrun + 1 : 0;
+    }
+    // the line is away from the box's edges across the sweep (no ghost copies
+    // but along the line on the final sweep)
+    const bool inner = a > 1 && a < g.nx && b > 1 && b < nb;
+#pragma unroll 2
+    for (int c = c0; c <= c1; ++c) {
+        // next iteration's operands (position c+4), loaded a march step ahead
+        const bool nx4 = c + 4 <= n + 1 && c < c1;
+        const float V4 = nx4 ? L.V(c + 4) : 0.0f, F4 = nx4 ? L.F(c + 4) : 0.0f;
+        // F == 0 at positions c-3 .. c+3 (velocities below vq): every stage
+        // value this iteration forms -- the flux of face c+3, Ftd(c+2), the
+        // ratios of c+1, the limiter of face c+1 and the new F(c) -- is zero
+        // (up to the sign of a zero, which no comparison sees and the final
+        // clamp01f removes), and so is the carried window.  Only dv(c+2) is
+        // needed later.  Most of a dam break is gas, far from the interface.
+        zrun = (F3 == 0.0f && fabsf(V3) < vq) ? zrun + 1 : 0;
+        const bool quiet = zrun >= 7;
+        const float dv2 = (c + 2 <= n) ? S.dv(V2, V3) : 1.0f;
+        float lo3 = 0.0f, a3f = 0.0f, T2 = 0.0f, rp1 = 0.0f, rm1 = 0.0f, cf1 = 0.0f, fnew = 0.0f;
+        if (!quiet) {
+            if (c + 3 <= n + 1) fct::flux(V3, F2, F3, dt, lo3, a3f);
+            if (c + 2 <= n) T2 = ftd_from(S, F2, lo2, lo3, dv2, __frcp_rn(dv2));
+            if (c + 1 <= n) limiter(S, T0, T1, T2, a1f, a2f, rp1, rm1);
+            cf1 = face_limit(a1f, rp0, rm0, rp1, rm1);
+            // (the reciprocal of dv(c) formed again here rather than carried:
+            // quiet positions skip it)
+            fnew = clamp01f(fct::stage4(S, T0, a0f, cf0, a1f, cf1, dv0, __frcp_rn(dv0)));
+        }
+        if (!FINAL) {
+            F[gi(a, b, c)] = fnew;
+        } else {
+            fnew = clamp01f(fnew);  // post_process_f_kernel, voftrial1.cu:502-507
+            if (inner && c > 1 && c < nm) {
+                F[gi(a, b, c)] = fnew;
+            } else {
+                // apply_bc_F (voftrial1.cu:1122-1135): every ghost takes the
+                // value at its clamped interior index
+                int qv[3], av[3], bv[3];
+                const int nq = mirrors(c, nm, qv), nav = mirrors(a, g.nx, av), nbv = mirrors(b, nb, bv);
+                for (int ib = 0; ib < nbv; ++ib)
+                    for (int ia = 0; ia < nav; ++ia)
+                        for (int iq = 0; iq < nq; ++iq) F[gi(av[ia], bv[ib], qv[iq])] = fnew;
+            }
+        }
+        lo2 = lo3;
+        a0f = a1f;
+        a1f = a2f;
+        a2f = a3f;
+        T0 = T1;
+        T1 = T2;
+        rp0 = rp1;
+        rm0 = rm1;
+        cf0 = cf1;
+        dv0 = dv1;
+        dv1 = dv2;
+        F2 = F3;
+        F3 = F4;
+        V2 = V3;
+        V3 = V4;
+    }
+}
+
+// ---- x sweeps out of place: a warp per window of a row ------------------------
+// An x line is contiguous in memory, so here the lanes run along the line: a
+// warp owns a window of XW = 32 * XC positions of one row (XC consecutive
+// cells per lane, one aligned vector load of F and of the face velocity),
+// evaluates every stage once per position -- fluxes, Ftd, Zalesak ratios, face
+// limiters, the new F -- and takes the neighbours of its first and last cell
+// from the adjacent lanes by shuffle.  A stage's value is exact wherever its
+// three-cell reach stays inside the window, so a window writes its positions
+// XC .. XW - XC - 1 and consecutive windows of a row overlap by 2 XC.  Same
+// per-cell expressions as k_fct; Fin and Fout must be different buffers.
+constexpr int XC = 4, XW = 32 * XC, XOUT = XW - 2 * XC;
+
+template <bool FINAL>
+__global__ void __launch_bounds__(256) k_fct_x(Geom g, const float* __restrict__ Fin, float* __restrict__ F,
+                                               const float* __restrict__ vel, int chunks) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const Sweep<0> S(g);
+    const int n = g.nx;
+    const int lane = threadIdx.x & 31;
+    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int chunk = (int)(wid % chunks);
+    const long long row = wid / chunks;
+    const int j = 1 + (int)(row % g.ny), k = 1 + (int)(row / g.ny);
+    if (k > g.nz) return;  // the whole warp
+    const int pa = chunk * XOUT - XC;  // first position of the window
+    const int x0 = pa + lane * XC;     // this lane's first position
+    const int rb = gidx(g, 0, j, k);
+    const float dt = S.dt;
+    float Fv[XC], Vv[XC];
+    if (x0 >= 0 && x0 + XC - 1 <= n + 1) {
+        const float4 f4 = *reinterpret_cast<const float4*>(Fin + rb + x0);
+        const float4 v4 = __ldg(reinterpret_cast<const float4*>(vel + rb + x0));
+        Fv[0] = f4.x; Fv[1] = f4.y; Fv[2] = f4.z; Fv[3] = f4.w;
+        Vv[0] = v4.x; Vv[1] = v4.y; Vv[2] = v4.z; Vv[3] = v4.w;
+    } else {
+#pragma unroll
+        for (int e = 0; e < XC; ++e) {
+            const int x = x0 + e;
+            const bool in = x >= 0 && x <= n + 1;
+            Fv[e] = in ? Fin[rb + x] : 0.0f;
+            Vv[e] = in ? __ldg(vel + rb + x) : 0.0f;
+        }
+    }
+    const int lo_out = pa + XC, hi_out = pa + XW - XC - 1;
+    float out[XC];
+    bool wr[XC];
+#pragma unroll
+    for (int e = 0; e < XC; ++e) {
+        const int x = x0 + e;
+        wr[e] = x >= 1 && x <= n && x >= lo_out && x <= hi_out;
+        out[e] = 0.0f;
+    }
+    // A window where F is 0 everywhere (face velocities below vq, which keeps
+    // every dv above 0.01 vol) gives 0 at each of its cells, as k_fct_march's
+    // quiet positions do: most windows of a dam break are gas.
+    const float vq = 0.49f * S.vol / S.dvfac;
+    bool zq = true;
+#pragma unroll
+    for (int e = 0; e < XC; ++e) {
+        const int x = x0 + e;
+        zq = zq && (x < 0 || x > n + 1 || (Fv[e] == 0.0f && fabsf(Vv[e]) < vq));
+    }
+    if (!__all_sync(FULL, zq)) {
+    // face fluxes through faces x0 .. x0+XC-1 (face x lies between cells x-1 and x)
+    const float Fm = __shfl_up_sync(FULL, Fv[XC - 1], 1);
+    float lo[XC], af[XC];
+#pragma unroll
+    for (int e = 0; e < XC; ++e) {
+        const int x = x0 + e;
+        lo[e] = 0.0f;
+        af[e] = 0.0f;
+        if (x >= 1 && x <= n + 1) fct::flux(Vv[e], e ? Fv[e - 1] : Fm, Fv[e], dt, lo[e], af[e]);
+    }
+    const float Vn = __shfl_down_sync(FULL, Vv[0], 1);
+    const float lon = __shfl_down_sync(FULL, lo[0], 1), an = __shfl_down_sync(FULL, af[0], 1);
+    // low-order update Ftd of cells x0 .. x0+XC-1 (0 outside 1..n)
+    float T[XC], dv[XC], rdv[XC];
+#pragma unroll
+    for (int e = 0; e < XC; ++e) {
+        const int x = x0 + e;
+        T[e] = 0.0f;
+        dv[e] = 1.0f;
+        rdv[e] = 1.0f;
+        if (x >= 1 && x <= n) {
+            dv[e] = S.dv(Vv[e], e < XC - 1 ? Vv[e + 1] : Vn);
+            rdv[e] = __frcp_rn(dv[e]);
+            T[e] = ftd_from(S, Fv[e], lo[e], e < XC - 1 ? lo[e + 1] : lon, dv[e], rdv[e]);
+        }
+    }
+    const float Tm = __shfl_up_sync(FULL, T[XC - 1], 1), Tn = __shfl_down_sync(FULL, T[0], 1);
+    // Zalesak ratios (0 outside 1..n)
+    float rp[XC], rm[XC];
+#pragma unroll
+    for (int e = 0; e < XC; ++e) {
+        const int x = x0 + e;
+        rp[e] = 0.0f;
+        rm[e] = 0.0f;
+        if (x >= 1 && x <= n)
+            limiter(S, e ? T[e - 1] : Tm, T[e], e < XC - 1 ? T[e + 1] : Tn, af[e], e < XC - 1 ? af[e + 1] : an,
+                    rp[e], rm[e]);
+    }
+    const float rpm = __shfl_up_sync(FULL, rp[XC - 1], 1), rmm = __shfl_up_sync(FULL, rm[XC - 1], 1);
+    // face limiters of faces 2 .. n+1 (c[1] is never written: 0)
+    float cf[XC];
+#pragma unroll
+    for (int e = 0; e < XC; ++e) {
+        const int x = x0 + e;
+        cf[e] = (x >= 2 && x <= n + 1) ? face_limit(af[e], e ? rp[e - 1] : rpm, e ? rm[e - 1] : rmm, rp[e], rm[e])
+                                       : 0.0f;
+    }
+    const float cfn = __shfl_down_sync(FULL, cf[0], 1);
+    // the new F of the window's own cells
+#pragma unroll
+    for (int e = 0; e < XC; ++e) {
+        if (wr[e]) {
+            out[e] = clamp01f(fct::stage4(S, T[e], af[e], cf[e], e < XC - 1 ? af[e + 1] : an,
+                                          e < XC - 1 ? cf[e + 1] : cfn, dv[e], rdv[e]));
+            if (FINAL) out[e] = clamp01f(out[e]);  // post_process_f_kernel, voftrial1.cu:502-507
+        }
+    }
+    }  // not a quiet window
+    if (!FINAL) {
+        if (wr[0] && wr[1] && wr[2] && wr[3]) {
+            *reinterpret_cast<float4*>(F + rb + x0) = make_float4(out[0], out[1], out[2], out[3]);
+        } else {
+#pragma unroll
+            for (int e = 0; e < XC; ++e)
+                if (wr[e]) F[rb + x0 + e] = out[e];
+        }
+    } else {
+        // apply_bc_F (voftrial1.cu:1122-1135): every ghost takes the value at
+        // its clamped interior index
+        int jv[3], kv[3];
+        const int nj = mirrors(j, g.ny, jv), nk = mirrors(k, g.nz, kv);
+        for (int b = 0; b < nk; ++b)
+            for (int q = 0; q < nj; ++q) {
+                const int r2 = gidx(g, 0, jv[q], kv[b]);
+#pragma unroll
+                for (int e = 0; e < XC; ++e) {
+                    if (!wr[e]) continue;
+                    const int x = x0 + e;
+                    F[r2 + x] = out[e];
+                    if (x == 1) F[r2] = out[e];
+                    if (x == n) F[r2 + n + 1] = out[e];
+                }
+            }
+    }
+}
+
+static int march_resident = 4 * 148;  // blocks of k_fct_march resident at once, set by fct_configure
+
+// Segments per line: the count (of 1 .. 16, segments of at least 16 cells)
+// whose launch fills its last wave of resident blocks best, the fewest
+// segments among equals (each segment start repeats a few cells of work).
+static int march_segment(const Geom& g, int axis) {
+    const int n = axis == 1 ? g.ny : g.nz;
+    const int nb = axis == 1 ? g.nz : g.ny;
+    const long long bx = ((long long)g.nx * nb + MARCH_THREADS - 1) / MARCH_THREADS;
+    int best = n;
+    double best_fill = -1.0;
+    for (int nseg = 1; nseg <= 16; ++nseg) {
+        const int seg = (n + nseg - 1) / nseg;
+        if (nseg > 1 && seg < 16) break;
+        const long long blocks = bx * ((n + seg - 1) / seg);
+        const long long waves = (blocks + march_resident - 1) / march_resident;
+        const double fill = (double)blocks / (double)(waves * march_resident);
+        if (fill > best_fill + 0.02) {
+            best_fill = fill;
+            best = seg;
+        }
+    }
+    return best;
+}
+
 size_t fct_smem_bytes(int axis, int n) {
     const int npos = n + 2;
     if (axis == 0) return sizeof(float) * 2u * (size_t)LANES * (size_t)odd_pitch(npos);
@@ -300,6 +629,23 @@ size_t fct_smem_bytes(int axis, int n) {
 
 template <int AXIS, bool FINAL>
 static cudaError_t launch_axis(const Geom& g, const float* Fsrc, float* F, const float* vel, cudaStream_t s) {
+    if (AXIS == 0 && Fsrc != F) {  // out of place along x: warps along the rows
+        const int chunks = (g.nx + 1 + XOUT - 1) / XOUT;
+        const long long warps = (long long)chunks * g.ny * g.nz;
+        k_fct_x<FINAL><<<(unsigned)((warps + 7) / 8), 256, 0, s>>>(g, Fsrc, F, vel, chunks);
+        return cudaGetLastError();
+    }
+    // out of place along y or z, with lines enough to fill the device (one
+    // thread per line segment): the march from memory; else the tiles below
+    if (AXIS != 0 && Fsrc != F && (long long)g.nx * (AXIS == 1 ? g.nz : g.ny) >= 16384) {
+        constexpr int A = AXIS == 0 ? 1 : AXIS;
+        const int n = A == 1 ? g.ny : g.nz, nb = A == 1 ? g.nz : g.ny;
+        const int seg = march_segment(g, A);
+        const dim3 grid((unsigned)(((long long)g.nx * nb + MARCH_THREADS - 1) / MARCH_THREADS),
+                        (unsigned)((n + seg - 1) / seg));
+        k_fct_march<A, FINAL><<<grid, MARCH_THREADS, 0, s>>>(g, Fsrc, F, vel, seg);
+        return cudaGetLastError();
+    }
     const int n = AXIS == 0 ? g.nx : (AXIS == 1 ? g.ny : g.nz);
     const int na = AXIS == 0 ? g.ny : g.nx;
     const int nb = AXIS == 2 ? g.ny : g.nz;
@@ -332,6 +678,12 @@ cudaError_t fct_configure() {
         return e;
     VOF_SET(0, false) VOF_SET(0, true) VOF_SET(1, false) VOF_SET(1, true) VOF_SET(2, false) VOF_SET(2, true)
 #undef VOF_SET
+    int sms = 0, occ = 0;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fct_march<2, false>, MARCH_THREADS, 0)) !=
+            cudaSuccess)
+        return e;
+    march_resident = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
     return cudaSuccess;
 }
 

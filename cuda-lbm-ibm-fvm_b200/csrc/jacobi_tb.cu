@@ -424,6 +424,225 @@ cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rh
     return cudaGetLastError();
 }
 
+// ---- two sweeps per launch, two cells per thread, marching z ----------------
+// The pressure and rhs of a plane are read from memory once for two sweeps,
+// so a pair of sweeps moves the bytes of one (read p, rhs; write p).
+//
+// A block owns a tile of `rows` rows by `tpx` pairs and a range of planes.
+// Its threads cover the tile plus a one-row halo above and below (and, when
+// a tile is narrower than a row, a one-pair halo left and right): the region
+// of rh x rw pairs, numbered flat (pair fastest), one thread per pair.  At
+// plane s a thread
+//   - computes the first sweep of its pair at plane s from the input planes
+//     s-1, s, s+1 of its own column (registers) and of its in-plane
+//     neighbours (the input plane s in shared memory; the rows beyond the
+//     region from memory),
+//   - stores it in a ring of three first-sweep planes in shared memory,
+//   - and, after the block's one barrier of the plane, computes the second
+//     sweep of its pair (tile pairs only) at plane s-1 from the first-sweep
+//     planes s-2, s-1, s of its own column (registers) and its neighbours'
+//     plane s-1 (shared memory).
+// The first sweep runs one plane beyond each end of the range.  Cells that
+// are not updated (ghost rows, columns and planes) carry the input's value,
+// as in k_jacobi_tb; they enter the second sweep only through zero
+// coefficients.  Every update is the scalar expression of k_jacobi_pairs in
+// the same operand order, so two sweeps here give the bits of two launches
+// of that kernel.
+//
+// Work is dealt to a persistent grid (one block of up to 1024 threads per
+// SM): the units are (tile, plane) with the plane fastest, and block b takes
+// the contiguous units [b U / G, (b + 1) U / G), one segment per tile it
+// touches, so every block marches the same number of planes.
+struct J2Plan {
+    int npair;     // pairs per row: columns 0 .. 2 npair - 1 cover 0 .. nx
+    int tpx, ntx;  // pairs per tile along x, tiles along x
+    int xh;        // halo pairs on each side along x (0: a tile is whole rows)
+    int rows, nty; // rows per tile, tiles along y
+    int rw, rh;    // region: pairs per row (tpx + 2 xh) and rows (rows + 2)
+    long long units;
+};
+
+constexpr int J2_THREADS = 1024;
+
+__global__ void __launch_bounds__(J2_THREADS, 1) k_jacobi_pairs2(Geom g, const float* __restrict__ pin,
+                                                               const float* __restrict__ rhs,
+                                                               float* __restrict__ pout, J2Plan pl) {
+    extern __shared__ float2 j2s[];
+    const int RS = pl.rw * pl.rh;  // pairs of one region plane
+    float2* s0 = j2s;              // [2][RS] input planes
+    float2* s1 = j2s + 2 * RS;     // [3][RS] first-sweep planes
+    const int t = threadIdx.x;
+    const bool tin = t < RS;
+    const int lr = tin ? t / pl.rw : 0, lm = tin ? t - lr * pl.rw : 0;
+    const float cx = g.dxi * g.dxi, cy = g.dyi * g.dyi, cz = g.dzi * g.dzi;
+    const int wp = g.plane >> 1, wr = g.px >> 1;
+    const float2* P = reinterpret_cast<const float2*>(pin);
+    const float2* R = reinterpret_cast<const float2*>(rhs);
+    float2* O = reinterpret_cast<float2*>(pout);
+    const float2 zero = make_float2(0.0f, 0.0f);
+    const long long G = gridDim.x;
+    const long long ub = pl.units * blockIdx.x / G, ue = pl.units * (blockIdx.x + 1) / G;
+    for (long long u = ub; u < ue;) {
+        const int tile = (int)(u / g.nz);
+        const long long tend = (long long)(tile + 1) * g.nz;
+        const long long uend = ue < tend ? ue : tend;
+        const int k0 = 1 + (int)(u - (long long)tile * g.nz), k1 = (int)(uend - (long long)tile * g.nz);
+        u = uend;
+        const int ty = tile / pl.ntx, tx = tile - ty * pl.ntx;
+        const int j = ty * pl.rows + lr;  // region row 0 is the row before the tile's first
+        const int m = tx * pl.tpx - pl.xh + lm;
+        const bool valid = tin && j <= g.ny + 1 && m >= 0 && m < pl.npair;
+        const int jc = valid ? j : 0, mc = valid ? m : 0;  // in-bounds addresses for every thread
+        const int i0 = 2 * mc, i1 = i0 + 1;
+        const bool rowin = valid && jc >= 1 && jc <= g.ny;
+        const bool a0 = rowin && i0 >= 1, a1 = rowin && i1 <= g.nx;
+        const bool out2 = rowin && lr >= 1 && lr <= pl.rows && lm >= pl.xh && lm < pl.xh + pl.tpx;
+        const float ae0 = (i0 != g.nx) ? cx : 0.0f, aw0 = (i0 != 1) ? cx : 0.0f;
+        const float ae1 = (i1 != g.nx) ? cx : 0.0f, aw1 = (i1 != 1) ? cx : 0.0f;
+        const float an = (jc != g.ny) ? cy : 0.0f, as = (jc != 1) ? cy : 0.0f;
+        const float2 dm = make_float2(-(ae0 + aw0 + an + as + cz + cz), -(ae1 + aw1 + an + as + cz + cz));
+        const float2 rm = make_float2(__frcp_rn(dm.x), __frcp_rn(dm.y));
+        const int w = ((jc * g.px) >> 1) + mc;
+        // the halo rows take their outer y neighbour from memory
+        const bool lo_edge = lr == 0, hi_edge = lr == pl.rh - 1;
+        const bool need_o = rowin && (lo_edge || hi_edge);
+        const int wo = lo_edge ? w - wr : w + wr;
+        const bool wpair = mc > 0 && lm > 0, epair = lm < pl.rw - 1;  // x neighbours inside the region
+        const int sa = k0 - 1, sb = k1 + 1;
+        auto cl = [&](int s) { return s > g.nz + 1 ? g.nz + 1 : s; };
+        float2 pm = P[w + (sa > 0 ? sa - 1 : 0) * wp], pc = P[w + sa * wp], pp = P[w + (sa + 1) * wp];
+        float2 po = need_o ? P[wo + sa * wp] : zero;
+        float2 rc = R[w + sa * wp], r1 = zero;
+        float2 qm = zero, qc = zero, qp = zero;  // first-sweep values at s-2, s-1, s
+        if (tin) s0[(sa & 1) * RS + t] = pc;
+        __syncthreads();
+        for (int s = sa; s <= sb; ++s) {
+            const bool more = s < sb;
+            const float2 pq = more ? P[w + cl(s + 2) * wp] : zero;
+            const float2 pon = (more && need_o) ? P[wo + (s + 1) * wp] : zero;
+            const float2 rn = more ? R[w + (s + 1) * wp] : zero;
+            // first sweep at plane s
+            float2 v = pc;
+            if (rowin && s >= 1 && s <= g.nz) {
+                const float2* S0 = s0 + (s & 1) * RS + t;
+                const float pw = wpair ? S0[-1].y : 0.0f;
+                const float pe = epair ? S0[1].x : 0.0f;
+                const float2 pS = lo_edge ? po : S0[-pl.rw];
+                const float2 pN = hi_edge ? po : S0[pl.rw];
+                const bool kb = s == 1, kt = s == g.nz;
+                const float af = kt ? 0.0f : cz, ab = kb ? 0.0f : cz;
+                float2 d = dm, rd = rm;
+                if (kb || kt) {
+                    d = make_float2(-(ae0 + aw0 + an + as + af + ab), -(ae1 + aw1 + an + as + af + ab));
+                    rd = make_float2(__frcp_rn(d.x), __frcp_rn(d.y));
+                }
+                if (a0)
+                    v.x = div_rn_pre(rc.x - ae0 * pc.y - aw0 * pw - an * pN.x - as * pS.x - af * pp.x - ab * pm.x,
+                                     d.x, rd.x);
+                if (a1)
+                    v.y = div_rn_pre(rc.y - ae1 * pe - aw1 * pc.x - an * pN.y - as * pS.y - af * pp.y - ab * pm.y,
+                                     d.y, rd.y);
+            }
+            qm = qc;
+            qc = qp;
+            qp = v;
+            if (tin) {
+                s1[(s % 3) * RS + t] = v;
+                if (more) s0[((s + 1) & 1) * RS + t] = pp;
+            }
+            __syncthreads();
+            // second sweep at plane s - 1
+            const int q = s - 1;
+            if (q >= k0 && out2) {
+                const float2* S1 = s1 + (q % 3) * RS + t;
+                const float pw = mc > 0 ? S1[-1].y : 0.0f;
+                const float pe = epair ? S1[1].x : 0.0f;
+                const float2 pS = S1[-pl.rw], pN = S1[pl.rw];
+                const bool kb = q == 1, kt = q == g.nz;
+                const float af = kt ? 0.0f : cz, ab = kb ? 0.0f : cz;
+                float2 d = dm, rd = rm;
+                if (kb || kt) {
+                    d = make_float2(-(ae0 + aw0 + an + as + af + ab), -(ae1 + aw1 + an + as + af + ab));
+                    rd = make_float2(__frcp_rn(d.x), __frcp_rn(d.y));
+                }
+                const float v0 =
+                    div_rn_pre(r1.x - ae0 * qc.y - aw0 * pw - an * pN.x - as * pS.x - af * qp.x - ab * qm.x, d.x, rd.x);
+                const float v1 =
+                    div_rn_pre(r1.y - ae1 * pe - aw1 * qc.x - an * pN.y - as * pS.y - af * qp.y - ab * qm.y, d.y, rd.y);
+                const int o = w + q * wp;
+                if (a0 && a1)
+                    O[o] = make_float2(v0, v1);
+                else if (a0)
+                    pout[2 * o] = v0;
+                else if (a1)
+                    pout[2 * o + 1] = v1;
+            }
+            r1 = rc;
+            rc = rn;
+            pm = pc;
+            pc = pp;
+            pp = pq;
+            po = pon;
+        }
+        __syncthreads();  // the next segment reuses the planes
+    }
+}
+
+static int j2_blocks = 148;  // resident blocks of k_jacobi_pairs2 (SMs x 1), set by jacobi_tb_configure
+
+// Tile shape: for 1, 2, 3 ... tiles along x, the widest region that fits a
+// block (at least four tile rows), keeping the shape with the least
+// first-sweep work per output pair.
+static J2Plan j2_plan(const Geom& g) {
+    J2Plan best{};
+    double best_cost = 1e300;
+    const int npair = g.nx / 2 + 1;
+    for (int ntx = 1; ntx <= 64; ++ntx) {
+        J2Plan p{};
+        p.npair = npair;
+        p.ntx = ntx;
+        p.tpx = (npair + ntx - 1) / ntx;
+        if (ntx > 1 && (p.tpx - 1) * ntx >= npair) continue;  // same tiles as fewer of them
+        p.xh = ntx > 1 ? 1 : 0;
+        p.rw = p.tpx + 2 * p.xh;
+        if (p.rw > J2_THREADS / 6) continue;
+        p.rh = J2_THREADS / p.rw;
+        p.rows = p.rh - 2;
+        if (p.rows > g.ny) {
+            p.rows = g.ny;
+            p.rh = p.rows + 2;
+        }
+        p.nty = (g.ny + p.rows - 1) / p.rows;
+        p.units = (long long)p.ntx * p.nty * g.nz;
+        const double cost = (double)p.rw * p.rh / ((double)p.tpx * p.rows);
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best = p;
+        }
+    }
+    return best;
+}
+
+// Also needs enough work to give every resident block four planes or more:
+// on smaller grids the single sweeps keep more of the device busy.
+bool jacobi_pairs2_supported(const Geom& g) {
+    const J2Plan p = j2_plan(g);
+    return p.rw > 0 && p.rows >= 1 && g.px % 2 == 0 && p.units / 4 >= j2_blocks;
+}
+
+cudaError_t jacobi_pairs2_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s) {
+    const J2Plan p = j2_plan(g);
+    if (p.rw <= 0) return cudaErrorInvalidValue;
+    // at least about four planes per block: shorter ranges spend most of
+    // their time on the extra first-sweep planes at their ends
+    long long nb = p.units / 4;
+    if (nb > j2_blocks) nb = j2_blocks;
+    if (nb < 1) nb = 1;
+    const size_t smem = sizeof(float2) * 5u * (size_t)p.rw * p.rh;
+    k_jacobi_pairs2<<<(unsigned)nb, J2_THREADS, smem, s>>>(g, pin, rhs, pout, p);
+    return cudaGetLastError();
+}
+
 size_t jacobi_tb_smem_bytes(int T) {
     switch (T) {
         case 1: return JTile<1>::SMEM;
@@ -442,6 +661,10 @@ cudaError_t jacobi_tb_configure() {
         (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_pairs, JP_THREADS, 0)) != cudaSuccess)
         return e;
     jp_wave = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_pairs2, J2_THREADS,
+                                                           sizeof(float2) * 5u * J2_THREADS)) != cudaSuccess)
+        return e;
+    j2_blocks = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
     if ((e = cudaFuncSetAttribute(k_jacobi_tb<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)JTile<1>::SMEM)) != cudaSuccess)
         return e;

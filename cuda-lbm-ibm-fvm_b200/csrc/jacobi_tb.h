@@ -27,6 +27,12 @@ cudaError_t jacobi_col_launch(const Geom& g, const float* pin, const float* rhs,
 // The same sweep with two cells per thread (packed FP32, same bits).
 cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);
 
+// Two sweeps in one launch (the first sweep's planes kept in shared memory),
+// same bits as two jacobi_pairs_launch calls; pout is a third buffer (not
+// pin), whose ghost cells are left as they are.
+cudaError_t jacobi_pairs2_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);
+bool jacobi_pairs2_supported(const Geom& g);
+
 // Dynamic shared memory of one block for T fused sweeps.
 size_t jacobi_tb_smem_bytes(int T);
 

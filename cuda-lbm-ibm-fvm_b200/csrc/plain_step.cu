@@ -415,26 +415,36 @@ static_assert(JACOBI_T >= 1 && JACOBI_T <= JACOBI_TB_MAX, "VOF_JACOBI_T out of r
 // Launches for `iters` sweeps: ceil(iters / JACOBI_T), except that a single
 // blocked launch cannot end in the buffer it reads, so iters == JACOBI_T
 // (even) runs as single sweeps.
-// Jacobi kernels: one streaming sweep per launch with two cells per thread
-// (k_jacobi_pairs, the default), the same with one cell per thread
-// (k_jacobi_col), or JACOBI_T blocked sweeps per launch (k_jacobi_tb).
-// VOF_JACOBI=pairs|col|tb forces one.
-enum { JACOBI_PAIRS = 0, JACOBI_COL = 1, JACOBI_TB = 2 };
-static int jacobi_kind(const Geom&) {
+// Jacobi kernels: two sweeps per launch with two cells per thread
+// (k_jacobi_pairs2, the default; an odd count starts with one single sweep),
+// one sweep per launch with two cells per thread (k_jacobi_pairs) or with
+// one (k_jacobi_col), or JACOBI_T blocked sweeps per launch through TMA
+// (k_jacobi_tb).  VOF_JACOBI=pairs2|pairs|col|tb forces one.  All give the
+// same bits.
+enum { JACOBI_PAIRS = 0, JACOBI_COL = 1, JACOBI_TB = 2, JACOBI_PAIRS2 = 3 };
+static int jacobi_kind(const Geom& g) {
     static int forced = -2;
     if (forced == -2) {
         const char* v = getenv("VOF_JACOBI");
-        forced = !v ? -1
-                    : (!strcmp(v, "pairs") ? JACOBI_PAIRS
-                                           : (!strcmp(v, "col") ? JACOBI_COL : (!strcmp(v, "tb") ? JACOBI_TB : -1)));
+        forced = -1;
+        if (v && !strcmp(v, "pairs")) forced = JACOBI_PAIRS;
+        if (v && !strcmp(v, "col")) forced = JACOBI_COL;
+        if (v && !strcmp(v, "tb")) forced = JACOBI_TB;
+        if (v && !strcmp(v, "pairs2")) forced = JACOBI_PAIRS2;
     }
-    return forced >= 0 ? forced : JACOBI_PAIRS;
+    const int k = forced >= 0 ? forced : JACOBI_PAIRS2;
+    return (k == JACOBI_PAIRS2 && !jacobi_pairs2_supported(g)) ? JACOBI_PAIRS : k;
 }
-static bool jacobi_streaming(const Geom& g) { return jacobi_kind(g) != JACOBI_TB; }
+static bool jacobi_streaming(const Geom& g) {
+    const int k = jacobi_kind(g);
+    return k == JACOBI_PAIRS || k == JACOBI_COL;
+}
+static int jacobi_per_launch(const Geom& g) { return jacobi_kind(g) == JACOBI_PAIRS2 ? 2 : JACOBI_T; }
 
 static int jacobi_launches(const Geom& g, int iters) {
     if (jacobi_streaming(g)) return iters;
-    const int L = (iters + JACOBI_T - 1) / JACOBI_T;
+    const int T = jacobi_per_launch(g);
+    const int L = (iters + T - 1) / T;
     return (L == 1 && iters % 2 == 0) ? iters : L;
 }
 
@@ -517,14 +527,24 @@ cudaError_t plain_back(const Geom& g, const PlainBuffers& b, int istep, const fl
     if ((e = mark(ev, 3, s)) != cudaSuccess) return e;
     if ((e = plain_correct(g, b, p, s)) != cudaSuccess || (e = mark(ev, 4, s)) != cudaSuccess) return e;
 
-    // Sweep order by istep % 3 (voftrial1.cu:1384-1396).
+    // Sweep order by istep % 3 (voftrial1.cu:1384-1396).  The sweeps run out
+    // of place, F -> s1 -> s2 -> F, through the two pressure buffers that do
+    // not hold the pressure: the next step's solve writes their interiors
+    // before it reads them, and their ghost cells (never written by a sweep or
+    // a Jacobi launch) hold finite values, which a sweep reads only through
+    // the zero velocity of a wall face.
     const int r = ((istep % 3) + 3) % 3;
     static const int order[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
+    float* s1 = (p == b.p0) ? b.p1 : b.p0;
+    float* s2 = b.p2;
+    const bool oop = s1 && s2 && p != b.p2;
+    const float* src[3] = {b.F, s1, s2};
+    float* dst[3] = {s1, s2, b.F};
     for (int q = 0; q < 3; ++q) {
         const int axis = order[r][q];
         const float* vel = axis == 0 ? b.u : (axis == 1 ? b.v : b.w);
-        if ((e = fct_launch(g, axis, q == 2, b.F, vel, s)) != cudaSuccess || (e = mark(ev, 5 + q, s)) != cudaSuccess)
-            return e;
+        e = oop ? fct_launch_to(g, axis, q == 2, src[q], dst[q], vel, s) : fct_launch(g, axis, q == 2, b.F, vel, s);
+        if (e != cudaSuccess || (e = mark(ev, 5 + q, s)) != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
@@ -541,11 +561,20 @@ cudaError_t plain_pressure(const Geom& g, const PlainBuffers& b, int jacobi_iter
     // reference's ghost entries in a download).
     float* pbuf[3] = {b.p0, b.p1, b.p2};
     const int src = *p_parity, dst = src ^ (jacobi_iters & 1);
-    const int L = (jacobi_iters + JACOBI_T - 1) / JACOBI_T;
+    const int T = jacobi_per_launch(g);
+    const int L = (jacobi_iters + T - 1) / T;
     int seq[64];
-    if (jacobi_streaming(g)) {
+    if (jacobi_kind(g) == JACOBI_PAIRS2 && L <= 62 && plan_buffers(src, dst, L, seq)) {
+        // an odd count starts with one single sweep
+        for (int q = 0; q < L; ++q) {
+            const bool single = q == 0 && (jacobi_iters & 1);
+            e = single ? jacobi_pairs_launch(g, pbuf[seq[q]], b.rhs, pbuf[seq[q + 1]], s)
+                       : jacobi_pairs2_launch(g, pbuf[seq[q]], b.rhs, pbuf[seq[q + 1]], s);
+            if (e != cudaSuccess) return e;
+        }
+    } else if (jacobi_streaming(g) || jacobi_kind(g) == JACOBI_PAIRS2) {
         int cur = src;
-        const bool pairs = jacobi_kind(g) == JACOBI_PAIRS;
+        const bool pairs = jacobi_kind(g) != JACOBI_COL;
         for (int it = 0; it < jacobi_iters; ++it) {
             e = pairs ? jacobi_pairs_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s)
                       : jacobi_col_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s);

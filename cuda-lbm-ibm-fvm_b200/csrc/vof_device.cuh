@@ -60,6 +60,10 @@ __host__ __device__ __forceinline__ float clamp01f(float v) {
 // provided nothing underflows or overflows.  Outside the range where that
 // holds (tiny, huge or non-finite operands) the IEEE division is used, and
 // +-0 numerators return x*rd, which carries the IEEE sign of 0/d.
+// The IEEE division outside that range, kept out of line: it is rare, and
+// inlined at every call site it would cost issue slots on every cell.
+static __device__ __noinline__ float div_rn_slow(float x, float d) { return __fdiv_rn(x, d); }
+
 __device__ __forceinline__ float div_rn_pre(float x, float d, float rd) {
     const float q0 = __fmul_rn(x, rd);
     const float r = __fmaf_rn(-q0, d, x);
@@ -67,7 +71,7 @@ __device__ __forceinline__ float div_rn_pre(float x, float d, float rd) {
     const float ax = fabsf(x), aq = fabsf(q0);
     if (ax >= 0x1p-96f && aq >= 0x1p-96f && aq <= 0x1p+96f) return q1;
     if (x == 0.0f) return q0;
-    return __fdiv_rn(x, d);
+    return div_rn_slow(x, d);
 }
 
 // 1/x for a positive normal FP64 x, to within about one ulp (not always

@@ -120,6 +120,9 @@ def _declare(lib):
         "vof_adjoint_keeps": (C.c_int, [vp]),
         "vof_debug_fail_alloc": (C.c_int, [C.c_int]),
         "vof_debug_wait_timeout": (C.c_int, [vp, C.c_uint]),
+        "vof_get_planes": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, C.c_int]),
+        "vof_put_planes": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, C.c_int]),
+        "vof_reduce_range": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, P(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -148,7 +151,8 @@ def exported_symbols():
             "vof_last_cuda_error", "vof_kernels_per_step", "vof_device_bytes",
             "vof_step_timed", "vof_phase_name", "vof_solver_stats", "vof_step_noalloc",
             "vof_forward_record", "vof_backward", "vof_adjoint_download", "vof_adjoint_kernels_per_step",
-            "vof_adjoint_storage", "vof_adjoint_keeps", "vof_debug_fail_alloc", "vof_debug_wait_timeout"]
+            "vof_adjoint_storage", "vof_adjoint_keeps", "vof_debug_fail_alloc", "vof_debug_wait_timeout",
+            "vof_get_planes", "vof_put_planes", "vof_reduce_range"]
 
 
 def default_params(nx: int, ny: int | None = None, nz: int | None = None, **overrides) -> Params:
@@ -241,6 +245,40 @@ class Solver:
 
     def state(self) -> dict:
         return {f: self.download(f) for f in STATE_FIELDS}
+
+    def get_planes(self, field, k0: int, nk: int, out=None, device_ptr: int | None = None):
+        """Planes k0 .. k0+nk-1 of a field (reference layout): into `out` (a
+        host float32 array of nk (ny+2)(nx+2) values, allocated when None) or
+        to a device pointer (stream-ordered)."""
+        fid = self._fid(field)
+        if device_ptr is not None:
+            self._check(self._lib.vof_get_planes(self._ctx, fid, k0, nk, C.c_void_p(device_ptr), 1), "vof_get_planes")
+            return None
+        if out is None:
+            out = np.empty((nk, self.prm.ny + 2, self.prm.nx + 2), dtype=np.float32)
+        assert out.dtype == np.float32 and out.flags.c_contiguous and out.size == nk * (self.prm.ny + 2) * (self.prm.nx + 2)
+        self._check(self._lib.vof_get_planes(self._ctx, fid, k0, nk, out.ctypes.data_as(C.c_void_p), 0),
+                    "vof_get_planes")
+        return out
+
+    def put_planes(self, field, k0: int, arr=None, device_ptr: int | None = None, nk: int | None = None):
+        """Write planes k0 .. from a host array (nk, ny+2, nx+2) or a device pointer (nk given)."""
+        fid = self._fid(field)
+        if device_ptr is not None:
+            self._check(self._lib.vof_put_planes(self._ctx, fid, k0, int(nk), C.c_void_p(device_ptr), 1),
+                        "vof_put_planes")
+            return
+        a = np.ascontiguousarray(arr, dtype=np.float32)
+        nk = a.size // ((self.prm.ny + 2) * (self.prm.nx + 2))
+        self._check(self._lib.vof_put_planes(self._ctx, fid, k0, nk, a.ctypes.data_as(C.c_void_p), 0),
+                    "vof_put_planes")
+        self._check(self._lib.vof_sync(self._ctx), "vof_sync")  # `a` may be a temporary
+
+    def reduce_range(self, what, k0: int, k1: int) -> float:
+        out = C.c_double()
+        w = REDUCTIONS[what] if isinstance(what, str) else int(what)
+        self._check(self._lib.vof_reduce_range(self._ctx, w, k0, k1, C.byref(out)), "vof_reduce_range")
+        return out.value
 
     # -- stepping ------------------------------------------------------------
     def step(self, istep: int):

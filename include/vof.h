@@ -154,6 +154,21 @@ int vof_upload(vof_ctx* ctx, int field, const float* src, int src_is_device);
 int vof_download(vof_ctx* ctx, int field, float* dst, int dst_is_device);
 
 /*
+ * Planes k0 .. k0+nk-1 (0 <= k0, k0+nk <= nz+2; ghost planes included) of
+ * one field, in the reference layout of a plane ((ny+2)(nx+2) floats, i
+ * fastest, planes consecutive), out of or into the context.  The halo
+ * exchange of a z-slab decomposition moves planes with these (no counterpart
+ * in the reference, which runs on one GPU; the host loop it would sit in is
+ * voftrial1.cu:1361-1401).  Device buffers: stream-ordered, no host
+ * synchronisation; host buffers: vof_get_planes waits for the copy,
+ * vof_put_planes needs the host memory valid until the stream reaches the
+ * copy.  vof_put_planes of VOF_FIELD_P: VOF_E_UNSUPPORTED in the convergent
+ * modes (their pressure state is the FP64 copy).
+ */
+int vof_get_planes(vof_ctx* ctx, int field, int k0, int nk, float* dst, int dst_is_device);
+int vof_put_planes(vof_ctx* ctx, int field, int k0, int nk, const float* src, int src_is_device);
+
+/*
  * One time step, exactly the sequence of voftrial1.cu:1364-1401 for the
  * given istep (the value the reference's loop has after `++istep`, so the
  * first step is istep = 1; istep % 3 picks the FCT sweep order,
@@ -190,6 +205,15 @@ int vof_sync(vof_ctx* ctx);
 
 /* Blocking reduction over the current state (VOF_RED_*); result in *out. */
 int vof_reduce(vof_ctx* ctx, int what, double* out);
+
+/*
+ * vof_reduce over the interior cells of planes k0..k1 only (1 <= k0 <= k1 <=
+ * nz), for VOF_RED_VOLUME, F_MIN, F_MAX, DIV_L2 and DIV_MAX (a plane's
+ * divergence uses the w faces above it); VOF_E_UNSUPPORTED for the others.
+ * The ranks of a z-slab decomposition reduce over the planes they own and
+ * combine (volumes add, DIV_L2 as the root of the summed squares).
+ */
+int vof_reduce_range(vof_ctx* ctx, int what, int k0, int k1, double* out);
 
 /*
  * Stream-ordered reduction: the result is written to *host_out (which should

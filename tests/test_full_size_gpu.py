@@ -7,10 +7,13 @@
   voftrial1.cu:1361-1401):
     - against the -fmad=false build: bit-identical in F, u, v, w and p;
     - against the build with nvcc's defaults (FMA contraction, the README's
-      kind of build): F max-abs <= 1e-3 and rel-L2 <= 1e-4; u, v, w rel-L2
-      <= 1e-3; p (mean removed, interior) rel-L2 <= 1e-3; the liquid volume
-      drift of the two runs differs by <= 1e-7 of the volume, and each stays
-      within 1e-5 of the initial volume.
+      kind of build): F max-abs <= 3e-4 and rel-L2 <= 3e-6; u, v, w rel-L2
+      <= 6e-6; p (mean removed, interior) rel-L2 <= 2e-5; the liquid volume
+      drift of the two runs differs by <= 1e-8 of the volume, and each stays
+      within 1e-5 of the initial volume.  (Measured on a B200: F max-abs
+      2.6e-5, rel-L2 3.0e-7; u, v 6.1e-7, w 4.2e-7; p 1.6e-6; drifts 3.220e-7
+      and 3.222e-7.  The bounds are ten times these: the differences are the
+      reference's own FMA rounding, the same in every run.)
 * MIXED convergent projection at 200^3 (the same inputs; BF16-stored /
   FP32-arithmetic multigrid inside FP64 defect correction to a relative
   residual <= 1e-8) against the FP64 oracle whose pressure is solved by
@@ -104,11 +107,11 @@ def test_dam_break_200_2000_steps_vs_reference_default_build(cuda, orc, workload
         "volume_drift_ref": (vr - v0) / v0,
     }
     report("dam_break_200_2000_vs_default_build", m)
-    assert m["F_max_abs"] <= 1e-3 and m["F_rel_l2"] <= 1e-4, m
+    assert m["F_max_abs"] <= 3e-4 and m["F_rel_l2"] <= 3e-6, m
     for k in ("u", "v", "w"):
-        assert m[f"{k}_rel_l2"] <= 1e-3, m
-    assert m["p_rel_l2_mean_removed"] <= 1e-3, m
-    assert abs(m["volume_drift_ours"] - m["volume_drift_ref"]) <= 1e-7, m
+        assert m[f"{k}_rel_l2"] <= 6e-6, m
+    assert m["p_rel_l2_mean_removed"] <= 2e-5, m
+    assert abs(m["volume_drift_ours"] - m["volume_drift_ref"]) <= 1e-8, m
     assert abs(m["volume_drift_ours"]) <= 1e-5 and abs(m["volume_drift_ref"]) <= 1e-5, m
 
 

@@ -72,12 +72,15 @@ def test_random_state_bitwise_vs_oracle(cuda, V, orc, nx, ny, nz, seed, dt, vs):
     assert_bitwise(got, want, STATE + ("ustar", "vstar", "wstar", "rhs"), f"{nx}x{ny}x{nz}")
 
 
-@pytest.mark.parametrize("env", [{"VOF_JACOBI": "tb"}, {"VOF_JACOBI": "col"}, {"VOF_JACOBI_KCHUNK": "1"},
-                                 {"VOF_JACOBI_KCHUNK": "5"}])
+@pytest.mark.parametrize("env", [{"VOF_JACOBI": "pairs"}, {"VOF_JACOBI": "tb"}, {"VOF_JACOBI": "col"},
+                                 {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "1"},
+                                 {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "5"}])
 def test_jacobi_kernel_choices_give_the_same_bits(cuda, V, orc, tmp_path, env):
-    """The Jacobi kernels a process may select (the blocked two-sweep kernel,
-    the one-cell streaming sweep, other z chunks of the paired sweep; read
-    once per process, so each runs in a child process) give the oracle's bits."""
+    """The Jacobi kernels a process may select (the default two-sweep paired
+    kernel runs in every other test; here the single-sweep paired kernel and
+    its z chunks, the TMA-blocked two-sweep kernel, the one-cell streaming
+    sweep; read once per process, so each runs in a child process) give the
+    oracle's bits."""
     import os
     import subprocess
     import sys
@@ -102,6 +105,31 @@ def test_jacobi_kernel_choices_give_the_same_bits(cuda, V, orc, tmp_path, env):
     got = dict(np.load(tmp_path / "out.npz"))
     want = orc.run_f32(prm, state, 1, 3)
     assert_bitwise(got, want, STATE, str(env))
+
+
+@pytest.mark.parametrize("shape,seed,vfrac", [((40, 36, 34), 41, 0.45), ((130, 17, 19), 42, 0.3),
+                                              ((17, 130, 9), 43, 0.6), ((9, 11, 140), 44, 0.45),
+                                              ((250, 12, 10), 45, 0.2)])
+def test_sparse_interface_bitwise_vs_oracle(cuda, V, orc, shape, seed, vfrac):
+    """F exactly 0 over irregular regions (runs of every length along every
+    axis, lines longer than one x window of the x sweep, a gas slab covering
+    whole x windows) next to mixed cells, velocities of both signs with a
+    standard deviation of vfrac times the sweeps' quiet-window velocity bound
+    (0.49 dx / dt), so some exceed it: the sweeps' zero-window shortcuts
+    against the full arithmetic of the oracle, every sweep order, bit for bit."""
+    prm = V.default_params(*shape, dt=1e-3, gy=0.0, gz=-9.81)
+    vq = 0.49 * float(prm.dx) / float(prm.dt)
+    st = ic.random_state(prm, seed=seed, vel_scale=vfrac * vq)
+    nz, ny, nx = prm.shape
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    ph = ic.uniform(seed, 6, 0.0, 2 * np.pi)
+    wave = (np.sin(0.37 * i + ph[0]) * np.sin(0.23 * j + ph[1]) * np.sin(0.31 * k + ph[2]) +
+            0.5 * np.sin(0.11 * (i + j + k) + ph[3]))
+    st["F"] = np.where(wave < 0.15, 0.0, st["F"]).astype(np.float32)
+    st["F"][:, :, nx // 2:] = 0.0  # gas slab
+    got = run_gpu(V, prm, st, 1, 3, extras=True)
+    want = orc.run_f32(prm, st, 1, 3, extras=True)
+    assert_bitwise(got, want, STATE + ("ustar", "vstar", "wstar", "rhs"), f"sparse {shape}")
 
 
 @pytest.mark.parametrize("istep", [1, 2, 3])
