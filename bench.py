@@ -23,8 +23,12 @@ reference: the reference's own voftrial1.cu kernels (oracle/_ref, built from
   the reference source; the reference has no CPU implementation of the path),
   sm_100a build and README build, better of the two; rank 0 only.
 
-Multi-GPU: independent replicas, one 200^3 problem per rank (weak scaling, no
-data-path collective); value = cells * steps * N / max-over-ranks time.
+Multi-GPU (--decomp slab, the default): one n x n x (n N) grid cut into z
+slabs of n planes per GPU, each rank stepping its slab plus a halo and
+exchanging the halos with its neighbours over NCCL after every step
+(vof_b200.slab; weak scaling); value = cells of the grid * steps / max-over-
+ranks time.  --decomp replicas: N independent n^3 problems, no data-path
+collective.
 """
 from __future__ import annotations
 
@@ -94,6 +98,9 @@ def parse_args(argv=None):
                     help="steps of the adjoint measurement at 64^3 (the bench size runs 1/8 of them; 0 disables)")
     ap.add_argument("--no-small", dest="small", action="store_false",
                     help="skip the 32^3 / 64^3 plain-step measurement")
+    ap.add_argument("--decomp", choices=("slab", "replicas"), default="slab",
+                    help="N > 1: one grid of n x n x (n N) cells cut into z slabs of n planes per GPU with a "
+                         "halo exchange every step (slab), or N independent n^3 problems (replicas)")
     ap.add_argument("--drive-steps", type=int, default=300,
                     help="steps of the drop-in program run (voftrial1.cu's main at 200^3 with a dump every "
                          "100 steps), timed end to end (0 disables)")
@@ -519,6 +526,12 @@ def run_ours(args):
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+        if args.decomp == "slab":
+            try:
+                run_slab(args, V, rank, world, dev)
+            finally:
+                dist.destroy_process_group()
+            return
 
     prm = workload_params(args.n)
     state = workload_state(prm)
@@ -625,6 +638,9 @@ def run_ours(args):
         Fout = torch.empty(prm.shape, dtype=torch.float32).pin_memory()
         solver2 = V.Solver(prm, stream=stream.cuda_stream)
         solver2.run(1, 3)  # graph capture outside the timed region
+        # the output buffer's first device write outside the timed region
+        # (the first DMA into freshly pinned pages runs at a few GB/s)
+        solver2.download("F", Fout.numpy())
         solver.run(istep, W_eff)  # the GPU busy right up to the timed region
         istep += W_eff
         barrier(world, dev)
@@ -700,6 +716,135 @@ def run_ours(args):
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# N GPUs, one grid: z slabs with a halo exchange every step (vof_b200.slab)
+# ---------------------------------------------------------------------------
+def slab_global_params(n, world):
+    """The n x n x (n world) dam break: the bench's constants, dz of the n^3
+    grid (the box is world times as tall)."""
+    prm = workload_params(n)
+    g = prm.copy()
+    g.nz = n * world
+    g.kmax = g.nz
+    g.nTot = (g.nx + 2) * (g.ny + 2) * (g.nz + 2)
+    g.Lz = float(np.float32(prm.Lz) * np.float32(world))
+    return g
+
+
+def run_slab(args, V, rank, world, dev):
+    """Weak scaling over one grid: each of the `world` ranks owns n planes of
+    an n x n x (n world) dam break (interface height 0.06 + 0.5 dx U(-1, 1),
+    seed 1: liquid in the lowest slab), steps them with a halo of
+    slab.halo_for(10) planes, and exchanges the halos with its neighbours over
+    NCCL (point-to-point) after every step.  value = owned cells of all ranks
+    x K / max over ranks of the device time of K steps (halo exchange
+    included)."""
+    import torch
+
+    from vof_b200 import ic, slab
+
+    stream = torch.cuda.current_stream(dev)
+    props = torch.cuda.get_device_properties(dev)
+    prm = slab_global_params(args.n, world)
+    state = ic.rest_state(prm, ic.dam_break(prm, height=ic.noisy_height(prm, seed=1)))
+    comm = slab.TorchComm()
+    r = slab.SlabRank(prm, comm, lambda q: V.Solver(q, stream=stream.cuda_stream), device=dev)
+    r.upload_global(state)
+    K, W = args.steps, max(3, args.warmup)
+    gpu_id = None
+    try:
+        gpu_id = "GPU-" + str(props.uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(gpu_id)
+    clocks.start()
+    clocks.wait_first()
+    istep = 1
+    r.run(istep, max(W, 20))
+    istep += max(W, 20)
+    W_eff = max(W, 20)
+    barrier(world, dev)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    r.run(istep, K)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    barrier(world, dev)
+    istep += K
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, world, dev)
+    own_cells = prm.nx * prm.ny * (r.slab.own1 - r.slab.own0 + 1)
+    cells_all = prm.nx * prm.ny * prm.nz
+    value = cells_all * K / (ms_max / 1e3) / 1e6
+    # the halo exchange alone (K of them) and the rank's step alone
+    barrier(world, dev)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(K):
+        r.exchange()
+    e1.record(stream)
+    e1.synchronize()
+    ex_ms = max_over_ranks(e0.elapsed_time(e1), world, dev) / K
+    barrier(world, dev)
+    e0.record(stream)
+    r.engine.run(istep, K)
+    e1.record(stream)
+    e1.synchronize()
+    step_ms = max_over_ranks(e0.elapsed_time(e1), world, dev) / K
+    istep += K
+    r.upload_global(state)
+    barrier(world, dev)
+    # e2e: the local state from pinned host memory, K steps with the liquid
+    # volume all-reduced and read on the host every step, the owned F back
+    host = {k: torch.from_numpy(v).pin_memory() for k, v in slab.local_state(state, r.slab).items()}
+    Fout = torch.empty((r.slab.own1 - r.slab.own0 + 1, prm.ny + 2, prm.nx + 2), dtype=torch.float32).pin_memory()
+    torch.cuda.synchronize(dev)
+    barrier(world, dev)
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for k in slab.STATE:
+        r.engine._check(r.engine._lib.vof_upload(r.engine._ctx, V.FIELDS[k], C.c_void_p(host[k].data_ptr()), 0),
+                        "vof_upload")
+    vols = []
+    for s in range(K):
+        r.run(1 + s, 1)
+        vols.append(r.volume())
+    r.engine.get_planes("F", r.slab.local(r.slab.own0), Fout.shape[0], out=Fout.numpy())
+    a1.record(stream)
+    a1.synchronize()
+    e2e_ms = max_over_ranks(a0.elapsed_time(a1), world, dev)
+    clk = clocks.stop()
+    nbytes = sum(v.numel() * 4 for v in host.values())
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": W_eff, "ms_per_step": round(ms_max / K, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": f"dam_break_{prm.nx}x{prm.ny}x{prm.nz}_plain_fp32",
+                   "grid": [prm.nx, prm.ny, prm.nz], "steps_timed": K, "dt": float(prm.dt),
+                   "jacobi_iters": prm.jacobi_iters, "gravity": [float(prm.gx), float(prm.gy), float(prm.gz)],
+                   "ic": "liquid x<0.04, y<0.04, z<0.06+0.5*dx*U(-1,1) (splitmix64 seed 1), u=v=w=p=0",
+                   "l2_policy": "inputs larger than L2: 10 resident fields x %.0f MB per GPU"
+                                % (r.lprm.nTot * 4 / 1e6),
+                   "parallelism": f"z slabs x{world}, halo {slab.halo_for(prm.jacobi_iters)} planes, "
+                                  "NCCL point-to-point halo exchange every step",
+                   "planes_per_rank": [[s.own0, s.own1, s.lo, s.hi] for s in r.slabs]},
+        "e2e": {"value": round(cells_all * K / (e2e_ms / 1e3) / 1e6, 1), "unit": UNIT,
+                "h2d_bytes_per_step": world * nbytes / K, "d2h_bytes_per_step": (world * Fout.numel() * 4 + 8 * K) / K,
+                "ms": round(e2e_ms, 3), "final_volume": vols[-1]},
+        "halo_exchange_ms_per_step": round(ex_ms, 5), "rank_step_ms": round(step_ms, 5),
+        "halo_bytes_per_step_per_rank": int(sum(b.numel() * 4 for b in r.sbuf.values())),
+        "owned_cells_per_rank": own_cells, "clocks": clk,
+        "gpu_launches": r.engine.kernels_per_step * K,
+        "native_so_loaded": mapped_libraries(), "device": props.name,
+    }
+    for rr in (r.engine,):
+        rr.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------------------

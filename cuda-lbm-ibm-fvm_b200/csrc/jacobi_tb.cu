@@ -464,6 +464,23 @@ struct J2Plan {
 
 constexpr int J2_THREADS = 1024;
 
+// Diagonals a_p = -(ae + aw + an + as + af + ab) (the reference's operand
+// order) and their IEEE reciprocals for every pattern of wall sides: index
+// (e*1 + w*2 + n*4 + s*8) * 4 + (bottom plane) + 2*(top plane), a bit set
+// where that side's coefficient is the full one (the neighbour is not
+// beyond a wall).  Built by the block's first 64 threads.
+__device__ __forceinline__ void j2_diag_table(float2* tab, float cx, float cy, float cz) {
+    const int e = threadIdx.x;
+    if (e < 64) {
+        const int pat = e >> 2, cls = e & 3;
+        const float ae = (pat & 1) ? cx : 0.0f, aw = (pat & 2) ? cx : 0.0f;
+        const float an = (pat & 4) ? cy : 0.0f, as = (pat & 8) ? cy : 0.0f;
+        const float ab = (cls & 1) ? 0.0f : cz, af = (cls & 2) ? 0.0f : cz;
+        const float d = -(ae + aw + an + as + af + ab);
+        tab[e] = make_float2(d, __frcp_rn(d));
+    }
+}
+
 __global__ void __launch_bounds__(J2_THREADS, 1) k_jacobi_pairs2(Geom g, const float* __restrict__ pin,
                                                                const float* __restrict__ rhs,
                                                                float* __restrict__ pout, J2Plan pl) {
@@ -471,10 +488,12 @@ __global__ void __launch_bounds__(J2_THREADS, 1) k_jacobi_pairs2(Geom g, const f
     const int RS = pl.rw * pl.rh;  // pairs of one region plane
     float2* s0 = j2s;              // [2][RS] input planes
     float2* s1 = j2s + 2 * RS;     // [3][RS] first-sweep planes
+    float2* tab = j2s + 5 * RS;    // [64] diagonals (j2_diag_table)
     const int t = threadIdx.x;
     const bool tin = t < RS;
     const int lr = tin ? t / pl.rw : 0, lm = tin ? t - lr * pl.rw : 0;
     const float cx = g.dxi * g.dxi, cy = g.dyi * g.dyi, cz = g.dzi * g.dzi;
+    j2_diag_table(tab, cx, cy, cz);
     const int wp = g.plane >> 1, wr = g.px >> 1;
     const float2* P = reinterpret_cast<const float2*>(pin);
     const float2* R = reinterpret_cast<const float2*>(rhs);
@@ -500,8 +519,9 @@ __global__ void __launch_bounds__(J2_THREADS, 1) k_jacobi_pairs2(Geom g, const f
         const float ae0 = (i0 != g.nx) ? cx : 0.0f, aw0 = (i0 != 1) ? cx : 0.0f;
         const float ae1 = (i1 != g.nx) ? cx : 0.0f, aw1 = (i1 != 1) ? cx : 0.0f;
         const float an = (jc != g.ny) ? cy : 0.0f, as = (jc != 1) ? cy : 0.0f;
-        const float2 dm = make_float2(-(ae0 + aw0 + an + as + cz + cz), -(ae1 + aw1 + an + as + cz + cz));
-        const float2 rm = make_float2(__frcp_rn(dm.x), __frcp_rn(dm.y));
+        const int pj = (jc != g.ny ? 4 : 0) | (jc != 1 ? 8 : 0);
+        const int t0 = ((i0 != g.nx ? 1 : 0) | (i0 != 1 ? 2 : 0) | pj) * 4;
+        const int t1 = ((i1 != g.nx ? 1 : 0) | (i1 != 1 ? 2 : 0) | pj) * 4;
         const int w = ((jc * g.px) >> 1) + mc;
         // the halo rows take their outer y neighbour from memory
         const bool lo_edge = lr == 0, hi_edge = lr == pl.rh - 1;
@@ -509,16 +529,17 @@ __global__ void __launch_bounds__(J2_THREADS, 1) k_jacobi_pairs2(Geom g, const f
         const int wo = lo_edge ? w - wr : w + wr;
         const bool wpair = mc > 0 && lm > 0, epair = lm < pl.rw - 1;  // x neighbours inside the region
         const int sa = k0 - 1, sb = k1 + 1;
-        auto cl = [&](int s) { return s > g.nz + 1 ? g.nz + 1 : s; };
         float2 pm = P[w + (sa > 0 ? sa - 1 : 0) * wp], pc = P[w + sa * wp], pp = P[w + (sa + 1) * wp];
         float2 po = need_o ? P[wo + sa * wp] : zero;
         float2 rc = R[w + sa * wp], r1 = zero;
         float2 qm = zero, qc = zero, qp = zero;  // first-sweep values at s-2, s-1, s
         if (tin) s0[(sa & 1) * RS + t] = pc;
         __syncthreads();
+        int s3 = sa % 3;  // s % 3
         for (int s = sa; s <= sb; ++s) {
             const bool more = s < sb;
-            const float2 pq = more ? P[w + cl(s + 2) * wp] : zero;
+            const int s2 = s + 2 > g.nz + 1 ? g.nz + 1 : s + 2;
+            const float2 pq = more ? P[w + s2 * wp] : zero;
             const float2 pon = (more && need_o) ? P[wo + (s + 1) * wp] : zero;
             const float2 rn = more ? R[w + (s + 1) * wp] : zero;
             // first sweep at plane s
@@ -531,44 +552,40 @@ __global__ void __launch_bounds__(J2_THREADS, 1) k_jacobi_pairs2(Geom g, const f
                 const float2 pN = hi_edge ? po : S0[pl.rw];
                 const bool kb = s == 1, kt = s == g.nz;
                 const float af = kt ? 0.0f : cz, ab = kb ? 0.0f : cz;
-                float2 d = dm, rd = rm;
-                if (kb || kt) {
-                    d = make_float2(-(ae0 + aw0 + an + as + af + ab), -(ae1 + aw1 + an + as + af + ab));
-                    rd = make_float2(__frcp_rn(d.x), __frcp_rn(d.y));
-                }
+                const int cls = (kb ? 1 : 0) | (kt ? 2 : 0);
+                const float2 d0 = tab[t0 + cls], d1 = tab[t1 + cls];
                 if (a0)
                     v.x = div_rn_pre(rc.x - ae0 * pc.y - aw0 * pw - an * pN.x - as * pS.x - af * pp.x - ab * pm.x,
-                                     d.x, rd.x);
+                                     d0.x, d0.y);
                 if (a1)
                     v.y = div_rn_pre(rc.y - ae1 * pe - aw1 * pc.x - an * pN.y - as * pS.y - af * pp.y - ab * pm.y,
-                                     d.y, rd.y);
+                                     d1.x, d1.y);
             }
             qm = qc;
             qc = qp;
             qp = v;
             if (tin) {
-                s1[(s % 3) * RS + t] = v;
+                s1[s3 * RS + t] = v;
                 if (more) s0[((s + 1) & 1) * RS + t] = pp;
             }
             __syncthreads();
             // second sweep at plane s - 1
             const int q = s - 1;
             if (q >= k0 && out2) {
-                const float2* S1 = s1 + (q % 3) * RS + t;
+                const float2* S1 = s1 + (s3 == 0 ? 2 : s3 - 1) * RS + t;
                 const float pw = mc > 0 ? S1[-1].y : 0.0f;
                 const float pe = epair ? S1[1].x : 0.0f;
                 const float2 pS = S1[-pl.rw], pN = S1[pl.rw];
                 const bool kb = q == 1, kt = q == g.nz;
                 const float af = kt ? 0.0f : cz, ab = kb ? 0.0f : cz;
-                float2 d = dm, rd = rm;
-                if (kb || kt) {
-                    d = make_float2(-(ae0 + aw0 + an + as + af + ab), -(ae1 + aw1 + an + as + af + ab));
-                    rd = make_float2(__frcp_rn(d.x), __frcp_rn(d.y));
-                }
+                const int cls = (kb ? 1 : 0) | (kt ? 2 : 0);
+                const float2 d0 = tab[t0 + cls], d1 = tab[t1 + cls];
                 const float v0 =
-                    div_rn_pre(r1.x - ae0 * qc.y - aw0 * pw - an * pN.x - as * pS.x - af * qp.x - ab * qm.x, d.x, rd.x);
+                    div_rn_pre(r1.x - ae0 * qc.y - aw0 * pw - an * pN.x - as * pS.x - af * qp.x - ab * qm.x, d0.x,
+                               d0.y);
                 const float v1 =
-                    div_rn_pre(r1.y - ae1 * pe - aw1 * qc.x - an * pN.y - as * pS.y - af * qp.y - ab * qm.y, d.y, rd.y);
+                    div_rn_pre(r1.y - ae1 * pe - aw1 * qc.x - an * pN.y - as * pS.y - af * qp.y - ab * qm.y, d1.x,
+                               d1.y);
                 const int o = w + q * wp;
                 if (a0 && a1)
                     O[o] = make_float2(v0, v1);
@@ -583,6 +600,7 @@ __global__ void __launch_bounds__(J2_THREADS, 1) k_jacobi_pairs2(Geom g, const f
             pc = pp;
             pp = pq;
             po = pon;
+            s3 = s3 == 2 ? 0 : s3 + 1;
         }
         __syncthreads();  // the next segment reuses the planes
     }
@@ -638,7 +656,7 @@ cudaError_t jacobi_pairs2_launch(const Geom& g, const float* pin, const float* r
     long long nb = p.units / 4;
     if (nb > j2_blocks) nb = j2_blocks;
     if (nb < 1) nb = 1;
-    const size_t smem = sizeof(float2) * 5u * (size_t)p.rw * p.rh;
+    const size_t smem = sizeof(float2) * (5u * (size_t)p.rw * p.rh + 64u);
     k_jacobi_pairs2<<<(unsigned)nb, J2_THREADS, smem, s>>>(g, pin, rhs, pout, p);
     return cudaGetLastError();
 }
@@ -662,7 +680,7 @@ cudaError_t jacobi_tb_configure() {
         return e;
     jp_wave = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_pairs2, J2_THREADS,
-                                                           sizeof(float2) * 5u * J2_THREADS)) != cudaSuccess)
+                                                           sizeof(float2) * (5u * J2_THREADS + 64u))) != cudaSuccess)
         return e;
     j2_blocks = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
     if ((e = cudaFuncSetAttribute(k_jacobi_tb<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -28,7 +28,9 @@ REF_LIBS = {
     "nofma": ORACLE_DIR / "_ref" / "libvofref_nofma.so",     # same, -fmad=false
     "readme": ORACLE_DIR / "_ref" / "libvofref_readme.so",   # README flags, PTX JIT
 }
-REFERENCE_SRC = Path(os.environ.get("VOF_REFERENCE_DIR", "/root/reference"))
+# The reference checkout (the directory holding voftrial1.cu), for building
+# the harness only: given by VOF_REFERENCE_DIR or by the caller of build().
+REFERENCE_SRC = Path(os.environ["VOF_REFERENCE_DIR"]) if os.environ.get("VOF_REFERENCE_DIR") else None
 
 STATE = ("F", "u", "v", "w", "p")
 
@@ -36,14 +38,20 @@ _oracle = None
 _refs = {}
 
 
-def build(ref: bool | None = None) -> None:
-    """make the oracle (always) and the reference harness (when its source exists)."""
+def build(ref: bool | None = None, ref_dir=None) -> None:
+    """make the oracle (always) and the reference harness from the reference
+    checkout `ref_dir` (or VOF_REFERENCE_DIR) when it holds voftrial1.cu."""
     targets = ["oracle"]
+    src = Path(ref_dir) if ref_dir else REFERENCE_SRC
     if ref is None:
-        ref = (REFERENCE_SRC / "voftrial1.cu").exists()
+        ref = src is not None and (src / "voftrial1.cu").exists()
     if ref:
+        if src is None or not (src / "voftrial1.cu").exists():
+            raise FileNotFoundError("reference harness: set VOF_REFERENCE_DIR (or pass ref_dir) to the directory "
+                                    "holding voftrial1.cu")
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), f"REF_DIR={REFERENCE_SRC}", *targets], check=True)
+    extra = [f"REF_DIR={src}"] if ref else []
+    subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), *extra, *targets], check=True)
 
 
 def _params_type():

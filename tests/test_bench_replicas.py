@@ -89,3 +89,22 @@ def test_clock_summary_flags_slowdowns():
     c = bench.summarize_clocks(lines)
     assert c["sm_mhz"] == 1320 and c["sm_max_mhz"] == 1965 and c["samples"] == 3
     assert c["reasons"] == ["hw_slowdown", "sw_power_cap"]
+
+
+def test_slab_bench_grid_keeps_the_cell_size():
+    """The multi-GPU bench's n x n x (n N) grid: the n^3 workload's constants
+    and cell size (dz and dzi bit for bit), N slabs of n owned planes."""
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(ROOT / "cuda-lbm-ibm-fvm_b200"))
+    import bench
+    from vof_b200 import slab
+
+    one = bench.workload_params(40)
+    for world in (2, 3, 8):
+        g = bench.slab_global_params(40, world)
+        assert (g.nx, g.ny, g.nz) == (40, 40, 40 * world)
+        assert (g.dz, g.dzi, g.dx, g.dt, g.gz) == (one.dz, one.dzi, one.dx, one.dt, one.gz)
+        assert g.nTot == 42 * 42 * (40 * world + 2)
+        sl = slab.plan(g.nz, world, slab.halo_for(g.jacobi_iters))
+        assert all(s.own1 - s.own0 + 1 == 40 for s in sl)
+    assert bench.parse_args(["--gpus", "2"]).decomp == "slab"

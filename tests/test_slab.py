@@ -87,6 +87,7 @@ def test_exchange_pairs_match():
 def test_local_group_matches_single_grid(orc, nranks, nz):
     prm, st = case(nz, seed=nranks)
     want = orc.run_f32(prm, st, 1, 6)
+    assert all(np.isfinite(want[k]).all() for k in STATE)
     grp = slab.LocalGroup(prm, nranks, OracleEngine)
     grp.upload_global(st)
     grp.run(1, 6)  # every sweep order, twice
