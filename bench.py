@@ -69,10 +69,10 @@ KERNEL_NAMES = {
     "predict": "k_predict", "rhs": "k_rhs", "jacobi": "k_jacobi_pairs", "correct": "k_correct",
     "sweep1": "k_fct", "sweep2": "k_fct", "sweep3": "k_fct",
 }
-# the Jacobi kernel the library runs at the bench size (VOF_JACOBI=pairs2|pairs|col|tb;
-# pairs2, two sweeps per launch, by default)
-KERNEL_NAMES["jacobi"] = {"col": "k_jacobi_col", "tb": "k_jacobi_tb", "pairs": "k_jacobi_pairs"}.get(
-    os.environ.get("VOF_JACOBI", ""), "k_jacobi_pairs2")
+# the Jacobi kernel the library runs at the bench size (VOF_JACOBI=pairs|ring|col|pairs2|tb;
+# pairs, one sweep per launch with two cells per thread, by default)
+KERNEL_NAMES["jacobi"] = {"col": "k_jacobi_col", "tb": "k_jacobi_tb", "pairs2": "k_jacobi_pairs2",
+                          "ring": "k_jacobi_ring"}.get(os.environ.get("VOF_JACOBI", ""), "k_jacobi_pairs")
 STEP_MODEL_BYTES = 188  # B per cell-step of the fused plain path (10 sweeps, FP32)
 WARM_MS = 60.0  # least GPU time of warm-up steps run back to back before a timed region
 

@@ -1866,10 +1866,16 @@ static void free_tape(AdjEngine* e) {
     free_states(e->cp, e->ncp);
     free_states(e->seg, e->every);
     free_mid(e->mid, e->every);
-    free_states(e->seg2, e->every);
-    free_mid(e->mid2, e->every);
-    e->cp = e->seg = e->seg2 = nullptr;
-    e->mid = e->mid2 = nullptr;
+    for (int i = 0; i < e->nkept; ++i) {
+        free_states(e->kseg[i], e->every);
+        free_mid(e->kmid[i], e->every);
+        e->kseg[i] = nullptr;
+        e->kmid[i] = nullptr;
+        e->kept[i] = false;
+    }
+    e->nkept = 0;
+    e->cp = e->seg = nullptr;
+    e->mid = nullptr;
     e->ncp = 0;
     e->keep = 0;
     e->tape_bytes = 0;
@@ -1980,32 +1986,37 @@ cudaError_t adj_tape(AdjEngine* e, int istep0, int nsteps, int every, cudaStream
             return r;
         if (keep && (r = alloc_mid(e->mid, every, e->elems, &e->tape_bytes, s)) != cudaSuccess) return r;
     }
-    // a second kept segment, where the record can keep one and memory allows
-    // (a tape that keeps intermediates, FP32 Jacobi with an even sweep count)
-    const bool want2 = keep && !e->conv && e->jacobi_iters % 2 == 0 && ncp >= 2;
-    if (!want2 && e->seg2) {
-        free_states(e->seg2, e->every);
-        free_mid(e->mid2, e->every);
-        e->seg2 = nullptr;
-        e->mid2 = nullptr;
+    // further kept segments, where the record can keep them and memory
+    // allows (a tape that keeps intermediates, FP32 Jacobi with an even sweep
+    // count): one set per segment before the last, from the last backwards
+    const bool want = keep && !e->conv && e->jacobi_iters % 2 == 0 && ncp >= 2;
+    int nwant = want ? ncp - 1 : 0;
+    if (nwant > AdjEngine::MAX_KEPT) nwant = AdjEngine::MAX_KEPT;
+    while (e->nkept > nwant) {
+        const int i = --e->nkept;
+        free_states(e->kseg[i], e->every);
+        free_mid(e->kmid[i], e->every);
+        e->kseg[i] = nullptr;
+        e->kmid[i] = nullptr;
     }
-    if (want2 && !e->seg2) {
+    while (e->nkept < nwant) {
         size_t fr = 0, tot = 0;
-        const size_t need2 = (size_t)(2 * every - 1) * 5 * fb;
-        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && need2 + tot / 32 <= fr) {
-            size_t b2 = 0;
-            r = alloc_states(e->seg2, every, 1, e->elems, false, &b2);
-            if (r == cudaSuccess) r = alloc_mid(e->mid2, every, e->elems, &b2, s);
-            if (r != cudaSuccess) {  // (only an optimisation: go without it)
-                free_states(e->seg2, e->every);
-                free_mid(e->mid2, e->every);
-                e->seg2 = nullptr;
-                e->mid2 = nullptr;
-                cudaGetLastError();
-            } else {
-                e->tape_bytes += b2;
-            }
+        const size_t need = (size_t)(2 * every - 1) * 5 * fb;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess || need + tot / 32 > fr) break;
+        const int i = e->nkept;
+        size_t bk = 0;
+        r = alloc_states(e->kseg[i], every, 1, e->elems, false, &bk);
+        if (r == cudaSuccess) r = alloc_mid(e->kmid[i], every, e->elems, &bk, s);
+        if (r != cudaSuccess) {  // (only an optimisation: go without it)
+            free_states(e->kseg[i], every);
+            free_mid(e->kmid[i], every);
+            e->kseg[i] = nullptr;
+            e->kmid[i] = nullptr;
+            cudaGetLastError();
+            break;
         }
+        e->tape_bytes += bk;
+        ++e->nkept;
     }
     e->istep0 = istep0;
     e->nsteps = nsteps;
@@ -2013,7 +2024,7 @@ cudaError_t adj_tape(AdjEngine* e, int istep0, int nsteps, int every, cudaStream
     e->recorded = false;
     e->tail_kept = false;
     e->tail_p = nullptr;
-    e->kept2 = false;
+    for (int i = 0; i < AdjEngine::MAX_KEPT; ++i) e->kept[i] = false;
     return cudaSuccess;
 }
 
@@ -2068,22 +2079,25 @@ cudaError_t adj_record_tail(AdjEngine* e, const AdjState& out, float* const extr
     return cudaSuccess;
 }
 
-bool adj_can_keep2(const AdjEngine& e) { return adj_can_record_tail(e) && e.ncp >= 2 && e.seg2 && e.mid2; }
+bool adj_can_keep(const AdjEngine& e, int m) {
+    const int i = e.ncp - 2 - m;
+    return adj_can_record_tail(e) && i >= 0 && i < e.nkept && e.kseg[i] && e.kmid[i];
+}
 
-cudaError_t adj_record_keep2(AdjEngine* e, const AdjState& out, cudaStream_t s) {
-    if (!adj_can_keep2(*e)) return cudaErrorNotSupported;
-    const int m = e->ncp - 2;
+cudaError_t adj_record_keep(AdjEngine* e, int m, const AdjState& out, cudaStream_t s) {
+    if (!adj_can_keep(*e, m)) return cudaErrorNotSupported;
+    const int i = e->ncp - 2 - m;
     const int first = adj_segment_first(*e, m), count = adj_segment_first(*e, m + 1) - first;
     cudaError_t r = load_state(*e, e->cp[m], s);
     int par = 0;
     const float* pa = nullptr;
     for (int q = 0; q < count && r == cudaSuccess; ++q)
-        r = replay_kept(*e, e->seg2, e->mid2, first, count, q, &par, &pa, s);
+        r = replay_kept(*e, e->kseg[i], e->kmid[i], first, count, q, &par, &pa, s);
     if (r != cudaSuccess) return r;
     const float* src[5] = {e->wb.F, e->wb.u, e->wb.v, e->wb.w, pa};
     for (int q = 0; q < 5; ++q)
         if ((r = copy_field(out.f[q], src[q], e->elems, s)) != cudaSuccess) return r;
-    e->kept2 = true;
+    e->kept[i] = true;
     return cudaSuccess;
 }
 
@@ -2126,13 +2140,14 @@ cudaError_t adj_backward(AdjEngine* e, const AdjState& fin, const double box[6],
             // replay every step of the segment from checkpoint m, keeping its
             // intermediates and the states after steps 0 .. count - 2; the
             // record did so already for the last segment when tail_kept, and
-            // for the one before it in seg2 / mid2 when kept2
+            // for the ones before it that have a kept set
             const bool tail = m == e->ncp - 1 && e->tail_kept;
-            const bool k2 = m == e->ncp - 2 && e->kept2;
-            AdjState* const seg = k2 ? e->seg2 : e->seg;
-            AdjMid* const mid = k2 ? e->mid2 : e->mid;
+            const int ki = e->ncp - 2 - m;
+            const bool k2 = ki >= 0 && ki < e->nkept && e->kept[ki];
+            AdjState* const seg = k2 ? e->kseg[ki] : e->seg;
+            AdjMid* const mid = k2 ? e->kmid[ki] : e->mid;
             // the state after the segment's last step: the replay's buffers,
-            // or checkpoint m + 1 for seg2
+            // or checkpoint m + 1 for a kept set
             const AdjState wbs{{e->wb.F, e->wb.u, e->wb.v, e->wb.w, nullptr}, nullptr};
             const AdjState& after = k2 ? e->cp[m + 1] : wbs;
             if (!tail && !k2 && (r = load_state(*e, e->cp[m], s)) != cudaSuccess) return r;

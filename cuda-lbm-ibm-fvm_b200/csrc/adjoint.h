@@ -71,13 +71,16 @@ struct AdjEngine {
     // that segment's last pressure (an engine buffer)
     bool tail_kept;
     const float* tail_p;
-    // a second set of segment states and intermediates (null unless the tape
-    // keeps intermediates and memory allows): the record keeps the segment
-    // before the last one there too (kept2), so the reverse pass replays
-    // neither of the last two segments
-    AdjState* seg2;
-    AdjMid* mid2;
-    bool kept2;
+    // further sets of segment states and intermediates (none unless the tape
+    // keeps intermediates; as many as memory allows, leaving 1/32 of the
+    // device free): set i holds segment ncp - 2 - i, which the record runs
+    // into it (kept[i]) as the reverse pass would replay it, so that pass
+    // replays none of those segments
+    static constexpr int MAX_KEPT = 64;
+    int nkept;
+    AdjState* kseg[MAX_KEPT];
+    AdjMid* kmid[MAX_KEPT];
+    bool kept[MAX_KEPT];
     size_t tape_bytes;       // device bytes of the tape
     bool recorded;
     // recompute buffers (FP32)
@@ -136,14 +139,14 @@ bool adj_can_record_tail(const AdjEngine& e);
 // The reverse pass then starts on this segment without a replay.
 cudaError_t adj_record_tail(AdjEngine* e, const AdjState& out, float* const extra[4], cudaStream_t s);
 
-// Whether the record may also keep the segment before the last one
-// (adj_record_keep2): adj_can_record_tail, at least two segments, seg2/mid2.
-bool adj_can_keep2(const AdjEngine& e);
+// Whether the record may keep segment m (< ncp - 1) in a set of its own
+// (adj_record_keep): adj_can_record_tail and a set allocated for it.
+bool adj_can_keep(const AdjEngine& e, int m);
 
-// The record's segment ncp - 2, from checkpoint ncp - 2 (saved before), run
-// like adj_record_tail into seg2 / mid2; the final state goes to `out`.  The
-// record then saves checkpoint ncp - 1 from `out` and runs adj_record_tail.
-cudaError_t adj_record_keep2(AdjEngine* e, const AdjState& out, cudaStream_t s);
+// The record's segment m, from checkpoint m (saved before), run like
+// adj_record_tail into its set; the final state goes to `out`.  The record
+// then saves checkpoint m + 1 from `out` and goes on with segment m + 1.
+cudaError_t adj_record_keep(AdjEngine* e, int m, const AdjState& out, cudaStream_t s);
 
 // Reverse the recorded run: L = sum over the box of F dV of the final state
 // `fin`; afterwards lF, lu, lv, lw, lp[lp_cur] hold dL/d(initial state) and

@@ -679,11 +679,11 @@ int vof_forward_record(vof_ctx* ctx, int istep0, int nsteps, int checkpoint_ever
                 if ((e = vof::adj_record_tail(A, x, extra, ctx->stream)) != cudaSuccess) return fail_cuda(ctx, e);
                 break;
             }
-            if (m == A->ncp - 2 && vof::adj_can_keep2(*A)) {
-                // so does the segment before it, into the second set of
-                // segment buffers; the next pass of the loop is at the last
+            if (vof::adj_can_keep(*A, m)) {
+                // so do the segments before it that have a set of kept
+                // buffers; the next pass of the loop is at the next
                 // segment's first step
-                if ((e = vof::adj_record_keep2(A, x, ctx->stream)) != cudaSuccess) return fail_cuda(ctx, e);
+                if ((e = vof::adj_record_keep(A, m, x, ctx->stream)) != cudaSuccess) return fail_cuda(ctx, e);
                 ++m;
                 n = vof::adj_segment_first(*A, m) - 1;
                 continue;

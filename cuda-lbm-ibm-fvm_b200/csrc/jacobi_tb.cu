@@ -383,6 +383,124 @@ __global__ void __launch_bounds__(JP_THREADS) k_jacobi_pairs(Geom g, const float
     }
 }
 
+// ---- the paired sweep with a deeper prefetch of its own column ---------------
+// k_jacobi_pairs keeps one plane of loads in flight per thread, which at
+// 200^3 leaves the sweep waiting on memory (about a third of the bytes in
+// flight that hide HBM latency at its occupancy).  Here each thread copies
+// its own column's pressure (JR_AHEAD + 1 planes ahead) and right-hand side
+// (JR_AHEAD planes ahead) into a ring of shared-memory slots of its own with
+// asynchronous copies (cp.async, cached in L1 on the way, where the other
+// rows' threads find them as their y neighbours), so JR_AHEAD planes of those
+// loads are in flight without holding registers; a thread reads only slots it
+// filled, so no barrier is needed.  Everything else -- the x neighbours by
+// shuffle, the y neighbours as loads one plane ahead, the per-cell expression
+// -- is k_jacobi_pairs', so the bits are the same.
+constexpr int JR_AHEAD = 4, JR_SLOTS = JR_AHEAD + 1;
+
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__global__ void __launch_bounds__(JP_THREADS) k_jacobi_ring(Geom g, const float* __restrict__ pin,
+                                                            const float* __restrict__ rhs,
+                                                            float* __restrict__ pout, int kchunk) {
+    __shared__ float2 ringP[JR_SLOTS][JP_THREADS];
+    __shared__ float2 ringR[JR_SLOTS][JP_THREADS];
+    const int npair = g.nx / 2 + 1;  // pairs covering columns 0 .. nx
+    const int nq = npair * g.ny;
+    const int t = threadIdx.x;
+    const int qt = blockIdx.x * JP_THREADS + t;
+    const bool qa = qt < nq;
+    const int q = qa ? qt : nq - 1;  // lanes past the end shadow the last pair
+    const int jr = q / npair, m = q - jr * npair;
+    const int j = jr + 1, i0 = 2 * m, i1 = i0 + 1;
+    const bool a0 = qa && i0 >= 1, a1 = qa && i1 <= g.nx;
+    const int lane = t & 31;
+    const bool ldw = lane == 0 && m > 0;             // x- neighbour of cell i0 from memory
+    const bool lde = lane == 31 || m == npair - 1;   // x+ neighbour of cell i1 from memory
+    const int k0 = 1 + blockIdx.y * kchunk, k1 = min(g.nz, k0 + kchunk - 1);
+    const int plane = g.plane;
+    const int c = gidx(g, i0, j, 0);  // even
+    const int cw = c - 1, ce = c + min(2, g.px - 1 - i0);
+    const float cx = g.dxi * g.dxi, cy = g.dyi * g.dyi, cz = g.dzi * g.dzi;
+    const float ae0 = (i0 != g.nx) ? cx : 0.0f, aw0 = (i0 != 1) ? cx : 0.0f;
+    const float ae1 = (i1 != g.nx) ? cx : 0.0f, aw1 = (i1 != 1) ? cx : 0.0f;
+    const float an = (j != g.ny) ? cy : 0.0f, as = (j != 1) ? cy : 0.0f;
+    const float2 dm = make_float2(-(ae0 + aw0 + an + as + cz + cz), -(ae1 + aw1 + an + as + cz + cz));
+    const float2 rm = make_float2(__frcp_rn(dm.x), __frcp_rn(dm.y));
+    const float2* P = reinterpret_cast<const float2*>(pin);
+    const float2* R = reinterpret_cast<const float2*>(rhs);
+    float2* O = reinterpret_cast<float2*>(pout);
+    const int w = c >> 1, wp = plane >> 1, wr = g.px >> 1;
+    const float2 zero = make_float2(0.0f, 0.0f);
+    // group gi (issued at iteration gi, or before the loop for gi < k0)
+    // copies the pressure of plane gi + JR_AHEAD + 1 and the rhs of plane
+    // gi + JR_AHEAD, which iteration gi + JR_AHEAD - 1 takes as the next
+    // plane's operands; planes nobody needs are not copied (empty group)
+    int slot_issue = 0, slot_use = 0;
+    auto issue = [&](int gi) {
+        const int kp = gi + JR_AHEAD + 1, kr = gi + JR_AHEAD;
+        if (kr - 1 < k1) {
+            if (kp <= g.nz + 1) cp_async8(&ringP[slot_issue][t], P + w + kp * wp);
+            cp_async8(&ringR[slot_issue][t], R + w + kr * wp);
+        }
+        cp_async_commit();
+        slot_issue = slot_issue + 1 == JR_SLOTS ? 0 : slot_issue + 1;
+    };
+    for (int gi = k0 + 1 - JR_AHEAD; gi < k0; ++gi) issue(gi);
+    float2 pm = P[w + (k0 - 1) * wp], pc = P[w + k0 * wp], pp = P[w + (k0 + 1) * wp];
+    float2 pS = P[w + k0 * wp - wr], pN = P[w + k0 * wp + wr], rc = R[w + k0 * wp];
+    float xw = ldw ? pin[cw + k0 * plane] : 0.0f, xe = lde ? pin[ce + k0 * plane] : 0.0f;
+    for (int k = k0; k <= k1; ++k) {
+        issue(k);
+        // operands of the next plane
+        const bool more = k < k1;
+        cp_async_wait<JR_AHEAD - 1>();  // the group of iteration k + 1 - JR_AHEAD has landed
+        const float2 pq = (more && k + 2 <= g.nz + 1) ? ringP[slot_use][t] : zero;
+        const float2 rn = more ? ringR[slot_use][t] : zero;
+        slot_use = slot_use + 1 == JR_SLOTS ? 0 : slot_use + 1;
+        const float2 sn = more ? P[w + (k + 1) * wp - wr] : zero;
+        const float2 nn = more ? P[w + (k + 1) * wp + wr] : zero;
+        const float xwn = (more && ldw) ? pin[cw + (k + 1) * plane] : 0.0f;
+        const float xen = (more && lde) ? pin[ce + (k + 1) * plane] : 0.0f;
+        float pw = __shfl_up_sync(0xffffffffu, pc.y, 1), pe = __shfl_down_sync(0xffffffffu, pc.x, 1);
+        if (ldw) pw = xw;
+        if (lde) pe = xe;
+        const bool kb = k == 1, kt = k == g.nz;
+        const float af = kt ? 0.0f : cz, ab = kb ? 0.0f : cz;
+        float2 d = dm, rd = rm;
+        if (kb || kt) {
+            d = make_float2(-(ae0 + aw0 + an + as + af + ab), -(ae1 + aw1 + an + as + af + ab));
+            rd = make_float2(__frcp_rn(d.x), __frcp_rn(d.y));
+        }
+        const float v0 =
+            div_rn_pre(rc.x - ae0 * pc.y - aw0 * pw - an * pN.x - as * pS.x - af * pp.x - ab * pm.x, d.x, rd.x);
+        const float v1 =
+            div_rn_pre(rc.y - ae1 * pe - aw1 * pc.x - an * pN.y - as * pS.y - af * pp.y - ab * pm.y, d.y, rd.y);
+        const int o = w + k * wp;
+        if (a0 && a1)
+            O[o] = make_float2(v0, v1);
+        else if (a0)
+            pout[2 * o] = v0;
+        else if (a1)
+            pout[2 * o + 1] = v1;
+        pm = pc;
+        pc = pp;
+        pp = pq;
+        pS = sn;
+        pN = nn;
+        rc = rn;
+        xw = xwn;
+        xe = xen;
+    }
+    cp_async_wait<0>();  // (no copy outlives the block)
+}
+
 // Blocks of k_jacobi_pairs resident on the device at once (SMs x blocks per
 // SM), set by jacobi_tb_configure.
 static int jp_wave = 4 * 148;
@@ -393,7 +511,9 @@ static int jp_wave = 4 * 148;
 // one wave, or 13 of 16 in 1.7 waves, 0.31 ms per 10 sweeps; 8 of 25 in 1.07
 // waves 0.39 ms).  Down to one plane on small grids.  VOF_JACOBI_KCHUNK
 // overrides.
-static int jacobi_pairs_kchunk(const Geom& g, int bx) {
+static int jr_wave = 4 * 148;  // the same for k_jacobi_ring
+
+static int jacobi_pairs_kchunk(const Geom& g, int bx, int wave = jp_wave) {
     static int forced = -1;
     if (forced < 0) {
         const char* v = getenv("VOF_JACOBI_KCHUNK");
@@ -405,8 +525,8 @@ static int jacobi_pairs_kchunk(const Geom& g, int bx) {
     for (int n = 1; n <= g.nz; ++n) {
         const int kc = (g.nz + n - 1) / n;  // n chunks of (nearly) equal length
         const long long blocks = (long long)bx * ((g.nz + kc - 1) / kc);
-        const long long waves = (blocks + jp_wave - 1) / jp_wave;
-        const double fill = (double)blocks / (double)(waves * jp_wave);
+        const long long waves = (blocks + wave - 1) / wave;
+        const double fill = (double)blocks / (double)(waves * wave);
         if (fill >= 0.85) return kc;
         if (fill > best_fill) {
             best_fill = fill;
@@ -421,6 +541,14 @@ cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rh
     const int bx = (nq + JP_THREADS - 1) / JP_THREADS;
     const int kchunk = jacobi_pairs_kchunk(g, bx);
     k_jacobi_pairs<<<dim3(bx, (g.nz + kchunk - 1) / kchunk), JP_THREADS, 0, s>>>(g, pin, rhs, pout, kchunk);
+    return cudaGetLastError();
+}
+
+cudaError_t jacobi_ring_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s) {
+    const int nq = (g.nx / 2 + 1) * g.ny;
+    const int bx = (nq + JP_THREADS - 1) / JP_THREADS;
+    const int kchunk = jacobi_pairs_kchunk(g, bx, jr_wave);
+    k_jacobi_ring<<<dim3(bx, (g.nz + kchunk - 1) / kchunk), JP_THREADS, 0, s>>>(g, pin, rhs, pout, kchunk);
     return cudaGetLastError();
 }
 
@@ -641,11 +769,9 @@ static J2Plan j2_plan(const Geom& g) {
     return best;
 }
 
-// Also needs enough work to give every resident block four planes or more:
-// on smaller grids the single sweeps keep more of the device busy.
 bool jacobi_pairs2_supported(const Geom& g) {
     const J2Plan p = j2_plan(g);
-    return p.rw > 0 && p.rows >= 1 && g.px % 2 == 0 && p.units / 4 >= j2_blocks;
+    return p.rw > 0 && p.rows >= 1 && g.px % 2 == 0;
 }
 
 cudaError_t jacobi_pairs2_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s) {
@@ -679,6 +805,9 @@ cudaError_t jacobi_tb_configure() {
         (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_pairs, JP_THREADS, 0)) != cudaSuccess)
         return e;
     jp_wave = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_ring, JP_THREADS, 0)) != cudaSuccess)
+        return e;
+    jr_wave = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_pairs2, J2_THREADS,
                                                            sizeof(float2) * (5u * J2_THREADS + 64u))) != cudaSuccess)
         return e;

@@ -72,14 +72,17 @@ def test_random_state_bitwise_vs_oracle(cuda, V, orc, nx, ny, nz, seed, dt, vs):
     assert_bitwise(got, want, STATE + ("ustar", "vstar", "wstar", "rhs"), f"{nx}x{ny}x{nz}")
 
 
-@pytest.mark.parametrize("env", [{"VOF_JACOBI": "pairs"}, {"VOF_JACOBI": "tb"}, {"VOF_JACOBI": "col"},
+@pytest.mark.parametrize("env", [{"VOF_JACOBI": "pairs2"}, {"VOF_JACOBI": "ring"}, {"VOF_JACOBI": "tb"},
+                                 {"VOF_JACOBI": "col"}, {"VOF_JACOBI": "ring", "VOF_JACOBI_KCHUNK": "1"},
+                                 {"VOF_JACOBI": "ring", "VOF_JACOBI_KCHUNK": "3"},
                                  {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "1"},
                                  {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "5"}])
 def test_jacobi_kernel_choices_give_the_same_bits(cuda, V, orc, tmp_path, env):
-    """The Jacobi kernels a process may select (the default two-sweep paired
-    kernel runs in every other test; here the single-sweep paired kernel and
-    its z chunks, the TMA-blocked two-sweep kernel, the one-cell streaming
-    sweep; read once per process, so each runs in a child process) give the
+    """The Jacobi kernels a process may select (the default single-sweep
+    paired kernel runs in every other test; here the two-sweep paired kernel,
+    the paired sweep with the cp.async ring and its z chunks, the TMA-blocked
+    two-sweep kernel, the one-cell streaming sweep, other z chunks of the
+    default; read once per process, so each runs in a child process) give the
     oracle's bits."""
     import os
     import subprocess
