@@ -336,9 +336,6 @@ constexpr int MARCH_THREADS = 256;
 #ifndef VOF_MARCH_UNROLL
 #define VOF_MARCH_UNROLL 2
 #endif
-#define VOF_PRAGMA_(x) _Pragma(#x)
-#define VOF_UNROLL_(n) VOF_PRAGMA_(unroll n)
-#define VOF_UNROLL(n) VOF_UNROLL_(n)
 
 // Lines are numbered flat, i fastest (a warp may span two rows of lines:
 // two coalesced pieces per load), blockIdx.y is the segment.

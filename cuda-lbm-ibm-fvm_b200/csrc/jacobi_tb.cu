@@ -383,6 +383,163 @@ __global__ void __launch_bounds__(JP_THREADS) k_jacobi_pairs(Geom g, const float
     }
 }
 
+// ---- the paired sweep with the plane cases peeled out of the march -----------
+// k_jacobi_pairs evaluates, on every plane, whether there is a next plane to
+// load (zeros otherwise) and whether the plane is a wall plane (its own
+// diagonal), and copies its plane registers one place down.  Here the march
+// is split: the first plane of the box (k = 1) and the last plane of the
+// chunk run through the general plane step; the planes between load their
+// successors unconditionally and take the inner diagonal, in a loop unrolled
+// U times so that the plane registers are renamed instead of copied.  The
+// per-cell expression and operand order are k_jacobi_pairs', so are the bits.
+struct JPLine {
+    const float2* P;
+    const float2* R;
+    float2* O;
+    const float* pin;
+    float* pout;
+    int w, wp, wr, cw, ce, plane;
+    float ae0, aw0, ae1, aw1, an, as, cz;
+    float2 dm, rm;
+    bool a0, a1, ldw, lde;
+};
+
+struct JPRegs {
+    float2 pm, pc, pp, pS, pN, rc;
+    float xw, xe;
+};
+
+// One plane k of the paired sweep.  MORE: load the next plane's operands (the
+// caller guarantees k < k1 <= nz, so plane k + 2 <= nz + 1 exists).  EDGE:
+// the plane may be the first or the last of the box.
+template <bool MORE, bool EDGE>
+__device__ __forceinline__ void jp_plane(const JPLine& L, const Geom& g, int k, JPRegs& s) {
+    float2 pq, sn, nn, rn;
+    float xwn = 0.0f, xen = 0.0f;
+    if constexpr (MORE) {
+        const int o1 = L.w + (k + 1) * L.wp;
+        pq = L.P[o1 + L.wp];
+        sn = L.P[o1 - L.wr];
+        nn = L.P[o1 + L.wr];
+        rn = L.R[o1];
+        if (L.ldw) xwn = L.pin[L.cw + (k + 1) * L.plane];
+        if (L.lde) xen = L.pin[L.ce + (k + 1) * L.plane];
+    }
+    float pw = __shfl_up_sync(0xffffffffu, s.pc.y, 1), pe = __shfl_down_sync(0xffffffffu, s.pc.x, 1);
+    if (L.ldw) pw = s.xw;
+    if (L.lde) pe = s.xe;
+    float af = L.cz, ab = L.cz;
+    float2 d = L.dm, rd = L.rm;
+    if constexpr (EDGE) {
+        const bool kb = k == 1, kt = k == g.nz;
+        af = kt ? 0.0f : L.cz;
+        ab = kb ? 0.0f : L.cz;
+        if (kb || kt) {
+            d = make_float2(-(L.ae0 + L.aw0 + L.an + L.as + af + ab), -(L.ae1 + L.aw1 + L.an + L.as + af + ab));
+            rd = make_float2(__frcp_rn(d.x), __frcp_rn(d.y));
+        }
+    }
+    const float v0 = div_rn_pre(s.rc.x - L.ae0 * s.pc.y - L.aw0 * pw - L.an * s.pN.x - L.as * s.pS.x -
+                                    af * s.pp.x - ab * s.pm.x,
+                                d.x, rd.x);
+    const float v1 = div_rn_pre(s.rc.y - L.ae1 * pe - L.aw1 * s.pc.x - L.an * s.pN.y - L.as * s.pS.y -
+                                    af * s.pp.y - ab * s.pm.y,
+                                d.y, rd.y);
+    const int o = L.w + k * L.wp;
+    if (L.a0 && L.a1)
+        L.O[o] = make_float2(v0, v1);
+    else if (L.a0)
+        L.pout[2 * o] = v0;
+    else if (L.a1)
+        L.pout[2 * o + 1] = v1;
+    if constexpr (MORE) {
+        s.pm = s.pc;
+        s.pc = s.pp;
+        s.pp = pq;
+        s.pS = sn;
+        s.pN = nn;
+        s.rc = rn;
+        s.xw = xwn;
+        s.xe = xen;
+    }
+}
+
+template <int U, int MINB>
+__global__ void __launch_bounds__(JP_THREADS, MINB) k_jacobi_peel(Geom g, const float* __restrict__ pin,
+                                                            const float* __restrict__ rhs,
+                                                            float* __restrict__ pout, int kchunk) {
+    const int npair = g.nx / 2 + 1;  // pairs covering columns 0 .. nx
+    const int nq = npair * g.ny;
+    const int qt = blockIdx.x * JP_THREADS + threadIdx.x;
+    const bool qa = qt < nq;
+    const int q = qa ? qt : nq - 1;  // lanes past the end shadow the last pair
+    const int jr = q / npair, m = q - jr * npair;
+    const int j = jr + 1, i0 = 2 * m, i1 = i0 + 1;
+    const int lane = threadIdx.x & 31;
+    const int k0 = 1 + blockIdx.y * kchunk, k1 = min(g.nz, k0 + kchunk - 1);
+    JPLine L;
+    L.P = reinterpret_cast<const float2*>(pin);
+    L.R = reinterpret_cast<const float2*>(rhs);
+    L.O = reinterpret_cast<float2*>(pout);
+    L.pin = pin;
+    L.pout = pout;
+    L.a0 = qa && i0 >= 1;
+    L.a1 = qa && i1 <= g.nx;
+    L.ldw = lane == 0 && m > 0;            // x- neighbour of cell i0 from memory
+    L.lde = lane == 31 || m == npair - 1;  // x+ neighbour of cell i1 from memory
+    L.plane = g.plane;
+    const int c = gidx(g, i0, j, 0);  // even
+    L.cw = c - 1;
+    L.ce = c + min(2, g.px - 1 - i0);
+    const float cx = g.dxi * g.dxi, cy = g.dyi * g.dyi;
+    L.cz = g.dzi * g.dzi;
+    L.ae0 = (i0 != g.nx) ? cx : 0.0f;
+    L.aw0 = (i0 != 1) ? cx : 0.0f;
+    L.ae1 = (i1 != g.nx) ? cx : 0.0f;
+    L.aw1 = (i1 != 1) ? cx : 0.0f;
+    L.an = (j != g.ny) ? cy : 0.0f;
+    L.as = (j != 1) ? cy : 0.0f;
+    L.dm = make_float2(-(L.ae0 + L.aw0 + L.an + L.as + L.cz + L.cz), -(L.ae1 + L.aw1 + L.an + L.as + L.cz + L.cz));
+    L.rm = make_float2(__frcp_rn(L.dm.x), __frcp_rn(L.dm.y));
+    L.w = c >> 1;
+    L.wp = g.plane >> 1;
+    L.wr = g.px >> 1;
+    JPRegs s;
+    s.pm = L.P[L.w + (k0 - 1) * L.wp];
+    s.pc = L.P[L.w + k0 * L.wp];
+    s.pp = L.P[L.w + (k0 + 1) * L.wp];
+    s.pS = L.P[L.w + k0 * L.wp - L.wr];
+    s.pN = L.P[L.w + k0 * L.wp + L.wr];
+    s.rc = L.R[L.w + k0 * L.wp];
+    s.xw = L.ldw ? pin[L.cw + k0 * L.plane] : 0.0f;
+    s.xe = L.lde ? pin[L.ce + k0 * L.plane] : 0.0f;
+    int k = k0;
+    if (k == 1 && k < k1) {
+        jp_plane<true, true>(L, g, k, s);
+        ++k;
+    }
+    VOF_UNROLL(U)
+    for (; k < k1; ++k) jp_plane<true, false>(L, g, k, s);
+    jp_plane<false, true>(L, g, k1, s);
+}
+
+// VOF_JP_UNROLL (1, 2 or 4) picks the unroll of the peeled march and
+// VOF_JP_MINB (1 or 4) the blocks per SM its registers are sized for.
+using JPKernel = void (*)(Geom, const float*, const float*, float*, int);
+static JPKernel jp_peel_kernel() {
+    static JPKernel k = nullptr;
+    if (!k) {
+        const char* v = getenv("VOF_JP_UNROLL");
+        const char* b = getenv("VOF_JP_MINB");
+        const int u = v ? atoi(v) : 2;
+        const int mb = b ? atoi(b) : 1;
+        k = u == 1 ? (mb == 4 ? k_jacobi_peel<1, 4> : k_jacobi_peel<1, 1>)
+            : u == 4 ? (mb == 4 ? k_jacobi_peel<4, 4> : k_jacobi_peel<4, 1>)
+                     : (mb == 4 ? k_jacobi_peel<2, 4> : k_jacobi_peel<2, 1>);
+    }
+    return k;
+}
+
 // ---- the paired sweep with a deeper prefetch of its own column ---------------
 // k_jacobi_pairs keeps one plane of loads in flight per thread, which at
 // 200^3 leaves the sweep waiting on memory (about a third of the bytes in
@@ -541,6 +698,16 @@ cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rh
     const int bx = (nq + JP_THREADS - 1) / JP_THREADS;
     const int kchunk = jacobi_pairs_kchunk(g, bx);
     k_jacobi_pairs<<<dim3(bx, (g.nz + kchunk - 1) / kchunk), JP_THREADS, 0, s>>>(g, pin, rhs, pout, kchunk);
+    return cudaGetLastError();
+}
+
+static int jpe_wave = 3 * 148;  // resident blocks of the chosen k_jacobi_peel, set by jacobi_tb_configure
+
+cudaError_t jacobi_peel_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s) {
+    const int nq = (g.nx / 2 + 1) * g.ny;
+    const int bx = (nq + JP_THREADS - 1) / JP_THREADS;
+    const int kchunk = jacobi_pairs_kchunk(g, bx, jpe_wave);
+    jp_peel_kernel()<<<dim3(bx, (g.nz + kchunk - 1) / kchunk), JP_THREADS, 0, s>>>(g, pin, rhs, pout, kchunk);
     return cudaGetLastError();
 }
 
@@ -808,6 +975,9 @@ cudaError_t jacobi_tb_configure() {
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_ring, JP_THREADS, 0)) != cudaSuccess)
         return e;
     jr_wave = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, jp_peel_kernel(), JP_THREADS, 0)) != cudaSuccess)
+        return e;
+    jpe_wave = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_pairs2, J2_THREADS,
                                                            sizeof(float2) * (5u * J2_THREADS + 64u))) != cudaSuccess)
         return e;

@@ -27,6 +27,10 @@ cudaError_t jacobi_col_launch(const Geom& g, const float* pin, const float* rhs,
 // The same sweep with two cells per thread (packed FP32, same bits).
 cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);
 
+// The paired sweep with its wall and last planes peeled out of the march
+// (unrolled VOF_JP_UNROLL times, default 4); same bits as jacobi_pairs_launch.
+cudaError_t jacobi_peel_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);
+
 // The paired sweep with its own column's loads copied several planes ahead
 // into shared memory (cp.async); same bits as jacobi_pairs_launch.
 cudaError_t jacobi_ring_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);

@@ -29,6 +29,11 @@ struct Geom {
     float sigma;
 };
 
+// #pragma unroll with a macro or template argument as the count.
+#define VOF_PRAGMA_(x) _Pragma(#x)
+#define VOF_UNROLL_(n) VOF_PRAGMA_(unroll n)
+#define VOF_UNROLL(n) VOF_UNROLL_(n)
+
 __host__ __device__ __forceinline__ int gidx(const Geom& g, int i, int j, int k) {
     return (k * g.py + j) * g.px + i;
 }
@@ -53,25 +58,64 @@ __host__ __device__ __forceinline__ float clamp01f(float v) {
 
 // Correctly rounded x / d from a precomputed rd = RN(1/d) (IEEE reciprocal,
 // __frcp_rn), for divisors that are constant or reused across several
-// quotients.  Method: P. Markstein, "Computation of elementary functions on
-// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990 -- with
-// rd = RN(1/d) and q0 = RN(x*rd) (within one ulp of x/d), the remainder
-// r = x - q0*d is exact in one FMA and q1 = RN(q0 + r*rd) equals RN(x/d),
-// provided nothing underflows or overflows.  Outside the range where that
-// holds (tiny, huge or non-finite operands) the IEEE division is used, and
-// +-0 numerators return x*rd, which carries the IEEE sign of 0/d.
-// The IEEE division outside that range, kept out of line: it is rare, and
-// inlined at every call site it would cost issue slots on every cell.
+// quotients and whose reciprocal is a normal number (|d| < 2^126).
+// Method: P. Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Dev. 34(1), 1990 -- with rd = RN(1/d)
+// and q0 = RN(x*rd) (within one ulp of x/d), the remainder r = x - q0*d is
+// exact in one FMA and q1 = RN(q0 + r*rd) equals RN(x/d), provided nothing
+// underflows or overflows.  The remainder is exact when x's exponent is at
+// least e_min + p - 1 = -103 (S. Boldo, M. Daumas, "Representable correcting
+// terms for possibly underflowing floating point operations", ARITH-16,
+// 2003); the fast path asks |x| >= 2^-100 and a normal quotient,
+// 2^-125 <= |q0| <= 2^96.
+// Tiny numerators (|x| < 2^-100, as in the cells a pressure front has not
+// reached yet) take div_rn_tiny below; +-0 numerators return x*rd, which
+// carries the IEEE sign of 0/d; what is left (huge quotients, non-finite
+// operands) takes the IEEE division, out of line: it is rare, and inlined at
+// every call site it would cost issue slots on every cell.
 static __device__ __noinline__ float div_rn_slow(float x, float d) { return __fdiv_rn(x, d); }
+
+// RN(x/d) for 0 < |x| < 2^-36: the quotient of xs = x * 2^64 (exact) by
+// Markstein's method, qs = RN(xs/d), scaled back by 2^-64.  When x/d is a
+// normal number the scaling is exact and commutes with rounding.  When it is
+// subnormal, y = RN(qs * 2^-64) rounds a second time, to the grid of 2^-149;
+// rounding qs first can only change the result when qs * 2^-64 is exactly a
+// midpoint of that grid (rounding is monotone and the midpoints lie on qs's
+// finer grid).  That case is detected exactly -- qs - y*2^64 (exact: both are
+// multiples of qs's quantum and they differ by at most 2^-86) equals +-2^-86
+// -- and settled by the sign of the exact remainder xs - qs*d: zero means
+// x/d is the midpoint itself (ties to even, as y already is), otherwise the
+// result is the grid point on the remainder's side, (qs +- 2^-86) * 2^-64,
+// exact.  Anything outside the scaled Markstein range goes to the IEEE
+// division.  Tested bit for bit against __fdiv_rn over every exponent and on
+// constructed subnormal midpoints.
+__device__ __forceinline__ float div_rn_tiny(float x, float d, float rd) {
+    if (!(fabsf(x) < 0x1p-36f)) return div_rn_slow(x, d);
+    const float xs = __fmul_rn(x, 0x1p+64f);
+    const float s0 = __fmul_rn(xs, rd);
+    const float as = fabsf(s0);
+    if (!(as >= 0x1p-125f && as <= 0x1p+96f)) return div_rn_slow(x, d);
+    const float qs = __fmaf_rn(__fmaf_rn(-s0, d, xs), rd, s0);
+    float y = __fmul_rn(qs, 0x1p-64f);
+    const float d2 = __fsub_rn(qs, __fmul_rn(y, 0x1p+64f));
+    if (fabsf(d2) == 0x1p-86f) {
+        const float rem = __fmaf_rn(-qs, d, xs);
+        if (rem != 0.0f) {
+            const bool up = (rem > 0.0f) == (d > 0.0f);
+            y = __fmul_rn(__fadd_rn(qs, up ? 0x1p-86f : -0x1p-86f), 0x1p-64f);
+        }
+    }
+    return y;
+}
 
 __device__ __forceinline__ float div_rn_pre(float x, float d, float rd) {
     const float q0 = __fmul_rn(x, rd);
     const float r = __fmaf_rn(-q0, d, x);
     const float q1 = __fmaf_rn(r, rd, q0);
     const float ax = fabsf(x), aq = fabsf(q0);
-    if (ax >= 0x1p-96f && aq >= 0x1p-96f && aq <= 0x1p+96f) return q1;
+    if (ax >= 0x1p-100f && aq >= 0x1p-125f && aq <= 0x1p+96f) return q1;
     if (x == 0.0f) return q0;
-    return div_rn_slow(x, d);
+    return div_rn_tiny(x, d, rd);
 }
 
 // 1/x for a positive normal FP64 x, to within about one ulp (not always

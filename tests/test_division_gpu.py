@@ -57,6 +57,33 @@ def test_constant_divisors_of_the_step(cuda, d):
     assert np.array_equal(fast.view(np.uint32), ieee.view(np.uint32))
 
 
+def test_tiny_numerators_and_subnormal_midpoints(cuda):
+    """The tiny-numerator path (|x| < 2^-100: scaled quotient, one more
+    rounding to the subnormal grid, midpoints settled by the remainder's sign)
+    against the IEEE division: x = k 2^-149 and its neighbours over divisors
+    that put x/d exactly on, just above and just below the midpoints of the
+    subnormal grid, and random tiny numerators over the Jacobi diagonals of
+    grids from 16 to 512 cells per side."""
+    ks = np.arange(1, 1 << 14, dtype=np.float64)
+    base = (ks * 2.0 ** -149).astype(np.float32)
+    up = np.nextafter(base, np.float32(1))
+    dn = np.nextafter(base, np.float32(0))
+    xs = np.concatenate([base, up, dn, -base, -up])
+    divs = [2.0, -2.0, 6.0, -6.0, 10.0, 0.375, 3.0 * 2 ** 20, -5.0 * 2 ** 23, 1.5, 2.0 ** -3, 7.0, 1.0 + 2 ** -23]
+    x = np.tile(xs, len(divs))
+    d = np.repeat(np.asarray(divs, dtype=np.float32), xs.size)
+    fast, ieee = run(x, d)
+    assert np.array_equal(fast.view(np.uint32), ieee.view(np.uint32))
+    rng = np.random.default_rng(7)
+    n = 1 << 20
+    x = (rng.uniform(1, 2, n) * np.exp2(rng.integers(-149, -90, n)) * rng.choice([-1, 1], n)).astype(np.float32)
+    h = (0.1 / rng.choice([16, 32, 48, 64, 100, 128, 200, 256, 320, 512], n)).astype(np.float32)
+    c = np.float32(1.0) / h
+    d = (-(c * c) * rng.choice([4, 5, 6], n).astype(np.float32)).astype(np.float32)
+    fast, ieee = run(x, d)
+    assert np.array_equal(fast.view(np.uint32), ieee.view(np.uint32))
+
+
 def test_fp64_reciprocal_within_one_ulp(cuda):
     """vof::rcp64 (Newton-Raphson from rcp.approx.ftz.f64, used for the FP64
     partial derivatives of the adjoint) against CUDA's correctly rounded

@@ -76,7 +76,17 @@ def test_random_state_bitwise_vs_oracle(cuda, V, orc, nx, ny, nz, seed, dt, vs):
                                  {"VOF_JACOBI": "col"}, {"VOF_JACOBI": "ring", "VOF_JACOBI_KCHUNK": "1"},
                                  {"VOF_JACOBI": "ring", "VOF_JACOBI_KCHUNK": "3"},
                                  {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "1"},
-                                 {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "5"}])
+                                 {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "5"},
+                                 {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "1"},
+                                 {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "1", "VOF_JP_MINB": "4"},
+                                 {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "2"},
+                                 {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "2", "VOF_JP_MINB": "4"},
+                                 {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "4"},
+                                 {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "4", "VOF_JP_MINB": "4"},
+                                 {"VOF_JACOBI": "peel", "VOF_JACOBI_KCHUNK": "1"},
+                                 {"VOF_JACOBI": "peel", "VOF_JACOBI_KCHUNK": "2"},
+                                 {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "4", "VOF_JACOBI_KCHUNK": "7"},
+                                 {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "4", "VOF_JACOBI_KCHUNK": "21"}])
 def test_jacobi_kernel_choices_give_the_same_bits(cuda, V, orc, tmp_path, env):
     """The Jacobi kernels a process may select (the default single-sweep
     paired kernel runs in every other test; here the two-sweep paired kernel,
