@@ -540,6 +540,141 @@ static JPKernel jp_peel_kernel() {
     return k;
 }
 
+// ---- the paired sweep fed by bulk copies of whole rows ------------------------
+// A block owns BY rows of the grid (whole padded rows, x complete) and a
+// chunk of planes.  One producer thread (the last warp's lane 0) streams, for
+// every plane k0-1 .. k1+1, the BY + 2 pressure rows j0-1 .. j0+BY and, for
+// the block's own planes, the BY rhs rows into a ring of JS_SLOTS
+// shared-memory slots with untiled bulk copies (cp.async.bulk; the rows of a
+// plane are contiguous, so one copy per field and plane, completing on the
+// slot's "full" mbarrier), up to JS_SLOTS planes ahead.  The consumer threads
+// own one pair of cells (i0 = 2m, i1 = i0 + 1) of one row each; at plane k
+// they read the pair and its x and y neighbours from plane k's slot, the
+// planes above and below from the slots beside it (the pair's own column of
+// plane k - 1 and k from registers), evaluate k_jacobi_pairs' per-cell
+// expression in its operand order (same bits), store the pair, and each warp
+// marks plane k's slot "empty" for the producer.  No register holds a
+// load in flight, so the bytes in flight are the ring's, not the occupancy's.
+// Every wait is bounded: a wait that runs out sets DEV_TMA_TIMEOUT in the
+// status word and ends the loop; the producer then waits (bounded) for the
+// copies it issued before the block exits.
+constexpr int JS_SLOTS = 8;
+
+template <int BY>
+__global__ void __launch_bounds__(512, 3) k_jacobi_bulk(Geom g, const float* __restrict__ pin,
+                                                      const float* __restrict__ rhs, float* __restrict__ pout,
+                                                      int kchunk, int* status) {
+    constexpr int slots = JS_SLOTS;
+    extern __shared__ __align__(128) unsigned char js_smem[];
+    const int px = g.px;
+    const int slot_floats = (2 * BY + 2) * px;  // BY + 2 pressure rows, BY rhs rows
+    float* ring = reinterpret_cast<float*>(js_smem);
+    uint64_t* full = reinterpret_cast<uint64_t*>(js_smem + (size_t)slots * slot_floats * sizeof(float));
+    uint64_t* empty = full + JS_SLOTS;
+    const int ncw = ((int)blockDim.x >> 5) - 1;  // consumer warps
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int j0 = 1 + blockIdx.x * BY;
+    const int nrow = min(BY, g.ny - j0 + 1);
+    const int k0 = 1 + blockIdx.y * kchunk, k1 = min(g.nz, k0 + kchunk - 1);
+    const int nplanes = k1 - k0 + 3;  // planes k0 - 1 .. k1 + 1
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < slots; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], ncw);
+        }
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    if (warp == ncw) {  // producer
+        if (lane != 0) return;
+        const uint32_t rowb = (uint32_t)px * sizeof(float);
+        bool ok = true;
+        int issued = 0;
+        for (int n = 0; n < nplanes; ++n) {
+            const int s = n % slots;
+            if (n >= slots && !(ok = mbar_wait(&empty[s], (uint32_t)((n / slots - 1) & 1)))) break;
+            const int kk = k0 - 1 + n;
+            const bool own = kk >= k0 && kk <= k1;
+            float* dst = ring + (size_t)s * slot_floats;
+            mbar_arrive_expect_tx(&full[s], rowb * (uint32_t)(nrow + 2 + (own ? nrow : 0)));
+            bulk_load(dst, pin + gidx(g, 0, j0 - 1, kk), rowb * (uint32_t)(nrow + 2), &full[s]);
+            if (own) bulk_load(dst + (BY + 2) * px, rhs + gidx(g, 0, j0, kk), rowb * (uint32_t)nrow, &full[s]);
+            issued = n + 1;
+        }
+        if (!ok) {
+            atomicOr(status, DEV_TMA_TIMEOUT);
+            // no copy may outlive the block: wait for the last fill of every slot
+            for (int n = issued - 1; n >= 0 && n >= issued - slots; --n)
+                mbar_wait(&full[n % slots], (uint32_t)((n / slots) & 1));
+        }
+        return;
+    }
+
+    // consumers: one pair per thread
+    const int npair = g.nx / 2 + 1;
+    const int t = threadIdx.x;
+    const bool act = t < nrow * npair;
+    const int r = act ? t / npair : 0, m = act ? t - r * npair : 0;
+    const int j = j0 + r, i0 = 2 * m, i1 = i0 + 1;
+    const bool a0 = act && i0 >= 1, a1 = act && i1 <= g.nx;
+    const float cx = g.dxi * g.dxi, cy = g.dyi * g.dyi, cz = g.dzi * g.dzi;
+    const float ae0 = (i0 != g.nx) ? cx : 0.0f, aw0 = (i0 != 1) ? cx : 0.0f;
+    const float ae1 = (i1 != g.nx) ? cx : 0.0f, aw1 = (i1 != 1) ? cx : 0.0f;
+    const float an = (j != g.ny) ? cy : 0.0f, as = (j != 1) ? cy : 0.0f;
+    const float2 dm = make_float2(-(ae0 + aw0 + an + as + cz + cz), -(ae1 + aw1 + an + as + cz + cz));
+    const float2 rm = make_float2(__frcp_rn(dm.x), __frcp_rn(dm.y));
+    const int off = (r + 1) * px + i0;     // the pair in a slot's pressure rows (even: float2-aligned)
+    const int roff = (BY + 2 + r) * px + i0;  // ... and in its rhs rows
+    float2* O = reinterpret_cast<float2*>(pout);
+    const int o0 = gidx(g, i0, j, 0) >> 1;
+    const int wp = g.plane >> 1;
+    bool ok = mbar_wait(&full[0], 0) && mbar_wait(&full[1], 0);
+    float2 pm = make_float2(0.0f, 0.0f), pc = pm;
+    if (ok) {
+        pm = *reinterpret_cast<const float2*>(ring + off);
+        pc = *reinterpret_cast<const float2*>(ring + (size_t)slot_floats + off);
+        // plane k0 - 1 is read by nobody any more (the pair's own column is in pm)
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[0]);
+    }
+    for (int k = k0; k <= k1 && ok; ++k) {
+        const int n = k - k0 + 2;  // plane k + 1
+        if (!(ok = mbar_wait(&full[n % slots], (uint32_t)((n / slots) & 1)))) break;
+        const float* Pc = ring + (size_t)((n - 1) % slots) * slot_floats;
+        const float* Pp = ring + (size_t)(n % slots) * slot_floats;
+        const float2 pp = *reinterpret_cast<const float2*>(Pp + off);
+        const float2 pN = *reinterpret_cast<const float2*>(Pc + off + px);
+        const float2 pS = *reinterpret_cast<const float2*>(Pc + off - px);
+        const float2 rc = *reinterpret_cast<const float2*>(Pc + roff);
+        const float pw = Pc[off - 1], pe = Pc[off + 2];
+        const bool kb = k == 1, kt = k == g.nz;
+        const float af = kt ? 0.0f : cz, ab = kb ? 0.0f : cz;
+        float2 d = dm, rd = rm;
+        if (kb || kt) {
+            d = make_float2(-(ae0 + aw0 + an + as + af + ab), -(ae1 + aw1 + an + as + af + ab));
+            rd = make_float2(__frcp_rn(d.x), __frcp_rn(d.y));
+        }
+        const float v0 =
+            div_rn_pre(rc.x - ae0 * pc.y - aw0 * pw - an * pN.x - as * pS.x - af * pp.x - ab * pm.x, d.x, rd.x);
+        const float v1 =
+            div_rn_pre(rc.y - ae1 * pe - aw1 * pc.x - an * pN.y - as * pS.y - af * pp.y - ab * pm.y, d.y, rd.y);
+        const int o = o0 + k * wp;
+        if (a0 && a1)
+            O[o] = make_float2(v0, v1);
+        else if (a0)
+            pout[2 * o] = v0;
+        else if (a1)
+            pout[2 * o + 1] = v1;
+        pm = pc;
+        pc = pp;
+        // plane k is read by nobody any more (its column goes on in pm)
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[(n - 1) % slots]);
+    }
+    if (!ok && lane == 0) atomicOr(status, DEV_TMA_TIMEOUT);
+}
+
 // ---- the paired sweep with a deeper prefetch of its own column ---------------
 // k_jacobi_pairs keeps one plane of loads in flight per thread, which at
 // 200^3 leaves the sweep waiting on memory (about a third of the bytes in
@@ -718,6 +853,80 @@ cudaError_t jacobi_ring_launch(const Geom& g, const float* pin, const float* rhs
     k_jacobi_ring<<<dim3(bx, (g.nz + kchunk - 1) / kchunk), JP_THREADS, 0, s>>>(g, pin, rhs, pout, kchunk);
     return cudaGetLastError();
 }
+
+// Launch shape of k_jacobi_bulk: rows per block (BY * npair pairs must fit
+// one block with its producer warp) and the z chunk from the resident-block
+// count (the occupancy of that shape).  Cached for the last grid.
+struct JSPlan {
+    int nx, ny, nz, px;
+    int by, slots, threads, kchunk, bx;
+    size_t smem;
+    bool ok;
+};
+
+static bool js_plan(const Geom& g, JSPlan* out) {
+    static JSPlan last{};
+    if (last.nx == g.nx && last.ny == g.ny && last.nz == g.nz && last.px == g.px && last.threads > 0) {
+        *out = last;
+        return last.ok;
+    }
+    JSPlan p{};
+    p.nx = g.nx;
+    p.ny = g.ny;
+    p.nz = g.nz;
+    p.px = g.px;
+    const int npair = g.nx / 2 + 1;
+    static int force_by = -1;
+    if (force_by < 0) {
+        const char* v = getenv("VOF_JS_BY");
+        force_by = v ? atoi(v) : 0;
+    }
+    int by = (force_by == 1 || force_by == 2 || force_by == 4) ? force_by : 4;
+    while (by > 1 && by * npair > 480) by >>= 1;
+    p.ok = by * npair <= 480;
+    const size_t bars = 2 * JS_SLOTS * sizeof(uint64_t);
+    const size_t slot_bytes = (size_t)(2 * by + 2) * g.px * sizeof(float);
+    const int slots = JS_SLOTS;
+    p.smem = slots * slot_bytes + bars;
+    p.ok = p.ok && p.smem <= (size_t)227 * 1024;
+    p.by = by;
+    p.slots = slots;
+    p.threads = ((by * npair + 31) / 32) * 32 + 32;
+    p.bx = (g.ny + by - 1) / by;
+    int occ = 0, dev = 0, sms = 148;
+    if (p.ok) {
+        const void* k = by == 4 ? (const void*)k_jacobi_bulk<4> : by == 2 ? (const void*)k_jacobi_bulk<2>
+                                                                          : (const void*)k_jacobi_bulk<1>;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, p.threads, p.smem) != cudaSuccess)
+            occ = 0;
+        p.ok = occ > 0;
+    }
+    p.kchunk = jacobi_pairs_kchunk(g, p.bx, (occ > 0 ? occ : 1) * sms);
+    last = p;
+    *out = p;
+    return p.ok;
+}
+
+bool jacobi_bulk_supported(const Geom& g) {
+    JSPlan p;
+    return js_plan(g, &p);
+}
+
+cudaError_t jacobi_bulk_launch(const Geom& g, const float* pin, const float* rhs, float* pout, int* status,
+                               cudaStream_t s) {
+    JSPlan p;
+    if (!js_plan(g, &p)) return cudaErrorInvalidValue;
+    const dim3 grid(p.bx, (g.nz + p.kchunk - 1) / p.kchunk);
+    switch (p.by) {
+        case 4: k_jacobi_bulk<4><<<grid, p.threads, p.smem, s>>>(g, pin, rhs, pout, p.kchunk, status); break;
+        case 2: k_jacobi_bulk<2><<<grid, p.threads, p.smem, s>>>(g, pin, rhs, pout, p.kchunk, status); break;
+        default: k_jacobi_bulk<1><<<grid, p.threads, p.smem, s>>>(g, pin, rhs, pout, p.kchunk, status); break;
+    }
+    return cudaGetLastError();
+}
+
 
 // ---- two sweeps per launch, two cells per thread, marching z ----------------
 // The pressure and rhs of a plane are read from memory once for two sweeps,
@@ -982,6 +1191,17 @@ cudaError_t jacobi_tb_configure() {
                                                            sizeof(float2) * (5u * J2_THREADS + 64u))) != cudaSuccess)
         return e;
     j2_blocks = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
+    for (const void* k : {(const void*)k_jacobi_bulk<4>, (const void*)k_jacobi_bulk<2>, (const void*)k_jacobi_bulk<1>})
+        if ((e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
+            return e;
+    if ((e = cudaFuncSetAttribute(k_jacobi_bulk<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024)) !=
+            cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_jacobi_bulk<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024)) !=
+            cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_jacobi_bulk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024)) !=
+            cudaSuccess)
+        return e;
     if ((e = cudaFuncSetAttribute(k_jacobi_tb<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)JTile<1>::SMEM)) != cudaSuccess)
         return e;

@@ -31,6 +31,13 @@ cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rh
 // (unrolled VOF_JP_UNROLL times, default 4); same bits as jacobi_pairs_launch.
 cudaError_t jacobi_peel_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);
 
+// The paired sweep fed by bulk copies of whole rows into a shared-memory
+// ring (one producer thread, bounded mbarrier waits that report
+// DEV_TMA_TIMEOUT in *status); same bits as jacobi_pairs_launch.
+bool jacobi_bulk_supported(const Geom& g);
+cudaError_t jacobi_bulk_launch(const Geom& g, const float* pin, const float* rhs, float* pout, int* status,
+                               cudaStream_t s);
+
 // The paired sweep with its own column's loads copied several planes ahead
 // into shared memory (cp.async); same bits as jacobi_pairs_launch.
 cudaError_t jacobi_ring_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);

@@ -423,7 +423,7 @@ static_assert(JACOBI_T >= 1 && JACOBI_T <= JACOBI_TB_MAX, "VOF_JACOBI_T out of r
 // blocked sweeps per launch through TMA (k_jacobi_tb).
 // VOF_JACOBI=pairs|ring|col|pairs2|tb forces one.  All give the same bits.
 // (Measured on a B200 at 200^3, 10 sweeps: pairs 0.275 ms, pairs2 0.290 ms.)
-enum { JACOBI_PAIRS = 0, JACOBI_COL = 1, JACOBI_TB = 2, JACOBI_PAIRS2 = 3, JACOBI_RING = 4, JACOBI_PEEL = 5 };
+enum { JACOBI_PAIRS = 0, JACOBI_COL = 1, JACOBI_TB = 2, JACOBI_PAIRS2 = 3, JACOBI_RING = 4, JACOBI_PEEL = 5, JACOBI_TB1 = 6, JACOBI_BULK = 7 };
 static int jacobi_kind(const Geom& g) {
     static int forced = -2;
     if (forced == -2) {
@@ -435,15 +435,21 @@ static int jacobi_kind(const Geom& g) {
         if (v && !strcmp(v, "pairs2")) forced = JACOBI_PAIRS2;
         if (v && !strcmp(v, "ring")) forced = JACOBI_RING;
         if (v && !strcmp(v, "peel")) forced = JACOBI_PEEL;
+        if (v && !strcmp(v, "tb1")) forced = JACOBI_TB1;
+        if (v && !strcmp(v, "bulk")) forced = JACOBI_BULK;
     }
     const int k = forced >= 0 ? forced : JACOBI_PAIRS;
+    if (k == JACOBI_BULK && !jacobi_bulk_supported(g)) return JACOBI_PAIRS;
     return (k == JACOBI_PAIRS2 && !jacobi_pairs2_supported(g)) ? JACOBI_PAIRS : k;
 }
 static bool jacobi_streaming(const Geom& g) {
     const int k = jacobi_kind(g);
-    return k == JACOBI_PAIRS || k == JACOBI_COL || k == JACOBI_RING || k == JACOBI_PEEL;
+    return k == JACOBI_PAIRS || k == JACOBI_COL || k == JACOBI_RING || k == JACOBI_PEEL || k == JACOBI_BULK;
 }
-static int jacobi_per_launch(const Geom& g) { return jacobi_kind(g) == JACOBI_PAIRS2 ? 2 : JACOBI_T; }
+static int jacobi_per_launch(const Geom& g) {
+    const int k = jacobi_kind(g);
+    return k == JACOBI_PAIRS2 ? 2 : k == JACOBI_TB1 ? 1 : JACOBI_T;
+}
 
 static int jacobi_launches(const Geom& g, int iters) {
     if (jacobi_streaming(g)) return iters;
@@ -583,6 +589,7 @@ cudaError_t plain_pressure(const Geom& g, const PlainBuffers& b, int jacobi_iter
             e = kind == JACOBI_COL    ? jacobi_col_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s)
                 : kind == JACOBI_RING ? jacobi_ring_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s)
                 : kind == JACOBI_PEEL ? jacobi_peel_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s)
+                : kind == JACOBI_BULK ? jacobi_bulk_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], b.status, s)
                                       : jacobi_pairs_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s);
             if (e != cudaSuccess) return e;
             cur ^= 1;
@@ -596,8 +603,9 @@ cudaError_t plain_pressure(const Geom& g, const PlainBuffers& b, int jacobi_iter
             cur ^= 1;
         }
     } else {
+        const int T1 = jacobi_per_launch(g);
         for (int q = 0; q < L; ++q) {
-            const int T = (q == 0 && jacobi_iters % JACOBI_T) ? jacobi_iters % JACOBI_T : JACOBI_T;
+            const int T = (q == 0 && jacobi_iters % T1) ? jacobi_iters % T1 : T1;
             if ((e = jacobi_tb_launch(g, T, b.maps[seq[q]], b.maps[3], pbuf[seq[q + 1]], b.status, s)) !=
                 cudaSuccess)
                 return e;

@@ -150,22 +150,38 @@ enum Post { POST_NONE = 0, POST_MEAN = 1, POST_SQRT = 2, POST_RATIO = 3, POST_SC
 
 // The fold of pass 2 by one block of RED_THREADS threads (partials read past
 // L1: they may have been written by other blocks of the same launch).
+// Each thread folds its strided partials in order, the warps fold their
+// lanes by a fixed shuffle tree, and thread 0 folds the warps in order.
 __device__ void fold_partials(const double* __restrict__ partial, int nblk, int nv, int op0, int op1, int op2,
                               int post, double scale, double* result) {
-    __shared__ double sh[3][RED_THREADS];
+    __shared__ double sh[3][RED_THREADS / 32];
     const int ops[3] = {op0, op1, op2};
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    // the partials of a thread loaded together, then folded in order
+    constexpr int PER = (RED_BLOCKS + RED_THREADS - 1) / RED_THREADS;
+    double xs[3][PER];
+#pragma unroll
+    for (int v = 0; v < 3; ++v)
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int b = threadIdx.x + q * RED_THREADS;
+            xs[v][q] = (v < nv && b < nblk) ? __ldcg(partial + (size_t)nv * b + v) : identity(ops[v]);
+        }
     for (int v = 0; v < nv; ++v) {
         double x = identity(ops[v]);
-        for (int b = threadIdx.x; b < nblk; b += RED_THREADS)
+#pragma unroll
+        for (int q = 0; q < PER; ++q) x = combine(x, xs[v][q], ops[v]);
+        for (int b = threadIdx.x + PER * RED_THREADS; b < nblk; b += RED_THREADS)
             x = combine(x, __ldcg(partial + (size_t)nv * b + v), ops[v]);
-        sh[v][threadIdx.x] = x;
+        for (int o = 16; o > 0; o >>= 1) x = combine(x, __shfl_down_sync(0xffffffffu, x, o), ops[v]);
+        if (lane == 0) sh[v][wid] = x;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         double r[3];
         for (int v = 0; v < nv; ++v) {
             double x = sh[v][0];
-            for (int q = 1; q < RED_THREADS; ++q) x = combine(x, sh[v][q], ops[v]);
+            for (int q = 1; q < RED_THREADS / 32; ++q) x = combine(x, sh[v][q], ops[v]);
             r[v] = x;
         }
         double out0 = r[0];
@@ -189,18 +205,67 @@ __global__ void __launch_bounds__(RED_THREADS) k_red_finish(const double* __rest
 // and counts itself done; the last one folds all partials in the same fixed
 // order as k_red_finish (the same bits), copies result[slot] to the mapped
 // host double when given, and clears the counter for the next launch.
-__global__ void __launch_bounds__(RED_THREADS) k_red_field_fold(Geom g, const float* __restrict__ a,
+// The field is read as aligned float4 words (a padded row starts on a
+// 128-byte boundary and holds at least round_up(nx + 2, 4) floats): rows
+// dealt to warps as in FOR_INTERIOR, the lanes on consecutive words of a row,
+// the ghost and padding entries masked out.  A warp loads RG rows x 2 words
+// per lane before it adds any of them, so that 4 loads of a lane are in
+// flight at once (more spill at 64 registers, the cap for 4 blocks per SM);
+// a row wider than 64 words takes several such passes.
+constexpr int RG = 2;
+
+__device__ __forceinline__ void field_words(const Geom& g, const float* __restrict__ a, double (&val)[3]) {
+    const int lane = threadIdx.x & 31;
+    const int nr = g.ny * g.nz, wpr = (g.nx + 5) >> 2;  // words covering columns 0 .. nx + 1
+    const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    auto take = [&](float f, int i) {
+        if (i >= 1 && i <= g.nx) {
+            const double x = (double)f;
+            val[0] += x;
+            val[1] = fmax(val[1], x);
+            val[2] = fmin(val[2], x);
+        }
+    };
+    for (int rb = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); rb < nr; rb += RG * nw) {
+        for (int q0 = 0; q0 < wpr; q0 += 64) {
+            float4 v[RG][2];
+            bool ok[RG][2];
+#pragma unroll
+            for (int u = 0; u < RG; ++u) {
+                const int r = rb + u * nw;
+                const bool rv = r < nr;
+                const int rr = rv ? r : rb;
+                const float4* w = reinterpret_cast<const float4*>(a + gidx(g, 0, 1 + rr % g.ny, 1 + rr / g.ny));
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int q = q0 + lane + 32 * h;
+                    ok[u][h] = rv && q < wpr;
+                    v[u][h] = ok[u][h] ? w[q] : zero;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < RG; ++u)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    if (ok[u][h]) {
+                        const int i = 4 * (q0 + lane + 32 * h);
+                        take(v[u][h].x, i);
+                        take(v[u][h].y, i + 1);
+                        take(v[u][h].z, i + 2);
+                        take(v[u][h].w, i + 3);
+                    }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(RED_THREADS, 4) k_red_field_fold(Geom g, const float* __restrict__ a,
                                                                 double* partial, unsigned* counter,
                                                                 double scale, double* result,
                                                                 double* host_alias, int slot) {
     double val[3] = {0.0, -INFINITY, INFINITY};
     const int op[3] = {OP_SUM, OP_MAX, OP_MIN};
-    FOR_INTERIOR(g, i, j, k) {
-        const double x = (double)a[gidx(g, i, j, k)];
-        val[0] += x;
-        val[1] = fmax(val[1], x);
-        val[2] = fmin(val[2], x);
-    }
+    field_words(g, a, val);
     block_reduce_store<3>(val, op, partial);
     __shared__ bool last;
     if (threadIdx.x == 0) {

@@ -2,7 +2,8 @@
 // mbarrier helpers for sm_100a, in inline PTX, plus host-side tensor-map
 // encoding through the driver entry point (no link against libcuda).
 //
-// Only plain (non-multicast) tiled loads of this GPU's own memory are used.
+// Only plain (non-multicast) tiled and untiled bulk loads of this GPU's own
+// memory are used.
 // Every wait is bounded: a wait that runs out of iterations reports failure
 // and the kernel records it in a device status word instead of hanging.
 #pragma once
@@ -59,6 +60,22 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
         if (done) return true;
     }
     return false;
+}
+
+// One arrival on the barrier (no transaction bytes).
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Untiled bulk copy of `bytes` bytes (a multiple of 16; both addresses
+// 16-byte aligned) from this GPU's global memory into shared memory,
+// completing on `bar` (complete_tx).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
 }
 
 // 3D tiled TMA load of one box at element coordinates (x, y, z) into shared

@@ -77,6 +77,10 @@ def test_random_state_bitwise_vs_oracle(cuda, V, orc, nx, ny, nz, seed, dt, vs):
                                  {"VOF_JACOBI": "ring", "VOF_JACOBI_KCHUNK": "3"},
                                  {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "1"},
                                  {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "5"},
+                                 {"VOF_JACOBI": "tb1"},
+                                 {"VOF_JACOBI": "bulk"}, {"VOF_JACOBI": "bulk", "VOF_JACOBI_KCHUNK": "1"},
+                                 {"VOF_JACOBI": "bulk", "VOF_JACOBI_KCHUNK": "7"},
+                                 {"VOF_JACOBI": "bulk", "VOF_JACOBI_KCHUNK": "21"},
                                  {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "1"},
                                  {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "1", "VOF_JP_MINB": "4"},
                                  {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "2"},
