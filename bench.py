@@ -66,14 +66,16 @@ ALG_BYTES = {
     "sweep3": 12,
 }
 KERNEL_NAMES = {
-    "predict": "k_predict", "rhs": "k_rhs", "jacobi": "k_jacobi_pairs", "correct": "k_correct",
+    "predict": "k_predict", "rhs": "k_rhs", "jacobi": "k_jacobi_peel", "correct": "k_correct4",
     "sweep1": "k_fct_x|k_fct_march", "sweep2": "k_fct_x|k_fct_march", "sweep3": "k_fct_x|k_fct_march",
 }
-# the Jacobi kernel the library runs at the bench size (VOF_JACOBI=pairs|peel|ring|col|pairs2|tb;
-# pairs, one sweep per launch with two cells per thread, by default)
-KERNEL_NAMES["jacobi"] = {"col": "k_jacobi_col", "tb": "k_jacobi_tb", "pairs2": "k_jacobi_pairs2",
-                          "ring": "k_jacobi_ring", "peel": "k_jacobi_peel"}.get(os.environ.get("VOF_JACOBI", ""),
-                                                                               "k_jacobi_pairs")
+# the Jacobi kernel the library runs at the bench size (VOF_JACOBI=peel|pairs|ring|bulk|col|pairs2|tb|tb1;
+# peel, one sweep per launch with two cells per thread, by default)
+KERNEL_NAMES["jacobi"] = {"col": "k_jacobi_col", "tb": "k_jacobi_tb", "tb1": "k_jacobi_tb", "pairs2": "k_jacobi_pairs2",
+                          "ring": "k_jacobi_ring", "bulk": "k_jacobi_bulk",
+                          "pairs": "k_jacobi_pairs"}.get(os.environ.get("VOF_JACOBI", ""), "k_jacobi_peel")
+if os.environ.get("VOF_CORRECT") == "1":
+    KERNEL_NAMES["correct"] = "k_correct"
 STEP_MODEL_BYTES = 188  # B per cell-step of the fused plain path (10 sweeps, FP32)
 WARM_MS = 60.0  # least GPU time of warm-up steps run back to back before a timed region
 

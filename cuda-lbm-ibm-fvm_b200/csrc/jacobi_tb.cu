@@ -532,7 +532,7 @@ static JPKernel jp_peel_kernel() {
         const char* v = getenv("VOF_JP_UNROLL");
         const char* b = getenv("VOF_JP_MINB");
         const int u = v ? atoi(v) : 2;
-        const int mb = b ? atoi(b) : 1;
+        const int mb = b ? atoi(b) : 4;
         k = u == 1 ? (mb == 4 ? k_jacobi_peel<1, 4> : k_jacobi_peel<1, 1>)
             : u == 4 ? (mb == 4 ? k_jacobi_peel<4, 4> : k_jacobi_peel<4, 1>)
                      : (mb == 4 ? k_jacobi_peel<2, 4> : k_jacobi_peel<2, 1>);
@@ -805,18 +805,12 @@ static int jp_wave = 4 * 148;
 // overrides.
 static int jr_wave = 4 * 148;  // the same for k_jacobi_ring
 
-static int jacobi_pairs_kchunk(const Geom& g, int bx, int wave = jp_wave) {
-    static int forced = -1;
-    if (forced < 0) {
-        const char* v = getenv("VOF_JACOBI_KCHUNK");
-        forced = v ? atoi(v) : 0;
-    }
-    if (forced > 0) return forced < g.nz ? forced : g.nz;
-    int best = g.nz;
+int wave_kchunk(int nz, int bx, int wave) {
+    int best = nz;
     double best_fill = -1.0;
-    for (int n = 1; n <= g.nz; ++n) {
-        const int kc = (g.nz + n - 1) / n;  // n chunks of (nearly) equal length
-        const long long blocks = (long long)bx * ((g.nz + kc - 1) / kc);
+    for (int n = 1; n <= nz; ++n) {
+        const int kc = (nz + n - 1) / n;  // n chunks of (nearly) equal length
+        const long long blocks = (long long)bx * ((nz + kc - 1) / kc);
         const long long waves = (blocks + wave - 1) / wave;
         const double fill = (double)blocks / (double)(waves * wave);
         if (fill >= 0.85) return kc;
@@ -827,6 +821,17 @@ static int jacobi_pairs_kchunk(const Geom& g, int bx, int wave = jp_wave) {
     }
     return best;
 }
+
+static int jacobi_pairs_kchunk(const Geom& g, int bx, int wave = jp_wave) {
+    static int forced = -1;
+    if (forced < 0) {
+        const char* v = getenv("VOF_JACOBI_KCHUNK");
+        forced = v ? atoi(v) : 0;
+    }
+    if (forced > 0) return forced < g.nz ? forced : g.nz;
+    return wave_kchunk(g.nz, bx, wave);
+}
+
 
 cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s) {
     const int nq = (g.nx / 2 + 1) * g.ny;

@@ -31,6 +31,11 @@ cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rh
 // (unrolled VOF_JP_UNROLL times, default 4); same bits as jacobi_pairs_launch.
 cudaError_t jacobi_peel_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);
 
+// z chunk of a launch of bx blocks per chunk whose resident blocks number
+// `wave`: the longest chunk whose last wave of blocks is 85 % full or more,
+// else the one that fills it best.
+int wave_kchunk(int nz, int bx, int wave);
+
 // The paired sweep fed by bulk copies of whole rows into a shared-memory
 // ring (one producer thread, bounded mbarrier waits that report
 // DEV_TMA_TIMEOUT in *status); same bits as jacobi_pairs_launch.

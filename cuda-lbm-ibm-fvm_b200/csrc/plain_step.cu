@@ -10,12 +10,14 @@
 // last bits of contracted expressions.
 //
 // Kernel map (reference kernels each one replaces):
-//   k_predict      advect_{u,v,w}_kernel + cal_nu_rho_kernel   voftrial1.cu:95-104, 230-399
-//   k_rhs          the rhs expression of solve_p_jacobi_kernel voftrial1.cu:418-422
-//   k_jacobi_pairs (jacobi_tb.cu) one solve_p_jacobi_kernel sweep per launch,  voftrial1.cu:401-439
-//                  two cells per thread (VOF_JACOBI=tb: k_jacobi_tb<T>, T sweeps
-//                  per launch; VOF_JACOBI=col: k_jacobi_col)
-//   k_correct      update_{u,v,w}_kernel + apply_bc_velocity   voftrial1.cu:441-493, 959-1051, 1107-1120
+//   k_predict2     advect_{u,v,w}_kernel + cal_nu_rho_kernel   voftrial1.cu:95-104, 230-399
+//                  two cells per thread (k_predict: one; VOF_PREDICT=1)
+//   k_rhs4         the rhs expression of solve_p_jacobi_kernel voftrial1.cu:418-422
+//                  four cells per thread (k_rhs: one, marching z; VOF_RHS=1)
+//   k_jacobi_peel  (jacobi_tb.cu) one solve_p_jacobi_kernel sweep per launch,  voftrial1.cu:401-439
+//                  two cells per thread (alternatives selected by VOF_JACOBI, below)
+//   k_correct4     update_{u,v,w}_kernel + apply_bc_velocity   voftrial1.cu:441-493, 959-1051, 1107-1120
+//                  four cells per thread (k_correct: one; VOF_CORRECT=1)
 //   k_fct<AXIS,FINAL>  (fct_sweep.cu) fct_{x,y,z}_sweep_stage1..4, and on
 //                  the last sweep post_process_f_kernel + apply_bc_F   voftrial1.cu:502-905, 1053-1135
 #include "plain_step.h"
@@ -55,11 +57,11 @@ struct Column {
 // Indices whose clamped value is x on an axis of n interior cells: x itself,
 // plus the ghost 0 when x == 1 and the ghost n+1 when x == n.
 __device__ __forceinline__ int mirrors(int x, int n, int* out) {
-    int m = 0;
-    out[m++] = x;
-    if (x == 1) out[m++] = 0;
-    if (x == n) out[m++] = n + 1;
-    return m;
+    // fixed positions (no runtime index: the list stays in registers)
+    out[0] = x;
+    out[1] = (x == 1) ? 0 : n + 1;
+    out[2] = n + 1;
+    return 1 + (x == 1) + (x == n);
 }
 
 // ---------------------------------------------------------------------------
@@ -138,6 +140,160 @@ __global__ void __launch_bounds__(256) k_predict(Geom g,
         w_km = w_c; w_c = w_kp;
         wim_c = wim_kp; wjm_c = wjm_kp;
         uip_km = uip_c; vjp_km = vjp_c;
+    }
+}
+
+// The predictor with two cells per thread.  Cells are paired by padded column
+// (2m, 2m + 1: one aligned 8-byte word), the pairs of all rows of a plane
+// numbered flat so that 32 consecutive pairs make a warp across row ends, and
+// a thread marches a chunk of planes, carrying its pair's k-1 / k values in
+// registers as k_predict does.  Every operand is a float2 load (10 per pair
+// and plane: u, v, w of the next plane, the rows j-1 and j+1 of u, v, w,
+// w of the next plane's row j-1, v of row j+1, and F); the x-1 and x+1
+// neighbours come from the lanes beside (a pair's left neighbour is the left
+// lane's second cell, its right neighbour the right lane's first), or from
+// memory at the ends of a warp and of a row.  Each cell's three updates keep
+// k_predict's expressions and operand order (same bits).
+// The pair's left (x-1 of the first cell) and right (x+1 of the second cell)
+// neighbours of a value held as a pair by every lane.
+__device__ __forceinline__ float left_of(float2 a, bool ldw, const float* __restrict__ p, int idl) {
+    const float s = __shfl_up_sync(0xffffffffu, a.y, 1);
+    return ldw ? __ldg(p + idl) : s;
+}
+__device__ __forceinline__ float right_of(float2 a, bool lde, const float* __restrict__ p, int idr) {
+    const float s = __shfl_down_sync(0xffffffffu, a.x, 1);
+    return lde ? __ldg(p + idr) : s;
+}
+
+__global__ void __launch_bounds__(256, 4) k_predict2(Geom g, const float* __restrict__ F,
+                                                     const float* __restrict__ u, const float* __restrict__ v,
+                                                     const float* __restrict__ w, float* __restrict__ us,
+                                                     float* __restrict__ vs, float* __restrict__ ws, int kchunk) {
+    const int npair = g.nx / 2 + 1;  // pairs covering columns 0 .. nx
+    const int nq = npair * g.ny;
+    const int qt = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool qa = qt < nq;
+    const int q = qa ? qt : nq - 1;  // lanes past the end shadow the last pair
+    const int jr = q / npair, m = q - jr * npair;
+    const int j = jr + 1, i0 = 2 * m;
+    const int lane = threadIdx.x & 31;
+    const bool ldw = lane == 0 && m > 0;            // x-1 neighbours from memory
+    const bool lde = lane == 31 || m == npair - 1;  // x+1 neighbours from memory
+    const int k0 = 1 + blockIdx.y * kchunk, k1 = min(g.nz, k0 + kchunk - 1);
+    const int sy = g.px, sz = g.plane;
+    // which cells of the pair are updated (u from i = 2, v and w from i = 1)
+    const bool a0 = qa && i0 >= 1 && i0 <= g.nx, a1 = qa && i0 + 1 <= g.nx;
+    const bool u0 = qa && i0 >= 2 && i0 <= g.nx, u1 = qa && i0 + 1 >= 2 && i0 + 1 <= g.nx;
+    auto L2 = [](const float* __restrict__ p, int id) { return __ldg(reinterpret_cast<const float2*>(p + id)); };
+    int id = gidx(g, i0, j, k0);  // even
+    // column windows along k (values of the pair's two cells)
+    float2 u_km = L2(u, id - sz), u_c = L2(u, id);
+    float2 v_km = L2(v, id - sz), v_c = L2(v, id);
+    float2 w_km = L2(w, id - sz), w_c = L2(w, id);
+    float2 wjm_c = L2(w, id - sy), vjp_km = L2(v, id + sy - sz);
+    // x neighbours carried from the previous plane
+    float wim_c = left_of(w_c, ldw, w, id - 1);
+    float uip_km = right_of(u_km, lde, u, id + 2 - sz);
+    for (int k = k0; k <= k1; ++k, id += sz) {
+        const float2 u_kp = L2(u, id + sz), v_kp = L2(v, id + sz), w_kp = L2(w, id + sz);
+        const float2 wjm_kp = L2(w, id - sy + sz), vjp_c = L2(v, id + sy);
+        const float2 ujm = L2(u, id - sy), ujp = L2(u, id + sy), vjm = L2(v, id - sy), wjp = L2(w, id + sy);
+        const float2 f2 = L2(F, id);
+        const float wim_kp = left_of(w_kp, ldw, w, id - 1 + sz);
+        const float uim0 = left_of(u_c, ldw, u, id - 1), uip1 = right_of(u_c, lde, u, id + 2);
+        const float vim0 = left_of(v_c, ldw, v, id - 1), vip1 = right_of(v_c, lde, v, id + 2);
+        const float vjp_im0 = left_of(vjp_c, ldw, v, id - 1 + sy);
+        const float ujm_ip1 = right_of(ujm, lde, u, id + 2 - sy);
+        const float wip1 = right_of(w_c, lde, w, id + 2);
+        float out_u[2], out_v[2], out_w[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            // this cell's values and its x neighbours
+            const float uc = e ? u_c.y : u_c.x, ukm = e ? u_km.y : u_km.x, ukp = e ? u_kp.y : u_kp.x;
+            const float vc = e ? v_c.y : v_c.x, vkm = e ? v_km.y : v_km.x, vkp = e ? v_kp.y : v_kp.x;
+            const float wc = e ? w_c.y : w_c.x, wkm = e ? w_km.y : w_km.x, wkp = e ? w_kp.y : w_kp.x;
+            const float uim = e ? u_c.x : uim0, uip_c = e ? uip1 : u_c.y;
+            const float vim = e ? v_c.x : vim0, vip = e ? vip1 : v_c.y;
+            const float wim_cc = e ? w_c.x : wim_c, wim_kpp = e ? w_kp.x : wim_kp;
+            const float wip = e ? wip1 : w_c.y;
+            const float vjpc = e ? vjp_c.y : vjp_c.x, vjp_im = e ? vjp_c.x : vjp_im0;
+            const float vjpkm = e ? vjp_km.y : vjp_km.x;
+            const float ujmc = e ? ujm.y : ujm.x, ujpc = e ? ujp.y : ujp.x, ujm_ip = e ? ujm_ip1 : ujm.y;
+            const float vjmc = e ? vjm.y : vjm.x;
+            const float wjmc = e ? wjm_c.y : wjm_c.x, wjmkp = e ? wjm_kp.y : wjm_kp.x;
+            const float wjpc = e ? wjp.y : wjp.x;
+            const float uipkm = e ? uip_km : u_km.y;
+            const float nu = nu_of(g, e ? f2.y : f2.x);
+            {  // advect_u_kernel, voftrial1.cu:230-285
+                const float v_here = 0.25f * (vim + vjp_im + vc + vjpc);
+                const float w_here = 0.25f * (wim_cc + wim_kpp + wc + wkp);
+                const float dudx = (uc > 0.0f) ? (uc - uim) * g.dxi : (uip_c - uc) * g.dxi;
+                const float dudy = (v_here > 0.0f) ? (uc - ujmc) * g.dyi : (ujpc - uc) * g.dyi;
+                const float dudz = (w_here > 0.0f) ? (uc - ukm) * g.dzi : (ukp - uc) * g.dzi;
+                const float visc = nu * (uim - 2.0f * uc + uip_c) * g.dxi * g.dxi +
+                                   nu * (ujmc - 2.0f * uc + ujpc) * g.dyi * g.dyi +
+                                   nu * (ukm - 2.0f * uc + ukp) * g.dzi * g.dzi;
+                const float adv = -uc * dudx - v_here * dudy - w_here * dudz;
+                out_u[e] = uc + g.dt * (visc + adv + g.gx);
+            }
+            {  // advect_v_kernel, voftrial1.cu:287-342
+                const float u_here = 0.25f * (ujmc + uc + ujm_ip + uip_c);
+                const float w_here = 0.25f * (wjmkp + wjmc + wc + wkp);
+                const float dvdx = (u_here > 0.0f) ? (vc - vim) * g.dxi : (vip - vc) * g.dxi;
+                const float dvdy = (vc > 0.0f) ? (vc - vjmc) * g.dyi : (vjpc - vc) * g.dyi;
+                const float dvdz = (w_here > 0.0f) ? (vc - vkm) * g.dzi : (vkp - vc) * g.dzi;
+                const float visc = nu * (vim - 2.0f * vc + vip) * g.dxi * g.dxi +
+                                   nu * (vjmc - 2.0f * vc + vjpc) * g.dyi * g.dyi +
+                                   nu * (vkm - 2.0f * vc + vkp) * g.dzi * g.dzi;
+                const float adv = -u_here * dvdx - vc * dvdy - w_here * dvdz;
+                out_v[e] = vc + g.dt * (visc + adv + g.gy);
+            }
+            {  // advect_w_kernel, voftrial1.cu:344-399
+                const float u_here = 0.25f * (uipkm + ukm + uip_c + uc);
+                const float v_here = 0.25f * (vjpkm + vkm + vc + vjpc);
+                const float dwdx = (u_here > 0.0f) ? (wc - wim_cc) * g.dxi : (wip - wc) * g.dxi;
+                const float dwdy = (v_here > 0.0f) ? (wc - wjmc) * g.dyi : (wjpc - wc) * g.dyi;
+                const float dwdz = (wc > 0.0f) ? (wc - wkm) * g.dzi : (wkp - wc) * g.dzi;
+                const float visc = nu * (wim_cc - 2.0f * wc + wip) * g.dxi * g.dxi +
+                                   nu * (wjmc - 2.0f * wc + wjpc) * g.dyi * g.dyi +
+                                   nu * (wkm - 2.0f * wc + wkp) * g.dzi * g.dzi;
+                const float adv = -u_here * dwdx - v_here * dwdy - wc * dwdz;
+                out_w[e] = wc + g.dt * (visc + adv + g.gz);
+            }
+        }
+        float2* US = reinterpret_cast<float2*>(us + id);
+        if (u0 && u1)
+            *US = make_float2(out_u[0], out_u[1]);
+        else if (u0)
+            us[id] = out_u[0];
+        else if (u1)
+            us[id + 1] = out_u[1];
+        if (j >= 2) {
+            if (a0 && a1)
+                *reinterpret_cast<float2*>(vs + id) = make_float2(out_v[0], out_v[1]);
+            else if (a0)
+                vs[id] = out_v[0];
+            else if (a1)
+                vs[id + 1] = out_v[1];
+        }
+        if (k >= 2) {
+            if (a0 && a1)
+                *reinterpret_cast<float2*>(ws + id) = make_float2(out_w[0], out_w[1]);
+            else if (a0)
+                ws[id] = out_w[0];
+            else if (a1)
+                ws[id + 1] = out_w[1];
+        }
+        u_km = u_c;
+        u_c = u_kp;
+        v_km = v_c;
+        v_c = v_kp;
+        w_km = w_c;
+        w_c = w_kp;
+        wim_c = wim_kp;
+        wjm_c = wjm_kp;
+        uip_km = uip1;
+        vjp_km = vjp_c;
     }
 }
 
@@ -238,6 +394,56 @@ __global__ void __launch_bounds__(256) k_rhs(Geom g,
     }
 }
 
+// The same with four cells per thread: quads of a row as in k_correct4 (one
+// aligned float4 word; quads of a plane numbered flat, one plane per
+// blockIdx.y), every operand an aligned float4 load -- F, u*, v* of the row
+// and of the row above, w* of the plane and of the plane above -- and the
+// u* east of the quad's last cell from the next lane, or from memory at the
+// end of a warp or of a row.  k_rhs's expression and operand order per cell.
+__device__ __forceinline__ float4 ld4g(const float* __restrict__ a) {
+    return __ldg(reinterpret_cast<const float4*>(a));
+}
+__device__ __forceinline__ float el4(const float4& v, int e) {
+    return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+
+__global__ void __launch_bounds__(256) k_rhs4(Geom g, const float* __restrict__ F, const float* __restrict__ us,
+                                              const float* __restrict__ vs, const float* __restrict__ ws,
+                                              float* __restrict__ rhs) {
+    const int nquad = g.nx / 4 + 1;  // quads covering columns 0 .. nx
+    const int total = nquad * g.ny;
+    const int qt = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool qa = qt < total;
+    const int q = qa ? qt : total - 1;  // lanes past the end shadow the last quad
+    const int jr = q / nquad, m = q - jr * nquad;
+    const int j = jr + 1, k = blockIdx.y + 1, i0 = 4 * m;
+    const int lane = threadIdx.x & 31;
+    const bool lde = lane == 31 || m == nquad - 1;  // u* east of the quad from memory
+    const int id = gidx(g, i0, j, k);  // a multiple of 4
+    const float4 f4 = ld4g(F + id), u4 = ld4g(us + id), v4 = ld4g(vs + id), vn4 = ld4g(vs + id + g.px);
+    const float4 w4 = ld4g(ws + id), wn4 = ld4g(ws + id + g.plane);
+    const float ue_m = lde ? __ldg(us + id + 4) : 0.0f;
+    float ue = __shfl_down_sync(0xffffffffu, u4.x, 1);
+    if (lde) ue = ue_m;
+    if (!qa) return;
+    const float rdt = __frcp_rn(g.dt);
+    float r[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const float rho = rho_of(g, el4(f4, e));
+        const float uip = e == 3 ? ue : el4(u4, e + 1);
+        r[e] = div_rn_pre(rho, g.dt, rdt) * ((uip - el4(u4, e)) * g.dxi + (el4(vn4, e) - el4(v4, e)) * g.dyi +
+                                             (el4(wn4, e) - el4(w4, e)) * g.dzi);
+    }
+    if (i0 >= 1 && i0 + 3 <= g.nx) {
+        *reinterpret_cast<float4*>(rhs + id) = make_float4(r[0], r[1], r[2], r[3]);
+        return;
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+        if (i0 + e >= 1 && i0 + e <= g.nx) rhs[id + e] = r[e];
+}
+
 // ---------------------------------------------------------------------------
 // Velocity correction fused with the free-slip boundary conditions.
 // update_{u,v,w}_kernel (voftrial1.cu:441-493) followed by apply_bc_velocity
@@ -277,9 +483,64 @@ __global__ void k_density_pairs(Geom g, float* out) {
     out[5] = g.dt / r2;
 }
 
+struct EdgeDims {
+    int nx, ny, nz, px, plane;
+    __device__ int at(int i, int j, int k) const { return k * plane + j * px + i; }
+};
+
+// The boundary copies of a cell on the domain's edge.
+__device__ __forceinline__ void store_edge_body(EdgeDims g, float* __restrict__ u, float* __restrict__ v,
+                                                float* __restrict__ w, int i, int j, int k, float un, float vn,
+                                                float wn) {
+    int mi[3], mj[3], mk[3];
+    const int nmi = mirrors(i, g.nx, mi), nmj = mirrors(j, g.ny, mj), nmk = mirrors(k, g.nz, mk);
+    for (int b = 0; b < nmk; ++b)
+        for (int a = 0; a < nmj; ++a) u[g.at(i, mj[a], mk[b])] = un;
+    for (int b = 0; b < nmk; ++b)
+        for (int a = 0; a < nmi; ++a) v[g.at(mi[a], j, mk[b])] = vn;
+    for (int b = 0; b < nmj; ++b)
+        for (int a = 0; a < nmi; ++a) w[g.at(mi[a], mj[b], k)] = wn;
+    // far walls and the never-updated first planes
+    if (i == g.nx)
+        for (int b = 0; b < nmk; ++b)
+            for (int a = 0; a < nmj; ++a) u[g.at(g.nx + 1, mj[a], mk[b])] = 0.0f;
+    if (j == g.ny)
+        for (int b = 0; b < nmk; ++b)
+            for (int a = 0; a < nmi; ++a) v[g.at(mi[a], g.ny + 1, mk[b])] = 0.0f;
+    if (k == g.nz)
+        for (int b = 0; b < nmj; ++b)
+            for (int a = 0; a < nmi; ++a) w[g.at(mi[a], mj[b], g.nz + 1)] = 0.0f;
+    if (i == 1 && (nmj > 1 || nmk > 1)) {
+        const float s0 = u[g.at(0, j, k)];
+        for (int b = 0; b < nmk; ++b)
+            for (int a = 0; a < nmj; ++a)
+                if (a || b) u[g.at(0, mj[a], mk[b])] = s0;
+    }
+    if (j == 1 && (nmi > 1 || nmk > 1)) {
+        const float s0 = v[g.at(i, 0, k)];
+        for (int b = 0; b < nmk; ++b)
+            for (int a = 0; a < nmi; ++a)
+                if (a || b) v[g.at(mi[a], 0, mk[b])] = s0;
+    }
+    if (k == 1 && (nmi > 1 || nmj > 1)) {
+        const float s0 = w[g.at(i, j, 0)];
+        for (int b = 0; b < nmj; ++b)
+            for (int a = 0; a < nmi; ++a)
+                if (a || b) w[g.at(mi[a], mj[b], 0)] = s0;
+    }
+}
+
+// The same out of line, for kernels that must not hold its registers.
+static __device__ __noinline__ void store_edge(EdgeDims g, float* __restrict__ u, float* __restrict__ v,
+                                               float* __restrict__ w, int i, int j, int k, float un, float vn,
+                                               float wn) {
+    store_edge_body(g, u, v, w, i, j, k, un, vn, wn);
+}
+
 // Writes the corrected face velocities of cell (i, j, k) and, on the domain
 // edges, the boundary copies of apply_bc_velocity (voftrial1.cu:959-1051,
-// 1107-1120) in closed form.
+// 1107-1120) in closed form.  OUTLINE: the edge copies through a call.
+template <bool OUTLINE>
 __device__ __forceinline__ void store_corrected(const Geom& g, float* __restrict__ u, float* __restrict__ v,
                                                 float* __restrict__ w, int i, int j, int k, int id, float un,
                                                 float vn, float wn) {
@@ -290,42 +551,11 @@ __device__ __forceinline__ void store_corrected(const Geom& g, float* __restrict
         w[id] = wn;
         return;
     }
-    int mi[3], mj[3], mk[3];
-    const int nmi = mirrors(i, g.nx, mi), nmj = mirrors(j, g.ny, mj), nmk = mirrors(k, g.nz, mk);
-    for (int b = 0; b < nmk; ++b)
-        for (int a = 0; a < nmj; ++a) u[gidx(g, i, mj[a], mk[b])] = un;
-    for (int b = 0; b < nmk; ++b)
-        for (int a = 0; a < nmi; ++a) v[gidx(g, mi[a], j, mk[b])] = vn;
-    for (int b = 0; b < nmj; ++b)
-        for (int a = 0; a < nmi; ++a) w[gidx(g, mi[a], mj[b], k)] = wn;
-    // far walls and the never-updated first planes
-    if (i == g.nx)
-        for (int b = 0; b < nmk; ++b)
-            for (int a = 0; a < nmj; ++a) u[gidx(g, g.nx + 1, mj[a], mk[b])] = 0.0f;
-    if (j == g.ny)
-        for (int b = 0; b < nmk; ++b)
-            for (int a = 0; a < nmi; ++a) v[gidx(g, mi[a], g.ny + 1, mk[b])] = 0.0f;
-    if (k == g.nz)
-        for (int b = 0; b < nmj; ++b)
-            for (int a = 0; a < nmi; ++a) w[gidx(g, mi[a], mj[b], g.nz + 1)] = 0.0f;
-    if (i == 1 && (nmj > 1 || nmk > 1)) {
-        const float s0 = u[gidx(g, 0, j, k)];
-        for (int b = 0; b < nmk; ++b)
-            for (int a = 0; a < nmj; ++a)
-                if (a || b) u[gidx(g, 0, mj[a], mk[b])] = s0;
-    }
-    if (j == 1 && (nmi > 1 || nmk > 1)) {
-        const float s0 = v[gidx(g, i, 0, k)];
-        for (int b = 0; b < nmk; ++b)
-            for (int a = 0; a < nmi; ++a)
-                if (a || b) v[gidx(g, mi[a], 0, mk[b])] = s0;
-    }
-    if (k == 1 && (nmi > 1 || nmj > 1)) {
-        const float s0 = w[gidx(g, i, j, 0)];
-        for (int b = 0; b < nmj; ++b)
-            for (int a = 0; a < nmi; ++a)
-                if (a || b) w[gidx(g, mi[a], mj[b], 0)] = s0;
-    }
+    const EdgeDims d{g.nx, g.ny, g.nz, g.px, g.plane};
+    if (OUTLINE)
+        store_edge(d, u, v, w, i, j, k, un, vn, wn);
+    else
+        store_edge_body(d, u, v, w, i, j, k, un, vn, wn);
 }
 
 __global__ void __launch_bounds__(256) k_correct(Geom g,
@@ -357,7 +587,79 @@ __global__ void __launch_bounds__(256) k_correct(Geom g,
         const float r = 0.5f * (rho_c + rho_of(g, __ldg(F + id - sz)));
         wn = __ldg(ws + id) - dt_over(g, r) * (p_c - __ldg(p + id - sz)) * g.dzi;
     }
-    store_corrected(g, u, v, w, i, j, k, id, un, vn, wn);
+    store_corrected<false>(g, u, v, w, i, j, k, id, un, vn, wn);
+}
+
+// The correction with four cells per thread: a quad i = 4m .. 4m+3 of a row
+// (one aligned float4 word of the padded layout; px is a multiple of 32), the
+// quads of all rows of a plane numbered flat so that 32 consecutive quads
+// make a warp across row ends, one plane per blockIdx.y.  Every operand is an
+// aligned float4 load (the cell, its y-1 and its z-1 neighbours of F and p;
+// u*, v*, w*); the x-1 neighbour of the quad's first cell comes from the
+// lane before (its last cell's density and pressure), or from memory at the
+// start of a warp.  Each face keeps k_correct's expression and operand order
+// (same bits).  Quads without an edge cell store float4 words; the others go
+// through store_corrected cell by cell.
+__global__ void __launch_bounds__(256, 4) k_correct4(Geom g, const float* __restrict__ F,
+                                                  const float* __restrict__ us, const float* __restrict__ vs,
+                                                  const float* __restrict__ ws, const float* __restrict__ p,
+                                                  float* __restrict__ u, float* __restrict__ v,
+                                                  float* __restrict__ w) {
+    const int nquad = g.nx / 4 + 1;  // quads covering columns 0 .. nx
+    const int total = nquad * g.ny;
+    const int qt = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool qa = qt < total;
+    const int q = qa ? qt : total - 1;  // lanes past the end shadow the last quad
+    const int jr = q / nquad, m = q - jr * nquad;
+    const int j = jr + 1, k = blockIdx.y + 1, i0 = 4 * m;
+    const int lane = threadIdx.x & 31;
+    const bool ldw = lane == 0 && m > 0;  // the x-1 neighbour from memory
+    const int sy = g.px, sz = g.plane;
+    const int id = gidx(g, i0, j, k);  // a multiple of 4
+    const float4 fc = ld4g(F + id), fs = ld4g(F + id - sy), fb = ld4g(F + id - sz);
+    const float4 pc = ld4g(p + id), ps = ld4g(p + id - sy), pb = ld4g(p + id - sz);
+    const float4 u4 = ld4g(us + id), v4 = ld4g(vs + id), w4 = ld4g(ws + id);
+    const float fl = ldw ? __ldg(F + id - 1) : 0.0f, pl = ldw ? __ldg(p + id - 1) : 0.0f;
+    float rc[4] = {rho_of(g, fc.x), rho_of(g, fc.y), rho_of(g, fc.z), rho_of(g, fc.w)};
+    float rl = __shfl_up_sync(0xffffffffu, rc[3], 1), pw = __shfl_up_sync(0xffffffffu, pc.w, 1);
+    if (ldw) {
+        rl = rho_of(g, fl);
+        pw = pl;
+    }
+    float un[4], vn[4], wn[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int i = i0 + e;
+        const float rho_c = rc[e], p_c = el4(pc, e);
+        un[e] = 0.0f;  // wall faces (i, j or k == 1) are 0
+        vn[e] = 0.0f;
+        wn[e] = 0.0f;
+        if (i >= 2) {
+            const float r = 0.5f * (rho_c + (e == 0 ? rl : rc[e - 1]));
+            un[e] = el4(u4, e) - dt_over(g, r) * (p_c - (e == 0 ? pw : el4(pc, e - 1))) * g.dxi;
+        }
+        if (j >= 2) {
+            const float r = 0.5f * (rho_c + rho_of(g, el4(fs, e)));
+            vn[e] = el4(v4, e) - dt_over(g, r) * (p_c - el4(ps, e)) * g.dyi;
+        }
+        if (k >= 2) {
+            const float r = 0.5f * (rho_c + rho_of(g, el4(fb, e)));
+            wn[e] = el4(w4, e) - dt_over(g, r) * (p_c - el4(pb, e)) * g.dzi;
+        }
+    }
+    if (!qa) return;
+    const bool bulk = i0 >= 2 && i0 + 3 <= g.nx - 1 && j != 1 && j != g.ny && k != 1 && k != g.nz;
+    if (bulk) {
+        *reinterpret_cast<float4*>(u + id) = make_float4(un[0], un[1], un[2], un[3]);
+        *reinterpret_cast<float4*>(v + id) = make_float4(vn[0], vn[1], vn[2], vn[3]);
+        *reinterpret_cast<float4*>(w + id) = make_float4(wn[0], wn[1], wn[2], wn[3]);
+        return;
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int i = i0 + e;
+        if (i >= 1 && i <= g.nx) store_corrected<true>(g, u, v, w, i, j, k, id + e, un[e], vn[e], wn[e]);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -438,7 +740,7 @@ static int jacobi_kind(const Geom& g) {
         if (v && !strcmp(v, "tb1")) forced = JACOBI_TB1;
         if (v && !strcmp(v, "bulk")) forced = JACOBI_BULK;
     }
-    const int k = forced >= 0 ? forced : JACOBI_PAIRS;
+    const int k = forced >= 0 ? forced : JACOBI_PEEL;
     if (k == JACOBI_BULK && !jacobi_bulk_supported(g)) return JACOBI_PAIRS;
     return (k == JACOBI_PAIRS2 && !jacobi_pairs2_supported(g)) ? JACOBI_PAIRS : k;
 }
@@ -503,6 +805,32 @@ static inline cudaError_t mark(cudaEvent_t* ev, int q, cudaStream_t s) {
     return ev ? cudaEventRecord(ev[q], s) : cudaSuccess;
 }
 
+// Four-cell kernels (k_rhs4, k_correct4) when their launch has at least
+// about 7 blocks per SM of a B200 (measured: faster from 128^3 up, slower at
+// 32^3 and 64^3, where the one-cell kernels' four times as many threads
+// fill the GPU better).  VOF_RHS / VOF_CORRECT = 1 or 4 force either.
+static bool quads_fill(const Geom& g) {
+    const long long blocks = (long long)(((g.nx / 4 + 1) * g.ny + 255) / 256) * g.nz;
+    return blocks >= 1024;
+}
+// SMs of the current device (queried once).
+static int sm_count() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) !=
+                                                      cudaSuccess)
+            n = 148;
+    }
+    return n;
+}
+
+// 1: the one-cell kernel, 4: the four-cell kernel, else by size.
+static int env_kernel(const char* name) {
+    const char* v = getenv(name);
+    return v ? atoi(v) : 0;
+}
+
 cudaError_t plain_front(const Geom& g, const PlainBuffers& b, cudaStream_t s, cudaEvent_t* ev) {
     const dim3 blk(TX, TY, 1);
     dim3 grid;
@@ -510,7 +838,15 @@ cudaError_t plain_front(const Geom& g, const PlainBuffers& b, cudaStream_t s, cu
     column_launch(g, grid, kchunk);
     cudaError_t e;
     if ((e = mark(ev, 0, s)) != cudaSuccess) return e;
-    k_predict<<<grid, blk, 0, s>>>(g, b.F, b.u, b.v, b.w, b.us, b.vs, b.ws, kchunk);
+    static int pforced = -1;  // VOF_PREDICT=1: k_predict (one cell per thread); else k_predict2
+    if (pforced < 0) pforced = env_kernel("VOF_PREDICT");
+    if (pforced == 1) {
+        k_predict<<<grid, blk, 0, s>>>(g, b.F, b.u, b.v, b.w, b.us, b.vs, b.ws, kchunk);
+    } else {
+        const int bx = ((g.nx / 2 + 1) * g.ny + 255) / 256;
+        const int kc = wave_kchunk(g.nz, bx, 4 * sm_count());
+        k_predict2<<<dim3(bx, (g.nz + kc - 1) / kc), 256, 0, s>>>(g, b.F, b.u, b.v, b.w, b.us, b.vs, b.ws, kc);
+    }
     if (g.csf && b.csf[0]) {  // surface tension (extension): normals, curvature, face accelerations
         const dim3 cb(32, 4, 2);
         const dim3 cg((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + 1) / 2);
@@ -519,15 +855,31 @@ cudaError_t plain_front(const Geom& g, const PlainBuffers& b, cudaStream_t s, cu
         k_csf_force<<<cg, cb, 0, s>>>(g, b.F, b.csf[3], b.us, b.vs, b.ws);
     }
     if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(ev, 1, s)) != cudaSuccess) return e;
-    k_rhs<<<grid, blk, 0, s>>>(g, b.F, b.us, b.vs, b.ws, b.rhs, kchunk);
+    static int forced = -1;  // VOF_RHS=1: k_rhs (one cell per thread, z march), 4: k_rhs4
+    if (forced < 0) forced = env_kernel("VOF_RHS");
+    if (forced == 1 || (forced != 4 && !quads_fill(g))) {
+        k_rhs<<<grid, blk, 0, s>>>(g, b.F, b.us, b.vs, b.ws, b.rhs, kchunk);
+    } else {
+        const int total = (g.nx / 4 + 1) * g.ny;
+        k_rhs4<<<dim3((total + 255) / 256, g.nz), 256, 0, s>>>(g, b.F, b.us, b.vs, b.ws, b.rhs);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess || (e = mark(ev, 2, s)) != cudaSuccess) return e;
     return cudaSuccess;
 }
 
+// The correction: k_correct4 (four cells per thread) on large grids, else
+// k_correct (one cell per thread).  Both give the same bits.
 cudaError_t plain_correct(const Geom& g, const PlainBuffers& b, const float* p, cudaStream_t s) {
-    const dim3 cb(32, 4, 2);
-    const dim3 cg((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + 1) / 2);
-    k_correct<<<cg, cb, 0, s>>>(g, b.F, b.us, b.vs, b.ws, p, b.u, b.v, b.w);
+    static int forced = -1;
+    if (forced < 0) forced = env_kernel("VOF_CORRECT");
+    if (forced == 1 || (forced != 4 && !quads_fill(g))) {
+        const dim3 cb(32, 4, 2);
+        const dim3 cg((g.nx + 31) / 32, (g.ny + 3) / 4, (g.nz + 1) / 2);
+        k_correct<<<cg, cb, 0, s>>>(g, b.F, b.us, b.vs, b.ws, p, b.u, b.v, b.w);
+    } else {
+        const int total = (g.nx / 4 + 1) * g.ny;
+        k_correct4<<<dim3((total + 255) / 256, g.nz), 256, 0, s>>>(g, b.F, b.us, b.vs, b.ws, p, b.u, b.v, b.w);
+    }
     return cudaGetLastError();
 }
 

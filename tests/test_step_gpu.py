@@ -77,7 +77,8 @@ def test_random_state_bitwise_vs_oracle(cuda, V, orc, nx, ny, nz, seed, dt, vs):
                                  {"VOF_JACOBI": "ring", "VOF_JACOBI_KCHUNK": "3"},
                                  {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "1"},
                                  {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "5"},
-                                 {"VOF_JACOBI": "tb1"},
+                                 {"VOF_JACOBI": "tb1"}, {"VOF_JACOBI": "pairs"}, {"VOF_CORRECT": "1"}, {"VOF_RHS": "1"},
+                                 {"VOF_PREDICT": "1"},
                                  {"VOF_JACOBI": "bulk"}, {"VOF_JACOBI": "bulk", "VOF_JACOBI_KCHUNK": "1"},
                                  {"VOF_JACOBI": "bulk", "VOF_JACOBI_KCHUNK": "7"},
                                  {"VOF_JACOBI": "bulk", "VOF_JACOBI_KCHUNK": "21"},
@@ -92,12 +93,14 @@ def test_random_state_bitwise_vs_oracle(cuda, V, orc, nx, ny, nz, seed, dt, vs):
                                  {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "4", "VOF_JACOBI_KCHUNK": "7"},
                                  {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "4", "VOF_JACOBI_KCHUNK": "21"}])
 def test_jacobi_kernel_choices_give_the_same_bits(cuda, V, orc, tmp_path, env):
-    """The Jacobi kernels a process may select (the default single-sweep
-    paired kernel runs in every other test; here the two-sweep paired kernel,
-    the paired sweep with the cp.async ring and its z chunks, the TMA-blocked
-    two-sweep kernel, the one-cell streaming sweep, other z chunks of the
-    default; read once per process, so each runs in a child process) give the
-    oracle's bits."""
+    """The kernels a process may select (the defaults -- the peeled paired
+    Jacobi sweep and the four-cell correction -- run in every other test;
+    here the other Jacobi kernels: the paired sweep, its peeled form at other
+    unrolls and register caps, the two-sweep paired kernel, the cp.async
+    ring, the bulk-copy ring, the TMA-blocked kernels, the one-cell streaming
+    sweep, and z chunks of several of them; and the one-cell correction; read
+    once per process, so each runs in a child process) give the oracle's
+    bits."""
     import os
     import subprocess
     import sys
@@ -122,6 +125,42 @@ def test_jacobi_kernel_choices_give_the_same_bits(cuda, V, orc, tmp_path, env):
     got = dict(np.load(tmp_path / "out.npz"))
     want = orc.run_f32(prm, state, 1, 3)
     assert_bitwise(got, want, STATE, str(env))
+
+
+@pytest.mark.parametrize("shape", [(1, 3, 2), (6, 5, 4), (17, 9, 13), (40, 33, 21), (64, 7, 5)])
+def test_four_cell_kernels_on_odd_grids(cuda, V, orc, tmp_path, shape):
+    """The four-cell right-hand side and correction (k_rhs4, k_correct4: the
+    defaults from about 128^3 up) forced on small and odd grids -- rows that
+    end inside a quad, warps that span rows, every edge and corner cell --
+    give the oracle's bits (child process: the switch is read once)."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    prm = V.default_params(*shape, dt=2e-4, gy=0.0, gz=-9.81)
+    state = ic.random_state(prm, seed=sum(shape), vel_scale=3.0)
+    np.savez(tmp_path / "in.npz", **state)
+    root = Path(__file__).resolve().parent.parent
+    code = (
+        "import sys, numpy as np\n"
+        f"sys.path.insert(0, {str(root / 'cuda-lbm-ibm-fvm_b200')!r})\n"
+        "import vof_b200 as V\n"
+        f"prm = V.default_params(*{shape!r}, dt=2e-4, gy=0.0, gz=-9.81)\n"
+        f"st = dict(np.load({str(tmp_path / 'in.npz')!r}))\n"
+        "with V.Solver(prm) as s:\n"
+        "    s.upload_state(**st)\n"
+        "    for t in range(3):\n"
+        "        s.step(1 + t)\n"
+        "    out = s.state()\n"
+        "    for k in ('ustar', 'vstar', 'wstar', 'rhs'):\n"
+        "        out[k] = s.download(k)\n"
+        f"    np.savez({str(tmp_path / 'out.npz')!r}, **out)\n")
+    env = {**os.environ, "VOF_CORRECT": "4", "VOF_RHS": "4"}
+    subprocess.run([sys.executable, "-c", code], env=env, check=True, timeout=600)
+    got = dict(np.load(tmp_path / "out.npz"))
+    want = orc.run_f32(prm, state, 1, 3, extras=True)
+    assert_bitwise(got, want, STATE + ("ustar", "vstar", "wstar", "rhs"), f"four-cell {shape}")
 
 
 @pytest.mark.parametrize("shape,seed,vfrac", [((40, 36, 34), 41, 0.45), ((130, 17, 19), 42, 0.3),
