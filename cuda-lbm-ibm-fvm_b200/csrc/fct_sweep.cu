@@ -105,11 +105,23 @@ __device__ void ratios_at(const Sweep<AXIS>& S, const Geom& g, const LineView& L
 // Indices whose clamped value is x on an axis of n interior cells: x itself,
 // plus the ghost 0 when x == 1 and the ghost n+1 when x == n.
 __device__ __forceinline__ int mirrors(int x, int n, int* out) {
-    int m = 0;
-    out[m++] = x;
-    if (x == 1) out[m++] = 0;
-    if (x == n) out[m++] = n + 1;
-    return m;
+    out[0] = x;  // fixed positions (no runtime index)
+    out[1] = (x == 1) ? 0 : n + 1;
+    out[2] = n + 1;
+    return 1 + (x == 1) + (x == n);
+}
+
+// apply_bc_F (voftrial1.cu:1122-1135) for one cell of the final sweep: the
+// cell (i, j, k) and every ghost whose clamped interior index is (i, j, k)
+// take f.  Out of line: only cells on the domain's edge come here, and inlined
+// it would hold registers in every thread of the marching kernels.
+__device__ __noinline__ void store_mirrored(float* __restrict__ F, int px, int plane, int nx, int ny, int nz, int i,
+                                            int j, int k, float f) {
+    int iv[3], jv[3], kv[3];
+    const int ni = mirrors(i, nx, iv), nj = mirrors(j, ny, jv), nk = mirrors(k, nz, kv);
+    for (int c = 0; c < nk; ++c)
+        for (int b = 0; b < nj; ++b)
+            for (int a = 0; a < ni; ++a) F[kv[c] * plane + jv[b] * px + iv[a]] = f;
 }
 
 }  // namespace
@@ -437,14 +449,10 @@ __global__ void __launch_bounds__(MARCH_THREADS, 4) k_fct_march(Geom g, const fl
             fnew = clamp01f(fnew);  // post_process_f_kernel, voftrial1.cu:502-507
             if (inner && c > 1 && c < nm) {
                 F[gi(a, b, c)] = fnew;
-            } else {
-                // apply_bc_F (voftrial1.cu:1122-1135): every ghost takes the
-                // value at its clamped interior index
-                int qv[3], av[3], bv[3];
-                const int nq = mirrors(c, nm, qv), nav = mirrors(a, g.nx, av), nbv = mirrors(b, nb, bv);
-                for (int ib = 0; ib < nbv; ++ib)
-                    for (int ia = 0; ia < nav; ++ia)
-                        for (int iq = 0; iq < nq; ++iq) F[gi(av[ia], bv[ib], qv[iq])] = fnew;
+            } else if (AXIS == 1) {  // (a, b, c) = (i, k, j)
+                store_mirrored(F, g.px, g.plane, g.nx, g.ny, g.nz, a, c, b, fnew);
+            } else {  // (a, b, c) = (i, j, k)
+                store_mirrored(F, g.px, g.plane, g.nx, g.ny, g.nz, a, b, c, fnew);
             }
         }
         lo2 = lo3;
@@ -598,23 +606,22 @@ __global__ void __launch_bounds__(256) k_fct_x(Geom g, const float* __restrict__
             for (int e = 0; e < XC; ++e)
                 if (wr[e]) F[rb + x0 + e] = out[e];
         }
+    } else if (j > 1 && j < g.ny && k > 1 && k < g.nz) {
+        // a row away from the y and z walls: only the x ghosts of the row
+#pragma unroll
+        for (int e = 0; e < XC; ++e) {
+            if (!wr[e]) continue;
+            const int x = x0 + e;
+            F[rb + x] = out[e];
+            if (x == 1) F[rb] = out[e];
+            if (x == n) F[rb + n + 1] = out[e];
+        }
     } else {
         // apply_bc_F (voftrial1.cu:1122-1135): every ghost takes the value at
         // its clamped interior index
-        int jv[3], kv[3];
-        const int nj = mirrors(j, g.ny, jv), nk = mirrors(k, g.nz, kv);
-        for (int b = 0; b < nk; ++b)
-            for (int q = 0; q < nj; ++q) {
-                const int r2 = gidx(g, 0, jv[q], kv[b]);
 #pragma unroll
-                for (int e = 0; e < XC; ++e) {
-                    if (!wr[e]) continue;
-                    const int x = x0 + e;
-                    F[r2 + x] = out[e];
-                    if (x == 1) F[r2] = out[e];
-                    if (x == n) F[r2 + n + 1] = out[e];
-                }
-            }
+        for (int e = 0; e < XC; ++e)
+            if (wr[e]) store_mirrored(F, g.px, g.plane, g.nx, g.ny, g.nz, x0 + e, j, k, out[e]);
     }
 }
 
