@@ -508,8 +508,6 @@ __global__ void __launch_bounds__(JP_THREADS, MINB) k_jacobi_peel(Geom g, const 
     s.pm = L.P[L.w + (k0 - 1) * L.wp];
     s.pc = L.P[L.w + k0 * L.wp];
     s.pp = L.P[L.w + (k0 + 1) * L.wp];
-    s.pS = L.P[L.w + k0 * L.wp - L.wr];
-    s.pN = L.P[L.w + k0 * L.wp + L.wr];
     s.rc = L.R[L.w + k0 * L.wp];
     s.xw = L.ldw ? pin[L.cw + k0 * L.plane] : 0.0f;
     s.xe = L.lde ? pin[L.ce + k0 * L.plane] : 0.0f;
@@ -538,6 +536,160 @@ static JPKernel jp_peel_kernel() {
                      : (mb == 4 ? k_jacobi_peel<2, 4> : k_jacobi_peel<2, 1>);
     }
     return k;
+}
+
+// ---- one sweep, four cells per thread, streaming along z ---------------------
+// The peeled march of k_jacobi_peel with a quad of cells per thread (i = 4m ..
+// 4m + 3: one aligned 16-byte word of the padded layout; the quads of all rows
+// numbered flat, so 32 consecutive quads make a warp across row ends), so that
+// every load in flight carries 16 bytes instead of 8: the sweep is bound by
+// memory latency at the occupancy its registers allow.  A cell's x neighbours
+// are the quad's own cells, the left lane's last cell and the right lane's
+// first (or memory at the ends of a warp and of a row).  The per-cell
+// coefficients and inner-plane diagonals are the thread's constants; each
+// cell's update is k_jacobi_pairs' expression in its operand order.
+struct JQLine {
+    const float4* P;
+    const float4* R;
+    float4* O;
+    const float* pin;
+    float* pout;
+    int w, wp, wr, cw, ce, plane;
+    int es;          // the quad's cell on an x wall (i == 1 or nx), or -1 (nx >= 4: at most one)
+    bool es_e, es_w;  // ... its east (i == nx) and west (i == 1) coefficients are 0
+    float cx, an, as, cz;
+    float dmi, rmi;  // inner-plane diagonal and reciprocal of a cell away from the x walls
+    float dms, rms;  // ... of the wall cell
+    int nact0, nact1;  // the active cells are nact0 .. nact1 - 1
+    bool ldw, lde;
+    __device__ float ae(int e) const { return (e == es && es_e) ? 0.0f : cx; }
+    __device__ float aw(int e) const { return (e == es && es_w) ? 0.0f : cx; }
+    __device__ bool act(int e) const { return e >= nact0 && e < nact1; }
+};
+
+struct JQRegs {
+    float4 pm, pc, pp, rc;
+    float xw, xe;
+};
+
+__device__ __forceinline__ float q4(const float4& v, int e) {
+    return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+
+template <bool MORE, bool EDGE>
+__device__ __forceinline__ void jq_plane(const JQLine& L, const Geom& g, int k, JQRegs& s) {
+    float4 pq, rn;
+    float xwn = 0.0f, xen = 0.0f;
+    // the y neighbours of this plane (L1 / L2: the rows of other warps)
+    const float4 pS = L.P[L.w + k * L.wp - L.wr], pN = L.P[L.w + k * L.wp + L.wr];
+    if constexpr (MORE) {
+        const int o1 = L.w + (k + 1) * L.wp;
+        pq = L.P[o1 + L.wp];
+        rn = L.R[o1];
+        if (L.ldw) xwn = L.pin[L.cw + (k + 1) * L.plane];
+        if (L.lde) xen = L.pin[L.ce + (k + 1) * L.plane];
+    }
+    float pw = __shfl_up_sync(0xffffffffu, s.pc.w, 1), pe = __shfl_down_sync(0xffffffffu, s.pc.x, 1);
+    if (L.ldw) pw = s.xw;
+    if (L.lde) pe = s.xe;
+    float af = L.cz, ab = L.cz;
+    bool wall = false;
+    if constexpr (EDGE) {
+        const bool kb = k == 1, kt = k == g.nz;
+        af = kt ? 0.0f : L.cz;
+        ab = kb ? 0.0f : L.cz;
+        wall = kb || kt;
+    }
+    float v[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const float ae = L.ae(e), aw = L.aw(e);
+        float d = (e == L.es) ? L.dms : L.dmi, rd = (e == L.es) ? L.rms : L.rmi;
+        if (EDGE && wall) {
+            d = -(ae + aw + L.an + L.as + af + ab);
+            rd = __frcp_rn(d);
+        }
+        const float pE = e == 3 ? pe : q4(s.pc, e + 1), pW = e == 0 ? pw : q4(s.pc, e - 1);
+        v[e] = div_rn_pre(q4(s.rc, e) - ae * pE - aw * pW - L.an * q4(pN, e) - L.as * q4(pS, e) -
+                              af * q4(s.pp, e) - ab * q4(s.pm, e),
+                          d, rd);
+    }
+    const int o = L.w + k * L.wp;
+    if (L.nact0 == 0 && L.nact1 == 4) {
+        L.O[o] = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if (L.act(e)) L.pout[4 * o + e] = v[e];
+    }
+    if constexpr (MORE) {
+        s.pm = s.pc;
+        s.pc = s.pp;
+        s.pp = pq;
+        s.rc = rn;
+        s.xw = xwn;
+        s.xe = xen;
+    }
+}
+
+__global__ void __launch_bounds__(256, 3) k_jacobi_quad(Geom g, const float* __restrict__ pin,
+                                                        const float* __restrict__ rhs, float* __restrict__ pout,
+                                                        int kchunk) {
+    const int nquad = g.nx / 4 + 1;  // quads covering columns 0 .. nx
+    const int nq = nquad * g.ny;
+    const int qt = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool qa = qt < nq;
+    const int q = qa ? qt : nq - 1;  // lanes past the end shadow the last quad
+    const int jr = q / nquad, m = q - jr * nquad;
+    const int j = jr + 1, i0 = 4 * m;
+    const int lane = threadIdx.x & 31;
+    const int k0 = 1 + blockIdx.y * kchunk, k1 = min(g.nz, k0 + kchunk - 1);
+    JQLine L;
+    L.P = reinterpret_cast<const float4*>(pin);
+    L.R = reinterpret_cast<const float4*>(rhs);
+    L.O = reinterpret_cast<float4*>(pout);
+    L.pin = pin;
+    L.pout = pout;
+    L.ldw = lane == 0 && m > 0;            // x- neighbour of the first cell from memory
+    L.lde = lane == 31 || m == nquad - 1;  // x+ neighbour of the last cell from memory
+    L.plane = g.plane;
+    const int c = gidx(g, i0, j, 0);  // a multiple of 4
+    L.cw = c - 1;
+    L.ce = c + 4;  // i0 + 4 <= nx + 3 < px: within the row
+    const float cy = g.dyi * g.dyi;
+    L.cx = g.dxi * g.dxi;
+    L.cz = g.dzi * g.dzi;
+    L.an = (j != g.ny) ? cy : 0.0f;
+    L.as = (j != 1) ? cy : 0.0f;
+    L.es = (i0 <= 1 && 1 <= i0 + 3) ? 1 - i0 : ((i0 <= g.nx && g.nx <= i0 + 3) ? g.nx - i0 : -1);
+    L.es_w = L.es >= 0 && i0 + L.es == 1;
+    L.es_e = L.es >= 0 && i0 + L.es == g.nx;
+    L.dmi = -(L.cx + L.cx + L.an + L.as + L.cz + L.cz);
+    L.rmi = __frcp_rn(L.dmi);
+    {
+        const float ae = L.es_e ? 0.0f : L.cx, aw = L.es_w ? 0.0f : L.cx;
+        L.dms = -(ae + aw + L.an + L.as + L.cz + L.cz);
+        L.rms = __frcp_rn(L.dms);
+    }
+    L.nact0 = qa ? max(0, 1 - i0) : 4;
+    L.nact1 = qa ? min(4, g.nx + 1 - i0) : 4;
+    L.w = c >> 2;
+    L.wp = g.plane >> 2;
+    L.wr = g.px >> 2;
+    JQRegs s;
+    s.pm = L.P[L.w + (k0 - 1) * L.wp];
+    s.pc = L.P[L.w + k0 * L.wp];
+    s.pp = L.P[L.w + (k0 + 1) * L.wp];
+    s.rc = L.R[L.w + k0 * L.wp];
+    s.xw = L.ldw ? pin[L.cw + k0 * L.plane] : 0.0f;
+    s.xe = L.lde ? pin[L.ce + k0 * L.plane] : 0.0f;
+    int k = k0;
+    if (k == 1 && k < k1) {
+        jq_plane<true, true>(L, g, k, s);
+        ++k;
+    }
+    for (; k < k1; ++k) jq_plane<true, false>(L, g, k, s);
+    jq_plane<false, true>(L, g, k1, s);
 }
 
 // ---- the paired sweep fed by bulk copies of whole rows ------------------------
@@ -842,6 +994,16 @@ cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rh
 }
 
 static int jpe_wave = 3 * 148;  // resident blocks of the chosen k_jacobi_peel, set by jacobi_tb_configure
+static int jq_wave = 3 * 148;   // the same for k_jacobi_quad
+
+cudaError_t jacobi_quad_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s) {
+    if (g.nx < 4) return jacobi_pairs_launch(g, pin, rhs, pout, s);  // two x-wall cells in one quad
+    const int nq = (g.nx / 4 + 1) * g.ny;
+    const int bx = (nq + 255) / 256;
+    const int kchunk = jacobi_pairs_kchunk(g, bx, jq_wave);
+    k_jacobi_quad<<<dim3(bx, (g.nz + kchunk - 1) / kchunk), 256, 0, s>>>(g, pin, rhs, pout, kchunk);
+    return cudaGetLastError();
+}
 
 cudaError_t jacobi_peel_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s) {
     const int nq = (g.nx / 2 + 1) * g.ny;
@@ -1192,6 +1354,8 @@ cudaError_t jacobi_tb_configure() {
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, jp_peel_kernel(), JP_THREADS, 0)) != cudaSuccess)
         return e;
     jpe_wave = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_quad, 256, 0)) != cudaSuccess) return e;
+    jq_wave = (sms > 0 ? sms : 148) * (occ > 0 ? occ : 1);
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_jacobi_pairs2, J2_THREADS,
                                                            sizeof(float2) * (5u * J2_THREADS + 64u))) != cudaSuccess)
         return e;

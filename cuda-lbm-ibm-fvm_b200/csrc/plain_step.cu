@@ -725,7 +725,7 @@ static_assert(JACOBI_T >= 1 && JACOBI_T <= JACOBI_TB_MAX, "VOF_JACOBI_T out of r
 // blocked sweeps per launch through TMA (k_jacobi_tb).
 // VOF_JACOBI=pairs|ring|col|pairs2|tb forces one.  All give the same bits.
 // (Measured on a B200 at 200^3, 10 sweeps: pairs 0.275 ms, pairs2 0.290 ms.)
-enum { JACOBI_PAIRS = 0, JACOBI_COL = 1, JACOBI_TB = 2, JACOBI_PAIRS2 = 3, JACOBI_RING = 4, JACOBI_PEEL = 5, JACOBI_TB1 = 6, JACOBI_BULK = 7 };
+enum { JACOBI_PAIRS = 0, JACOBI_COL = 1, JACOBI_TB = 2, JACOBI_PAIRS2 = 3, JACOBI_RING = 4, JACOBI_PEEL = 5, JACOBI_TB1 = 6, JACOBI_BULK = 7, JACOBI_QUAD = 8 };
 static int jacobi_kind(const Geom& g) {
     static int forced = -2;
     if (forced == -2) {
@@ -739,6 +739,7 @@ static int jacobi_kind(const Geom& g) {
         if (v && !strcmp(v, "peel")) forced = JACOBI_PEEL;
         if (v && !strcmp(v, "tb1")) forced = JACOBI_TB1;
         if (v && !strcmp(v, "bulk")) forced = JACOBI_BULK;
+        if (v && !strcmp(v, "quad")) forced = JACOBI_QUAD;
     }
     const int k = forced >= 0 ? forced : JACOBI_PEEL;
     if (k == JACOBI_BULK && !jacobi_bulk_supported(g)) return JACOBI_PAIRS;
@@ -746,7 +747,8 @@ static int jacobi_kind(const Geom& g) {
 }
 static bool jacobi_streaming(const Geom& g) {
     const int k = jacobi_kind(g);
-    return k == JACOBI_PAIRS || k == JACOBI_COL || k == JACOBI_RING || k == JACOBI_PEEL || k == JACOBI_BULK;
+    return k == JACOBI_PAIRS || k == JACOBI_COL || k == JACOBI_RING || k == JACOBI_PEEL || k == JACOBI_BULK ||
+           k == JACOBI_QUAD;
 }
 static int jacobi_per_launch(const Geom& g) {
     const int k = jacobi_kind(g);
@@ -942,6 +944,7 @@ cudaError_t plain_pressure(const Geom& g, const PlainBuffers& b, int jacobi_iter
                 : kind == JACOBI_RING ? jacobi_ring_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s)
                 : kind == JACOBI_PEEL ? jacobi_peel_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s)
                 : kind == JACOBI_BULK ? jacobi_bulk_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], b.status, s)
+                : kind == JACOBI_QUAD ? jacobi_quad_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s)
                                       : jacobi_pairs_launch(g, pbuf[cur], b.rhs, pbuf[cur ^ 1], s);
             if (e != cudaSuccess) return e;
             cur ^= 1;

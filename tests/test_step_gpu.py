@@ -78,7 +78,9 @@ def test_random_state_bitwise_vs_oracle(cuda, V, orc, nx, ny, nz, seed, dt, vs):
                                  {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "1"},
                                  {"VOF_JACOBI": "pairs", "VOF_JACOBI_KCHUNK": "5"},
                                  {"VOF_JACOBI": "tb1"}, {"VOF_JACOBI": "pairs"}, {"VOF_CORRECT": "1"}, {"VOF_RHS": "1"},
-                                 {"VOF_PREDICT": "1"},
+                                 {"VOF_PREDICT": "1"}, {"VOF_JACOBI": "quad"},
+                                 {"VOF_JACOBI": "quad", "VOF_JACOBI_KCHUNK": "1"},
+                                 {"VOF_JACOBI": "quad", "VOF_JACOBI_KCHUNK": "21"},
                                  {"VOF_JACOBI": "bulk"}, {"VOF_JACOBI": "bulk", "VOF_JACOBI_KCHUNK": "1"},
                                  {"VOF_JACOBI": "bulk", "VOF_JACOBI_KCHUNK": "7"},
                                  {"VOF_JACOBI": "bulk", "VOF_JACOBI_KCHUNK": "21"},
@@ -130,9 +132,10 @@ def test_jacobi_kernel_choices_give_the_same_bits(cuda, V, orc, tmp_path, env):
 @pytest.mark.parametrize("shape", [(1, 3, 2), (6, 5, 4), (17, 9, 13), (40, 33, 21), (64, 7, 5)])
 def test_four_cell_kernels_on_odd_grids(cuda, V, orc, tmp_path, shape):
     """The four-cell right-hand side and correction (k_rhs4, k_correct4: the
-    defaults from about 128^3 up) forced on small and odd grids -- rows that
-    end inside a quad, warps that span rows, every edge and corner cell --
-    give the oracle's bits (child process: the switch is read once)."""
+    defaults from about 128^3 up) and the four-cell Jacobi sweep forced on
+    small and odd grids -- rows that end inside a quad, warps that span rows,
+    every edge and corner cell -- give the oracle's bits (child process: the
+    switches are read once)."""
     import os
     import subprocess
     import sys
@@ -156,7 +159,7 @@ def test_four_cell_kernels_on_odd_grids(cuda, V, orc, tmp_path, shape):
         "    for k in ('ustar', 'vstar', 'wstar', 'rhs'):\n"
         "        out[k] = s.download(k)\n"
         f"    np.savez({str(tmp_path / 'out.npz')!r}, **out)\n")
-    env = {**os.environ, "VOF_CORRECT": "4", "VOF_RHS": "4"}
+    env = {**os.environ, "VOF_CORRECT": "4", "VOF_RHS": "4", "VOF_JACOBI": "quad"}
     subprocess.run([sys.executable, "-c", code], env=env, check=True, timeout=600)
     got = dict(np.load(tmp_path / "out.npz"))
     want = orc.run_f32(prm, state, 1, 3, extras=True)
