@@ -508,6 +508,8 @@ __global__ void __launch_bounds__(JP_THREADS, MINB) k_jacobi_peel(Geom g, const 
     s.pm = L.P[L.w + (k0 - 1) * L.wp];
     s.pc = L.P[L.w + k0 * L.wp];
     s.pp = L.P[L.w + (k0 + 1) * L.wp];
+    s.pS = L.P[L.w + k0 * L.wp - L.wr];
+    s.pN = L.P[L.w + k0 * L.wp + L.wr];
     s.rc = L.R[L.w + k0 * L.wp];
     s.xw = L.ldw ? pin[L.cw + k0 * L.plane] : 0.0f;
     s.xe = L.lde ? pin[L.ce + k0 * L.plane] : 0.0f;
