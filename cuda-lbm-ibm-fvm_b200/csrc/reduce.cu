@@ -219,12 +219,14 @@ __device__ __forceinline__ void field_words(const Geom& g, const float* __restri
     const int nr = g.ny * g.nz, wpr = (g.nx + 5) >> 2;  // words covering columns 0 .. nx + 1
     const int nw = (int)((gridDim.x * blockDim.x) >> 5);
     const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    // the sum in FP64; max and min of FP32 values in FP32 (exact, and off the
+    // FP64 pipe, which the sum alone keeps busy), widened at the end
+    float mx = -INFINITY, mn = INFINITY;
     auto take = [&](float f, int i) {
         if (i >= 1 && i <= g.nx) {
-            const double x = (double)f;
-            val[0] += x;
-            val[1] = fmax(val[1], x);
-            val[2] = fmin(val[2], x);
+            val[0] += (double)f;
+            mx = fmaxf(mx, f);
+            mn = fminf(mn, f);
         }
     };
     for (int rb = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); rb < nr; rb += RG * nw) {
@@ -257,6 +259,8 @@ __device__ __forceinline__ void field_words(const Geom& g, const float* __restri
                     }
         }
     }
+    val[1] = fmax(val[1], (double)mx);
+    val[2] = fmin(val[2], (double)mn);
 }
 
 __global__ void __launch_bounds__(RED_THREADS, 4) k_red_field_fold(Geom g, const float* __restrict__ a,
