@@ -565,51 +565,11 @@ int vof_sync(vof_ctx* ctx) {
     return check_status(ctx);
 }
 
-int vof_reduce_async(vof_ctx* ctx, int what, double* host_out) {
-    if (!ctx || !host_out) return VOF_E_INVALID;
-    if (what < 0 || what >= VOF_NUM_REDUCTIONS) return VOF_E_INVALID;
-    DeviceGuard dg(ctx->device);
-    vof::ReduceInputs in;
-    in.F = ctx->b.F;
-    in.u = ctx->b.u;
-    in.v = ctx->b.v;
-    in.w = ctx->b.w;
-    in.p = ctx->p_parity ? ctx->b.p1 : ctx->b.p0;
-    in.rhs = ctx->b.rhs;
-    // page-locked host memory mapped into the device: the reduction kernel
-    // writes the value there itself (no copy in the stream)
-    double* alias = nullptr;
-    cudaPointerAttributes pa{};
-    if (cudaPointerGetAttributes(&pa, host_out) == cudaSuccess) {
-        if (pa.type == cudaMemoryTypeHost && pa.devicePointer) alias = static_cast<double*>(pa.devicePointer);
-    } else {
-        cudaGetLastError();  // not a pointer CUDA knows: an ordinary host address
-    }
-    bool wrote = false;
-    cudaError_t e = vof::reduce_launch(ctx->g, in, what, ctx->d_red_scratch, ctx->d_red_result,
-                                       ctx->stream, alias, &wrote);
-    if (e != cudaSuccess) return fail_cuda(ctx, e);
-    if (wrote) return VOF_OK;
-    e = cudaMemcpyAsync(host_out, ctx->d_red_result + vof::reduce_result_slot(what), sizeof(double),
-                        cudaMemcpyDeviceToHost, ctx->stream);
-    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
-}
-
-int vof_reduce(vof_ctx* ctx, int what, double* out) {
-    if (!ctx || !out) return VOF_E_INVALID;
-    int st = vof_reduce_async(ctx, what, ctx->h_red_result);
-    if (st != VOF_OK) return st;
-    st = vof_sync(ctx);
-    if (st != VOF_OK) return st;
-    *out = ctx->h_red_result[0];
-    return VOF_OK;
-}
-
-int vof_reduce_range(vof_ctx* ctx, int what, int k0, int k1, double* out) {
-    if (!ctx || !out || k0 < 1 || k1 > ctx->g.nz || k0 > k1) return VOF_E_INVALID;
-    if (what != VOF_RED_VOLUME && what != VOF_RED_F_MIN && what != VOF_RED_F_MAX && what != VOF_RED_DIV_L2 &&
-        what != VOF_RED_DIV_MAX)
-        return what >= 0 && what < VOF_NUM_REDUCTIONS ? VOF_E_UNSUPPORTED : VOF_E_INVALID;
+// The reduction `what` over the interior cells of planes k0..k1 (1..nz: the
+// whole grid), stream-ordered, its value written to *host_out when the stream
+// gets there.  Page-locked host memory mapped into the device is written by
+// the reduction kernel itself; any other address gets a copy in the stream.
+static int reduce_planes_async(vof_ctx* ctx, int what, int k0, int k1, double* host_out) {
     DeviceGuard dg(ctx->device);
     // the planes k0..k1 as a grid of their own: the same rows, the base moved
     // k0 - 1 planes up (every reduction here reads a cell and its upper faces)
@@ -623,12 +583,61 @@ int vof_reduce_range(vof_ctx* ctx, int what, int k0, int k1, double* out) {
     in.w = ctx->b.w + off;
     in.p = (ctx->p_parity ? ctx->b.p1 : ctx->b.p0) + off;
     in.rhs = ctx->b.rhs + off;
-    cudaError_t e = vof::reduce_launch(sub, in, what, ctx->d_red_scratch, ctx->d_red_result, ctx->stream);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(ctx->h_red_result, ctx->d_red_result + vof::reduce_result_slot(what), sizeof(double),
-                            cudaMemcpyDeviceToHost, ctx->stream);
+    double* alias = nullptr;
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, host_out) == cudaSuccess) {
+        if (pa.type == cudaMemoryTypeHost && pa.devicePointer) alias = static_cast<double*>(pa.devicePointer);
+    } else {
+        cudaGetLastError();  // not a pointer CUDA knows: an ordinary host address
+    }
+    bool wrote = false;
+    cudaError_t e = vof::reduce_launch(sub, in, what, ctx->d_red_scratch, ctx->d_red_result, ctx->stream, alias,
+                                       &wrote);
     if (e != cudaSuccess) return fail_cuda(ctx, e);
-    const int st = vof_sync(ctx);
+    if (wrote) return VOF_OK;
+    e = cudaMemcpyAsync(host_out, ctx->d_red_result + vof::reduce_result_slot(what), sizeof(double),
+                        cudaMemcpyDeviceToHost, ctx->stream);
+    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
+}
+
+// The reductions a plane range supports: those whose every term is one cell
+// and the faces above it.
+static int check_range(const vof_ctx* ctx, int what, int k0, int k1) {
+    if (k0 < 1 || k1 > ctx->g.nz || k0 > k1) return VOF_E_INVALID;
+    if (what != VOF_RED_VOLUME && what != VOF_RED_F_MIN && what != VOF_RED_F_MAX && what != VOF_RED_DIV_L2 &&
+        what != VOF_RED_DIV_MAX)
+        return what >= 0 && what < VOF_NUM_REDUCTIONS ? VOF_E_UNSUPPORTED : VOF_E_INVALID;
+    return VOF_OK;
+}
+
+int vof_reduce_async(vof_ctx* ctx, int what, double* host_out) {
+    if (!ctx || !host_out) return VOF_E_INVALID;
+    if (what < 0 || what >= VOF_NUM_REDUCTIONS) return VOF_E_INVALID;
+    return reduce_planes_async(ctx, what, 1, ctx->g.nz, host_out);
+}
+
+int vof_reduce(vof_ctx* ctx, int what, double* out) {
+    if (!ctx || !out) return VOF_E_INVALID;
+    int st = vof_reduce_async(ctx, what, ctx->h_red_result);
+    if (st != VOF_OK) return st;
+    st = vof_sync(ctx);
+    if (st != VOF_OK) return st;
+    *out = ctx->h_red_result[0];
+    return VOF_OK;
+}
+
+int vof_reduce_range_async(vof_ctx* ctx, int what, int k0, int k1, double* host_out) {
+    if (!ctx || !host_out) return VOF_E_INVALID;
+    const int st = check_range(ctx, what, k0, k1);
+    if (st != VOF_OK) return st;
+    return reduce_planes_async(ctx, what, k0, k1, host_out);
+}
+
+int vof_reduce_range(vof_ctx* ctx, int what, int k0, int k1, double* out) {
+    if (!ctx || !out) return VOF_E_INVALID;
+    int st = vof_reduce_range_async(ctx, what, k0, k1, ctx->h_red_result);
+    if (st != VOF_OK) return st;
+    st = vof_sync(ctx);
     if (st != VOF_OK) return st;
     *out = ctx->h_red_result[0];
     return VOF_OK;

@@ -123,6 +123,7 @@ def _declare(lib):
         "vof_get_planes": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, C.c_int]),
         "vof_put_planes": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, C.c_int]),
         "vof_reduce_range": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, P(C.c_double)]),
+        "vof_reduce_range_async": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -152,7 +153,7 @@ def exported_symbols():
             "vof_step_timed", "vof_phase_name", "vof_solver_stats", "vof_step_noalloc",
             "vof_forward_record", "vof_backward", "vof_adjoint_download", "vof_adjoint_kernels_per_step",
             "vof_adjoint_storage", "vof_adjoint_keeps", "vof_debug_fail_alloc", "vof_debug_wait_timeout",
-            "vof_get_planes", "vof_put_planes", "vof_reduce_range"]
+            "vof_get_planes", "vof_put_planes", "vof_reduce_range", "vof_reduce_range_async"]
 
 
 def default_params(nx: int, ny: int | None = None, nz: int | None = None, **overrides) -> Params:
@@ -279,6 +280,12 @@ class Solver:
         w = REDUCTIONS[what] if isinstance(what, str) else int(what)
         self._check(self._lib.vof_reduce_range(self._ctx, w, k0, k1, C.byref(out)), "vof_reduce_range")
         return out.value
+
+    def reduce_range_async(self, what, k0: int, k1: int, host_ptr: int):
+        """reduce_range written to host_ptr (pinned) in stream order; sync before reading."""
+        w = REDUCTIONS[what] if isinstance(what, str) else int(what)
+        self._check(self._lib.vof_reduce_range_async(self._ctx, w, k0, k1, C.c_void_p(host_ptr)),
+                    "vof_reduce_range_async")
 
     # -- stepping ------------------------------------------------------------
     def step(self, istep: int):

@@ -216,6 +216,14 @@ int vof_reduce(vof_ctx* ctx, int what, double* out);
 int vof_reduce_range(vof_ctx* ctx, int what, int k0, int k1, double* out);
 
 /*
+ * vof_reduce_range, stream-ordered like vof_reduce_async: *host_out receives
+ * the value when the stream gets there (mapped pinned memory is written by the
+ * reduction kernel itself), and the host must vof_sync before reading it.  A
+ * slab rank reads its partial volume every step with no host synchronisation.
+ */
+int vof_reduce_range_async(vof_ctx* ctx, int what, int k0, int k1, double* host_out);
+
+/*
  * Stream-ordered reduction: the result is written to *host_out (which should
  * be pinned host memory) when the stream reaches this point; the host must
  * vof_sync before reading it.  No host synchronisation inside.  For pinned

@@ -49,7 +49,23 @@ def test_plane_copies_and_range_reductions(cuda, V):
         assert s.reduce_range("f_max", 6, 6) == F[6, 1:-1, 1:-1].max()
         tot = sum(s.reduce_range("volume", a, b) for a, b in ((1, 8), (9, 9), (10, 23)))
         assert tot == pytest.approx(s.reduce("volume"), rel=1e-12)
+        # stream-ordered: mapped pinned memory (written by the kernel) and an
+        # ordinary host array (a copy in the stream), both equal to the blocking call
+        ranges = (("volume", 3, 17), ("f_max", 6, 6), ("f_min", 1, 23), ("div_l2", 2, 9), ("div_max", 4, 12))
+        pinned = torch.zeros(len(ranges), dtype=torch.float64).pin_memory()
+        plain = np.zeros(len(ranges), dtype=np.float64)
+        for i, (what, a, b) in enumerate(ranges):
+            s.reduce_range_async(what, a, b, pinned.data_ptr() + 8 * i)
+            s.reduce_range_async(what, a, b, plain.ctypes.data + 8 * i)
+        s.sync()
+        want = [s.reduce_range(what, a, b) for what, a, b in ranges]
+        assert pinned.tolist() == want and plain.tolist() == want
         lib = s._lib
+        assert lib.vof_reduce_range_async(s._ctx, 0, 0, 3, plain.ctypes.data) == V.E_INVALID
+        assert lib.vof_reduce_range_async(s._ctx, 0, 1, 3, None) == V.E_INVALID
+        with pytest.raises(V.VofError) as e:
+            s.reduce_range_async("nonfinite", 1, 3, plain.ctypes.data)
+        assert e.value.status == V.E_UNSUPPORTED
         assert lib.vof_get_planes(s._ctx, 0, -1, 2, d.data_ptr(), 1) == V.E_INVALID
         assert lib.vof_get_planes(s._ctx, 0, prm.nz + 1, 2, d.data_ptr(), 1) == V.E_INVALID
         assert lib.vof_reduce_range(s._ctx, 0, 0, 3, None) == V.E_INVALID
