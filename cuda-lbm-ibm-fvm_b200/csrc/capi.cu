@@ -14,6 +14,7 @@
 #include "../../include/vof.h"
 #include "jacobi_tb.h"
 #include "adjoint.h"
+#include "apply_bc.h"
 #include "mg_solve.h"
 #include "plain_step.h"
 #include "reduce.h"
@@ -641,6 +642,35 @@ int vof_reduce_range(vof_ctx* ctx, int what, int k0, int k1, double* out) {
     if (st != VOF_OK) return st;
     *out = ctx->h_red_result[0];
     return VOF_OK;
+}
+
+int vof_apply_bc(vof_ctx* ctx) {
+    if (!ctx) return VOF_E_INVALID;
+    if (ctx->conv) return VOF_E_UNSUPPORTED;  // the pressure state is its FP64 copy there
+    DeviceGuard dg(ctx->device);
+    vof::BcFields f;
+    f.u = field_ptr(ctx, VOF_FIELD_U);
+    f.v = field_ptr(ctx, VOF_FIELD_V);
+    f.w = field_ptr(ctx, VOF_FIELD_W);
+    f.F = field_ptr(ctx, VOF_FIELD_F);
+    f.p = field_ptr(ctx, VOF_FIELD_P);
+    f.rho = nullptr;  // never stored: every kernel forms rho from F
+    const cudaError_t e = vof::apply_bc_launch(ctx->g.nx, ctx->g.ny, ctx->g.nz, ctx->g.px, f, ctx->stream);
+    return e == cudaSuccess ? VOF_OK : fail_cuda(ctx, e);
+}
+
+int vof_apply_bc_fields(const vof_params* p, float* u, float* v, float* w, float* F, float* pres, float* rho,
+                        void* stream) {
+    if (!p) return VOF_E_INVALID;
+    if (p->nx < 1 || p->ny < 1 || p->nz < 1) return VOF_E_SIZE;
+    if ((long long)(p->nx + 2) * (p->ny + 2) * (long long)(p->nz + 2) > kMaxCells) return VOF_E_SIZE;
+    if (p->imin != 1 || p->jmin != 1 || p->kmin != 1 || p->imax != p->nx || p->jmax != p->ny || p->kmax != p->nz)
+        return VOF_E_INVALID;
+    if ((long long)p->nTot != (long long)(p->nx + 2) * (p->ny + 2) * (p->nz + 2)) return VOF_E_INVALID;
+    const vof::BcFields f{u, v, w, F, pres, rho};
+    const cudaError_t e =
+        vof::apply_bc_launch(p->nx, p->ny, p->nz, p->nx + 2, f, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? VOF_OK : VOF_E_CUDA;
 }
 
 int vof_solver_stats(const vof_ctx* ctx, int* outer, double* rel_initial, double* rel_final) {

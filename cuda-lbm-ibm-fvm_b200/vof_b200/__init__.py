@@ -124,6 +124,8 @@ def _declare(lib):
         "vof_put_planes": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, C.c_int]),
         "vof_reduce_range": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, P(C.c_double)]),
         "vof_reduce_range_async": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp]),
+        "vof_apply_bc": (C.c_int, [vp]),
+        "vof_apply_bc_fields": (C.c_int, [P(Params), vp, vp, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -153,7 +155,24 @@ def exported_symbols():
             "vof_step_timed", "vof_phase_name", "vof_solver_stats", "vof_step_noalloc",
             "vof_forward_record", "vof_backward", "vof_adjoint_download", "vof_adjoint_kernels_per_step",
             "vof_adjoint_storage", "vof_adjoint_keeps", "vof_debug_fail_alloc", "vof_debug_wait_timeout",
-            "vof_get_planes", "vof_put_planes", "vof_reduce_range", "vof_reduce_range_async"]
+            "vof_get_planes", "vof_put_planes", "vof_reduce_range", "vof_reduce_range_async",
+            "vof_apply_bc", "vof_apply_bc_fields"]
+
+
+BC_FIELDS = ("u", "v", "w", "F", "p", "rho")  # apply_bc's argument order (voftrial1.cu:943)
+
+
+def apply_bc_fields(prm, stream: int = 0, **device_ptrs):
+    """The reference's apply_bc on caller-owned device buffers in the reference
+    layout, given as device pointers by name (u, v, w, F, p, rho; a name left
+    out is skipped), enqueued on `stream` (0: the legacy default stream)."""
+    unknown = set(device_ptrs) - set(BC_FIELDS)
+    if unknown:
+        raise ValueError(f"unknown fields {sorted(unknown)}")
+    ptrs = [C.c_void_p(device_ptrs[k]) if device_ptrs.get(k) else None for k in BC_FIELDS]
+    st = lib().vof_apply_bc_fields(C.byref(prm), *ptrs, C.c_void_p(stream) if stream else None)
+    if st != OK:
+        raise VofError(st, "vof_apply_bc_fields")
 
 
 def default_params(nx: int, ny: int | None = None, nz: int | None = None, **overrides) -> Params:
@@ -296,6 +315,10 @@ class Solver:
 
     def sync(self):
         self._check(self._lib.vof_sync(self._ctx), "vof_sync")
+
+    def apply_bc(self):
+        """The reference's apply_bc on the current state (stream-ordered)."""
+        self._check(self._lib.vof_apply_bc(self._ctx), "vof_apply_bc")
 
     def reduce(self, what) -> float:
         out = C.c_double()

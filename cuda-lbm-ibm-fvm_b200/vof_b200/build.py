@@ -39,9 +39,10 @@ SOURCES = {
     "reduce.cu": [],
     "capi.cu": [],
     "noalloc.cu": [],
+    "apply_bc.cu": [],
 }
 HEADERS = ["vof_device.cuh", "tma.cuh", "plain_step.h", "fct_sweep.h", "fct_line.cuh", "jacobi_tb.h", "mg_solve.h",
-           "reduce.h", "adjoint.h"]
+           "reduce.h", "adjoint.h", "apply_bc.h"]
 
 
 def nvcc() -> str:

@@ -256,6 +256,34 @@ int vof_reduce_async(vof_ctx* ctx, int what, double* host_out);
 int vof_step_noalloc(const vof_params* p, float* F, float* u, float* v, float* w, float* pres, int istep,
                      void* stream);
 
+/* ---- boundary conditions ------------------------------------------------ */
+/*
+ * The reference's apply_bc (voftrial1.cu:943-956: set_bc_j_kernel,
+ * set_bc_i_kernel, set_bc_k_kernel of :105-228, in that order), as one
+ * stream-ordered launch with the same result.  Ghost cells of F, p (and rho)
+ * copy the nearest interior cell, edges and corners included.  The
+ * wall-normal velocity is zeroed on the first and last faces (u at i = imin
+ * and imax+1, v at j = jmin and jmax+1, w at k = kmin and kmax+1).  The other
+ * velocity components' ghosts copy the neighbouring row as the three passes
+ * leave them.  The reference's time loop never calls apply_bc; these calls
+ * are for callers that do.
+ *
+ * vof_apply_bc: on the context's current state (F, u, v, w, p; rho is never
+ * stored).  VOF_E_UNSUPPORTED in the convergent modes, where the pressure
+ * state is its FP64 copy.
+ */
+int vof_apply_bc(vof_ctx* ctx);
+
+/*
+ * vof_apply_bc_fields: apply_bc's own signature, on caller-owned device
+ * buffers in the reference layout (p->nTot floats each).  A NULL pointer
+ * skips that field.  Enqueued on `stream` (NULL: the legacy default stream,
+ * as the reference launches); no host synchronisation.  VOF_E_SIZE for an
+ * empty or oversized grid, VOF_E_INVALID for inconsistent parameters.
+ */
+int vof_apply_bc_fields(const vof_params* p, float* u, float* v, float* w, float* F, float* pres, float* rho,
+                        void* stream);
+
 /*
  * Convergent modes (VOF_MODE_MIXED, VOF_MODE_FP64; no counterpart in the
  * reference): V-cycles done by the last pressure solve and its relative

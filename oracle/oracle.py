@@ -97,6 +97,8 @@ def oracle_lib():
             fn = getattr(lib, name)
             fn.restype = C.c_int
             fn.argtypes = [C.c_void_p, C.c_int, C.POINTER(Params)] + [C.POINTER(T)] * 5 + [C.c_int, C.c_int, D, D]
+        lib.oracle_apply_bc_f32.restype = C.c_int
+        lib.oracle_apply_bc_f32.argtypes = [C.POINTER(Params)] + [C.POINTER(C.c_float)] * 6
         lib.oracle_clamp01f.restype = C.c_float
         lib.oracle_clamp01f.argtypes = [C.c_float]
         lib.oracle_clamp01d.restype = C.c_double
@@ -237,6 +239,19 @@ class SwitchTape:
             pass
 
 
+BC_FIELDS = ("u", "v", "w", "F", "p", "rho")  # apply_bc's argument order (voftrial1.cu:943)
+
+
+def apply_bc(prm, fields: dict) -> dict:
+    """The reference's apply_bc (voftrial1.cu:943-956) on copies of the six
+    fields (reference layout): set_bc_j, then set_bc_i, then set_bc_k."""
+    st = {k: np.ascontiguousarray(fields[k], dtype=np.float32).copy() for k in BC_FIELDS}
+    rc = oracle_lib().oracle_apply_bc_f32(C.byref(prm), *(_ptr(st[k], C.c_float) for k in BC_FIELDS))
+    if rc != 0:
+        raise RuntimeError(f"oracle apply_bc failed: {rc}")
+    return st
+
+
 def clamp01f(x: float) -> float:
     return oracle_lib().oracle_clamp01f(x)
 
@@ -269,6 +284,8 @@ def ref_lib(variant: str = "sm100a"):
         lib.ref_initial_F.argtypes = [C.POINTER(Params), C.c_int, F]
         lib.ref_write_vtk.restype = C.c_int
         lib.ref_write_vtk.argtypes = [C.c_char_p, F, C.c_int, C.c_int, C.c_int]
+        lib.ref_apply_bc.restype = C.c_int
+        lib.ref_apply_bc.argtypes = [C.POINTER(Params)] + [F] * 6
         _refs[variant] = lib
     return _refs[variant]
 
@@ -289,6 +306,15 @@ def ref_write_vtk(path, F: np.ndarray, variant: str = "sm100a") -> None:
     rc = ref_lib(variant).ref_write_vtk(str(path).encode(), _ptr(F, C.c_float), nx, ny, nz)
     if rc != 0:
         raise RuntimeError(f"ref_write_vtk failed: {rc}")
+
+
+def ref_apply_bc(prm, fields: dict, variant: str = "sm100a") -> dict:
+    """The reference's own apply_bc kernels (GPU) on copies of the six fields."""
+    st = {k: np.ascontiguousarray(fields[k], dtype=np.float32).copy() for k in BC_FIELDS}
+    rc = ref_lib(variant).ref_apply_bc(C.byref(prm), *(_ptr(st[k], C.c_float) for k in BC_FIELDS))
+    if rc != 0:
+        raise RuntimeError(f"ref_apply_bc failed: {rc}")
+    return st
 
 
 def ref_run(prm, state, istep0: int, nsteps: int, variant: str = "sm100a", extras: bool = False) -> dict:

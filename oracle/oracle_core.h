@@ -348,6 +348,65 @@ struct Oracle {
             }
     }
 
+    // set_bc_{j,i,k}_kernel (voftrial1.cu:105-228) in the order of apply_bc
+    // (voftrial1.cu:943-956): the ghost cells of u, v, w, F, p and rho, and
+    // the wall-normal velocity on the first and last faces.  The reference's
+    // time loop never calls it.
+    void bc_all() {
+        const int jb = 0, jt = P.ny + 1, ib = 0, ir = P.nx + 1, kb = 0, kf = P.nz + 1;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+        for (int k = 0; k < NZ; ++k)
+            for (int i = 0; i < NX; ++i) {
+                const size_t bg = id(i, jb, k), bi = id(i, 1, k), tg = id(i, jt, k), ti = id(i, P.ny, k);
+                u[bg] = u[bi];
+                v[bi] = T(0);
+                w[bg] = w[bi];
+                F[bg] = F[bi];
+                p[bg] = p[bi];
+                rho[bg] = rho[bi];
+                u[tg] = u[ti];
+                v[tg] = T(0);
+                w[tg] = w[ti];
+                F[tg] = F[ti];
+                p[tg] = p[ti];
+                rho[tg] = rho[ti];
+            }
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+        for (int k = 0; k < NZ; ++k)
+            for (int j = 0; j < NY; ++j) {
+                const size_t lg = id(ib, j, k), li = id(1, j, k), rg = id(ir, j, k), ri = id(P.nx, j, k);
+                u[li] = T(0);
+                v[lg] = v[li];
+                w[lg] = w[li];
+                F[lg] = F[li];
+                p[lg] = p[li];
+                rho[lg] = rho[li];
+                u[rg] = T(0);
+                v[rg] = v[ri];
+                w[rg] = w[ri];
+                F[rg] = F[ri];
+                p[rg] = p[ri];
+                rho[rg] = rho[ri];
+            }
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+        for (int j = 0; j < NY; ++j)
+            for (int i = 0; i < NX; ++i) {
+                const size_t bg = id(i, j, kb), bi = id(i, j, 1), fg = id(i, j, kf), fi = id(i, j, P.nz);
+                u[bg] = u[bi];
+                v[bg] = v[bi];
+                w[bi] = T(0);
+                F[bg] = F[bi];
+                p[bg] = p[bi];
+                rho[bg] = rho[bi];
+                u[fg] = u[fi];
+                v[fg] = v[fi];
+                w[fg] = T(0);
+                F[fg] = F[fi];
+                p[fg] = p[fi];
+                rho[fg] = rho[fi];
+            }
+    }
+
     // post_process_f_kernel, voftrial1.cu:502-507
     void post_process() {
 #pragma omp parallel for num_threads(nthreads) schedule(static)

@@ -222,6 +222,27 @@ int ref_initial_F(const vof_params* prm, int ic, float* F_out) {
     return VOF_OK;
 }
 
+// The reference's apply_bc (voftrial1.cu:943-956, set_bc_{j,i,k}_kernel) on
+// six host fields in the reference layout, updated in place.
+int ref_apply_bc(const vof_params* prm, float* u, float* v, float* w, float* F, float* p, float* rho) {
+    if (!prm || !u || !v || !w || !F || !p || !rho) return VOF_E_INVALID;
+    load_params(prm);
+    const size_t bytes = (size_t)prm->nTot * sizeof(float);
+    float* host[6] = {u, v, w, F, p, rho};
+    float* dev[6] = {};
+    for (int q = 0; q < 6; ++q) {
+        alloc_field(&dev[q], bytes);
+        CHECK_CUDA(cudaMemcpy(dev[q], host[q], bytes, cudaMemcpyHostToDevice));
+    }
+    apply_bc(dev[0], dev[1], dev[2], dev[3], dev[4], dev[5]);
+    CHECK_CUDA(cudaDeviceSynchronize());
+    for (int q = 0; q < 6; ++q) {
+        CHECK_CUDA(cudaMemcpy(host[q], dev[q], bytes, cudaMemcpyDeviceToHost));
+        cudaFree(dev[q]);
+    }
+    return VOF_OK;
+}
+
 // The reference's dump writer (write_legacy_vtk, voftrial1.cu:907-941) on a
 // host field of nxTot * nyTot * nzTot floats; host code only, no GPU needed.
 int ref_write_vtk(const char* path, const float* field, int nxTot, int nyTot, int nzTot) {

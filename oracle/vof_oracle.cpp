@@ -67,6 +67,20 @@ int oracle_run_conv_f64(const vof_params* prm, double* F, double* u, double* v, 
     return run<double>(prm, F, u, v, w, p, istep0, nsteps, nullptr, nullptr, nullptr, nullptr, nthreads, tol);
 }
 
+// The reference's apply_bc (voftrial1.cu:943-956) on six host fields in the
+// reference layout, updated in place.
+int oracle_apply_bc_f32(const vof_params* prm, float* u, float* v, float* w, float* F, float* p, float* rho) {
+    if (!prm || !u || !v || !w || !F || !p || !rho) return VOF_E_INVALID;
+    if (prm->nx < 1 || prm->ny < 1 || prm->nz < 1) return VOF_E_SIZE;
+    Oracle<float> o(make_prm(prm, 0.0f), 1);
+    float* fields[6] = {u, v, w, F, p, rho};
+    std::vector<float>* mine[6] = {&o.u, &o.v, &o.w, &o.F, &o.p, &o.rho};
+    for (int q = 0; q < 6; ++q) std::copy(fields[q], fields[q] + o.N, mine[q]->begin());
+    o.bc_all();
+    for (int q = 0; q < 6; ++q) std::copy(mine[q]->begin(), mine[q]->end(), fields[q]);
+    return VOF_OK;
+}
+
 // clamp01f of the reference on one value, in float and in double.
 float oracle_clamp01f(float v) { return clamp01<float>(v); }
 double oracle_clamp01d(double v) { return clamp01<double>(v); }

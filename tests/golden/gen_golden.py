@@ -11,7 +11,11 @@ and writes index.json with the parameters, the tolerance the tests apply to
 the FMA build (fma_rel_l2, a stated bound) and the measured difference
 between the two builds.
 
-    python tests/golden/gen_golden.py [outdir]
+It also runs the reference's apply_bc (voftrial1.cu:943-956, never called by
+its time loop) on seeded random fields and stores in_/out_{u,v,w,F,p,rho} per
+case in apply_bc_*.npz, listed in apply_bc.json.
+
+    python tests/golden/gen_golden.py [outdir] [--only steps|apply_bc]
 """
 from __future__ import annotations
 
@@ -42,6 +46,34 @@ CASES = [
     dict(name="dam_32_200", nx=32, ny=32, nz=32, overrides=dict(gy=0.0, gz=-9.81),
          input=dict(kind="dam_break"), istep0=1, nsteps=200, fma_rel_l2=1e-5),
 ]
+
+
+BC_CASES = [
+    # name, grid, seed of the six standard-normal float32 input fields
+    dict(name="apply_bc_7x5x4_s1", nx=7, ny=5, nz=4, seed=1),
+    dict(name="apply_bc_1x3x2_s2", nx=1, ny=3, nz=2, seed=2),
+    dict(name="apply_bc_16x12x10_s3", nx=16, ny=12, nz=10, seed=3),
+]
+
+
+def bc_input(prm, seed):
+    rng = np.random.default_rng(seed)
+    return {k: rng.standard_normal(prm.shape).astype(np.float32) for k in orc.BC_FIELDS}
+
+
+def gen_apply_bc(outdir: Path):
+    index = {"generator": "tests/golden/gen_golden.py --only apply_bc", "cases": []}
+    for c in BC_CASES:
+        prm = V.default_params(c["nx"], c["ny"], c["nz"])
+        inp = bc_input(prm, c["seed"])
+        out = orc.ref_apply_bc(prm, inp)
+        arrays = {**{"in_" + k: inp[k] for k in orc.BC_FIELDS}, **{"out_" + k: out[k] for k in orc.BC_FIELDS}}
+        fname = c["name"] + ".npz"
+        np.savez_compressed(outdir / fname, **arrays)
+        changed = {k: int((out[k] != inp[k]).sum()) for k in orc.BC_FIELDS}
+        index["cases"].append({**c, "file": fname, "changed_cells": changed})
+        print(c["name"], json.dumps(changed))
+    (outdir / "apply_bc.json").write_text(json.dumps(index, indent=1) + "\n")
 
 
 def make_input(prm, spec):
@@ -90,4 +122,15 @@ def main(outdir: Path):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).resolve().parent)
+    import argparse
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("outdir", nargs="?", default=str(Path(__file__).resolve().parent))
+    ap.add_argument("--only", choices=("steps", "apply_bc"))
+    a = ap.parse_args()
+    out = Path(a.outdir)
+    out.mkdir(parents=True, exist_ok=True)
+    if a.only in (None, "steps"):
+        main(out)
+    if a.only in (None, "apply_bc"):
+        gen_apply_bc(out)

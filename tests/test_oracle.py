@@ -119,5 +119,57 @@ def test_oracle_matches_reference_golden(V, orc, case):
 def test_golden_index_present_when_fixtures_exist():
     files = sorted(p.name for p in GOLDEN.glob("*.npz"))
     if files:
-        names = {c["file"] for c in golden_cases()}
+        names = {c["file"] for c in golden_cases()} | {c["file"] for c in bc_cases()}
         assert set(files) <= names
+
+
+# ---- apply_bc (voftrial1.cu:943-956) -------------------------------------
+BC = ("u", "v", "w", "F", "p", "rho")
+
+
+def bc_cases():
+    idx = GOLDEN / "apply_bc.json"
+    return json.loads(idx.read_text())["cases"] if idx.exists() else []
+
+
+def bc_closed_form(inp):
+    """What set_bc_j, set_bc_i and set_bc_k leave, in one numpy expression per
+    field: ghosts of F, p, rho from the clamped interior cell; u, v, w zero on
+    their first and last faces, their other ghosts clamped in the two
+    tangential directions only."""
+    nz2, ny2, nx2 = inp["F"].shape
+    ci = np.clip(np.arange(nx2), 1, nx2 - 2)
+    cj = np.clip(np.arange(ny2), 1, ny2 - 2)
+    ck = np.clip(np.arange(nz2), 1, nz2 - 2)
+    out = {k: inp[k][np.ix_(ck, cj, ci)] for k in ("F", "p", "rho")}
+    out["u"] = inp["u"][np.ix_(ck, cj, np.arange(nx2))]
+    out["u"][:, :, [1, nx2 - 1]] = 0
+    out["v"] = inp["v"][np.ix_(ck, np.arange(ny2), ci)]
+    out["v"][:, [1, ny2 - 1], :] = 0
+    out["w"] = inp["w"][np.ix_(np.arange(nz2), cj, ci)]
+    out["w"][[1, nz2 - 1], :, :] = 0
+    return out
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (1, 3, 2), (4, 1, 3), (5, 6, 1), (9, 7, 5)])
+def test_apply_bc_oracle_is_the_closed_form(V, orc, shape):
+    prm = V.default_params(*shape)
+    rng = np.random.default_rng(sum(shape))
+    inp = {k: rng.standard_normal(prm.shape).astype(np.float32) for k in BC}
+    got = orc.apply_bc(prm, inp)
+    want = bc_closed_form(inp)
+    for k in BC:
+        assert np.array_equal(got[k], want[k]), k
+    again = orc.apply_bc(prm, got)  # idempotent
+    for k in BC:
+        assert np.array_equal(again[k], got[k]), k
+
+
+@pytest.mark.parametrize("case", bc_cases(), ids=lambda c: c["name"])
+def test_apply_bc_oracle_matches_reference_golden(V, orc, case):
+    """The oracle's apply_bc reproduces the reference's own kernels bit for bit."""
+    data = np.load(GOLDEN / case["file"])
+    prm = V.default_params(case["nx"], case["ny"], case["nz"])
+    got = orc.apply_bc(prm, {k: data["in_" + k] for k in BC})
+    for k in BC:
+        assert np.array_equal(got[k], data["out_" + k]), k
