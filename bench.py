@@ -66,7 +66,7 @@ ALG_BYTES = {
     "sweep3": 12,
 }
 KERNEL_NAMES = {
-    "predict": "k_predict", "rhs": "k_rhs", "jacobi": "k_jacobi_peel", "correct": "k_correct4",
+    "predict": "k_predict2", "rhs": "k_rhs4", "jacobi": "k_jacobi_peel", "correct": "k_correct4",
     "sweep1": "k_fct_x|k_fct_march", "sweep2": "k_fct_x|k_fct_march", "sweep3": "k_fct_x|k_fct_march",
 }
 # the Jacobi kernel the library runs at the bench size (VOF_JACOBI=peel|pairs|ring|bulk|col|pairs2|tb|tb1;
@@ -76,6 +76,10 @@ KERNEL_NAMES["jacobi"] = {"col": "k_jacobi_col", "tb": "k_jacobi_tb", "tb1": "k_
                           "pairs": "k_jacobi_pairs"}.get(os.environ.get("VOF_JACOBI", ""), "k_jacobi_peel")
 if os.environ.get("VOF_CORRECT") == "1":
     KERNEL_NAMES["correct"] = "k_correct"
+if os.environ.get("VOF_RHS") == "1":
+    KERNEL_NAMES["rhs"] = "k_rhs"
+if os.environ.get("VOF_PREDICT") == "1":
+    KERNEL_NAMES["predict"] = "k_predict"
 STEP_MODEL_BYTES = 188  # B per cell-step of the fused plain path (10 sweeps, FP32)
 WARM_MS = 60.0  # least GPU time of warm-up steps run back to back before a timed region
 

@@ -407,9 +407,10 @@ __global__ void __launch_bounds__(MARCH_THREADS, 4) k_fct_march(Geom g, const fl
         const bool in = q >= 0 && q <= n + 1;
         zrun = (!in || (L.F(q) == 0.0f && fabsf(L.V(q)) < vq)) ? zrun + 1 : 0;
     }
-    // the line is away from the box's edges across the sweep (no ghost copies
-    // but along the line on the final sweep)
-    const bool inner = a > 1 && a < g.nx && b > 1 && b < nb;
+    // the line is away from the walls across b: on the final sweep its cells
+    // away from the line's ends have no ghost copies but the i ghost (a = 1
+    // or a = nx)
+    const bool binner = b > 1 && b < nb;
 #if VOF_MARCH_AHEAD >= 2
     float F4 = (c0 + 4 <= n + 1) ? L.F(c0 + 4) : 0.0f, V4 = (c0 + 4 <= n + 1) ? L.V(c0 + 4) : 0.0f;
 #endif
@@ -447,8 +448,13 @@ __global__ void __launch_bounds__(MARCH_THREADS, 4) k_fct_march(Geom g, const fl
             F[gi(a, b, c)] = fnew;
         } else {
             fnew = clamp01f(fnew);  // post_process_f_kernel, voftrial1.cu:502-507
-            if (inner && c > 1 && c < nm) {
-                F[gi(a, b, c)] = fnew;
+            if (binner && c > 1 && c < nm) {
+                // inline, so that the warps holding a line at a = 1 or nx do
+                // not leave their other lanes for a call at every position
+                const int o = gi(a, b, c);
+                F[o] = fnew;
+                if (a == 1) F[o - 1] = fnew;
+                if (a == g.nx) F[o + 1] = fnew;
             } else if (AXIS == 1) {  // (a, b, c) = (i, k, j)
                 store_mirrored(F, g.px, g.plane, g.nx, g.ny, g.nz, a, c, b, fnew);
             } else {  // (a, b, c) = (i, j, k)

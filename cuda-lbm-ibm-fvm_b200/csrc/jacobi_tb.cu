@@ -410,20 +410,24 @@ struct JPRegs {
 };
 
 // One plane k of the paired sweep.  MORE: load the next plane's operands (the
-// caller guarantees k < k1 <= nz, so plane k + 2 <= nz + 1 exists).  EDGE:
-// the plane may be the first or the last of the box.
-template <bool MORE, bool EDGE>
+// caller guarantees k < k1 <= nz, so plane k + 2 <= nz + 1 exists; marching
+// DOWN, k > k0 >= 1, so plane k - 2 >= 0 exists).  EDGE: the plane may be the
+// first or the last of the box.  DOWN marches k downwards: the next plane is
+// k - 1, and the window pm, pc, pp turns the other way; each cell's
+// expression is the same.
+template <bool MORE, bool EDGE, bool DOWN = false>
 __device__ __forceinline__ void jp_plane(const JPLine& L, const Geom& g, int k, JPRegs& s) {
     float2 pq, sn, nn, rn;
     float xwn = 0.0f, xen = 0.0f;
     if constexpr (MORE) {
-        const int o1 = L.w + (k + 1) * L.wp;
-        pq = L.P[o1 + L.wp];
+        const int kn = DOWN ? k - 1 : k + 1;
+        const int o1 = L.w + kn * L.wp;
+        pq = L.P[DOWN ? o1 - L.wp : o1 + L.wp];
         sn = L.P[o1 - L.wr];
         nn = L.P[o1 + L.wr];
         rn = L.R[o1];
-        if (L.ldw) xwn = L.pin[L.cw + (k + 1) * L.plane];
-        if (L.lde) xen = L.pin[L.ce + (k + 1) * L.plane];
+        if (L.ldw) xwn = L.pin[L.cw + kn * L.plane];
+        if (L.lde) xen = L.pin[L.ce + kn * L.plane];
     }
     float pw = __shfl_up_sync(0xffffffffu, s.pc.y, 1), pe = __shfl_down_sync(0xffffffffu, s.pc.x, 1);
     if (L.ldw) pw = s.xw;
@@ -453,9 +457,15 @@ __device__ __forceinline__ void jp_plane(const JPLine& L, const Geom& g, int k, 
     else if (L.a1)
         L.pout[2 * o + 1] = v1;
     if constexpr (MORE) {
-        s.pm = s.pc;
-        s.pc = s.pp;
-        s.pp = pq;
+        if constexpr (DOWN) {
+            s.pp = s.pc;
+            s.pc = s.pm;
+            s.pm = pq;
+        } else {
+            s.pm = s.pc;
+            s.pc = s.pp;
+            s.pp = pq;
+        }
         s.pS = sn;
         s.pN = nn;
         s.rc = rn;
@@ -464,7 +474,7 @@ __device__ __forceinline__ void jp_plane(const JPLine& L, const Geom& g, int k, 
     }
 }
 
-template <int U, int MINB>
+template <int U, int MINB, bool DOWN = false>
 __global__ void __launch_bounds__(JP_THREADS, MINB) k_jacobi_peel(Geom g, const float* __restrict__ pin,
                                                             const float* __restrict__ rhs,
                                                             float* __restrict__ pout, int kchunk) {
@@ -505,26 +515,39 @@ __global__ void __launch_bounds__(JP_THREADS, MINB) k_jacobi_peel(Geom g, const 
     L.wp = g.plane >> 1;
     L.wr = g.px >> 1;
     JPRegs s;
-    s.pm = L.P[L.w + (k0 - 1) * L.wp];
-    s.pc = L.P[L.w + k0 * L.wp];
-    s.pp = L.P[L.w + (k0 + 1) * L.wp];
-    s.pS = L.P[L.w + k0 * L.wp - L.wr];
-    s.pN = L.P[L.w + k0 * L.wp + L.wr];
-    s.rc = L.R[L.w + k0 * L.wp];
-    s.xw = L.ldw ? pin[L.cw + k0 * L.plane] : 0.0f;
-    s.xe = L.lde ? pin[L.ce + k0 * L.plane] : 0.0f;
-    int k = k0;
-    if (k == 1 && k < k1) {
-        jp_plane<true, true>(L, g, k, s);
-        ++k;
+    const int ks = DOWN ? k1 : k0;  // the march's first plane
+    s.pm = L.P[L.w + (ks - 1) * L.wp];
+    s.pc = L.P[L.w + ks * L.wp];
+    s.pp = L.P[L.w + (ks + 1) * L.wp];
+    s.pS = L.P[L.w + ks * L.wp - L.wr];
+    s.pN = L.P[L.w + ks * L.wp + L.wr];
+    s.rc = L.R[L.w + ks * L.wp];
+    s.xw = L.ldw ? pin[L.cw + ks * L.plane] : 0.0f;
+    s.xe = L.lde ? pin[L.ce + ks * L.plane] : 0.0f;
+    int k = ks;
+    if constexpr (DOWN) {
+        if (k == g.nz && k > k0) {
+            jp_plane<true, true, true>(L, g, k, s);
+            --k;
+        }
+        VOF_UNROLL(U)
+        for (; k > k0; --k) jp_plane<true, false, true>(L, g, k, s);
+        jp_plane<false, true, true>(L, g, k0, s);
+    } else {
+        if (k == 1 && k < k1) {
+            jp_plane<true, true>(L, g, k, s);
+            ++k;
+        }
+        VOF_UNROLL(U)
+        for (; k < k1; ++k) jp_plane<true, false>(L, g, k, s);
+        jp_plane<false, true>(L, g, k1, s);
     }
-    VOF_UNROLL(U)
-    for (; k < k1; ++k) jp_plane<true, false>(L, g, k, s);
-    jp_plane<false, true>(L, g, k1, s);
 }
 
 // VOF_JP_UNROLL (1, 2 or 4) picks the unroll of the peeled march and
 // VOF_JP_MINB (1 or 4) the blocks per SM its registers are sized for.
+// The downward march (the sweeps' alternating direction) is built for the
+// default shape only.
 using JPKernel = void (*)(Geom, const float*, const float*, float*, int);
 static JPKernel jp_peel_kernel() {
     static JPKernel k = nullptr;
@@ -1007,11 +1030,16 @@ cudaError_t jacobi_quad_launch(const Geom& g, const float* pin, const float* rhs
     return cudaGetLastError();
 }
 
-cudaError_t jacobi_peel_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s) {
+cudaError_t jacobi_peel_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s,
+                               bool down) {
     const int nq = (g.nx / 2 + 1) * g.ny;
     const int bx = (nq + JP_THREADS - 1) / JP_THREADS;
     const int kchunk = jacobi_pairs_kchunk(g, bx, jpe_wave);
-    jp_peel_kernel()<<<dim3(bx, (g.nz + kchunk - 1) / kchunk), JP_THREADS, 0, s>>>(g, pin, rhs, pout, kchunk);
+    const dim3 grid(bx, (g.nz + kchunk - 1) / kchunk);
+    if (down)
+        k_jacobi_peel<2, 4, true><<<grid, JP_THREADS, 0, s>>>(g, pin, rhs, pout, kchunk);
+    else
+        jp_peel_kernel()<<<grid, JP_THREADS, 0, s>>>(g, pin, rhs, pout, kchunk);
     return cudaGetLastError();
 }
 

@@ -24,12 +24,14 @@ cudaError_t jacobi_tb_launch(const Geom& g, int T, const CUtensorMap& map_in, co
 // buffer; its ghost cells are left as they are), streaming along z.
 cudaError_t jacobi_col_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);
 
-// The same sweep with two cells per thread (packed FP32, same bits).
+// The same sweep with two cells per thread (scalar FP32, same bits).
 cudaError_t jacobi_pairs_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);
 
 // The paired sweep with its wall and last planes peeled out of the march
-// (unrolled VOF_JP_UNROLL times, default 4); same bits as jacobi_pairs_launch.
-cudaError_t jacobi_peel_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s);
+// (unrolled VOF_JP_UNROLL times, default 2); same bits as jacobi_pairs_launch.
+// down: march z downwards (the default shape only); same bits.
+cudaError_t jacobi_peel_launch(const Geom& g, const float* pin, const float* rhs, float* pout, cudaStream_t s,
+                               bool down = false);
 
 // z chunk of a launch of bx blocks per chunk whose resident blocks number
 // `wave`: the longest chunk whose last wave of blocks is 85 % full or more,

@@ -93,16 +93,21 @@ def test_random_state_bitwise_vs_oracle(cuda, V, orc, nx, ny, nz, seed, dt, vs):
                                  {"VOF_JACOBI": "peel", "VOF_JACOBI_KCHUNK": "1"},
                                  {"VOF_JACOBI": "peel", "VOF_JACOBI_KCHUNK": "2"},
                                  {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "4", "VOF_JACOBI_KCHUNK": "7"},
-                                 {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "4", "VOF_JACOBI_KCHUNK": "21"}])
+                                 {"VOF_JACOBI": "peel", "VOF_JP_UNROLL": "4", "VOF_JACOBI_KCHUNK": "21"},
+                                 {"VOF_JACOBI_ALT": "0"}, {"VOF_JACOBI_ALT": "1", "VOF_JACOBI_KCHUNK": "1"},
+                                 {"VOF_JACOBI_ALT": "1", "VOF_JACOBI_KCHUNK": "2"},
+                                 {"VOF_JACOBI_ALT": "1", "VOF_JACOBI_KCHUNK": "7"}])
 def test_jacobi_kernel_choices_give_the_same_bits(cuda, V, orc, tmp_path, env):
-    """The kernels a process may select (the defaults -- the peeled paired
-    Jacobi sweep and the four-cell correction -- run in every other test;
-    here the other Jacobi kernels: the paired sweep, its peeled form at other
-    unrolls and register caps, the two-sweep paired kernel, the cp.async
-    ring, the bulk-copy ring, the TMA-blocked kernels, the one-cell streaming
-    sweep, and z chunks of several of them; and the one-cell correction; read
-    once per process, so each runs in a child process) give the oracle's
-    bits."""
+    """The kernels a process may select give the oracle's bits.  The defaults
+    (the peeled paired Jacobi sweep, marching z down on every second sweep at
+    these sizes, and the size-chosen predictor, rhs and correction kernels)
+    run in every other test; here the other Jacobi kernels: the paired sweep,
+    the peeled form at other unrolls and register caps and with every sweep
+    marching up, the downward march over short z chunks, the four-cell sweep,
+    the two-sweep paired kernel, the cp.async ring, the bulk-copy ring, the
+    TMA-blocked kernels, the one-cell streaming sweep, and z chunks of
+    several of them; and the one-cell predictor, rhs and correction.  The
+    choice is read once per process, so each runs in a child process."""
     import os
     import subprocess
     import sys
