@@ -407,10 +407,15 @@ __global__ void __launch_bounds__(MARCH_THREADS, 4) k_fct_march(Geom g, const fl
         const bool in = q >= 0 && q <= n + 1;
         zrun = (!in || (L.F(q) == 0.0f && fabsf(L.V(q)) < vq)) ? zrun + 1 : 0;
     }
-    // the line is away from the walls across b: on the final sweep its cells
-    // away from the line's ends have no ghost copies but the i ghost (a = 1
-    // or a = nx)
-    const bool binner = b > 1 && b < nb;
+    // Final sweep, apply_bc_F (voftrial1.cu:1122-1135): every ghost takes the
+    // value at its clamped interior index.  Across the line, a cell at a = 1
+    // or nx, b = 1 or nb has ghost copies on those sides (and their corner),
+    // written inline by the lines at the box's edge; the line's own ghosts
+    // (c = 0 and n + 1, with their copies across) are written after the march
+    // from the values kept at c = 1 and c = n.  No call inside the loop.
+    const int bs = AXIS == 1 ? g.plane : g.px;  // b's stride
+    const bool edge = a == 1 || a == g.nx || b == 1 || b == nb;
+    float f_lo = 0.0f, f_hi = 0.0f;
 #if VOF_MARCH_AHEAD >= 2
     float F4 = (c0 + 4 <= n + 1) ? L.F(c0 + 4) : 0.0f, V4 = (c0 + 4 <= n + 1) ? L.V(c0 + 4) : 0.0f;
 #endif
@@ -448,18 +453,24 @@ __global__ void __launch_bounds__(MARCH_THREADS, 4) k_fct_march(Geom g, const fl
             F[gi(a, b, c)] = fnew;
         } else {
             fnew = clamp01f(fnew);  // post_process_f_kernel, voftrial1.cu:502-507
-            if (binner && c > 1 && c < nm) {
-                // inline, so that the warps holding a line at a = 1 or nx do
-                // not leave their other lanes for a call at every position
-                const int o = gi(a, b, c);
-                F[o] = fnew;
+            const int o = gi(a, b, c);
+            F[o] = fnew;
+            if (edge) {
                 if (a == 1) F[o - 1] = fnew;
                 if (a == g.nx) F[o + 1] = fnew;
-            } else if (AXIS == 1) {  // (a, b, c) = (i, k, j)
-                store_mirrored(F, g.px, g.plane, g.nx, g.ny, g.nz, a, c, b, fnew);
-            } else {  // (a, b, c) = (i, j, k)
-                store_mirrored(F, g.px, g.plane, g.nx, g.ny, g.nz, a, b, c, fnew);
+                if (b == 1) {
+                    F[o - bs] = fnew;
+                    if (a == 1) F[o - bs - 1] = fnew;
+                    if (a == g.nx) F[o - bs + 1] = fnew;
+                }
+                if (b == nb) {
+                    F[o + bs] = fnew;
+                    if (a == 1) F[o + bs - 1] = fnew;
+                    if (a == g.nx) F[o + bs + 1] = fnew;
+                }
             }
+            if (c == 1) f_lo = fnew;
+            if (c == nm) f_hi = fnew;
         }
         lo2 = lo3;
         a0f = a1f;
@@ -480,6 +491,15 @@ __global__ void __launch_bounds__(MARCH_THREADS, 4) k_fct_march(Geom g, const fl
         F4 = F5;
         V4 = V5;
 #endif
+    }
+    if (FINAL) {
+        if (AXIS == 1) {  // (a, b, c) = (i, k, j)
+            if (c0 == 1) store_mirrored(F, g.px, g.plane, g.nx, g.ny, g.nz, a, 1, b, f_lo);
+            if (c1 == nm) store_mirrored(F, g.px, g.plane, g.nx, g.ny, g.nz, a, nm, b, f_hi);
+        } else {  // (a, b, c) = (i, j, k)
+            if (c0 == 1) store_mirrored(F, g.px, g.plane, g.nx, g.ny, g.nz, a, b, 1, f_lo);
+            if (c1 == nm) store_mirrored(F, g.px, g.plane, g.nx, g.ny, g.nz, a, b, nm, f_hi);
+        }
     }
 }
 
