@@ -333,6 +333,52 @@ def test_async_reductions_into_mapped_and_pageable_memory(cuda, V):
         assert list(got_p[rep]) == want and list(got_h[rep]) == want, (rep, got_p[rep], got_h[rep], want)
 
 
+@pytest.mark.parametrize("env", [{}, {"VOF_JACOBI_ALT": "0"}, {"VOF_JACOBI": "pairs"}])
+def test_jacobi_ieee_division_cells(cuda, V, orc, tmp_path, env):
+    """Pressures near 1e31 give Jacobi quotients above 2^96, outside the fast
+    division's range: those cells take the IEEE division.  The pressure after
+    one step is the sweeps' output and must be the oracle's bit for bit; the
+    other fields (the correction and the sweeps then see huge gradients) must
+    agree wherever they are not NaN and be NaN at the same cells."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    shape = (12, 10, 9)
+    prm = V.default_params(*shape, dt=2e-4, gy=0.0, gz=-9.81)
+    state = ic.random_state(prm, seed=21, vel_scale=1.0)
+    rng = np.random.default_rng(21)
+    p = state["p"]
+    idx = tuple(rng.integers(1, n + 1, 40) for n in (shape[2], shape[1], shape[0]))
+    p[idx] = (rng.standard_normal(40) * 1e31).astype(np.float32)
+    p[2, 3, 4], p[5, 5, 5], p[7, 1, 11] = 3.0e33, -2.0e33, 1.5e32
+    np.savez(tmp_path / "in.npz", **state)
+    root = Path(__file__).resolve().parent.parent
+    code = (
+        "import sys, numpy as np\n"
+        f"sys.path.insert(0, {str(root / 'cuda-lbm-ibm-fvm_b200')!r})\n"
+        "import vof_b200 as V\n"
+        f"prm = V.default_params(*{shape!r}, dt=2e-4, gy=0.0, gz=-9.81)\n"
+        f"st = dict(np.load({str(tmp_path / 'in.npz')!r}))\n"
+        "with V.Solver(prm) as s:\n"
+        "    s.upload_state(**st)\n"
+        "    s.step(1)\n"
+        f"    np.savez({str(tmp_path / 'out.npz')!r}, **s.state())\n")
+    subprocess.run([sys.executable, "-c", code], env={**os.environ, **env}, check=True, timeout=600)
+    got = dict(np.load(tmp_path / "out.npz"))
+    want = orc.run_f32(prm, state, 1, 1)
+    assert np.isfinite(want["p"]).all() and np.abs(want["p"]).max() > 1e24  # still far outside the fast range's reach
+    assert_bitwise(got, want, ("p",), f"pressure {env}")
+    for k in ("F", "u", "v", "w"):
+        gn, wn = np.isnan(got[k]), np.isnan(want[k])
+        assert np.array_equal(gn, wn), (k, int((gn != wn).sum()))
+        g, w = got[k].copy(), want[k].copy()
+        g[gn] = 0.0
+        w[wn] = 0.0
+        assert_bitwise({k: g}, {k: w}, (k,), f"{k} {env}")
+
+
 def test_nonfinite_watchdog(cuda, V):
     prm = V.default_params(10, 10, 10)
     state = ic.random_state(prm, seed=3)
