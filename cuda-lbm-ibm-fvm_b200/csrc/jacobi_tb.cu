@@ -1,8 +1,13 @@
 // jacobi_tb.cu -- Jacobi sweeps of the pressure system (solve_p_jacobi_kernel,
-// voftrial1.cu:401-439, with the ping-pong of voftrial1.cu:1371-1375): one
-// sweep per launch with two cells per thread (k_jacobi_pairs, the default),
-// one sweep per launch with one cell per thread (k_jacobi_col), or T sweeps
-// per launch temporally blocked in shared memory (k_jacobi_tb<T>, below).
+// voftrial1.cu:401-439, with the ping-pong of voftrial1.cu:1371-1375).  The
+// default is one sweep per launch with two cells per thread and the plane
+// cases peeled out of the z march (k_jacobi_peel), marching up or down.  The
+// other kernels here, all with the same bits: the same without the peeling
+// (k_jacobi_pairs), four cells per thread (k_jacobi_quad), own-column
+// cp.async ring (k_jacobi_ring), rows fed by bulk copies (k_jacobi_bulk),
+// one cell per thread (k_jacobi_col), two sweeps per launch
+// (k_jacobi_pairs2), and T sweeps per launch temporally blocked in shared
+// memory through TMA (k_jacobi_tb<T>, described below).
 //
 // Compiled with -fmad=false: each cell update keeps the reference's
 //     pt = (rhs - ae*pE - aw*pW - an*pN - as*pS - af*pF - ab*pB) / ap
