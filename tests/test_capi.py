@@ -111,7 +111,29 @@ def test_null_context_calls_return_invalid(V):
     assert lib.vof_upload(None, 0, None, 0) == V.E_INVALID
     assert lib.vof_download(None, 0, None, 0) == V.E_INVALID
     assert lib.vof_kernels_per_step(None) == V.E_INVALID
+    assert lib.vof_reduce_range(None, 0, 1, 2, None) == V.E_INVALID
+    assert lib.vof_reduce_range_async(None, 0, 1, 2, None) == V.E_INVALID
+    assert lib.vof_apply_bc(None) == V.E_INVALID
     lib.vof_destroy(None)  # no-op
+
+
+def test_apply_bc_fields_rejects_bad_params_without_touching_device(V):
+    """vof_apply_bc_fields checks its parameters before any CUDA call."""
+    lib = V.lib()
+    nulls = [None] * 7
+    assert lib.vof_apply_bc_fields(None, *nulls) == V.E_INVALID
+    p = V.default_params(6, 5, 4)
+    p.nTot += 1
+    assert lib.vof_apply_bc_fields(C.byref(p), *nulls) == V.E_INVALID
+    p = V.default_params(6, 5, 4)
+    p.imax = 5
+    assert lib.vof_apply_bc_fields(C.byref(p), *nulls) == V.E_INVALID
+    p = V.default_params(6, 5, 4)
+    p.nz = 0
+    assert lib.vof_apply_bc_fields(C.byref(p), *nulls) == V.E_SIZE
+    p = V.default_params(6, 5, 4)
+    p.nx = p.ny = p.nz = 1300  # (nx+2)(ny+2)(nz+2) beyond the cell limit
+    assert lib.vof_apply_bc_fields(C.byref(p), *nulls) == V.E_SIZE
 
 
 def test_error_strings(V):
