@@ -70,6 +70,29 @@ def test_plan_covers_the_grid_and_halos_come_from_one_neighbour():
     assert slab.halo_for(10) == 16 and slab.halo_for(40) == 46
 
 
+@pytest.mark.parametrize("world", [2, 4, 8])
+def test_bench_slab_plans_for_the_scaling_run(world):
+    """The plans `bench.py --gpus N` makes (200 planes per rank, the halo of
+    ten Jacobi sweeps): every rank owns 200 planes, steps those plus one
+    halo per cut, and exchanges exactly its halo depth with each neighbour."""
+    import bench
+
+    g = bench.slab_global_params(200, world)
+    assert g.nz == 200 * world and g.nTot == 202 * 202 * (200 * world + 2)
+    h = slab.halo_for(g.jacobi_iters)
+    assert h == 16
+    sl = slab.plan(g.nz, world, h)
+    assert [s.own1 - s.own0 + 1 for s in sl] == [200] * world
+    for r, s in enumerate(sl):
+        cuts = (r > 0) + (r < world - 1)
+        q = slab.local_params(g, s)
+        assert q.nz == s.nz == 200 + h * cuts
+        assert q.nTot == (q.nx + 2) * (q.ny + 2) * (q.nz + 2)
+        ex = slab.Exchange(sl, r)
+        assert sorted(p for p, _, _ in ex.sends) == sorted(p for p, _, _ in ex.recvs)
+        assert [nk for _, _, nk in ex.sends] == [h] * cuts and [nk for _, _, nk in ex.recvs] == [h] * cuts
+
+
 def test_exchange_pairs_match():
     sl = slab.plan(60, 3)
     ex = [slab.Exchange(sl, r) for r in range(3)]
