@@ -123,6 +123,30 @@ def test_tangent_against_finite_differences(V, orc):
         assert abs(fd - tl) <= 1e-4 * abs(tl), (name, fd, tl)
 
 
+def test_adjoint_against_finite_differences_along_sixteen_directions(V, orc):
+    """The form of the 64^3 adjoint gradient check at a CPU size: the initial
+    velocity perturbed by N(0, (1e-3 m/s)^2) on interior faces, 16 seeded
+    directions (seed 4) in the joint u, v, w interior-face space with the same
+    std, central differences with eps = 1e-4 (1e-7 m/s per face) of the
+    unfrozen FP64 forward against the FP64 adjoint's <dL/du, d>: relative
+    1e-4."""
+    prm, st = dam_state(V, 12, 12, 12, amp=1e-3)
+    box = box_of(prm)
+    steps, eps = 6, 1e-4
+    A = orc.adjoint(prm, st, 1, steps, box, "f64")
+    assert A["loss"] > 0
+    rng = np.random.default_rng(4)
+    for n in range(16):
+        d = {c: interior_faces(prm, c, rng, sigma=1e-3) for c in ("u", "v", "w")}
+        adj = sum(float(np.sum(A["l" + c] * d[c])) for c in d)
+        sp = {k: (st[k] + eps * d[k] if k in d else st[k]) for k in STATE}
+        sm = {k: (st[k] - eps * d[k] if k in d else st[k]) for k in STATE}
+        fd = (box_loss(prm, orc.run_f64(prm, sp, 1, steps)["F"], box) -
+              box_loss(prm, orc.run_f64(prm, sm, 1, steps)["F"], box)) / (2 * eps)
+        rel = abs(fd - adj) / abs(adj)
+        assert rel <= 1e-4, (n, fd, adj, rel)
+
+
 def test_fp32_and_fp64_trajectories_give_close_gradients(V, orc):
     prm, st = dam_state(V, 12, 12, 12)
     box = box_of(prm)
